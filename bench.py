@@ -1,0 +1,383 @@
+"""Benchmark: SIMPLE iterations per second of the flow-solver pass on a B200.
+
+Workload (BASELINE metric configuration): box of 2*128 x 128 x 128 =
+4,194,304 hexahedral cells on a 0.2 x 0.1 x 0.1 m domain, inlet u = 50 m/s on
+x-min, zero-gradient outlet on x-max, walls elsewhere, rho 1.2, mu 1.8e-5,
+T0 1500 K; initial u, v, w, p, T = inlet state + seeded uniform noise +-1%;
+1,000 seeded Gaussian particle-source blobs (momentum, energy, mass; sigma 2
+cells, amplitude 1e-3 of the cell inflow); the corrected SIMPLE pass
+(MC_MODE_SIMPLE), momentum URF 0.7, pressure URF 0.3, pressure PCG + Jacobi to
+rtol 1e-8, momentum/temperature BiCGStab to rtol 1e-8.  Synthetic data (the
+reference has no dataset); the working set (about 4.5 GB) is far larger than
+L2, so consecutive iterations stream from HBM.
+
+One step = one SIMPLE pass (gradients, momentum assembly and three solves,
+Rhie-Chow mass flux, pressure-correction assembly, PCG solve(s) and
+corrections, temperature assembly and solve).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs N independent replicas (the path is single-GPU),
+one per rank under torchrun, and reports the whole-job rate.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SIMPLE iters/s at 4.2M cells"
+UNIT = "iters/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--m", type=int, default=128, help="mesh modifier: 2m x m x m cells")
+    ap.add_argument("--blobs", type=int, default=1000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-roofline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ inputs
+
+def noisy_fields(n, seed, t0=1500.0, u_in=50.0, p0=4000.0, amplitude=0.01):
+    rng = np.random.default_rng(seed)
+    out = {}
+    for name, base in (("U", u_in), ("V", 0.0), ("W", 0.0), ("P", p0), ("TEM", t0)):
+        noise = rng.uniform(-amplitude, amplitude, size=n)
+        out[name] = u_in * noise if base == 0.0 else base * (1.0 + noise)
+    return out
+
+
+def gaussian_blobs(dims, lengths, k, seed, rel_amplitude=1e-3, rho=1.2, u_in=50.0, sigma_cells=2.0):
+    """k Gaussian blobs centred at uniform-random cells; amplitude = rel_amplitude
+    x the cell inflow rho u_in A_x; momentum along +x, energy and mass scaled
+    from it.  Returned as particle_aos rows [cells][5]."""
+    ex, ey, ez = dims
+    dx, dy, dz = (lengths[0] / ex, lengths[1] / ey, lengths[2] / ez)
+    amp = rel_amplitude * rho * u_in * dy * dz
+    rng = np.random.default_rng(seed)
+    centres = rng.choice(ex * ey * ez, size=k, replace=False)
+    g = np.zeros((ez, ey, ex))
+    r = int(np.ceil(3 * sigma_cells))
+    off = np.arange(-r, r + 1)
+    w1 = np.exp(-0.5 * (off / sigma_cells) ** 2)
+    for c in centres:
+        x, y, z = c % ex, (c // ex) % ey, c // (ex * ey)
+        xs, ys, zs = x + off, y + off, z + off
+        mx, my, mz = (xs >= 0) & (xs < ex), (ys >= 0) & (ys < ey), (zs >= 0) & (zs < ez)
+        g[np.ix_(zs[mz], ys[my], xs[mx])] += amp * w1[mz][:, None, None] * w1[my][None, :, None] * w1[mx][None, None, :]
+    g = g.reshape(-1)
+    src = np.zeros((ex * ey * ez, 5))
+    src[:, 0] = g
+    src[:, 3] = 1.0e3 * g
+    src[:, 4] = 1.0e-2 * g
+    return src
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------- roofline
+
+def kernel_bytes(name, N, F, nnz_off):
+    """Algorithmic (unique-touch) bytes of one launch: each stored input
+    element read once, each output written once, at its stored type."""
+    return {
+        "pcg_iter1_spmv": 12 * nnz_off + 40 * N,   # diag, off+col, z, p_old -> p_new, q
+        "pcg_iter2_update": 64 * N,                # x rw, r rw, p, q, diag -> z
+        "bicg3_1_spmv": 12 * nnz_off + 8 * N + 3 * 48 * N,
+        "bicg3_2_spmv": 12 * nnz_off + 8 * N + 3 * 32 * N,
+        "bicg3_3_update": 3 * 56 * N,
+        "lsq_gradients_uvwpt": 208 * N,
+        "momentum_assemble": 56 * F + 296 * N,
+        "mass_flux": 88 * F + 176 * N,
+        "pressure_rows": 24 * F + 120 * N,
+        "temperature_assemble": 40 * F + 168 * N,
+    }.get(name)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------- reference arm
+
+def reference_sample(m, passes):
+    """The reference's own CPU FlowSolver (oracle/_ref) on the same mesh; each
+    sample is `passes` SIMPLE passes after construction and one warm pass."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from checkers import Reference, noisy_initial_fields, ref_available
+    if not ref_available():
+        return None
+    ref = Reference(2 * m, m, m, 0.2, 0.1, 0.1, delta=1.0e-5, bcgs_rtol=1e-8, cg_rtol=1e-8)
+    init = noisy_initial_fields(ref.N, {"U": 50.0, "V": 0.0, "W": 0.0, "P": 4000.0, "TEM": 2000.0}, 0)
+    for name, vals in init.items():
+        a = ref.field(name)
+        a[:ref.N] = vals
+        ref.set_field(name, a)
+    ref.step()  # first pass includes set_up_field
+    t0 = time.perf_counter()
+    for _ in range(passes):
+        ref.step()
+    dt = time.perf_counter() - t0
+    ref.close()
+    return dt / passes
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from checkers import ref_available
+    if not ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmcref.so (the reference compiled "
+                                                              "from its sources) is not built"}))
+        return
+    sample_m = 32
+    times = []
+    for _ in range(max(1, args.warmup // 3)):
+        reference_sample(sample_m, 1)
+    for _ in range(args.steps):
+        times.append(reference_sample(sample_m, 1))
+    per_pass_small = float(np.mean(times))
+    scale = (2 * args.m ** 3) / (2 * sample_m ** 3)
+    value = 1.0 / (per_pass_small * scale)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"reference CPU FlowSolver, box 2*{args.m}^3 cells (sampled at 2*{sample_m}^3, "
+                                   "scaled by cell count)", "cells": 2 * args.m ** 3, "mode": "reference physics"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": f"{args.steps} single SIMPLE passes of the reference on 2*{sample_m}^3 "
+                                       f"cells, time per pass x {scale:.0f} (cell-count scaling)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------- main
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        dist = tdist
+    torch.cuda.set_device(local)
+
+    from minicombust_app_b200 import build as mcbuild
+    from minicombust_app_b200 import flow
+    if not os.path.exists(flow.LIB_PATH):
+        mcbuild.build()
+
+    m = args.m
+    dims, lengths = (2 * m, m, m), (0.2, 0.1, 0.1)
+    mesh = flow.Mesh.box(*dims, *lengths)
+    params = flow.default_params(flow.MODE_SIMPLE, device=local, p_rtol=1e-8, u_rtol=1e-8)
+    solver = flow.FlowSolver(mesh, params=params)
+    N = solver.N
+    init = noisy_fields(N, seed=rank)
+    for name, vals in init.items():
+        a = solver.field(name)
+        a[:N] = vals
+        solver.set_field(name, a)
+    solver.set_sources(gaussian_blobs(dims, lengths, args.blobs, seed=rank))
+
+    stream = torch.cuda.ExternalStream(solver.stream(), device=torch.device("cuda", local))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        solver.simple_iteration()
+
+    # ---- device-resident throughput (value)
+    stats = []
+    launches0 = solver.launch_count()
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        solver.simple_iteration()
+        stats.append(solver.last_stats.as_dict())
+    ev1.record(stream)
+    barrier()
+    clocks = sampler.stop()
+    launches = solver.launch_count() - launches0
+    t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    value = world * args.steps / t_dev
+
+    # ---- end to end through the C ABI with host buffers
+    names = ("U", "V", "W", "P", "TEM")
+    pinned = {n: torch.empty(N + 6, dtype=torch.float64, pin_memory=True) for n in names}
+    for n in names:
+        pinned[n].numpy()[:] = solver.field(n)
+    h2d = 5 * (N + 6) * 8
+    d2h = 5 * (N + 6) * 8
+    L = flow.library()
+    h = solver.h
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        for i, n in enumerate(names):
+            flow._check(L.mc_flow_set_field(h, flow.FIELDS[n], pinned[n].data_ptr()), h, "set_field")
+        solver.simple_iteration()
+        for n in names:
+            flow._check(L.mc_flow_get_field(h, flow.FIELDS[n], pinned[n].data_ptr()), h, "get_field")
+    e1.record(stream)
+    barrier()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    e2e = world * args.steps / t_e2e
+
+    line = None
+    if rank == 0:
+        # ---- roofline of the dominant kernel (separate instrumented pass)
+        roof = None
+        kt = {}
+        if not args.no_roofline:
+            solver.reset_kernel_times()
+            solver.set_timing(True)
+            solver.simple_iteration()
+            solver.set_timing(False)
+            kt = solver.kernel_times()
+            nnz_off = int(np.sum(mesh.face_cells[:, 1] < N)) * 2
+            ranked = sorted(((ms, name, cnt) for name, (ms, cnt) in kt.items() if cnt > 0), reverse=True)
+            for ms, name, cnt in ranked:
+                b = kernel_bytes(name, N, mesh.n_faces, nnz_off)
+                if b is None:
+                    continue
+                avg_s = ms / cnt / 1e3
+                peak, kind = measured_peaks()
+                achieved = b / avg_s / 1e9
+                roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_source": kind, "traffic": None,
+                        "bytes_per_launch": b, "avg_launch_us": avg_s * 1e6, "launches_per_step": cnt,
+                        "share_of_step": ms / sum(v[0] for v in kt.values())}
+                break
+        cpu = None
+        if not args.no_cpu_baseline:
+            per_pass = reference_sample(32, 3)
+            if per_pass is not None:
+                scale = (2 * m ** 3) / (2 * 32 ** 3)
+                cpu = {"value": 1.0 / (per_pass * scale), "unit": UNIT, "cores": 1, "kind": "reference",
+                       "sample": f"3 SIMPLE passes of the reference CPU FlowSolver (its own physics) on 2*32^3 "
+                                 f"cells, time per pass x {scale:.0f} (cell-count scaling)"}
+        pit = [s["pressure_iters_total"] for s in stats]
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"simple-mode SIMPLE pass, box 2*{m}x{m}x{m} = {N} cells, {args.blobs} "
+                                       "source blobs, plain FP64 path (PCG+Jacobi pressure, BiCGStab momentum/T, "
+                                       "rtol 1e-8)",
+                           "cells": N, "faces": mesh.n_faces, "l2": "inputs larger than L2 (~4.5 GB working set)",
+                           "parallelism": "replicas" if world > 1 else "single GPU"},
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": launches,
+                "clocks": clocks,
+                "roofline": roof,
+                "cpu_baseline": cpu,
+                "solver": {"pressure_iters_per_step": float(np.mean(pit)), "momentum_iters": stats[-1]["momentum_iters"],
+                           "temperature_iters": stats[-1]["temperature_iters"],
+                           "mass_imbalance": stats[-1]["mass_imbalance"]},
+                "kernel_ms_one_step": {k: round(v[0], 4) for k, v in kt.items() if v[1] > 0}}
+        print(json.dumps(line))
+    solver.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

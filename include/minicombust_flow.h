@@ -1,0 +1,186 @@
+/*
+ * minicombust_flow.h -- C ABI of the B200 (sm_100a) flow-solver SIMPLE pass.
+ *
+ * This is the drop-in boundary for miniCOMBUST's flow solver.  It replaces:
+ *   - the reference CPU solver's per-pass work (include/flow/FlowSolver.inl,
+ *     timestep loop :3188-3268, stages cited per entry point below), and
+ *   - the reference GPU back-end's launch shims (include/flow/gpu/gpu_kernels.cuh:11-82,
+ *     "void C_kernel_*(int block_count, int thread_count, device pointers...)")
+ *     together with the AmgX calls of include/flow/gpu/FlowSolver.inl:644-1025.
+ * Those shims take raw device pointers, return nothing and exit() on error
+ * (gpu_kernels.cu:24-32).  Here a handle owns every device buffer, inputs and
+ * outputs are host arrays in the reference layout, every call returns a status
+ * code and nothing exits the process.
+ *
+ * Layout contract (the reference's, Mesh.hpp:86-106 and utils.hpp:158-174):
+ *   - cells are indexed 0..cells-1; a face is {cell0, cell1} with cell0 < cell1;
+ *     a boundary face has cell1 = cells + d, d = 0..5 the boundary side
+ *     FRONT, BACK, LEFT, RIGHT, DOWN, UP, whose type is boundary_types[d]
+ *     (1 wall, 2 inlet, 3 outlet);
+ *   - a field is an array of cells + 6 doubles: interior values, then the
+ *     value of each boundary side at index cells + d;
+ *   - particle source terms are particle_aos<double> per cell:
+ *     {momentum.x, momentum.y, momentum.z, energy, fuel (mass)}.
+ *
+ * Threading: one host thread per handle at a time; each handle owns one CUDA
+ * stream on the device chosen at creation.  Calls are synchronous unless noted.
+ */
+#ifndef MINICOMBUST_FLOW_H
+#define MINICOMBUST_FLOW_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MC_FLOW_ABI_VERSION 1
+
+typedef enum mc_status {
+    MC_OK = 0,
+    MC_ERR_ARG = -1,            /* bad argument or handle */
+    MC_ERR_CUDA = -2,           /* a CUDA call failed; see mc_flow_last_error */
+    MC_ERR_NOT_CONVERGED = -3,  /* a Krylov solve reached max_iters */
+    MC_ERR_NONFINITE = -4,      /* a residual or reduction became NaN/Inf */
+    MC_ERR_MESH = -5,           /* mesh arrays inconsistent */
+    MC_ERR_NOMEM = -6,          /* device or host allocation failed */
+    MC_ERR_UNSUPPORTED = -7     /* option not available in this build */
+} mc_status;
+
+enum { MC_MODE_COMPAT = 0, MC_MODE_SIMPLE = 1 };
+enum { MC_PSOLVER_PCG_JACOBI = 0, MC_PSOLVER_PCG_AMG = 1 };
+enum { MC_PRECISION_FP64 = 0, MC_PRECISION_FP32_REFINED = 1 };
+enum { MC_GUESS_ZERO = 0, MC_GUESS_PREVIOUS = 1, MC_GUESS_LEARNED = 2 };
+
+/* Field ids: the member order of phi_vector<T> (utils.hpp:158-174). */
+enum {
+    MC_FIELD_U = 0, MC_FIELD_V = 1, MC_FIELD_W = 2, MC_FIELD_P = 3, MC_FIELD_PP = 4,
+    MC_FIELD_TE = 5, MC_FIELD_ED = 6, MC_FIELD_TP = 7, MC_FIELD_TEM = 8,
+    MC_FIELD_FUL = 9, MC_FIELD_PRO = 10, MC_FIELD_VARF = 11, MC_FIELD_VARP = 12
+};
+
+/* Linear systems readable with mc_flow_get_csr. */
+enum { MC_SYSTEM_MOMENTUM = 0, MC_SYSTEM_PRESSURE = 1, MC_SYSTEM_TEMPERATURE = 2 };
+
+/* Mesh in the reference layout (Mesh<T> public arrays, Mesh.hpp:86-106). */
+typedef struct mc_mesh_view {
+    uint64_t cells;                  /* Mesh::mesh_size */
+    uint64_t faces;                  /* Mesh::faces_size */
+    uint64_t points;                 /* Mesh::points_size */
+    const double *points_xyz;        /* [points][3]  Mesh::points */
+    const uint64_t *cell_nodes;      /* [cells][8]   Mesh::cells, vertex order A..H */
+    const uint64_t *face_cells;      /* [faces][2]   Mesh::faces */
+    const uint64_t *cell_faces;      /* [cells][6]   Mesh::cell_faces */
+    const uint64_t *cell_neighbours; /* [cells][6]   Mesh::cell_neighbours (UINT64_MAX on the boundary) */
+    const double *cell_centers;      /* [cells][3]   Mesh::cell_centers */
+    uint64_t boundary_types[6];      /* Mesh::boundary_types */
+} mc_mesh_view;
+
+/* Physics and solver settings.  mc_flow_default_params fills the reference's
+ * constants (FlowSolver.hpp:296,342; Mesh.hpp:114-116; FlowSolver.inl:1731,
+ * 1871, 2425, 2939-2946; minicombust.cpp:120) for MC_MODE_COMPAT and the
+ * benchmark physics for MC_MODE_SIMPLE. */
+typedef struct mc_flow_params {
+    int mode;                 /* MC_MODE_COMPAT: the reference's control flow and quirks;
+                                 MC_MODE_SIMPLE: corrected SIMPLE pass (see below) */
+    double delta;             /* time step */
+    double density;
+    double viscosity;
+    double inlet_u;           /* inlet velocity (x); v = w = 0 */
+    double pressure0;         /* initial and boundary pressure */
+    double temperature0;      /* initial, inlet and buoyancy-reference temperature */
+    double urf_momentum;
+    double urf_pressure;
+    double urf_temperature;
+    double flux_corr;         /* non-orthogonal flux-correction factor */
+    double u_rtol;            /* momentum and temperature BiCGStab: ||r|| <= u_rtol ||b|| */
+    double p_rtol;            /* pressure-correction PCG: ||r|| <= p_rtol ||b|| */
+    int max_iters;            /* per Krylov solve */
+    int pressure_solver;      /* MC_PSOLVER_* */
+    int precision;            /* MC_PRECISION_* */
+    int initial_guess;        /* MC_GUESS_* for the pressure correction */
+    int device;               /* CUDA device ordinal */
+} mc_flow_params;
+
+/* Per-pass statistics. */
+typedef struct mc_iter_stats {
+    int momentum_iters[3];
+    int temperature_iters;
+    int pressure_solves;
+    int pressure_iters_total;
+    int pressure_iters_first;
+    double pressure_correction_max_first;
+    double pressure_rel_residual;    /* last pressure solve, ||r|| / ||b|| */
+    double mass_imbalance;           /* max over cells |div(mdot) - mass source| after the pass */
+} mc_iter_stats;
+
+typedef struct mc_flow mc_flow;
+
+/* Fill params with the defaults of a mode. */
+void mc_flow_default_params(mc_flow_params *params, int mode);
+
+/* Replaces the FlowSolver constructor (FlowSolver.hpp:147-539; GPU back-end
+ * gpu/FlowSolver.hpp:274-1118): face geometry, cell volumes, initial fields,
+ * matrix pattern, device buffers.  The mesh is copied; the caller keeps it. */
+int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_flow **out);
+int mc_flow_destroy(mc_flow *flow);
+
+/* Field access, cells + 6 doubles (FlowSolver::phi).  Fields outside the
+ * coupled set U, V, W, P, PP, TEM return MC_ERR_UNSUPPORTED. */
+int mc_flow_set_field(mc_flow *flow, int field, const double *host_values);
+int mc_flow_get_field(mc_flow *flow, int field, double *host_values);
+/* Least-squares gradient of U, V, W, P, PP or TEM, [cells][3]. */
+int mc_flow_get_gradient(mc_flow *flow, int field, double *host_values);
+/* Particle source terms, [cells][5] particle_aos<double> (Mesh::particle_terms). */
+int mc_flow_set_sources(mc_flow *flow, const double *host_particle_terms);
+/* Face arrays in reference face order.  which: 0 mass flux [faces], 1 area,
+ * 2 lambda, 3 rlencos, 4 face_fields [faces][2], 5 normals [faces][3], 6 centres [faces][3]. */
+int mc_flow_get_face_array(mc_flow *flow, int which, double *host_values);
+/* which: 0 A_phi.U (momentum diagonal after under-relaxation), 1 pressure
+ * diagonal, 2 cell volumes, 3 cell densities; [cells]. */
+int mc_flow_get_cell_array(mc_flow *flow, int which, double *host_values);
+/* Assembled system as CSR with ascending columns (the PETSc AIJ pattern the
+ * reference builds, FlowSolver.inl:1186-1297 and 2106-2201) and its right-hand
+ * side.  Pass NULL arrays to query n and nnz. */
+int mc_flow_get_csr(mc_flow *flow, int system, int *n, int *nnz, int *row_ptr, int *col, double *val, double *rhs);
+
+/* One SIMPLE pass: the body of FlowSolver::timestep's loop (FlowSolver.inl:3188-3268)
+ * for the coupled fields u, v, w, p, T.  stats may be NULL. */
+int mc_flow_simple_iteration(mc_flow *flow, mc_iter_stats *stats);
+/* FlowSolver::timestep (FlowSolver.inl:3148-3356): three SIMPLE passes. */
+int mc_flow_timestep(mc_flow *flow, mc_iter_stats *stats);
+
+/* The stages of a pass, callable one at a time (same order as in a pass). */
+int mc_flow_stage_gradients(mc_flow *flow);   /* get_phi_gradients, FlowSolver.inl:917-1063 */
+int mc_flow_stage_set_up_field(mc_flow *flow);/* set_up_field, FlowSolver.inl:1106-1113 */
+int mc_flow_stage_momentum(mc_flow *flow, mc_iter_stats *stats);    /* calculate_UVW, :1655-1810 */
+int mc_flow_stage_pressure(mc_flow *flow, mc_iter_stats *stats);    /* calculate_pressure, :2317-2514 */
+int mc_flow_stage_temperature(mc_flow *flow, mc_iter_stats *stats); /* Scalar_solve(TEMP), :2885-3076 */
+
+/* Kernel timing on the handle's stream (CUDA events around each launch).
+ * While enabled, passes run without graph replay.  Times accumulate until
+ * reset; ids are dense from 0 to mc_flow_kernel_count()-1. */
+int mc_flow_set_timing(mc_flow *flow, int enable);
+int mc_flow_kernel_count(void);
+const char *mc_flow_kernel_name(int id);
+int mc_flow_get_kernel_times(mc_flow *flow, double *total_ms, long *launches);
+int mc_flow_reset_kernel_times(mc_flow *flow);
+/* The handle's cudaStream_t, for callers that time around it. */
+void *mc_flow_stream(mc_flow *flow);
+/* Number of this library's kernel launches since creation. */
+long mc_flow_launch_count(mc_flow *flow);
+
+const char *mc_flow_last_error(mc_flow *flow);
+const char *mc_status_string(int status);
+
+/* Box mesh in the reference layout: load_mesh for one flow rank
+ * (src/examples/mesh_examples.cpp:120-571), x-min inlet, x-max outlet, walls
+ * elsewhere.  Arrays are allocated by the library; release them with
+ * mc_mesh_box_destroy. */
+int mc_mesh_box_create(uint64_t ex, uint64_t ey, uint64_t ez, double lx, double ly, double lz, mc_mesh_view *out);
+void mc_mesh_box_destroy(mc_mesh_view *mesh);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MINICOMBUST_FLOW_H */

@@ -1,0 +1,1047 @@
+// C ABI of the B200 flow solver (include/minicombust_flow.h): handle
+// lifetime, device memory arena, the SIMPLE pass orchestration and the host
+// side of the Krylov solves (batched iterations captured in CUDA graphs, one
+// status read per batch).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "flow_kernels.cuh"
+#include "krylov.cuh"
+#include "mc_internal.h"
+#include "mc_reduce.cuh"
+#include "mesh_setup.h"
+#include "minicombust_flow.h"
+
+using namespace mcb;
+
+namespace {
+
+enum KernelId {
+    K_GRAD5, K_GRAD1, K_PRECOMP_AU, K_MOMENTUM, K_MASS_FLUX, K_OUTLET_FIX, K_PRESSURE_ROWS, K_PP_FACES,
+    K_PP_CELLS, K_P_BOUNDARY, K_PP_MAX, K_TEMPERATURE, K_IMBALANCE, K_PCG_MEAN, K_PCG_INIT, K_PCG_ITER1,
+    K_PCG_ITER2, K_PCG_XMEAN, K_PCG_SUBMEAN, K_BICG3_INIT, K_BICG3_1, K_BICG3_2, K_BICG3_3, K_BICG1_INIT,
+    K_BICG1_1, K_BICG1_2, K_BICG1_3, K_COUNT
+};
+
+const char *kKernelNames[K_COUNT] = {
+    "lsq_gradients_uvwpt", "lsq_gradient_single", "precomp_au", "momentum_assemble", "mass_flux",
+    "outlet_fix", "pressure_rows", "pp_correct_faces", "pp_correct_cells", "update_p_boundary", "pp_max",
+    "temperature_assemble", "mass_imbalance", "pcg_mean", "pcg_init", "pcg_iter1_spmv", "pcg_iter2_update",
+    "pcg_xmean", "pcg_sub_xmean", "bicg3_init", "bicg3_1_spmv", "bicg3_2_spmv", "bicg3_3_update",
+    "bicg1_init", "bicg1_1_spmv", "bicg1_2_spmv", "bicg1_3_update"};
+
+constexpr int PCG_BATCH = 16;   // iterations per status read (even: ping-pong buffers)
+constexpr int BICG_BATCH = 8;
+
+// One cudaMalloc carved into aligned sub-buffers.
+struct Arena {
+    char *base = nullptr;
+    size_t size = 0, used = 0;
+    size_t reserve(size_t bytes)
+    {
+        const size_t off = used;
+        used += (bytes + 255) & ~(size_t)255;
+        return off;
+    }
+};
+
+struct Timing {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> ids;
+    size_t used = 0;
+    double total_ms[K_COUNT] = {0};
+    long count[K_COUNT] = {0};
+};
+
+} // namespace
+
+struct mc_flow {
+    mc_flow_params prm{};
+    int N = 0, F = 0;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    Physics ph{};
+    MeshArgs margs{};
+    Arena arena;
+    std::vector<int> hcol;   // ELL columns with -1 on boundary slots (CSR export)
+
+    // mesh
+    int *fc0, *fc1, *nbr, *sface, *col, *outlet_faces;
+    double *area, *lam, *rl, *Sx, *Sy, *Sz, *xf, *yf, *zf, *xc, *yc, *zc, *vol, *rho;
+    // fields and gradients (G_U..G_T x 3 components)
+    double *phi[G_NFIELDS];
+    double *grad[G_NFIELDS][3];
+    double *mdot, *ff0, *ff1, *fcorr;
+    double *AU, *off_m, *b_m;
+    double *off_p, *diag_p, *b_p;
+    double *off_t, *diag_t, *b_t;
+    double *src;
+    // reductions
+    double *partials;
+    unsigned int *counter;
+    FluxBalance *balance;
+    double *scalars;   // [0] max|PP|, [1] mass imbalance
+    // Krylov
+    PcgVectors pv{};
+    BicgVectors<3> b3{};
+    BicgVectors<1> b1{};
+    PcgState *h_pcg = nullptr;         // pinned
+    BicgState<3> *h_b3 = nullptr;      // pinned
+    BicgState<1> *h_b1 = nullptr;      // pinned
+    double *h_scalars = nullptr;       // pinned
+    cudaGraphExec_t g_pcg = nullptr, g_b3 = nullptr, g_b1 = nullptr;
+
+    // state of the reference's control flow
+    int first_pressure = 1;
+    uint64_t timestep_count = 0;
+    int pass_in_step = 0;
+    int sources_set = 0;
+    double mass_source_total = 0.0;
+    double p_bnorm_ref = 0.0;
+    long launches = 0;
+    Timing timing;
+};
+
+namespace {
+
+int fail(mc_flow *h, int code, const std::string &msg)
+{
+    if (h) h->err = msg;
+    return code;
+}
+
+#define CUDA_TRY(h, call)                                                                              \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return fail((h), MC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));         \
+    } while (0)
+
+// Kernel launch with launch counting and optional event timing.
+template <typename Fn>
+void launch(mc_flow *h, int kid, Fn &&fn)
+{
+    Timing &t = h->timing;
+    if (t.on) {
+        if (t.used * 2 + 2 > t.ev.size()) {
+            for (int i = 0; i < 64; i++) {
+                cudaEvent_t e;
+                cudaEventCreate(&e);
+                t.ev.push_back(e);
+            }
+        }
+        cudaEventRecord(t.ev[2 * t.used], h->stream);
+        fn();
+        cudaEventRecord(t.ev[2 * t.used + 1], h->stream);
+        t.ids.push_back(kid);
+        t.used++;
+    } else {
+        fn();
+    }
+    h->launches++;
+}
+
+void flush_timing(mc_flow *h)
+{
+    Timing &t = h->timing;
+    if (!t.on || t.used == 0) return;
+    cudaStreamSynchronize(h->stream);
+    for (size_t i = 0; i < t.used; i++) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t.ev[2 * i], t.ev[2 * i + 1]);
+        t.total_ms[t.ids[i]] += ms;
+        t.count[t.ids[i]] += 1;
+    }
+    t.used = 0;
+    t.ids.clear();
+}
+
+int check_launch(mc_flow *h)
+{
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h, MC_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return MC_OK;
+}
+
+inline int blocks_for(int n) { return std::max(1, (n + MCB_THREADS - 1) / MCB_THREADS); }
+
+int grad_index(int field)
+{
+    switch (field) {
+    case MC_FIELD_U: return G_U;
+    case MC_FIELD_V: return G_V;
+    case MC_FIELD_W: return G_W;
+    case MC_FIELD_P: return G_P;
+    case MC_FIELD_PP: return G_PP;
+    case MC_FIELD_TEM: return G_T;
+    default: return -1;
+    }
+}
+
+Ell momentum_matrix(mc_flow *h) { return Ell{h->N, h->AU, h->off_m, h->col}; }
+Ell pressure_matrix(mc_flow *h) { return Ell{h->N, h->diag_p, h->off_p, h->col}; }
+Ell temperature_matrix(mc_flow *h) { return Ell{h->N, h->diag_t, h->off_t, h->col}; }
+
+// ------------------------------------------------------------ Krylov drivers
+
+int krylov_status_to_mc(int s)
+{
+    return s == KRYLOV_OK ? MC_OK : (s == KRYLOV_NONFINITE ? MC_ERR_NONFINITE : MC_ERR_NOT_CONVERGED);
+}
+
+// Graph of one batch of iterations, captured on first use.
+template <typename Body>
+int run_batch(mc_flow *h, cudaGraphExec_t *exec, int kernels_in_batch, Body &&body)
+{
+    if (h->timing.on) {
+        body();
+        return check_launch(h);
+    }
+    if (!*exec) {
+        cudaGraph_t g;
+        CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        const long before = h->launches;
+        body();
+        h->launches = before;
+        CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
+        CUDA_TRY(h, cudaGraphInstantiate(exec, g, 0));
+        cudaGraphDestroy(g);
+    }
+    CUDA_TRY(h, cudaGraphLaunch(*exec, h->stream));
+    h->launches += kernels_in_batch;
+    return MC_OK;
+}
+
+int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, double *bnorm)
+{
+    const Ell A = pressure_matrix(h);
+    PcgVectors v = h->pv;
+    launch(h, K_PCG_MEAN, [&] { pcg_mean(h->stream, A, v); });
+    launch(h, K_PCG_INIT, [&] { pcg_init(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, 0, 1); });
+    int rc = check_launch(h);
+    if (rc) return rc;
+    // The device marks the solve done at max_iters; the host bound is a second guard.
+    const long max_batches = h->prm.max_iters / PCG_BATCH + 2;
+    for (long batch = 0;; batch++) {
+        CUDA_TRY(h, cudaMemcpyAsync(h->h_pcg, v.st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        flush_timing(h);
+        if (h->h_pcg->done) break;
+        if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "pressure solve state did not advance");
+        rc = run_batch(h, &h->g_pcg, PCG_BATCH * PCG_KERNELS_PER_ITER, [&] {
+            for (int it = 0; it < PCG_BATCH; it++) {
+                const int pin = it & 1;
+                launch(h, K_PCG_ITER1, [&] { pcg_iter1(h->stream, A, v, pin); });
+                launch(h, K_PCG_ITER2, [&] { pcg_iter2(h->stream, A, v, pin ^ 1); });
+            }
+        });
+        if (rc) return rc;
+    }
+    launch(h, K_PCG_XMEAN, [&] { pcg_xmean(h->stream, h->N, v); });
+    launch(h, K_PCG_SUBMEAN, [&] { pcg_sub_xmean(h->stream, h->N, v); });
+    rc = check_launch(h);
+    if (rc) return rc;
+    const PcgState &s = *h->h_pcg;
+    *iters = s.iter;
+    *bnorm = std::sqrt(s.bb);
+    *relres = s.bb > 0 ? std::sqrt(s.rr / s.bb) : 0.0;
+    return krylov_status_to_mc(s.status);
+}
+
+template <int R>
+int solve_bicg(mc_flow *h, const Ell &A, const BicgVectors<R> &v, BicgState<R> *hs, cudaGraphExec_t *exec,
+               int kid_init, int kid1, int iters_out[R])
+{
+    launch(h, kid_init, [&] { bicg_init<R>(h->stream, A, v, h->prm.u_rtol, h->prm.max_iters); });
+    int rc = check_launch(h);
+    if (rc) return rc;
+    const long max_batches = h->prm.max_iters / BICG_BATCH + 2;
+    for (long batch = 0;; batch++) {
+        CUDA_TRY(h, cudaMemcpyAsync(hs, v.st, sizeof(BicgState<R>), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        flush_timing(h);
+        if (hs->all_done) break;
+        if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "BiCGStab state did not advance");
+        rc = run_batch(h, exec, BICG_BATCH * BICG_KERNELS_PER_ITER, [&] {
+            for (int it = 0; it < BICG_BATCH; it++) {
+                const int pin = it & 1;
+                launch(h, kid1, [&] { bicg_1<R>(h->stream, A, v, pin); });
+                launch(h, kid1 + 1, [&] { bicg_2<R>(h->stream, A, v, pin ^ 1); });
+                launch(h, kid1 + 2, [&] { bicg_3<R>(h->stream, A, v, pin ^ 1); });
+            }
+        });
+        if (rc) return rc;
+    }
+    int worst = MC_OK;
+    for (int j = 0; j < R; j++) {
+        iters_out[j] = hs->iter[j];
+        const int s = krylov_status_to_mc(hs->status[j]);
+        if (s == MC_ERR_NONFINITE || worst == MC_OK) worst = (s != MC_OK) ? s : worst;
+    }
+    return worst;
+}
+
+// -------------------------------------------------------------- SIMPLE stages
+
+void launch_gradients5(mc_flow *h)
+{
+    GradArgs<5> a{};
+    const int fields[5] = {G_U, G_V, G_W, G_P, G_T};
+    for (int k = 0; k < 5; k++) {
+        a.phi[k] = h->phi[fields[k]];
+        a.gx[k] = h->grad[fields[k]][0];
+        a.gy[k] = h->grad[fields[k]][1];
+        a.gz[k] = h->grad[fields[k]][2];
+    }
+    a.zero_boundary = 1u << 3;  // pressure: dphi = 0 on boundary faces (FlowSolver.inl:980)
+    launch(h, K_GRAD5, [&] {
+        k_lsq_gradients<5><<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->N, h->nbr, h->fc1, h->xc, h->yc,
+                                                                             h->zc, h->xf, h->yf, h->zf, a);
+    });
+}
+
+void launch_gradient_pressure(mc_flow *h, int g)
+{
+    GradArgs<1> a{};
+    a.phi[0] = h->phi[g];
+    a.gx[0] = h->grad[g][0];
+    a.gy[0] = h->grad[g][1];
+    a.gz[0] = h->grad[g][2];
+    a.zero_boundary = 1u;
+    launch(h, K_GRAD1, [&] {
+        k_lsq_gradients<1><<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->N, h->nbr, h->fc1, h->xc, h->yc,
+                                                                             h->zc, h->xf, h->yf, h->zf, a);
+    });
+}
+
+void launch_mass_flux(mc_flow *h)
+{
+    MassFluxArgs a{};
+    a.U = h->phi[G_U];
+    a.V = h->phi[G_V];
+    a.W = h->phi[G_W];
+    a.P = h->phi[G_P];
+    a.AU = h->AU;
+    for (int d = 0; d < 3; d++) {
+        a.gU[d] = h->grad[G_U][d];
+        a.gV[d] = h->grad[G_V][d];
+        a.gW[d] = h->grad[G_W][d];
+        a.gP[d] = h->grad[G_P][d];
+    }
+    a.mdot = h->mdot;
+    a.ff0 = h->ff0;
+    a.ff1 = h->ff1;
+    a.partials = h->partials;
+    a.counter = h->counter;
+    a.balance = h->balance;
+    a.mass_source_total = (h->prm.mode == MC_MODE_SIMPLE && h->sources_set) ? h->mass_source_total : 0.0;
+    const int grid = std::min(blocks_for(h->F), krylov_grid(h->F));
+    launch(h, K_MASS_FLUX, [&] { k_mass_flux<<<grid, MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a); });
+    if (h->margs.n_outlet > 0)
+        launch(h, K_OUTLET_FIX, [&] {
+            k_outlet_fix<<<blocks_for(h->margs.n_outlet), MCB_THREADS, 0, h->stream>>>(
+                h->ph, h->margs, h->mdot, h->phi[G_U], h->phi[G_V], h->phi[G_W], h->balance);
+        });
+}
+
+int stage_gradients(mc_flow *h)
+{
+    launch_gradients5(h);
+    return check_launch(h);
+}
+
+int stage_set_up_field(mc_flow *h)
+{
+    launch(h, K_PRECOMP_AU, [&] {
+        k_precomp_au<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, h->mdot, h->AU);
+    });
+    launch_mass_flux(h);
+    return check_launch(h);
+}
+
+int stage_momentum(mc_flow *h, mc_iter_stats *st)
+{
+    MomentumArgs a{};
+    a.U = h->phi[G_U];
+    a.V = h->phi[G_V];
+    a.W = h->phi[G_W];
+    a.T = h->phi[G_T];
+    for (int d = 0; d < 3; d++) {
+        a.gU[d] = h->grad[G_U][d];
+        a.gV[d] = h->grad[G_V][d];
+        a.gW[d] = h->grad[G_W][d];
+        a.gP[d] = h->grad[G_P][d];
+    }
+    a.mdot = h->mdot;
+    a.src = h->sources_set ? h->src : nullptr;
+    a.off = h->off_m;
+    a.AU = h->AU;
+    a.b = h->b_m;
+    launch(h, K_MOMENTUM, [&] { k_momentum_assemble<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a); });
+    int rc = check_launch(h);
+    if (rc) return rc;
+    int its[3] = {0, 0, 0};
+    rc = solve_bicg<3>(h, momentum_matrix(h), h->b3, h->h_b3, &h->g_b3, K_BICG3_INIT, K_BICG3_1, its);
+    if (st)
+        for (int j = 0; j < 3; j++) st->momentum_iters[j] = its[j];
+    return rc;
+}
+
+int stage_pressure(mc_flow *h, mc_iter_stats *st)
+{
+    const int simple = h->prm.mode == MC_MODE_SIMPLE;
+    launch_mass_flux(h);
+    if (simple || h->first_pressure) {
+        PressureRowArgs a{};
+        a.mdot = h->mdot;
+        a.ff0 = h->ff0;
+        a.ff1 = h->ff1;
+        a.src = h->sources_set ? h->src : nullptr;
+        a.off = h->off_p;
+        a.diag = h->diag_p;
+        a.b = h->b_p;
+        launch(h, K_PRESSURE_ROWS, [&] {
+            k_pressure_rows<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a);
+        });
+    }
+    int rc = check_launch(h);
+    if (rc) return rc;
+    int loop = 0, worst = MC_OK;
+    double pc_ref = 0.0;
+    for (;;) {
+        loop++;
+        int its = 0;
+        double relres = 0.0, bnorm = 0.0;
+        const double floor = (simple && loop > 1) ? h->prm.p_rtol * h->p_bnorm_ref : 0.0;
+        rc = solve_pressure(h, floor, &its, &relres, &bnorm);
+        if (rc == MC_ERR_CUDA) return rc;
+        if (rc != MC_OK && worst == MC_OK) worst = rc;
+        if (loop == 1) h->p_bnorm_ref = bnorm;
+        if (st) {
+            st->pressure_solves++;
+            st->pressure_iters_total += its;
+            if (loop == 1) st->pressure_iters_first = its;
+            st->pressure_rel_residual = relres;
+        }
+        launch(h, K_PP_MAX, [&] {
+            k_pp_max<<<krylov_grid(h->N), MCB_THREADS, 0, h->stream>>>(h->N, h->phi[G_PP], h->partials, h->counter,
+                                                                       h->scalars);
+        });
+        CUDA_TRY(h, cudaMemcpyAsync(h->h_scalars, h->scalars, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        launch_gradient_pressure(h, G_PP);
+        CorrectArgs c{};
+        c.PP = h->phi[G_PP];
+        c.P = h->phi[G_P];
+        c.U = h->phi[G_U];
+        c.V = h->phi[G_V];
+        c.W = h->phi[G_W];
+        c.AU = h->AU;
+        for (int d = 0; d < 3; d++) c.gPP[d] = h->grad[G_PP][d];
+        c.ff0 = h->ff0;
+        c.mdot = h->mdot;
+        c.fcorr = h->fcorr;
+        c.next_rhs = simple ? h->b_p : nullptr;
+        const int grid_f = std::min(blocks_for(h->F), krylov_grid(h->F));
+        launch(h, K_PP_FACES, [&] { k_pp_correct_faces<<<grid_f, MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, c); });
+        const int cell0 = (!simple && h->first_pressure) ? 1 : 0;
+        launch(h, K_PP_CELLS, [&] {
+            k_pp_correct_cells<<<blocks_for(h->N + 6), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, c, simple, cell0);
+        });
+        if (cell0) h->first_pressure = 0;
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        flush_timing(h);
+        rc = check_launch(h);
+        if (rc) return rc;
+        const double pc_max = h->h_scalars[0];
+        if (loop == 1) {
+            pc_ref = pc_max;
+            if (st) st->pressure_correction_max_first = pc_max;
+        }
+        if (!std::isfinite(pc_max)) return fail(h, MC_ERR_NONFINITE, "pressure correction is not finite");
+        if (loop >= 4 || pc_max <= 0.25 * pc_ref) break;
+    }
+    launch_gradient_pressure(h, G_P);
+    launch(h, K_P_BOUNDARY, [&] {
+        k_update_p_boundary<<<1, 32, 0, h->stream>>>(h->ph, h->margs, h->phi[G_P], h->grad[G_P][0], h->grad[G_P][1],
+                                                     h->grad[G_P][2]);
+    });
+    rc = check_launch(h);
+    return rc ? rc : worst;
+}
+
+int stage_temperature(mc_flow *h, mc_iter_stats *st)
+{
+    ScalarArgs a{};
+    a.phi = h->phi[G_T];
+    for (int d = 0; d < 3; d++) a.g[d] = h->grad[G_T][d];
+    a.mdot = h->mdot;
+    a.src = h->sources_set ? h->src : nullptr;
+    a.off = h->off_t;
+    a.diag = h->diag_t;
+    a.b = h->b_t;
+    launch(h, K_TEMPERATURE, [&] {
+        k_temperature_assemble<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a);
+    });
+    int rc = check_launch(h);
+    if (rc) return rc;
+    int its[1] = {0};
+    rc = solve_bicg<1>(h, temperature_matrix(h), h->b1, h->h_b1, &h->g_b1, K_BICG1_INIT, K_BICG1_1, its);
+    if (st) st->temperature_iters = its[0];
+    return rc;
+}
+
+// ------------------------------------------------------------------ create
+
+int allocate(mc_flow *h)
+{
+    const size_t N = (size_t)h->N, F = (size_t)h->F, NB = N + 6;
+    Arena &A = h->arena;
+    const int G = krylov_grid(std::max(h->N, h->F));
+    struct Item { void **p; size_t bytes; };
+    std::vector<Item> items;
+    auto add = [&](void *pp, size_t bytes) { items.push_back({(void **)pp, bytes}); };
+    add(&h->fc0, F * 4); add(&h->fc1, F * 4);
+    add(&h->nbr, 6 * N * 4); add(&h->sface, 6 * N * 4); add(&h->col, 6 * N * 4);
+    add(&h->outlet_faces, std::max<size_t>(1, (size_t)h->margs.n_outlet) * 4);
+    for (double **p : {&h->area, &h->lam, &h->rl, &h->Sx, &h->Sy, &h->Sz, &h->xf, &h->yf, &h->zf}) add(p, F * 8);
+    for (double **p : {&h->xc, &h->yc, &h->zc, &h->vol, &h->rho}) add(p, N * 8);
+    for (int g = 0; g < G_NFIELDS; g++) {
+        add(&h->phi[g], NB * 8);
+        for (int d = 0; d < 3; d++) add(&h->grad[g][d], N * 8);
+    }
+    for (double **p : {&h->mdot, &h->ff0, &h->ff1, &h->fcorr}) add(p, F * 8);
+    add(&h->AU, N * 8); add(&h->off_m, 6 * N * 8); add(&h->b_m, 3 * N * 8);
+    add(&h->off_p, 6 * N * 8); add(&h->diag_p, N * 8); add(&h->b_p, N * 8);
+    add(&h->off_t, 6 * N * 8); add(&h->diag_t, N * 8); add(&h->b_t, N * 8);
+    add(&h->src, 5 * N * 8);
+    add(&h->partials, (size_t)G * 8 * 8);
+    add(&h->counter, 256);
+    add(&h->balance, sizeof(FluxBalance));
+    add(&h->scalars, 8 * 8);
+    // PCG
+    add(&h->pv.r, N * 8); add(&h->pv.z, N * 8); add(&h->pv.p[0], N * 8); add(&h->pv.p[1], N * 8);
+    add(&h->pv.q, N * 8); add(&h->pv.st, sizeof(PcgState));
+    // BiCGStab, three right-hand sides; the single-RHS solver shares the vectors
+    double *bic[8];
+    for (int k = 0; k < 8; k++) add(&bic[k], 3 * N * 8);
+    add(&h->b3.st, sizeof(BicgState<3>));
+    add(&h->b1.st, sizeof(BicgState<1>));
+    size_t total = 0;
+    std::vector<size_t> offs;
+    for (auto &it : items) offs.push_back(A.reserve(it.bytes));
+    total = A.used;
+    cudaError_t e = cudaMalloc((void **)&A.base, total);
+    if (e != cudaSuccess) return fail(h, MC_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    A.size = total;
+    for (size_t i = 0; i < items.size(); i++) *items[i].p = A.base + offs[i];
+    CUDA_TRY(h, cudaMemsetAsync(A.base, 0, total, h->stream));
+    h->pv.partials = h->partials;
+    h->pv.counter = h->counter;
+    h->b3.partials = h->b1.partials = h->partials;
+    h->b3.counter = h->b1.counter = h->counter;
+    h->b3.r = bic[0]; h->b3.r0 = bic[1]; h->b3.p[0] = bic[2]; h->b3.p[1] = bic[3];
+    h->b3.v[0] = bic[4]; h->b3.v[1] = bic[5]; h->b3.s = bic[6]; h->b3.t = bic[7];
+    h->b1.r = bic[0]; h->b1.r0 = bic[1]; h->b1.p[0] = bic[2]; h->b1.p[1] = bic[3];
+    h->b1.v[0] = bic[4]; h->b1.v[1] = bic[5]; h->b1.s = bic[6]; h->b1.t = bic[7];
+    h->b3.b = h->b_m;
+    h->b3.x[0] = h->phi[G_U];
+    h->b3.x[1] = h->phi[G_V];
+    h->b3.x[2] = h->phi[G_W];
+    h->b1.b = h->b_t;
+    h->b1.x[0] = h->phi[G_T];
+    h->pv.b = h->b_p;
+    h->pv.x = h->phi[G_PP];
+    CUDA_TRY(h, cudaMallocHost((void **)&h->h_pcg, sizeof(PcgState)));
+    CUDA_TRY(h, cudaMallocHost((void **)&h->h_b3, sizeof(BicgState<3>)));
+    CUDA_TRY(h, cudaMallocHost((void **)&h->h_b1, sizeof(BicgState<1>)));
+    CUDA_TRY(h, cudaMallocHost((void **)&h->h_scalars, 8 * sizeof(double)));
+    return MC_OK;
+}
+
+template <typename T>
+int upload(mc_flow *h, T *dst, const T *src, size_t n)
+{
+    CUDA_TRY(h, cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+    return MC_OK;
+}
+
+// Split [n][3] host data into three device arrays.
+int upload3(mc_flow *h, double *x, double *y, double *z, const std::vector<double> &v, size_t n)
+{
+    std::vector<double> tmp(n);
+    double *dst[3] = {x, y, z};
+    for (int d = 0; d < 3; d++) {
+        for (size_t i = 0; i < n; i++) tmp[i] = v[3 * i + d];
+        CUDA_TRY(h, cudaMemcpy(dst[d], tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    return MC_OK;
+}
+
+// Initial state of the FlowSolver constructor (FlowSolver.hpp:315-327 interior,
+// :403-471 boundary slots).
+int initial_fields(mc_flow *h, const int btype[6])
+{
+    const size_t NB = (size_t)h->N + 6;
+    std::vector<double> v(NB);
+    auto put = [&](int g, double interior, double inlet, double outlet, double wall) -> int {
+        std::fill(v.begin(), v.begin() + h->N, interior);
+        for (int s = 0; s < 6; s++) v[h->N + s] = btype[s] == INLET ? inlet : (btype[s] == OUTLET ? outlet : wall);
+        CUDA_TRY(h, cudaMemcpy(h->phi[g], v.data(), NB * sizeof(double), cudaMemcpyHostToDevice));
+        return MC_OK;
+    };
+    const mc_flow_params &p = h->prm;
+    int rc = put(G_U, p.inlet_u, p.inlet_u, p.inlet_u, 0.0);
+    rc = rc ? rc : put(G_V, 0.0, 0.0, 0.0, 0.0);
+    rc = rc ? rc : put(G_W, 0.0, 0.0, 0.0, 0.0);
+    rc = rc ? rc : put(G_P, p.pressure0, p.pressure0, p.pressure0, p.pressure0);
+    rc = rc ? rc : put(G_PP, 0.0, 0.0, 0.0, 0.0);
+    rc = rc ? rc : put(G_T, p.temperature0, p.temperature0, p.temperature0, p.temperature0);
+    return rc;
+}
+
+} // namespace
+
+// =================================================================== C ABI
+
+extern "C" {
+
+void mc_flow_default_params(mc_flow_params *p, int mode)
+{
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->mode = mode;
+    p->delta = 1.0e-5;
+    p->density = 1.2;
+    p->inlet_u = 50.0;
+    p->pressure0 = 4000.0;
+    p->flux_corr = 0.8;
+    p->urf_temperature = 0.95;
+    p->max_iters = 10000;
+    p->pressure_solver = MC_PSOLVER_PCG_JACOBI;
+    p->precision = MC_PRECISION_FP64;
+    p->initial_guess = MC_GUESS_ZERO;
+    if (mode == MC_MODE_COMPAT) {
+        p->viscosity = 0.000014;
+        p->temperature0 = 2000.0;
+        p->urf_momentum = 0.5;
+        p->urf_pressure = 0.2;
+        p->u_rtol = 1e-13;
+        p->p_rtol = 1e-13;
+    } else {
+        p->viscosity = 1.8e-5;
+        p->temperature0 = 1500.0;
+        p->urf_momentum = 0.7;
+        p->urf_pressure = 0.3;
+        p->u_rtol = 1e-8;
+        p->p_rtol = 1e-8;
+    }
+}
+
+int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_flow **out)
+{
+    if (!mesh || !params || !out) return MC_ERR_ARG;
+    *out = nullptr;
+    if (params->mode != MC_MODE_COMPAT && params->mode != MC_MODE_SIMPLE) return MC_ERR_ARG;
+    if (params->pressure_solver != MC_PSOLVER_PCG_JACOBI || params->precision != MC_PRECISION_FP64 ||
+        params->initial_guess != MC_GUESS_ZERO)
+        return MC_ERR_UNSUPPORTED;
+    if (!(params->delta > 0) || !(params->urf_momentum > 0) || !(params->urf_temperature > 0) ||
+        !(params->u_rtol > 0) || !(params->p_rtol > 0) || params->max_iters <= 0)
+        return MC_ERR_ARG;
+    mc_flow *h = new (std::nothrow) mc_flow();
+    if (!h) return MC_ERR_NOMEM;
+    h->prm = *params;
+    int rc = MC_OK;
+    {
+        HostMesh hm;
+        std::string err;
+        HostPhysics hp{params->density};
+        rc = build_host_mesh(mesh, hp, hm, err);
+        if (rc) {
+            h->err = err;
+            mc_flow_destroy(h);
+            return rc;
+        }
+        cudaError_t e = cudaSetDevice(params->device);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            mc_flow_destroy(h);
+            return MC_ERR_CUDA;
+        }
+        h->dev = params->device;
+        h->N = hm.N;
+        h->F = hm.F;
+        h->margs.n_outlet = (int)hm.outlet_faces.size();
+        rc = allocate(h);
+        if (!rc) {
+            const size_t N = hm.N, F = hm.F;
+            rc = upload(h, h->fc0, hm.fc0.data(), F);
+            rc = rc ? rc : upload(h, h->fc1, hm.fc1.data(), F);
+            rc = rc ? rc : upload(h, h->nbr, hm.nbr.data(), 6 * N);
+            rc = rc ? rc : upload(h, h->sface, hm.sface.data(), 6 * N);
+            rc = rc ? rc : upload(h, h->col, hm.col.data(), 6 * N);
+            if (!rc && !hm.outlet_faces.empty()) rc = upload(h, h->outlet_faces, hm.outlet_faces.data(), hm.outlet_faces.size());
+            rc = rc ? rc : upload(h, h->area, hm.area.data(), F);
+            rc = rc ? rc : upload(h, h->lam, hm.lam.data(), F);
+            rc = rc ? rc : upload(h, h->rl, hm.rl.data(), F);
+            rc = rc ? rc : upload(h, h->vol, hm.vol.data(), N);
+            rc = rc ? rc : upload(h, h->rho, hm.rho.data(), N);
+            if (!rc) cudaStreamSynchronize(h->stream);
+            rc = rc ? rc : upload3(h, h->Sx, h->Sy, h->Sz, hm.S, F);
+            rc = rc ? rc : upload3(h, h->xf, h->yf, h->zf, hm.xf, F);
+            rc = rc ? rc : upload3(h, h->xc, h->yc, h->zc, hm.xc, N);
+            rc = rc ? rc : initial_fields(h, hm.btype);
+        }
+        if (!rc) {
+            h->hcol.assign((size_t)6 * hm.N, -1);
+            for (int k = 0; k < 6; k++)
+                for (int c = 0; c < hm.N; c++) {
+                    const int f = hm.sface[(size_t)k * hm.N + c];
+                    if (hm.fc1[f] < hm.N) h->hcol[(size_t)k * hm.N + c] = hm.col[(size_t)k * hm.N + c];
+                }
+            Physics &ph = h->ph;
+            ph.N = hm.N;
+            ph.mode = params->mode;
+            for (int s = 0; s < 6; s++) {
+                ph.btype[s] = hm.btype[s];
+                ph.last_bface[s] = hm.last_bface[s];
+            }
+            ph.mu = params->viscosity;
+            ph.inlet_mu = inlet_effective_viscosity(params->viscosity, params->inlet_u);
+            ph.u_in = params->inlet_u;
+            ph.rho_in = params->density;
+            ph.T_ref = params->temperature0;
+            ph.rdelta = 1.0 / params->delta;
+            ph.urf_u = params->urf_momentum;
+            ph.urf_T = params->urf_temperature;
+            ph.urf_p = params->urf_pressure;
+            ph.flux_corr = params->flux_corr;
+            MeshArgs &m = h->margs;
+            m.F = hm.F;
+            m.fc0 = h->fc0; m.fc1 = h->fc1; m.sface = h->sface;
+            m.area = h->area; m.lam = h->lam; m.rl = h->rl;
+            m.Sx = h->Sx; m.Sy = h->Sy; m.Sz = h->Sz;
+            m.xf = h->xf; m.yf = h->yf; m.zf = h->zf;
+            m.xc = h->xc; m.yc = h->yc; m.zc = h->zc;
+            m.vol = h->vol; m.rho = h->rho;
+            m.outlet_faces = h->outlet_faces;
+        }
+    }
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) rc = fail(h, MC_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (rc) {
+        mc_flow_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return MC_OK;
+}
+
+int mc_flow_destroy(mc_flow *h)
+{
+    if (!h) return MC_ERR_ARG;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (cudaGraphExec_t g : {h->g_pcg, h->g_b3, h->g_b1})
+        if (g) cudaGraphExecDestroy(g);
+    for (cudaEvent_t e : h->timing.ev) cudaEventDestroy(e);
+    if (h->arena.base) cudaFree(h->arena.base);
+    if (h->h_pcg) cudaFreeHost(h->h_pcg);
+    if (h->h_b3) cudaFreeHost(h->h_b3);
+    if (h->h_b1) cudaFreeHost(h->h_b1);
+    if (h->h_scalars) cudaFreeHost(h->h_scalars);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return MC_OK;
+}
+
+int mc_flow_set_field(mc_flow *h, int field, const double *vals)
+{
+    if (!h || !vals) return MC_ERR_ARG;
+    const int g = grad_index(field);
+    if (g < 0) return MC_ERR_UNSUPPORTED;
+    CUDA_TRY(h, cudaMemcpyAsync(h->phi[g], vals, ((size_t)h->N + 6) * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return MC_OK;
+}
+
+int mc_flow_get_field(mc_flow *h, int field, double *vals)
+{
+    if (!h || !vals) return MC_ERR_ARG;
+    const int g = grad_index(field);
+    if (g < 0) return MC_ERR_UNSUPPORTED;
+    CUDA_TRY(h, cudaMemcpyAsync(vals, h->phi[g], ((size_t)h->N + 6) * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return MC_OK;
+}
+
+int mc_flow_get_gradient(mc_flow *h, int field, double *vals)
+{
+    if (!h || !vals) return MC_ERR_ARG;
+    const int g = grad_index(field);
+    if (g < 0) return MC_ERR_UNSUPPORTED;
+    std::vector<double> tmp((size_t)h->N);
+    for (int d = 0; d < 3; d++) {
+        CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), h->grad[g][d], (size_t)h->N * 8, cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        for (int i = 0; i < h->N; i++) vals[3 * (size_t)i + d] = tmp[i];
+    }
+    return MC_OK;
+}
+
+int mc_flow_set_sources(mc_flow *h, const double *terms)
+{
+    if (!h || !terms) return MC_ERR_ARG;
+    const size_t N = (size_t)h->N;
+    std::vector<double> soa(5 * N);
+    double total = 0.0;
+    for (size_t i = 0; i < N; i++) {
+        for (int k = 0; k < 5; k++) soa[k * N + i] = terms[5 * i + k];
+        total += terms[5 * i + 4];
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(h->src, soa.data(), 5 * N * 8, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->mass_source_total = total;
+    h->sources_set = 1;
+    return MC_OK;
+}
+
+int mc_flow_get_face_array(mc_flow *h, int which, double *vals)
+{
+    if (!h || !vals) return MC_ERR_ARG;
+    const size_t F = (size_t)h->F;
+    auto get1 = [&](const double *d, int stride, int comp) -> int {
+        std::vector<double> tmp(F);
+        CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), d, F * 8, cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        for (size_t i = 0; i < F; i++) vals[stride * i + comp] = tmp[i];
+        return MC_OK;
+    };
+    switch (which) {
+    case 0: return get1(h->mdot, 1, 0);
+    case 1: return get1(h->area, 1, 0);
+    case 2: return get1(h->lam, 1, 0);
+    case 3: return get1(h->rl, 1, 0);
+    case 4: { int rc = get1(h->ff0, 2, 0); return rc ? rc : get1(h->ff1, 2, 1); }
+    case 5: { int rc = get1(h->Sx, 3, 0); rc = rc ? rc : get1(h->Sy, 3, 1); return rc ? rc : get1(h->Sz, 3, 2); }
+    case 6: { int rc = get1(h->xf, 3, 0); rc = rc ? rc : get1(h->yf, 3, 1); return rc ? rc : get1(h->zf, 3, 2); }
+    default: return MC_ERR_ARG;
+    }
+}
+
+int mc_flow_get_cell_array(mc_flow *h, int which, double *vals)
+{
+    if (!h || !vals) return MC_ERR_ARG;
+    const double *src = which == 0 ? h->AU : which == 1 ? h->diag_p : which == 2 ? h->vol : which == 3 ? h->rho : nullptr;
+    if (!src) return MC_ERR_ARG;
+    CUDA_TRY(h, cudaMemcpyAsync(vals, src, (size_t)h->N * 8, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return MC_OK;
+}
+
+int mc_flow_get_csr(mc_flow *h, int system, int *n, int *nnz, int *row_ptr, int *col, double *val, double *rhs)
+{
+    if (!h || !n || !nnz) return MC_ERR_ARG;
+    const size_t N = (size_t)h->N;
+    const double *d_diag, *d_off, *d_rhs;
+    switch (system) {
+    case MC_SYSTEM_MOMENTUM: d_diag = h->AU; d_off = h->off_m; d_rhs = h->b_m; break;
+    case MC_SYSTEM_PRESSURE: d_diag = h->diag_p; d_off = h->off_p; d_rhs = h->b_p; break;
+    case MC_SYSTEM_TEMPERATURE: d_diag = h->diag_t; d_off = h->off_t; d_rhs = h->b_t; break;
+    case 3: d_diag = h->AU; d_off = h->off_m; d_rhs = h->b_m + N; break;      // momentum, V right-hand side
+    case 4: d_diag = h->AU; d_off = h->off_m; d_rhs = h->b_m + 2 * N; break;  // momentum, W right-hand side
+    default: return MC_ERR_ARG;
+    }
+    size_t count = N;
+    for (int c : h->hcol) count += c >= 0;
+    *n = (int)N;
+    *nnz = (int)count;
+    if (!row_ptr && !col && !val && !rhs) return MC_OK;
+    std::vector<double> diag(N), off(6 * N);
+    CUDA_TRY(h, cudaMemcpyAsync(diag.data(), d_diag, N * 8, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(off.data(), d_off, 6 * N * 8, cudaMemcpyDeviceToHost, h->stream));
+    if (rhs) CUDA_TRY(h, cudaMemcpyAsync(rhs, d_rhs, N * 8, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    size_t pos = 0;
+    std::vector<std::pair<int, double>> row;
+    for (size_t i = 0; i < N; i++) {
+        row.clear();
+        row.push_back({(int)i, diag[i]});
+        for (int k = 0; k < 6; k++) {
+            const int c = h->hcol[k * N + i];
+            if (c >= 0) row.push_back({c, off[k * N + i]});
+        }
+        std::sort(row.begin(), row.end(), [](const std::pair<int, double> &a, const std::pair<int, double> &b) {
+            return a.first < b.first;
+        });
+        if (row_ptr) row_ptr[i] = (int)pos;
+        for (auto &e : row) {
+            if (col) col[pos] = e.first;
+            if (val) val[pos] = e.second;
+            pos++;
+        }
+    }
+    if (row_ptr) row_ptr[N] = (int)pos;
+    return MC_OK;
+}
+
+int mc_flow_stage_gradients(mc_flow *h)
+{
+    if (!h) return MC_ERR_ARG;
+    int rc = stage_gradients(h);
+    if (!rc) CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    flush_timing(h);
+    return rc;
+}
+
+int mc_flow_stage_set_up_field(mc_flow *h)
+{
+    if (!h) return MC_ERR_ARG;
+    int rc = stage_set_up_field(h);
+    if (!rc) CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    flush_timing(h);
+    return rc;
+}
+
+int mc_flow_stage_momentum(mc_flow *h, mc_iter_stats *st)
+{
+    if (!h) return MC_ERR_ARG;
+    const int rc = stage_momentum(h, st);
+    flush_timing(h);
+    return rc;
+}
+
+int mc_flow_stage_pressure(mc_flow *h, mc_iter_stats *st)
+{
+    if (!h) return MC_ERR_ARG;
+    const int rc = stage_pressure(h, st);
+    if (rc != MC_ERR_CUDA) CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    flush_timing(h);
+    return rc;
+}
+
+int mc_flow_stage_temperature(mc_flow *h, mc_iter_stats *st)
+{
+    if (!h) return MC_ERR_ARG;
+    const int rc = stage_temperature(h, st);
+    flush_timing(h);
+    return rc;
+}
+
+// One pass of FlowSolver::timestep's loop (FlowSolver.inl:3188-3268).
+int mc_flow_simple_iteration(mc_flow *h, mc_iter_stats *st)
+{
+    if (!h) return MC_ERR_ARG;
+    mc_iter_stats local{};
+    mc_iter_stats *s = st ? st : &local;
+    memset(s, 0, sizeof(*s));
+    int worst = MC_OK;
+    auto track = [&](int rc) -> int {
+        if (rc == MC_ERR_CUDA || rc == MC_ERR_NONFINITE) return rc;
+        if (rc != MC_OK && worst == MC_OK) worst = rc;
+        return MC_OK;
+    };
+    int rc = stage_gradients(h);
+    if (rc) return rc;
+    if (h->timestep_count == 0 && h->pass_in_step == 0) {
+        rc = stage_set_up_field(h);
+        if (rc) return rc;
+    }
+    if ((rc = track(stage_momentum(h, s)))) return rc;
+    if ((rc = track(stage_pressure(h, s)))) return rc;
+    if ((rc = track(stage_temperature(h, s)))) return rc;
+    launch(h, K_IMBALANCE, [&] {
+        k_mass_imbalance<<<krylov_grid(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, h->mdot,
+                                                                           h->sources_set ? h->src : nullptr,
+                                                                           h->partials, h->counter, h->scalars + 1);
+    });
+    CUDA_TRY(h, cudaMemcpyAsync(h->h_scalars + 1, h->scalars + 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    flush_timing(h);
+    rc = check_launch(h);
+    if (rc) return rc;
+    s->mass_imbalance = h->h_scalars[1];
+    h->pass_in_step++;
+    if (h->pass_in_step == 3) {
+        h->pass_in_step = 0;
+        h->timestep_count++;
+    }
+    return worst;
+}
+
+int mc_flow_timestep(mc_flow *h, mc_iter_stats *st)
+{
+    if (!h) return MC_ERR_ARG;
+    int worst = MC_OK;
+    do {
+        const int rc = mc_flow_simple_iteration(h, st);
+        if (rc == MC_ERR_CUDA || rc == MC_ERR_NONFINITE || rc == MC_ERR_ARG) return rc;
+        if (rc != MC_OK && worst == MC_OK) worst = rc;
+    } while (h->pass_in_step != 0);
+    return worst;
+}
+
+int mc_flow_set_timing(mc_flow *h, int enable)
+{
+    if (!h) return MC_ERR_ARG;
+    flush_timing(h);
+    h->timing.on = enable != 0;
+    return MC_OK;
+}
+
+int mc_flow_kernel_count(void) { return K_COUNT; }
+
+const char *mc_flow_kernel_name(int id) { return (id >= 0 && id < K_COUNT) ? kKernelNames[id] : ""; }
+
+int mc_flow_get_kernel_times(mc_flow *h, double *total_ms, long *launches)
+{
+    if (!h) return MC_ERR_ARG;
+    flush_timing(h);
+    for (int i = 0; i < K_COUNT; i++) {
+        if (total_ms) total_ms[i] = h->timing.total_ms[i];
+        if (launches) launches[i] = h->timing.count[i];
+    }
+    return MC_OK;
+}
+
+int mc_flow_reset_kernel_times(mc_flow *h)
+{
+    if (!h) return MC_ERR_ARG;
+    flush_timing(h);
+    for (int i = 0; i < K_COUNT; i++) {
+        h->timing.total_ms[i] = 0.0;
+        h->timing.count[i] = 0;
+    }
+    return MC_OK;
+}
+
+void *mc_flow_stream(mc_flow *h) { return h ? (void *)h->stream : nullptr; }
+long mc_flow_launch_count(mc_flow *h) { return h ? h->launches : 0; }
+const char *mc_flow_last_error(mc_flow *h) { return h ? h->err.c_str() : ""; }
+
+const char *mc_status_string(int s)
+{
+    switch (s) {
+    case MC_OK: return "ok";
+    case MC_ERR_ARG: return "invalid argument";
+    case MC_ERR_CUDA: return "CUDA error";
+    case MC_ERR_NOT_CONVERGED: return "linear solve did not converge";
+    case MC_ERR_NONFINITE: return "non-finite value";
+    case MC_ERR_MESH: return "inconsistent mesh";
+    case MC_ERR_NOMEM: return "out of memory";
+    case MC_ERR_UNSUPPORTED: return "unsupported option";
+    default: return "unknown status";
+    }
+}
+
+} // extern "C"

@@ -1,0 +1,685 @@
+// SIMPLE-pass assembly kernels for sm_100a (FP64).  Built with -fmad=false:
+// every expression below is evaluated as the plain IEEE sequence the
+// reference's C++ spells out (FlowSolver.inl), so the assembled coefficients
+// equal the CPU oracle's bit for bit.
+//
+// Design: cell-centric gathers.  One thread owns one cell and walks its six
+// faces in reference face order (sface), recomputing the face quantity it
+// needs from face geometry and the two adjacent cells.  Every accumulation a
+// reference face loop scatters into a cell happens here inside that cell's
+// thread in the same order, so there are no atomics and results are
+// deterministic.  Face-owned outputs (mass flux) come from face-parallel
+// kernels.  All kernels are HBM-bandwidth bound.
+#include "flow_kernels.cuh"
+#include "mc_reduce.cuh"
+
+namespace mcb {
+
+namespace {
+
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }  // std::min
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }  // std::max
+
+// solve (FlowSolver.inl:895-915): Cramer's rule on the symmetric LSQ matrix.
+__device__ __forceinline__ void cramer(double A00, double A10, double A20, double A11, double A21, double A22,
+                                       const double b0, const double b1, const double b2, double &o0, double &o1,
+                                       double &o2)
+{
+    const double A01 = A10, A02 = A20, A12 = A21;
+    const double det = (A00 * (A11 * A22 - A21 * A12)) - (A01 * (A10 * A22 - A20 * A12)) +
+                       (A02 * (A10 * A21 - A20 * A11));
+    double invdet = 0.0;
+    if (det != 0.0) invdet = 1 / det;
+    o0 = (b0 * invdet * (A11 * A22 - A21 * A12)) + (b1 * invdet * (A21 * A02 - A01 * A22)) +
+         (b2 * invdet * (A01 * A12 - A11 * A02));
+    o1 = (b0 * invdet * (A12 * A20 - A10 * A22)) + (b1 * invdet * (A00 * A22 - A20 * A02)) +
+         (b2 * invdet * (A10 * A02 - A00 * A12));
+    o2 = (b0 * invdet * (A10 * A21 - A20 * A11)) + (b1 * invdet * (A20 * A01 - A00 * A21)) +
+         (b2 * invdet * (A00 * A11 - A10 * A01));
+}
+
+__device__ __forceinline__ int grid_stride_start() { return blockIdx.x * blockDim.x + threadIdx.x; }
+
+} // namespace
+
+// ------------------------------------------------------------- gradients
+// get_phi_gradients / get_phi_gradient (FlowSolver.inl:738-803, 917-1063).
+// Over slot f in cell_faces order: dX = x_nbr - x_c (equal to the reference's
+// mask * (x1 - x0)), boundary dX = x_face - x_c; dphi likewise, or 0 on
+// boundary faces for pressure-like fields.
+template <int NF>
+__global__ void __launch_bounds__(MCB_THREADS) k_lsq_gradients(int N, const int *__restrict__ nbr,
+                                                              const int *__restrict__ fc1, const double *__restrict__ xc,
+                                                              const double *__restrict__ yc,
+                                                              const double *__restrict__ zc,
+                                                              const double *__restrict__ xf,
+                                                              const double *__restrict__ yf,
+                                                              const double *__restrict__ zf, GradArgs<NF> a)
+{
+    const int c = grid_stride_start();
+    if (c >= N) return;
+    const double x = xc[c], y = yc[c], z = zc[c];
+    double pc[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) pc[k] = a.phi[k][c];
+    double A00 = 0.0, A10 = 0.0, A20 = 0.0, A11 = 0.0, A21 = 0.0, A22 = 0.0;
+    double b[NF][3];
+#pragma unroll
+    for (int k = 0; k < NF; k++) b[k][0] = b[k][1] = b[k][2] = 0.0;
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        const int n = nbr[(size_t)f * N + c];
+        double dx, dy, dz, dphi[NF];
+        if (n >= 0) {
+            dx = xc[n] - x;
+            dy = yc[n] - y;
+            dz = zc[n] - z;
+#pragma unroll
+            for (int k = 0; k < NF; k++) dphi[k] = a.phi[k][n] - pc[k];
+        } else {
+            const int face = -1 - n;
+            dx = xf[face] - x;
+            dy = yf[face] - y;
+            dz = zf[face] - z;
+            const int slot = fc1[face];
+#pragma unroll
+            for (int k = 0; k < NF; k++) dphi[k] = ((a.zero_boundary >> k) & 1) ? 0.0 : a.phi[k][slot] - pc[k];
+        }
+        A00 += (dx * dx);
+        A10 += (dx * dy);
+        A20 += (dx * dz);
+        A11 += (dy * dy);
+        A21 += (dy * dz);
+        A22 += (dz * dz);
+#pragma unroll
+        for (int k = 0; k < NF; k++) {
+            b[k][0] += (dx * dphi[k]);
+            b[k][1] += (dy * dphi[k]);
+            b[k][2] += (dz * dphi[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+        double gx, gy, gz;
+        cramer(A00, A10, A20, A11, A21, A22, b[k][0], b[k][1], b[k][2], gx, gy, gz);
+        a.gx[k][c] = gx;
+        a.gy[k][c] = gy;
+        a.gz[k][c] = gz;
+    }
+}
+
+template __global__ void k_lsq_gradients<5>(int, const int *, const int *, const double *, const double *,
+                                            const double *, const double *, const double *, const double *,
+                                            GradArgs<5>);
+template __global__ void k_lsq_gradients<1>(int, const int *, const int *, const double *, const double *,
+                                            const double *, const double *, const double *, const double *,
+                                            GradArgs<1>);
+
+// -------------------------------------------------------------- precomp_AU
+// precomp_AU (FlowSolver.inl:1065-1104): inlet/outlet viscous part plus rho V / dt.
+__global__ void __launch_bounds__(MCB_THREADS) k_precomp_au(Physics ph, MeshArgs m, const double *__restrict__ mdot,
+                                                            double *__restrict__ AU)
+{
+    const int N = ph.N;
+    const int c = grid_stride_start();
+    if (c >= N) return;
+    double a = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        const int face = m.sface[(size_t)k * N + c];
+        const int c1 = m.fc1[face];
+        if (c1 < N) continue;
+        const int t = ph.btype[c1 - N];
+        if (t == INLET || t == OUTLET) {
+            const double VisFace = ph.mu * m.rl[face];
+            const double f = -VisFace + smin(mdot[face], 0.0);
+            a = a - f;
+        }
+    }
+    const double f = m.rho[c] * m.vol[c] * ph.rdelta;
+    a += f;
+    AU[c] = a;
+}
+
+// ---------------------------------------------------------------- momentum
+// calculate_flux_UVW (FlowSolver.inl:1377-1653), the cell source terms of
+// calculate_UVW (:1689-1729) and setup/update_sparse_matrix (:1186-1339) for
+// the three velocity components at once.  The U, V and W systems share the
+// off-diagonal coefficients and, bit for bit, the diagonal.
+__global__ void __launch_bounds__(MCB_THREADS) k_momentum_assemble(Physics ph, MeshArgs m, MomentumArgs a)
+{
+    const int N = ph.N;
+    const int c = grid_stride_start();
+    if (c >= N) return;
+    const double xcc = m.xc[c], ycc = m.yc[c], zcc = m.zc[c];
+    const double Uc = a.U[c], Vc = a.V[c], Wc = a.W[c];
+    double su = 0.0, sv = 0.0, sw = 0.0, ac = 0.0;
+    double offv[6];
+    unsigned internal = 0u;
+    const double mu = ph.mu;
+    for (int k = 0; k < 6; k++) {
+        const int face = m.sface[(size_t)k * N + c];
+        const int c0 = m.fc0[face], c1 = m.fc1[face];
+        const double Sx = m.Sx[face], Sy = m.Sy[face], Sz = m.Sz[face];
+        if (c1 < N) {
+            internal |= 1u << k;
+            const double l0 = m.lam[face];
+            const double l1 = 1.0 - l0;
+            const double dUx = a.gU[0][c0] * l0 + a.gU[0][c1] * l1;
+            const double dUy = a.gU[1][c0] * l0 + a.gU[1][c1] * l1;
+            const double dUz = a.gU[2][c0] * l0 + a.gU[2][c1] * l1;
+            const double dVx = a.gV[0][c0] * l0 + a.gV[0][c1] * l1;
+            const double dVy = a.gV[1][c0] * l0 + a.gV[1][c1] * l1;
+            const double dVz = a.gV[2][c0] * l0 + a.gV[2][c1] * l1;
+            const double dWx = a.gW[0][c0] * l0 + a.gW[0][c1] * l1;
+            const double dWy = a.gW[1][c0] * l0 + a.gW[1][c1] * l1;
+            const double dWz = a.gW[2][c0] * l0 + a.gW[2][c1] * l1;
+            const double Visac = mu * l0 + mu * l1;
+            const double VisFace = Visac * m.rl[face];
+            const double Xx = m.xc[c1] - m.xc[c0], Xy = m.yc[c1] - m.yc[c0], Xz = m.zc[c1] - m.zc[c0];
+            const double md = a.mdot[face];
+            const double fude = Visac * ((dUx + dUx) * Sx + (dUy + dVx) * Sy + (dUz + dWx) * Sz);
+            const double fvde = Visac * ((dUy + dVx) * Sx + (dVy + dVy) * Sy + (dVz + dWy) * Sz);
+            const double fwde = Visac * ((dUz + dWx) * Sx + (dWy + dVz) * Sy + (dWz + dWz) * Sz);
+            const double fudi = VisFace * (dUx * Xx + dUy * Xy + dUz * Xz);
+            const double fvdi = VisFace * (dVx * Xx + dVy * Xy + dVz * Xz);
+            const double fwdi = VisFace * (dWx * Xx + dWy * Xy + dWz * Xz);
+            // The deferred-correction blend is GammaBlend = 0 (:1387) and is omitted.
+            if (c == c0) {
+                su = su + fude - fudi;
+                sv = sv + fvde - fvdi;
+                sw = sw + fwde - fwdi;
+                offv[k] = -VisFace + smin(md, 0.0);  // face_fields.cell1, column c1
+            } else {
+                su = su - fude + fudi;
+                sv = sv - fvde + fvdi;
+                sw = sw - fwde + fwdi;
+                offv[k] = -VisFace - smax(md, 0.0);  // face_fields.cell0, column c0
+            }
+        } else {
+            offv[k] = 0.0;
+            const int side = c1 - N;
+            const int t = ph.btype[side];
+            const double Xx = m.xf[face] - xcc, Xy = m.yf[face] - ycc, Xz = m.zf[face] - zcc;
+            if (t == INLET || t == OUTLET) {
+                const double dUx = a.gU[0][c], dUy = a.gU[1][c], dUz = a.gU[2][c];
+                const double dVx = a.gV[0][c], dVy = a.gV[1][c], dVz = a.gV[2][c];
+                const double dWx = a.gW[0][c], dWy = a.gW[1][c], dWz = a.gW[2][c];
+                double UF, VF, WF, Visac;
+                if (t == INLET) {
+                    UF = ph.u_in;
+                    VF = 0.0;
+                    WF = 0.0;
+                    Visac = ph.inlet_mu;
+                } else {
+                    UF = Uc;
+                    VF = Vc;
+                    WF = Wc;
+                    Visac = mu;
+                }
+                const double VisFace = Visac * m.rl[face];
+                const double fude = Visac * ((dUx + dUx) * Sx + (dUy + dVx) * Sy + (dUz + dWx) * Sz);
+                const double fvde = Visac * ((dUy + dVx) * Sx + (dVy + dVy) * Sy + (dVz + dWy) * Sz);
+                const double fwde = Visac * ((dUz + dWx) * Sx + (dWy + dVz) * Sy + (dWz + dWz) * Sz);
+                const double fudi = VisFace * (dUx * Xx + dUy * Xy + dUz * Xz);
+                const double fvdi = VisFace * (dVx * Xx + dVy * Xy + dVz * Xz);
+                const double fwdi = VisFace * (dWx * Xx + dWy * Xy + dWz * Xz);
+                double md = a.mdot[face];
+                if (t == OUTLET && md < 0.0) {  // :1576-1580
+                    md = 1e-15;
+                    a.mdot[face] = md;
+                }
+                const double f = -VisFace + smin(md, 0.0);
+                ac = ac - f;
+                su = su - f * UF + fude - fudi;
+                sv = sv - f * VF + fvde - fvdi;
+                sw = sw - f * WF + fwde - fwdi;
+                if (face == ph.last_bface[side]) {
+                    a.U[c1] = UF;
+                    a.V[c1] = VF;
+                    a.W[c1] = WF;
+                }
+            } else if (t == WALL) {
+                const double Visac = mu;
+                const double coef = Visac * m.rl[face];
+                const double Upx = Uc - 0., Upy = Vc - 0., Upz = Wc - 0.;
+                const double smag = sqrt(Sx * Sx + Sy * Sy + Sz * Sz);
+                const double nx = Sx / smag, ny = Sy / smag, nz = Sz / smag;
+                const double dp = Upx * nx + Upy * ny + Upz * nz;
+                const double Utx = Upx - nx * dp, Uty = Upy - ny * dp, Utz = Upz - nz * dp;
+                const double Uvel = fabs(Utx) + fabs(Uty) + fabs(Utz);
+                double fx = 0.0, fy = 0.0, fz = 0.0;
+                if (Uvel > 0.0) {
+                    const double dist = sqrt(Xx * Xx + Xy * Xy + Xz * Xz);
+                    const double s = m.area[face] * Visac;
+                    fx = Utx * s / dist;
+                    fy = Uty * s / dist;
+                    fz = Utz * s / dist;
+                }
+                ac = ac + coef;
+                su = su + coef * Uc - fx;
+                sv = sv + coef * Vc - fy;
+                sw = sw + coef * Wc - fz;
+                if (face == ph.last_bface[side]) {
+                    a.U[c1] = 0.;
+                    a.V[c1] = 0.;
+                    a.W[c1] = 0.;
+                }
+            }
+        }
+    }
+    const double vol = m.vol[c], rho = m.rho[c];
+    const double BodyForce = -0.001 * rho * vol * (a.T[c] - ph.T_ref);  // :1689-1697
+    su += 0.0 * BodyForce;
+    sv += -9.81 * BodyForce;
+    sw += 0.0 * BodyForce;
+    su -= a.gP[0][c] * vol;  // :1700-1705
+    sv -= a.gP[1][c] * vol;
+    sw -= a.gP[2][c] * vol;
+    const double f = rho * vol * ph.rdelta;  // :1708-1721
+    su += f * Uc;
+    sv += f * Vc;
+    sw += f * Wc;
+    ac += f;
+    if (ph.mode == 1 && a.src) {  // particle momentum (left commented out at :1723-1729)
+        su += a.src[c];
+        sv += a.src[(size_t)N + c];
+        sw += a.src[2 * (size_t)N + c];
+    }
+    for (int k = 0; k < 6; k++)  // setup_sparse_matrix diagonal, :1242-1243
+        if ((internal >> k) & 1u) ac -= offv[k];
+    const double URF = ph.urf_u;
+    const double RURF = 1. / URF;
+    ac *= RURF;
+    a.b[c] = su + (1.0 - URF) * ac * Uc;
+    a.b[(size_t)N + c] = sv + (1.0 - URF) * ac * Vc;
+    a.b[2 * (size_t)N + c] = sw + (1.0 - URF) * ac * Wc;
+    a.AU[c] = ac;
+#pragma unroll
+    for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
+}
+
+// ------------------------------------------------------------- temperature
+// FluxScalar(TEMP) (FlowSolver.inl:2516-2744), unsteady term and
+// setup_sparse_matrix of Scalar_solve (:2885-2953).
+__global__ void __launch_bounds__(MCB_THREADS) k_temperature_assemble(Physics ph, MeshArgs m, ScalarArgs a)
+{
+    const int N = ph.N;
+    const int c = grid_stride_start();
+    if (c >= N) return;
+    const double xcc = m.xc[c], ycc = m.yc[c], zcc = m.zc[c];
+    const double Tc = a.phi[c];
+    const double mu = ph.mu;
+    double st = 0.0, at = 0.0, offv[6];
+    unsigned internal = 0u;
+    for (int k = 0; k < 6; k++) {
+        const int face = m.sface[(size_t)k * N + c];
+        const int c0 = m.fc0[face], c1 = m.fc1[face];
+        const double Sx = m.Sx[face], Sy = m.Sy[face], Sz = m.Sz[face];
+        const double md = a.mdot[face];
+        if (c1 < N) {
+            internal |= 1u << k;
+            const double l0 = m.lam[face];
+            const double l1 = 1.0 - l0;
+            double Visac = mu * l0 + mu * l1;
+            Visac -= mu;
+            Visac = (mu + Visac / 0.9) / 0.6905;
+            const double dx = a.g[0][c0] * l0 + a.g[0][c1] * l1;
+            const double dy = a.g[1][c0] * l0 + a.g[1][c1] * l1;
+            const double dz = a.g[2][c0] * l0 + a.g[2][c1] * l1;
+            const double Xx = m.xc[c1] - m.xc[c0], Xy = m.yc[c1] - m.yc[c0], Xz = m.zc[c1] - m.zc[c0];
+            const double VisFace = Visac * m.rl[face];
+            const double fde1 = Visac * (dx * Sx + dy * Sy + dz * Sz);
+            const double fdi = VisFace * (dx * Xx + dy * Xy + dz * Xz);
+            if (c == c0) {
+                st = st + fde1 - fdi;
+                offv[k] = -VisFace + smin(md, 0.0);
+            } else {
+                st = st - fde1 + fdi;
+                offv[k] = -VisFace - smax(md, 0.0);
+            }
+        } else {
+            offv[k] = 0.0;
+            const int side = c1 - N;
+            const int t = ph.btype[side];
+            const double dx = a.g[0][c], dy = a.g[1][c], dz = a.g[2][c];
+            const double Xx = m.xf[face] - xcc, Xy = m.yf[face] - ycc, Xz = m.zf[face] - zcc;
+            if (t == INLET) {
+                const double PhiFace = ph.T_ref;
+                double Visac = ph.inlet_mu;
+                Visac -= mu;
+                Visac = (mu + Visac / 0.9) / 0.6905;
+                const double VisFace = Visac * m.rl[face];
+                const double fde = Visac * (dx * Sx + dy * Sy + dz * Sz);
+                const double fdi = VisFace * (dx * Xx + dy * Xy + dz * Xz);
+                const double f = -VisFace + smin(md, 0.0);
+                at = at - f;
+                st = st - f * PhiFace + fde - fdi;
+                if (face == ph.last_bface[side]) a.phi[c1] = PhiFace;
+            } else if (t == OUTLET) {
+                double Visac = mu;
+                Visac -= mu;
+                Visac = (mu + Visac / 0.9) / 0.6905;
+                const double PhiFace = Tc + (dx * Xx + dy * Xy + dz * Xz);
+                const double VisFace = Visac * m.rl[face];
+                const double fde = Visac * (dx * Sx + dy * Sy + dz * Sz);
+                const double fdi = VisFace * (dx * Xx + dy * Xy + dz * Xz);
+                st = st + fde - fdi;
+                if (face == ph.last_bface[side]) a.phi[c1] = PhiFace;
+            } else if (t == WALL) {
+                if (face == ph.last_bface[side]) a.phi[c1] = Tc;
+            }
+        }
+    }
+    const double f = m.rho[c] * m.vol[c] * ph.rdelta;
+    st += f * Tc;
+    at += f;
+    if (ph.mode == 1 && a.src) st += a.src[3 * (size_t)N + c];  // particle energy (commented out at :2919-2925)
+    for (int k = 0; k < 6; k++)
+        if ((internal >> k) & 1u) at -= offv[k];
+    const double URF = ph.urf_T;
+    const double RURF = 1. / URF;
+    at *= RURF;
+    a.b[c] = st + (1.0 - URF) * at * Tc;
+    a.diag[c] = at;
+#pragma unroll
+    for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
+}
+
+// --------------------------------------------------------------- mass flux
+// calculate_mass_flux face loop (FlowSolver.inl:1885-2007): Rhie-Chow flux
+// and -ApV on internal faces; inlet, outlet and wall fluxes; partial sums
+// of the boundary balance (:2010-2034), finished by the last block.
+__global__ void __launch_bounds__(MCB_THREADS) k_mass_flux(Physics ph, MeshArgs m, MassFluxArgs a)
+{
+    __shared__ double sh[3][MCB_THREADS];
+    const int N = ph.N, F = m.F;
+    double part[3] = {0.0, 0.0, 0.0};  // flow_in, flow_out, area_out
+    for (int face = grid_stride_start(); face < F; face += gridDim.x * blockDim.x) {
+        const int c0 = m.fc0[face], c1 = m.fc1[face];
+        const double Sx = m.Sx[face], Sy = m.Sy[face], Sz = m.Sz[face];
+        if (c1 < N) {
+            const double l0 = m.lam[face];
+            const double l1 = 1.0 - l0;
+            const double dUx = a.gU[0][c0] * l0 + a.gU[0][c1] * l1;
+            const double dUy = a.gU[1][c0] * l0 + a.gU[1][c1] * l1;
+            const double dUz = a.gU[2][c0] * l0 + a.gU[2][c1] * l1;
+            const double dVx = a.gV[0][c0] * l0 + a.gV[0][c1] * l1;
+            const double dVy = a.gV[1][c0] * l0 + a.gV[1][c1] * l1;
+            const double dVz = a.gV[2][c0] * l0 + a.gV[2][c1] * l1;
+            const double dWx = a.gW[0][c0] * l0 + a.gW[0][c1] * l1;
+            const double dWy = a.gW[1][c0] * l0 + a.gW[1][c1] * l1;
+            const double dWz = a.gW[2][c0] * l0 + a.gW[2][c1] * l1;
+            const double x0 = m.xc[c0], y0 = m.yc[c0], z0 = m.zc[c0];
+            const double x1 = m.xc[c1], y1 = m.yc[c1], z1 = m.zc[c1];
+            const double xf = m.xf[face], yf = m.yf[face], zf = m.zf[face];
+            const double Xacx = x1 * l1 + x0 * l0, Xacy = y1 * l1 + y0 * l0, Xacz = z1 * l1 + z0 * l0;
+            const double dlx = xf - Xacx, dly = yf - Xacy, dlz = zf - Xacz;
+            const double UF = a.U[c1] * l1 + a.U[c0] * l0 + (dUx * dlx + dUy * dly + dUz * dlz);
+            const double VF = a.V[c1] * l1 + a.V[c0] * l0 + (dVx * dlx + dVy * dly + dVz * dlz);
+            const double WF = a.W[c1] * l1 + a.W[c0] * l0 + (dWx * dlx + dWy * dly + dWz * dlz);
+            const double densityf = m.rho[c0] * l0 + m.rho[c1] * l1;
+            double md = densityf * (UF * Sx + VF * Sy + WF * Sz);
+            const double smag = sqrt(Sx * Sx + Sy * Sy + Sz * Sz);
+            const double nx = Sx / smag, ny = Sy / smag, nz = Sz / smag;
+            const double d0 = (xf - x0) * nx + (yf - y0) * ny + (zf - z0) * nz;
+            const double d1 = (xf - x1) * nx + (yf - y1) * ny + (zf - z1) * nz;
+            const double Xpacx = xf - nx * d0, Xpacy = yf - ny * d0, Xpacz = zf - nz * d0;
+            const double Xnacx = xf - nx * d1, Xnacy = yf - ny * d1, Xnacz = zf - nz * d1;
+            const double delpx = Xpacx - x0, delpy = Xpacy - y0, delpz = Xpacz - z0;
+            const double delnx = Xnacx - x1, delny = Xnacy - y1, delnz = Xnacz - z1;
+            const double gP0x = a.gP[0][c0], gP0y = a.gP[1][c0], gP0z = a.gP[2][c0];
+            const double gP1x = a.gP[0][c1], gP1y = a.gP[1][c1], gP1z = a.gP[2][c1];
+            const double cell0_P = a.P[c0] + (gP0x * delpx + gP0y * delpy + gP0z * delpz);
+            const double cell1_P = a.P[c1] + (gP1x * delnx + gP1y * delny + gP1z * delnz);
+            const double Xpnx = Xnacx - Xpacx, Xpny = Xnacy - Xpacy, Xpnz = Xnacz - Xpacz;
+            const double X2x = x1 - x0, X2y = y1 - y0, X2z = z1 - z0;
+            const double A0 = a.AU[c0], A1 = a.AU[c1];
+            const double ApV0 = (A0 != 0.0) ? 1.0 / A0 : 0.0;
+            const double ApV1 = (A1 != 0.0) ? 1.0 / A1 : 0.0;
+            double ApV = m.rho[c0] * ApV0 * l0 + m.rho[c1] * ApV1 * l1;
+            const double volume_avg = m.vol[c0] * l0 + m.vol[c1] * l1;
+            ApV = ApV * m.area[face] * volume_avg / (X2x * nx + X2y * ny + X2z * nz);
+            const double dpx = (gP1x * l1 + gP0x * l0) * Xpnx;
+            const double dpy = (gP1y * l1 + gP0y * l0) * Xpny;
+            const double dpz = (gP1z * l1 + gP0z * l0) * Xpnz;
+            md -= ApV * ((cell1_P - cell0_P) - dpx - dpy - dpz);
+            a.mdot[face] = md;
+            a.ff0[face] = -ApV;
+            a.ff1[face] = -ApV;
+        } else {
+            const int t = ph.btype[c1 - N];
+            double md = 0.0;
+            if (t == INLET) {
+                md = ph.rho_in * (ph.u_in * Sx + 0.0 * Sy + 0.0 * Sz);
+                part[0] += md;
+            } else if (t == OUTLET) {
+                if (ph.mode == 1)  // zero-gradient outlet
+                    md = ph.rho_in * (a.U[c0] * Sx + a.V[c0] * Sy + a.W[c0] * Sz);
+                else  // the reference's fixed outlet flux (:1969-1985)
+                    md = ph.rho_in * (ph.u_in * Sx + 0.0 * Sy + 0.0 * Sz);
+                if (md < 0.0) md = 1e-15;
+                part[1] += md;
+                part[2] += m.area[face];
+            }
+            a.mdot[face] = md;
+        }
+    }
+    if (publish_partials<3>(part, a.partials, a.counter)) {
+        double tot[3];
+        reduce_partials<3>(tot, a.partials, a.counter, sh);
+        if (threadIdx.x == 0) {
+            FluxBalance *bal = a.balance;
+            bal->flow_in = tot[0];
+            bal->flow_out = tot[1];
+            bal->area_out = tot[2];
+            bal->fallback = tot[1] < 0.0000000001;
+            bal->rate_area = -tot[0] / tot[2];
+            bal->outlet_scale = (ph.mode == 1 && !bal->fallback) ? (a.mass_source_total - tot[0]) / tot[1] : 1.0;
+        }
+    }
+}
+
+// Outlet fluxes after the balance (:2049-2079; simple mode: scale so that the
+// boundary fluxes balance the particle mass source).
+__global__ void k_outlet_fix(Physics ph, MeshArgs m, double *__restrict__ mdot, double *U, double *V, double *W,
+                             const FluxBalance *__restrict__ bal)
+{
+    const int i = grid_stride_start();
+    if (i >= m.n_outlet) return;
+    const int face = m.outlet_faces[i];
+    if (bal->fallback) {
+        mdot[face] = bal->rate_area * m.area[face];
+        const int slot = m.fc1[face];
+        if (face == ph.last_bface[slot - ph.N]) {
+            U[slot] = ph.u_in;
+            V[slot] = 0.0;
+            W[slot] = 0.0;
+        }
+    } else if (ph.mode == 1) {
+        mdot[face] *= bal->outlet_scale;
+    }
+}
+
+// Pressure-correction rows (the S_U accumulation of calculate_mass_flux,
+// :1964 and :2101, and setup_pressure_matrix, :2139-2189).
+__global__ void __launch_bounds__(MCB_THREADS) k_pressure_rows(Physics ph, MeshArgs m, PressureRowArgs a)
+{
+    const int N = ph.N;
+    const int c = grid_stride_start();
+    if (c >= N) return;
+    int faces[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) faces[k] = m.sface[(size_t)k * N + c];
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        const int c1 = m.fc1[faces[k]];
+        if (c1 >= N && ph.btype[c1 - N] == INLET) s = s - a.mdot[faces[k]];
+    }
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        const int c1 = m.fc1[faces[k]];
+        if (c1 >= N && ph.btype[c1 - N] == OUTLET) s -= a.mdot[faces[k]];
+    }
+    if (ph.mode == 1 && a.src) s += a.src[4 * (size_t)N + c];
+    double diag = 0.0;
+    double offv[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        const int face = faces[k];
+        const int c0 = m.fc0[face], c1 = m.fc1[face];
+        offv[k] = 0.0;
+        if (c1 >= N) continue;
+        const double md = a.mdot[face];
+        if (c == c0) {
+            s -= md;
+            offv[k] = a.ff1[face];
+            diag -= offv[k];
+        } else {
+            s += md;
+            offv[k] = a.ff0[face];
+            diag -= offv[k];
+        }
+    }
+    a.b[c] = s;
+    a.diag[c] = diag;
+#pragma unroll
+    for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
+}
+
+// ------------------------------------------------------- corrector updates
+// Face part of one corrector pass of calculate_pressure: mass flux += a_f
+// (PP_N - PP_P) (:2402-2412) then update_mass_flux (:1812-1878).
+__global__ void __launch_bounds__(MCB_THREADS) k_pp_correct_faces(Physics ph, MeshArgs m, CorrectArgs a)
+{
+    const int N = ph.N, F = m.F;
+    for (int face = grid_stride_start(); face < F; face += gridDim.x * blockDim.x) {
+        const int c0 = m.fc0[face], c1 = m.fc1[face];
+        if (c1 >= N) continue;
+        const double fact = a.ff0[face];
+        double md = a.mdot[face];
+        md += (fact * (a.PP[c1] - a.PP[c0]));
+        const double Sx = m.Sx[face], Sy = m.Sy[face], Sz = m.Sz[face];
+        const double smag = sqrt(Sx * Sx + Sy * Sy + Sz * Sz);
+        const double nx = Sx / smag, ny = Sy / smag, nz = Sz / smag;
+        const double x0 = m.xc[c0], y0 = m.yc[c0], z0 = m.zc[c0];
+        const double x1 = m.xc[c1], y1 = m.yc[c1], z1 = m.zc[c1];
+        const double xf = m.xf[face], yf = m.yf[face], zf = m.zf[face];
+        const double d0 = (xf - x0) * nx + (yf - y0) * ny + (zf - z0) * nz;
+        const double d1 = (xf - x1) * nx + (yf - y1) * ny + (zf - z1) * nz;
+        double Xnx = (xf - nx * d1) - x1, Xny = (yf - ny * d1) - y1, Xnz = (zf - nz * d1) - z1;
+        double Xpx = (xf - nx * d0) - x0, Xpy = (yf - ny * d0) - y0, Xpz = (zf - nz * d0) - z0;
+        if (fabs(Xnx) < 0.0000000000000003) Xnx = 0.0;
+        if (fabs(Xny) < 0.0000000000000003) Xny = 0.0;
+        if (fabs(Xnz) < 0.0000000000000003) Xnz = 0.0;
+        if (fabs(Xpx) < 0.0000000000000003) Xpx = 0.0;
+        if (fabs(Xpy) < 0.0000000000000003) Xpy = 0.0;
+        if (fabs(Xpz) < 0.0000000000000003) Xpz = 0.0;
+        const double dpx = a.gPP[0][c1] * Xnx - a.gPP[0][c0] * Xpx;
+        const double dpy = a.gPP[1][c1] * Xny - a.gPP[1][c0] * Xpy;
+        const double dpz = a.gPP[2][c1] * Xnz - a.gPP[2][c0] * Xpz;
+        const double fc = fact * (dpx + dpy + dpz) * ph.flux_corr;
+        md += fc;
+        a.mdot[face] = md;
+        a.fcorr[face] = fc;
+    }
+}
+
+// Cell part: P += urf_p PP and u -= V/A grad(PP) (:2416-2433; every cell in
+// simple mode, only cell 0 on the first call in compat mode), the next
+// corrector's right-hand side from the non-orthogonal flux corrections
+// (:1875-1876, simple mode), and PP = 0 (:2447-2450).
+__global__ void __launch_bounds__(MCB_THREADS) k_pp_correct_cells(Physics ph, MeshArgs m, CorrectArgs a,
+                                                                  int correct_all, int correct_cell0)
+{
+    const int N = ph.N;
+    const int c = grid_stride_start();
+    if (c < N) {
+        if (correct_all || (correct_cell0 && c == 0)) {
+            const double A = a.AU[c];
+            const double Ar = (A != 0.0) ? 1.0 / A : 0.0;
+            const double fact = m.vol[c] * Ar;
+            a.P[c] += ph.urf_p * a.PP[c];
+            a.U[c] -= a.gPP[0][c] * fact;
+            a.V[c] -= a.gPP[1][c] * fact;
+            a.W[c] -= a.gPP[2][c] * fact;
+        }
+        if (a.next_rhs) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                const int face = m.sface[(size_t)k * N + c];
+                const int c0 = m.fc0[face], c1 = m.fc1[face];
+                if (c1 >= N) continue;
+                if (c == c0)
+                    s -= a.fcorr[face];
+                else
+                    s += a.fcorr[face];
+            }
+            a.next_rhs[c] = s;
+        }
+        a.PP[c] = 0.0;
+    } else if (c < N + 6) {
+        a.PP[c] = 0.0;
+    }
+}
+
+// update_P (FlowSolver.inl:2292-2315): boundary pressure from the last face
+// of each side.
+__global__ void k_update_p_boundary(Physics ph, MeshArgs m, double *P, const double *gPx, const double *gPy,
+                                    const double *gPz)
+{
+    const int side = threadIdx.x;
+    if (side >= 6) return;
+    const int face = ph.last_bface[side];
+    if (face < 0) return;
+    const int c0 = m.fc0[face];
+    if (ph.btype[side] == OUTLET) {
+        P[ph.N + side] = P[c0];
+    } else {
+        const double dsx = m.xf[face] - m.xc[c0], dsy = m.yf[face] - m.yc[c0], dsz = m.zf[face] - m.zc[c0];
+        P[ph.N + side] = P[c0] + (gPx[c0] * dsx + gPy[c0] * dsy + gPz[c0] * dsz);
+    }
+}
+
+// Largest pressure correction, as the reference computes it (:2371-2378):
+// max(PP[0], max_{i >= 1} |PP[i]|).
+__global__ void __launch_bounds__(MCB_THREADS) k_pp_max(int N, const double *__restrict__ PP, double *partials,
+                                                        unsigned int *counter, double *out)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    double v[1] = {-1.0e308};
+    for (int i = grid_stride_start(); i < N; i += gridDim.x * blockDim.x) v[0] = fmax(v[0], i == 0 ? PP[0] : fabs(PP[i]));
+    if (publish_partials<1>(v, partials, counter)) {
+        double tot[1];
+        reduce_partials<1, true>(tot, partials, counter, sh);
+        if (threadIdx.x == 0) *out = tot[0];
+    }
+}
+
+// max over cells of |net outflow - mass source| (a diagnostic of the pass).
+__global__ void __launch_bounds__(MCB_THREADS) k_mass_imbalance(Physics ph, MeshArgs m, const double *__restrict__ mdot,
+                                                                const double *__restrict__ src, double *partials,
+                                                                unsigned int *counter, double *out)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    const int N = ph.N;
+    double v[1] = {0.0};
+    for (int c = grid_stride_start(); c < N; c += gridDim.x * blockDim.x) {
+        double div = 0.0;
+        for (int k = 0; k < 6; k++) {
+            const int face = m.sface[(size_t)k * N + c];
+            div += (m.fc0[face] == c) ? mdot[face] : -mdot[face];
+        }
+        if (ph.mode == 1 && src) div -= src[4 * (size_t)N + c];
+        v[0] = fmax(v[0], fabs(div));
+    }
+    if (publish_partials<1>(v, partials, counter)) {
+        double tot[1];
+        reduce_partials<1, true>(tot, partials, counter, sh);
+        if (threadIdx.x == 0) *out = tot[0];
+    }
+}
+
+} // namespace mcb

@@ -1,0 +1,89 @@
+// Declarations and argument blocks of the SIMPLE-pass assembly kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "mc_internal.h"
+
+namespace mcb {
+
+// Device view of the mesh passed to kernels by value.
+struct MeshArgs {
+    int F;
+    const int *fc0, *fc1, *sface;
+    const double *area, *lam, *rl, *Sx, *Sy, *Sz, *xf, *yf, *zf;
+    const double *xc, *yc, *zc, *vol, *rho;
+    const int *outlet_faces;
+    int n_outlet;
+};
+
+template <int NF>
+struct GradArgs {
+    const double *phi[NF];
+    double *gx[NF], *gy[NF], *gz[NF];
+    unsigned zero_boundary;  // bit k: dphi = 0 on boundary faces for field k
+};
+
+struct MomentumArgs {
+    double *U, *V, *W;          // interior read, boundary slots written
+    const double *T;
+    const double *gU[3], *gV[3], *gW[3], *gP[3];
+    double *mdot;               // outlet clamp write (:1576-1580)
+    const double *src;          // [5][N] particle terms or null
+    double *off;                // [6][N]
+    double *AU;                 // diagonal after under-relaxation (A_phi.U)
+    double *b;                  // [3][N]
+};
+
+struct ScalarArgs {
+    double *phi;                // T: interior read, boundary slots written
+    const double *g[3];
+    const double *mdot;
+    const double *src;
+    double *off, *diag, *b;
+};
+
+struct MassFluxArgs {
+    const double *U, *V, *W, *P, *AU;
+    const double *gU[3], *gV[3], *gW[3], *gP[3];
+    double *mdot, *ff0, *ff1;
+    double *partials;
+    unsigned int *counter;
+    FluxBalance *balance;
+    double mass_source_total;
+};
+
+struct PressureRowArgs {
+    const double *mdot, *ff0, *ff1, *src;
+    double *off, *diag, *b;
+};
+
+struct CorrectArgs {
+    double *PP, *P, *U, *V, *W;
+    const double *AU;
+    const double *gPP[3];
+    const double *ff0;
+    double *mdot, *fcorr;
+    double *next_rhs;           // null: do not build the next corrector's right-hand side
+};
+
+template <int NF>
+__global__ void k_lsq_gradients(int N, const int *nbr, const int *fc1, const double *xc, const double *yc,
+                                const double *zc, const double *xf, const double *yf, const double *zf,
+                                GradArgs<NF> a);
+__global__ void k_precomp_au(Physics ph, MeshArgs m, const double *mdot, double *AU);
+__global__ void k_momentum_assemble(Physics ph, MeshArgs m, MomentumArgs a);
+__global__ void k_temperature_assemble(Physics ph, MeshArgs m, ScalarArgs a);
+__global__ void k_mass_flux(Physics ph, MeshArgs m, MassFluxArgs a);
+__global__ void k_outlet_fix(Physics ph, MeshArgs m, double *mdot, double *U, double *V, double *W,
+                             const FluxBalance *bal);
+__global__ void k_pressure_rows(Physics ph, MeshArgs m, PressureRowArgs a);
+__global__ void k_pp_correct_faces(Physics ph, MeshArgs m, CorrectArgs a);
+__global__ void k_pp_correct_cells(Physics ph, MeshArgs m, CorrectArgs a, int correct_all, int correct_cell0);
+__global__ void k_update_p_boundary(Physics ph, MeshArgs m, double *P, const double *gPx, const double *gPy,
+                                    const double *gPz);
+__global__ void k_pp_max(int N, const double *PP, double *partials, unsigned int *counter, double *out);
+__global__ void k_mass_imbalance(Physics ph, MeshArgs m, const double *mdot, const double *src, double *partials,
+                                 unsigned int *counter, double *out);
+
+} // namespace mcb

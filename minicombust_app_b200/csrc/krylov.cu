@@ -1,0 +1,482 @@
+// Krylov solvers (see krylov.cuh).  FP64 throughout; bandwidth bound: an
+// iteration streams the 7-point matrix (12 bytes per entry) and a handful of
+// vectors.
+#include "krylov.cuh"
+#include "mc_reduce.cuh"
+
+#include <algorithm>
+
+namespace mcb {
+
+namespace {
+
+__device__ __forceinline__ bool finite(double x) { return isfinite(x); }
+
+} // namespace
+
+int krylov_grid(int N)
+{
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    const int need = (N + MCB_THREADS - 1) / MCB_THREADS;
+    return std::max(1, std::min(need, sms * 4));
+}
+
+// ---------------------------------------------------------------------- PCG
+
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_mean(int N, const double *__restrict__ b, PcgVectors v)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) acc[0] += b[i];
+    if (publish_partials<1>(acc, v.partials, v.counter)) {
+        double tot[1];
+        reduce_partials<1>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) v.st->mean = tot[0] / (double)N;
+    }
+}
+
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_init(Ell A, PcgVectors v, double rtol, double abs_floor,
+                                                          int max_iters, int use_x0, int project)
+{
+    __shared__ double sh[3][MCB_THREADS];
+    const int N = A.N;
+    const double mean = project ? v.st->mean : 0.0;
+    double acc[3] = {0.0, 0.0, 0.0};  // b.b, r.z, r.r
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double bi = v.b[i] - mean;
+        double ri = bi;
+        if (use_x0) {
+            double ax = A.diag[i] * v.x[i];
+#pragma unroll
+            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * v.x[A.col[(size_t)k * N + i]];
+            ri = bi - ax;
+        } else {
+            v.x[i] = 0.0;
+        }
+        const double di = A.diag[i];
+        const double zi = (di != 0.0) ? ri / di : ri;  // a zero row (isolated cell) is left unpreconditioned
+        v.r[i] = ri;
+        v.z[i] = zi;
+        v.p[0][i] = 0.0;
+        v.p[1][i] = 0.0;
+        acc[0] += bi * bi;
+        acc[1] += ri * zi;
+        acc[2] += ri * ri;
+    }
+    if (publish_partials<3>(acc, v.partials, v.counter)) {
+        double tot[3];
+        reduce_partials<3>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) {
+            PcgState *st = v.st;
+            st->bb = tot[0];
+            st->rz = tot[1];
+            st->rz_old = 1.0;
+            st->rr = tot[2];
+            const double t = fmax(rtol * sqrt(tot[0]), abs_floor);
+            st->tol2 = t * t;
+            st->iter = 0;
+            st->max_iters = max_iters;
+            st->status = KRYLOV_OK;
+            st->done = (tot[0] == 0.0 || tot[2] <= st->tol2) ? 1 : 0;
+            if (!finite(tot[0]) || !finite(tot[1])) {
+                st->done = 1;
+                st->status = KRYLOV_NONFINITE;
+            }
+        }
+    }
+}
+
+// p_new = z + beta p_old (own row and, on the fly, neighbour rows); q = A p_new.
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(Ell A, PcgVectors v, int pin)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    const PcgState *st = v.st;
+    if (st->done) return;
+    const int N = A.N;
+    const double beta = (st->iter == 0) ? 0.0 : st->rz / st->rz_old;
+    const double *__restrict__ po = v.p[pin];
+    double *__restrict__ pn = v.p[pin ^ 1];
+    const double *__restrict__ z = v.z;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double pi = z[i] + beta * po[i];
+        double qi = A.diag[i] * pi;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const int j = A.col[(size_t)k * N + i];
+            qi += A.off[(size_t)k * N + i] * (z[j] + beta * po[j]);
+        }
+        pn[i] = pi;
+        v.q[i] = qi;
+        acc[0] += pi * qi;
+    }
+    if (publish_partials<1>(acc, v.partials, v.counter)) {
+        double tot[1];
+        reduce_partials<1>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) {
+            PcgState *s = v.st;
+            s->pq = tot[0];
+            s->alpha = s->rz / tot[0];
+            if (!finite(s->alpha)) {
+                s->done = 1;
+                s->status = KRYLOV_NONFINITE;
+            }
+        }
+    }
+}
+
+// x += alpha p; r -= alpha q; z = r / diag; convergence on ||r||.
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2(Ell A, PcgVectors v, int pnew)
+{
+    __shared__ double sh[2][MCB_THREADS];
+    const PcgState *st = v.st;
+    if (st->done) return;
+    const int N = A.N;
+    const double alpha = st->alpha;
+    const double *__restrict__ p = v.p[pnew];
+    double acc[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        v.x[i] += alpha * p[i];
+        const double ri = v.r[i] - alpha * v.q[i];
+        const double di = A.diag[i];
+        const double zi = (di != 0.0) ? ri / di : ri;  // a zero row (isolated cell) is left unpreconditioned
+        v.r[i] = ri;
+        v.z[i] = zi;
+        acc[0] += ri * zi;
+        acc[1] += ri * ri;
+    }
+    if (publish_partials<2>(acc, v.partials, v.counter)) {
+        double tot[2];
+        reduce_partials<2>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) {
+            PcgState *s = v.st;
+            s->rz_old = s->rz;
+            s->rz = tot[0];
+            s->rr = tot[1];
+            s->iter += 1;
+            if (!finite(tot[0]) || !finite(tot[1])) {
+                s->done = 1;
+                s->status = KRYLOV_NONFINITE;
+            } else if (tot[1] <= s->tol2) {
+                s->done = 1;
+            } else if (s->iter >= s->max_iters) {
+                s->done = 1;
+                s->status = KRYLOV_NOT_CONVERGED;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_xmean(int N, PcgVectors v)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) acc[0] += v.x[i];
+    if (publish_partials<1>(acc, v.partials, v.counter)) {
+        double tot[1];
+        reduce_partials<1>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) v.st->xmean = tot[0] / (double)N;
+    }
+}
+
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_sub_xmean(int N, PcgVectors v)
+{
+    const double m = v.st->xmean;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) v.x[i] -= m;
+}
+
+void pcg_mean(cudaStream_t s, const Ell &A, const PcgVectors &v)
+{
+    k_pcg_mean<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A.N, v.b, v);
+}
+void pcg_init(cudaStream_t s, const Ell &A, const PcgVectors &v, double rtol, double abs_floor, int max_iters,
+              int use_x0, int project)
+{
+    k_pcg_init<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, abs_floor, max_iters, use_x0, project);
+}
+void pcg_iter1(cudaStream_t s, const Ell &A, const PcgVectors &v, int pin)
+{
+    k_pcg_iter1<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, pin);
+}
+void pcg_iter2(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew)
+{
+    k_pcg_iter2<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, pnew);
+}
+void pcg_xmean(cudaStream_t s, int N, const PcgVectors &v) { k_pcg_xmean<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, v); }
+void pcg_sub_xmean(cudaStream_t s, int N, const PcgVectors &v)
+{
+    k_pcg_sub_xmean<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, v);
+}
+
+// ----------------------------------------------------------------- BiCGStab
+
+template <int R>
+__global__ void __launch_bounds__(MCB_THREADS) k_bicg_init(Ell A, BicgVectors<R> v, double rtol, int max_iters)
+{
+    __shared__ double sh[R][MCB_THREADS];
+    const int N = A.N;
+    double acc[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) acc[j] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const size_t o = (size_t)j * N + i;
+            const double bi = v.b[o];
+            v.x[j][i] = 0.0;
+            v.r[o] = bi;
+            v.r0[o] = bi;
+            v.p[0][o] = 0.0;
+            v.p[1][o] = 0.0;
+            v.v[0][o] = 0.0;
+            v.v[1][o] = 0.0;
+            acc[j] += bi * bi;
+        }
+    }
+    if (publish_partials<R>(acc, v.partials, v.counter)) {
+        double tot[R];
+        reduce_partials<R>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) {
+            BicgState<R> *st = v.st;
+            int all = 1;
+            for (int j = 0; j < R; j++) {
+                st->bb[j] = tot[j];
+                st->rr[j] = tot[j];
+                st->rho_new[j] = tot[j];
+                st->rho[j] = 1.0;
+                st->alpha[j] = 1.0;
+                st->omega[j] = 1.0;
+                st->tol2[j] = rtol * rtol * tot[j];
+                st->iter[j] = 0;
+                st->status[j] = finite(tot[j]) ? KRYLOV_OK : KRYLOV_NONFINITE;
+                st->done[j] = (tot[j] == 0.0 || !finite(tot[j])) ? 1 : 0;
+                all &= st->done[j];
+            }
+            st->all_done = all;
+            st->max_iters = max_iters;
+        }
+    }
+}
+
+// p_new = r + beta (p_old - omega v_old); v_new = A p_new.
+template <int R>
+__global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(Ell A, BicgVectors<R> v, int pin)
+{
+    __shared__ double sh[R][MCB_THREADS];
+    const BicgState<R> *st = v.st;
+    if (st->all_done) return;
+    const int N = A.N;
+    double beta[R], omega[R];
+    bool act[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        act[j] = !st->done[j];
+        beta[j] = (st->rho_new[j] / st->rho[j]) * (st->alpha[j] / st->omega[j]);
+        omega[j] = st->omega[j];
+    }
+    const double *__restrict__ po = v.p[pin];
+    const double *__restrict__ vo = v.v[pin];
+    double *__restrict__ pn = v.p[pin ^ 1];
+    double *__restrict__ vn = v.v[pin ^ 1];
+    double acc[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) acc[j] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double d = A.diag[i];
+        double offk[6];
+        int colk[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            offk[k] = A.off[(size_t)k * N + i];
+            colk[k] = A.col[(size_t)k * N + i];
+        }
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            if (!act[j]) continue;
+            const size_t base = (size_t)j * N;
+            const double pi = v.r[base + i] + beta[j] * (po[base + i] - omega[j] * vo[base + i]);
+            double vi = d * pi;
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                const size_t q = base + colk[k];
+                vi += offk[k] * (v.r[q] + beta[j] * (po[q] - omega[j] * vo[q]));
+            }
+            pn[base + i] = pi;
+            vn[base + i] = vi;
+            acc[j] += v.r0[base + i] * vi;
+        }
+    }
+    if (publish_partials<R>(acc, v.partials, v.counter)) {
+        double tot[R];
+        reduce_partials<R>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) {
+            BicgState<R> *s = v.st;
+            for (int j = 0; j < R; j++) {
+                if (s->done[j]) continue;
+                s->alpha[j] = s->rho_new[j] / tot[j];
+                if (!finite(s->alpha[j])) {
+                    s->done[j] = 1;
+                    s->status[j] = KRYLOV_NONFINITE;
+                }
+            }
+        }
+    }
+}
+
+// s = r - alpha v; t = A s.
+template <int R>
+__global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(Ell A, BicgVectors<R> v, int vnew)
+{
+    __shared__ double sh[2 * R][MCB_THREADS];
+    const BicgState<R> *st = v.st;
+    if (st->all_done) return;
+    const int N = A.N;
+    double alpha[R];
+    bool act[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        act[j] = !st->done[j];
+        alpha[j] = st->alpha[j];
+    }
+    const double *__restrict__ vv = v.v[vnew];
+    double acc[2 * R];
+#pragma unroll
+    for (int j = 0; j < 2 * R; j++) acc[j] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double d = A.diag[i];
+        double offk[6];
+        int colk[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            offk[k] = A.off[(size_t)k * N + i];
+            colk[k] = A.col[(size_t)k * N + i];
+        }
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            if (!act[j]) continue;
+            const size_t base = (size_t)j * N;
+            const double si = v.r[base + i] - alpha[j] * vv[base + i];
+            double ti = d * si;
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                const size_t q = base + colk[k];
+                ti += offk[k] * (v.r[q] - alpha[j] * vv[q]);
+            }
+            v.s[base + i] = si;
+            v.t[base + i] = ti;
+            acc[2 * j] += ti * si;
+            acc[2 * j + 1] += ti * ti;
+        }
+    }
+    if (publish_partials<2 * R>(acc, v.partials, v.counter)) {
+        double tot[2 * R];
+        reduce_partials<2 * R>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) {
+            BicgState<R> *s = v.st;
+            for (int j = 0; j < R; j++) {
+                if (s->done[j]) continue;
+                const double tt = tot[2 * j + 1];
+                s->omega[j] = (tt != 0.0) ? tot[2 * j] / tt : 0.0;
+            }
+        }
+    }
+}
+
+// x += alpha p + omega s; r = s - omega t; convergence on ||r||.
+template <int R>
+__global__ void __launch_bounds__(MCB_THREADS) k_bicg_3(Ell A, BicgVectors<R> v, int pnew)
+{
+    __shared__ double sh[2 * R][MCB_THREADS];
+    const BicgState<R> *st = v.st;
+    if (st->all_done) return;
+    const int N = A.N;
+    double alpha[R], omega[R];
+    bool act[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        act[j] = !st->done[j];
+        alpha[j] = st->alpha[j];
+        omega[j] = st->omega[j];
+    }
+    const double *__restrict__ p = v.p[pnew];
+    double acc[2 * R];
+#pragma unroll
+    for (int j = 0; j < 2 * R; j++) acc[j] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            if (!act[j]) continue;
+            const size_t o = (size_t)j * N + i;
+            const double si = v.s[o];
+            v.x[j][i] += alpha[j] * p[o] + omega[j] * si;
+            const double ri = si - omega[j] * v.t[o];
+            v.r[o] = ri;
+            acc[2 * j] += v.r0[o] * ri;
+            acc[2 * j + 1] += ri * ri;
+        }
+    }
+    if (publish_partials<2 * R>(acc, v.partials, v.counter)) {
+        double tot[2 * R];
+        reduce_partials<2 * R>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) {
+            BicgState<R> *s = v.st;
+            int all = 1;
+            for (int j = 0; j < R; j++) {
+                if (!s->done[j]) {
+                    s->rho[j] = s->rho_new[j];
+                    s->rho_new[j] = tot[2 * j];
+                    s->rr[j] = tot[2 * j + 1];
+                    s->iter[j] += 1;
+                    if (!finite(tot[2 * j]) || !finite(tot[2 * j + 1])) {
+                        s->done[j] = 1;
+                        s->status[j] = KRYLOV_NONFINITE;
+                    } else if (tot[2 * j + 1] <= s->tol2[j]) {
+                        s->done[j] = 1;
+                    } else if (s->omega[j] == 0.0 || tot[2 * j] == 0.0 || s->iter[j] >= s->max_iters) {
+                        s->done[j] = 1;
+                        s->status[j] = KRYLOV_NOT_CONVERGED;
+                    }
+                }
+                all &= s->done[j];
+            }
+            s->all_done = all;
+        }
+    }
+}
+
+template <int R>
+void bicg_init(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, double rtol, int max_iters)
+{
+    k_bicg_init<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, max_iters);
+}
+template <int R>
+void bicg_1(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, int pin)
+{
+    k_bicg_1<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, pin);
+}
+template <int R>
+void bicg_2(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, int vnew)
+{
+    k_bicg_2<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, vnew);
+}
+template <int R>
+void bicg_3(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, int pnew)
+{
+    k_bicg_3<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, pnew);
+}
+
+#define MCB_INSTANTIATE_BICG(R)                                                                  \
+    template void bicg_init<R>(cudaStream_t, const Ell &, const BicgVectors<R> &, double, int); \
+    template void bicg_1<R>(cudaStream_t, const Ell &, const BicgVectors<R> &, int);            \
+    template void bicg_2<R>(cudaStream_t, const Ell &, const BicgVectors<R> &, int);            \
+    template void bicg_3<R>(cudaStream_t, const Ell &, const BicgVectors<R> &, int);
+MCB_INSTANTIATE_BICG(1)
+MCB_INSTANTIATE_BICG(3)
+
+} // namespace mcb

@@ -1002,7 +1002,7 @@ static void calculate_mass_flux(mco_solver *s)
         const double fact = (msrc - FlowIn) / FlowOut;
         for (uint64_t face = 0; face < s->F; face++) {
             const uint64_t c1 = s->faces[2 * face + 1];
-            if (c1 >= N || (int)s->btype[c1 - N] != OUTLET) continue;
+            if (c1 < N || (int)s->btype[c1 - N] != OUTLET) continue;
             s->mdot[face] *= fact;
         }
     }
