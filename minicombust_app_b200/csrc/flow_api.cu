@@ -304,8 +304,7 @@ void launch_gradients5(mc_flow *h)
     }
     a.zero_boundary = 1u << 3;  // pressure: dphi = 0 on boundary faces (FlowSolver.inl:980)
     launch(h, K_GRAD5, [&] {
-        k_lsq_gradients<5><<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->N, h->nbr, h->fc1, h->xc, h->yc,
-                                                                             h->zc, h->xf, h->yf, h->zf, a);
+        launch_lsq_gradients5(h->stream, h->N, h->nbr, h->fc1, h->xc, h->yc, h->zc, h->xf, h->yf, h->zf, a);
     });
 }
 
@@ -318,8 +317,7 @@ void launch_gradient_pressure(mc_flow *h, int g)
     a.gz[0] = h->grad[g][2];
     a.zero_boundary = 1u;
     launch(h, K_GRAD1, [&] {
-        k_lsq_gradients<1><<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->N, h->nbr, h->fc1, h->xc, h->yc,
-                                                                             h->zc, h->xf, h->yf, h->zf, a);
+        launch_lsq_gradients1(h->stream, h->N, h->nbr, h->fc1, h->xc, h->yc, h->zc, h->xf, h->yf, h->zf, a);
     });
 }
 

@@ -108,12 +108,21 @@ __global__ void __launch_bounds__(MCB_THREADS) k_lsq_gradients(int N, const int 
     }
 }
 
-template __global__ void k_lsq_gradients<5>(int, const int *, const int *, const double *, const double *,
-                                            const double *, const double *, const double *, const double *,
-                                            GradArgs<5>);
-template __global__ void k_lsq_gradients<1>(int, const int *, const int *, const double *, const double *,
-                                            const double *, const double *, const double *, const double *,
-                                            GradArgs<1>);
+void launch_lsq_gradients5(cudaStream_t s, int N, const int *nbr, const int *fc1, const double *xc,
+                           const double *yc, const double *zc, const double *xf, const double *yf, const double *zf,
+                           const GradArgs<5> &a)
+{
+    k_lsq_gradients<5><<<(N + MCB_THREADS - 1) / MCB_THREADS, MCB_THREADS, 0, s>>>(N, nbr, fc1, xc, yc, zc, xf, yf,
+                                                                                  zf, a);
+}
+
+void launch_lsq_gradients1(cudaStream_t s, int N, const int *nbr, const int *fc1, const double *xc,
+                           const double *yc, const double *zc, const double *xf, const double *yf, const double *zf,
+                           const GradArgs<1> &a)
+{
+    k_lsq_gradients<1><<<(N + MCB_THREADS - 1) / MCB_THREADS, MCB_THREADS, 0, s>>>(N, nbr, fc1, xc, yc, zc, xf, yf,
+                                                                                  zf, a);
+}
 
 // -------------------------------------------------------------- precomp_AU
 // precomp_AU (FlowSolver.inl:1065-1104): inlet/outlet viscous part plus rho V / dt.
@@ -465,7 +474,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_mass_flux(Physics ph, MeshArgs 
             a.mdot[face] = md;
         }
     }
-    if (publish_partials<3>(part, a.partials, a.counter)) {
+    if (publish_partials<3>(part, a.partials, a.counter, sh)) {
         double tot[3];
         reduce_partials<3>(tot, a.partials, a.counter, sh);
         if (threadIdx.x == 0) {
@@ -651,7 +660,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pp_max(int N, const double *__r
     __shared__ double sh[1][MCB_THREADS];
     double v[1] = {-1.0e308};
     for (int i = grid_stride_start(); i < N; i += gridDim.x * blockDim.x) v[0] = fmax(v[0], i == 0 ? PP[0] : fabs(PP[i]));
-    if (publish_partials<1>(v, partials, counter)) {
+    if (publish_partials<1, true>(v, partials, counter, sh)) {
         double tot[1];
         reduce_partials<1, true>(tot, partials, counter, sh);
         if (threadIdx.x == 0) *out = tot[0];
@@ -675,7 +684,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_mass_imbalance(Physics ph, Mesh
         if (ph.mode == 1 && src) div -= src[4 * (size_t)N + c];
         v[0] = fmax(v[0], fabs(div));
     }
-    if (publish_partials<1>(v, partials, counter)) {
+    if (publish_partials<1, true>(v, partials, counter, sh)) {
         double tot[1];
         reduce_partials<1, true>(tot, partials, counter, sh);
         if (threadIdx.x == 0) *out = tot[0];

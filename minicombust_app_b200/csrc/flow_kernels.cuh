@@ -67,10 +67,15 @@ struct CorrectArgs {
     double *next_rhs;           // null: do not build the next corrector's right-hand side
 };
 
-template <int NF>
-__global__ void k_lsq_gradients(int N, const int *nbr, const int *fc1, const double *xc, const double *yc,
-                                const double *zc, const double *xf, const double *yf, const double *zf,
-                                GradArgs<NF> a);
+// The gradient kernel is a template; it is launched from its own translation
+// unit (a template kernel launched elsewhere without relocatable device code
+// would register a stub with no device code).
+void launch_lsq_gradients5(cudaStream_t s, int N, const int *nbr, const int *fc1, const double *xc,
+                           const double *yc, const double *zc, const double *xf, const double *yf, const double *zf,
+                           const GradArgs<5> &a);
+void launch_lsq_gradients1(cudaStream_t s, int N, const int *nbr, const int *fc1, const double *xc,
+                           const double *yc, const double *zc, const double *xf, const double *yf, const double *zf,
+                           const GradArgs<1> &a);
 __global__ void k_precomp_au(Physics ph, MeshArgs m, const double *mdot, double *AU);
 __global__ void k_momentum_assemble(Physics ph, MeshArgs m, MomentumArgs a);
 __global__ void k_temperature_assemble(Physics ph, MeshArgs m, ScalarArgs a);

@@ -34,7 +34,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_mean(int N, const double *_
     __shared__ double sh[1][MCB_THREADS];
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) acc[0] += b[i];
-    if (publish_partials<1>(acc, v.partials, v.counter)) {
+    if (publish_partials<1>(acc, v.partials, v.counter, sh)) {
         double tot[1];
         reduce_partials<1>(tot, v.partials, v.counter, sh);
         if (threadIdx.x == 0) v.st->mean = tot[0] / (double)N;
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_init(Ell A, PcgVectors v, d
         acc[1] += ri * zi;
         acc[2] += ri * ri;
     }
-    if (publish_partials<3>(acc, v.partials, v.counter)) {
+    if (publish_partials<3>(acc, v.partials, v.counter, sh)) {
         double tot[3];
         reduce_partials<3>(tot, v.partials, v.counter, sh);
         if (threadIdx.x == 0) {
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(Ell A, PcgVectors v, 
         v.q[i] = qi;
         acc[0] += pi * qi;
     }
-    if (publish_partials<1>(acc, v.partials, v.counter)) {
+    if (publish_partials<1>(acc, v.partials, v.counter, sh)) {
         double tot[1];
         reduce_partials<1>(tot, v.partials, v.counter, sh);
         if (threadIdx.x == 0) {
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2(Ell A, PcgVectors v, 
         acc[0] += ri * zi;
         acc[1] += ri * ri;
     }
-    if (publish_partials<2>(acc, v.partials, v.counter)) {
+    if (publish_partials<2>(acc, v.partials, v.counter, sh)) {
         double tot[2];
         reduce_partials<2>(tot, v.partials, v.counter, sh);
         if (threadIdx.x == 0) {
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_xmean(int N, PcgVectors v)
     __shared__ double sh[1][MCB_THREADS];
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) acc[0] += v.x[i];
-    if (publish_partials<1>(acc, v.partials, v.counter)) {
+    if (publish_partials<1>(acc, v.partials, v.counter, sh)) {
         double tot[1];
         reduce_partials<1>(tot, v.partials, v.counter, sh);
         if (threadIdx.x == 0) v.st->xmean = tot[0] / (double)N;
@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_init(Ell A, BicgVectors<R>
             acc[j] += bi * bi;
         }
     }
-    if (publish_partials<R>(acc, v.partials, v.counter)) {
+    if (publish_partials<R>(acc, v.partials, v.counter, sh)) {
         double tot[R];
         reduce_partials<R>(tot, v.partials, v.counter, sh);
         if (threadIdx.x == 0) {
@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(Ell A, BicgVectors<R> v,
             acc[j] += v.r0[base + i] * vi;
         }
     }
-    if (publish_partials<R>(acc, v.partials, v.counter)) {
+    if (publish_partials<R>(acc, v.partials, v.counter, sh)) {
         double tot[R];
         reduce_partials<R>(tot, v.partials, v.counter, sh);
         if (threadIdx.x == 0) {
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(Ell A, BicgVectors<R> v,
             acc[2 * j + 1] += ti * ti;
         }
     }
-    if (publish_partials<2 * R>(acc, v.partials, v.counter)) {
+    if (publish_partials<2 * R>(acc, v.partials, v.counter, sh)) {
         double tot[2 * R];
         reduce_partials<2 * R>(tot, v.partials, v.counter, sh);
         if (threadIdx.x == 0) {
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_3(Ell A, BicgVectors<R> v,
             acc[2 * j + 1] += ri * ri;
         }
     }
-    if (publish_partials<2 * R>(acc, v.partials, v.counter)) {
+    if (publish_partials<2 * R>(acc, v.partials, v.counter, sh)) {
         double tot[2 * R];
         reduce_partials<2 * R>(tot, v.partials, v.counter, sh);
         if (threadIdx.x == 0) {

@@ -47,16 +47,25 @@ __device__ inline void block_max(double (&v)[K], double (*sh)[MCB_THREADS])
     for (int k = 0; k < K; k++) v[k] = sh[k][0];
 }
 
-// Publish this block's K partials and report whether it is the last block.
+// Reduce the threads' values across the block, publish the block's K
+// partials and report whether this block is the last to arrive.
 // partials: [gridDim.x][K]; counter must be zero before the launch and is
 // reset by the last block.
-template <int K>
-__device__ inline bool publish_partials(const double (&v)[K], double *partials, unsigned int *counter)
+template <int K, bool MAX = false>
+__device__ inline bool publish_partials(const double (&v)[K], double *partials, unsigned int *counter,
+                                        double (*sh)[MCB_THREADS])
 {
     __shared__ bool am_last;
+    double b[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) b[k] = v[k];
+    if (MAX)
+        block_max<K>(b, sh);
+    else
+        block_sum<K>(b, sh);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < K; k++) partials[(size_t)blockIdx.x * K + k] = v[k];
+        for (int k = 0; k < K; k++) partials[(size_t)blockIdx.x * K + k] = b[k];
         __threadfence();
         const unsigned int prev = atomicAdd(counter, 1u);
         am_last = (prev == gridDim.x - 1);
