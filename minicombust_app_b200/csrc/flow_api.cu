@@ -526,7 +526,7 @@ int allocate(mc_flow *h)
     add(&h->balance, sizeof(FluxBalance));
     add(&h->scalars, 8 * 8);
     // PCG
-    add(&h->pv.r, N * 8); add(&h->pv.z, N * 8); add(&h->pv.p[0], N * 8); add(&h->pv.p[1], N * 8);
+    add(&h->pv.r, N * 8); add(&h->pv.zp[0], N * 16); add(&h->pv.zp[1], N * 16);
     add(&h->pv.q, N * 8); add(&h->pv.st, sizeof(PcgState));
     // BiCGStab, three right-hand sides; the single-RHS solver shares the vectors
     double *bic[8];

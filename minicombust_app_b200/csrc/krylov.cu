@@ -6,6 +6,11 @@
 
 #include <algorithm>
 
+// Resident blocks per SM the grid-stride Krylov kernels are sized for.
+#ifndef MCB_KRYLOV_BLOCKS_PER_SM
+#define MCB_KRYLOV_BLOCKS_PER_SM 8
+#endif
+
 namespace mcb {
 
 namespace {
@@ -24,7 +29,7 @@ int krylov_grid(int N)
         if (sms <= 0) sms = 148;
     }
     const int need = (N + MCB_THREADS - 1) / MCB_THREADS;
-    return std::max(1, std::min(need, sms * 4));
+    return std::max(1, std::min(need, sms * MCB_KRYLOV_BLOCKS_PER_SM));
 }
 
 // ---------------------------------------------------------------------- PCG
@@ -62,9 +67,8 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_init(Ell A, PcgVectors v, d
         const double di = A.diag[i];
         const double zi = (di != 0.0) ? ri / di : ri;  // a zero row (isolated cell) is left unpreconditioned
         v.r[i] = ri;
-        v.z[i] = zi;
-        v.p[0][i] = 0.0;
-        v.p[1][i] = 0.0;
+        v.zp[0][i] = make_double2(zi, 0.0);
+        v.zp[1][i] = make_double2(0.0, 0.0);
         acc[0] += bi * bi;
         acc[1] += ri * zi;
         acc[2] += ri * ri;
@@ -93,28 +97,47 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_init(Ell A, PcgVectors v, d
 }
 
 // p_new = z + beta p_old (own row and, on the fly, neighbour rows); q = A p_new.
-__global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(Ell A, PcgVectors v, int pin)
+// Two rows per thread are kept in flight so that their gathers overlap.
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(Ell A, PcgVectors v, const double2 *__restrict__ X,
+                                                           double2 *__restrict__ Y)
 {
     __shared__ double sh[1][MCB_THREADS];
     const PcgState *st = v.st;
     if (st->done) return;
     const int N = A.N;
     const double beta = (st->iter == 0) ? 0.0 : st->rz / st->rz_old;
-    const double *__restrict__ po = v.p[pin];
-    double *__restrict__ pn = v.p[pin ^ 1];
-    const double *__restrict__ z = v.z;
+    const int stride = gridDim.x * blockDim.x;
     double acc[1] = {0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const double pi = z[i] + beta * po[i];
-        double qi = A.diag[i] * pi;
+    for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < N; i0 += 2 * stride) {
+        const int i1 = i0 + stride;
+        const bool has1 = i1 < N;
+        const int j1 = has1 ? i1 : i0;
+        int ca[6], cb[6];
+        double oa[6], ob[6];
 #pragma unroll
         for (int k = 0; k < 6; k++) {
-            const int j = A.col[(size_t)k * N + i];
-            qi += A.off[(size_t)k * N + i] * (z[j] + beta * po[j]);
+            ca[k] = A.col[(size_t)k * N + i0];
+            cb[k] = A.col[(size_t)k * N + j1];
+            oa[k] = A.off[(size_t)k * N + i0];
+            ob[k] = A.off[(size_t)k * N + j1];
         }
-        pn[i] = pi;
-        v.q[i] = qi;
-        acc[0] += pi * qi;
+        const double2 sa = X[i0], sb = X[j1];
+        const double pa = sa.x + beta * sa.y, pb = sb.x + beta * sb.y;
+        double qa = A.diag[i0] * pa, qb = A.diag[j1] * pb;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const double2 ga = X[ca[k]], gb = X[cb[k]];
+            qa += oa[k] * (ga.x + beta * ga.y);
+            qb += ob[k] * (gb.x + beta * gb.y);
+        }
+        Y[i0].y = pa;
+        v.q[i0] = qa;
+        acc[0] += pa * qa;
+        if (has1) {
+            Y[i1].y = pb;
+            v.q[i1] = qb;
+            acc[0] += pb * qb;
+        }
     }
     if (publish_partials<1>(acc, v.partials, v.counter, sh)) {
         double tot[1];
@@ -132,22 +155,22 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(Ell A, PcgVectors v, 
 }
 
 // x += alpha p; r -= alpha q; z = r / diag; convergence on ||r||.
-__global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2(Ell A, PcgVectors v, int pnew)
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2(Ell A, PcgVectors v, double2 *__restrict__ Y)
 {
     __shared__ double sh[2][MCB_THREADS];
     const PcgState *st = v.st;
     if (st->done) return;
     const int N = A.N;
     const double alpha = st->alpha;
-    const double *__restrict__ p = v.p[pnew];
     double acc[2] = {0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        v.x[i] += alpha * p[i];
+        const double p = Y[i].y;
+        v.x[i] += alpha * p;
         const double ri = v.r[i] - alpha * v.q[i];
         const double di = A.diag[i];
         const double zi = (di != 0.0) ? ri / di : ri;  // a zero row (isolated cell) is left unpreconditioned
         v.r[i] = ri;
-        v.z[i] = zi;
+        Y[i].x = zi;
         acc[0] += ri * zi;
         acc[1] += ri * ri;
     }
@@ -202,11 +225,11 @@ void pcg_init(cudaStream_t s, const Ell &A, const PcgVectors &v, double rtol, do
 }
 void pcg_iter1(cudaStream_t s, const Ell &A, const PcgVectors &v, int pin)
 {
-    k_pcg_iter1<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, pin);
+    k_pcg_iter1<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.zp[pin], v.zp[pin ^ 1]);
 }
 void pcg_iter2(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew)
 {
-    k_pcg_iter2<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, pnew);
+    k_pcg_iter2<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.zp[pnew]);
 }
 void pcg_xmean(cudaStream_t s, int N, const PcgVectors &v) { k_pcg_xmean<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, v); }
 void pcg_sub_xmean(cudaStream_t s, int N, const PcgVectors &v)
@@ -266,7 +289,9 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_init(Ell A, BicgVectors<R>
 
 // p_new = r + beta (p_old - omega v_old); v_new = A p_new.
 template <int R>
-__global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(Ell A, BicgVectors<R> v, int pin)
+__global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(Ell A, BicgVectors<R> v, const double *__restrict__ po,
+                                                        const double *__restrict__ vo, double *__restrict__ pn,
+                                                        double *__restrict__ vn)
 {
     __shared__ double sh[R][MCB_THREADS];
     const BicgState<R> *st = v.st;
@@ -280,10 +305,6 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(Ell A, BicgVectors<R> v,
         beta[j] = (st->rho_new[j] / st->rho[j]) * (st->alpha[j] / st->omega[j]);
         omega[j] = st->omega[j];
     }
-    const double *__restrict__ po = v.p[pin];
-    const double *__restrict__ vo = v.v[pin];
-    double *__restrict__ pn = v.p[pin ^ 1];
-    double *__restrict__ vn = v.v[pin ^ 1];
     double acc[R];
 #pragma unroll
     for (int j = 0; j < R; j++) acc[j] = 0.0;
@@ -331,7 +352,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(Ell A, BicgVectors<R> v,
 
 // s = r - alpha v; t = A s.
 template <int R>
-__global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(Ell A, BicgVectors<R> v, int vnew)
+__global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(Ell A, BicgVectors<R> v, const double *__restrict__ vv)
 {
     __shared__ double sh[2 * R][MCB_THREADS];
     const BicgState<R> *st = v.st;
@@ -344,7 +365,6 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(Ell A, BicgVectors<R> v,
         act[j] = !st->done[j];
         alpha[j] = st->alpha[j];
     }
-    const double *__restrict__ vv = v.v[vnew];
     double acc[2 * R];
 #pragma unroll
     for (int j = 0; j < 2 * R; j++) acc[j] = 0.0;
@@ -390,7 +410,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(Ell A, BicgVectors<R> v,
 
 // x += alpha p + omega s; r = s - omega t; convergence on ||r||.
 template <int R>
-__global__ void __launch_bounds__(MCB_THREADS) k_bicg_3(Ell A, BicgVectors<R> v, int pnew)
+__global__ void __launch_bounds__(MCB_THREADS) k_bicg_3(Ell A, BicgVectors<R> v, const double *__restrict__ p)
 {
     __shared__ double sh[2 * R][MCB_THREADS];
     const BicgState<R> *st = v.st;
@@ -404,7 +424,6 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_3(Ell A, BicgVectors<R> v,
         alpha[j] = st->alpha[j];
         omega[j] = st->omega[j];
     }
-    const double *__restrict__ p = v.p[pnew];
     double acc[2 * R];
 #pragma unroll
     for (int j = 0; j < 2 * R; j++) acc[j] = 0.0;
@@ -458,17 +477,17 @@ void bicg_init(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, double rto
 template <int R>
 void bicg_1(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, int pin)
 {
-    k_bicg_1<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, pin);
+    k_bicg_1<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.p[pin], v.v[pin], v.p[pin ^ 1], v.v[pin ^ 1]);
 }
 template <int R>
 void bicg_2(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, int vnew)
 {
-    k_bicg_2<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, vnew);
+    k_bicg_2<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.v[vnew]);
 }
 template <int R>
 void bicg_3(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, int pnew)
 {
-    k_bicg_3<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, pnew);
+    k_bicg_3<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.p[pnew]);
 }
 
 #define MCB_INSTANTIATE_BICG(R)                                                                  \

@@ -32,8 +32,13 @@ struct BicgState {
     int all_done, max_iters;
 };
 
+// zp[k][i] = (z_i, p_i): the preconditioned residual and the search
+// direction interleaved, so that a neighbour costs one 16-byte gather.
+// Iteration k reads zp[k & 1] and writes p into zp[(k & 1) ^ 1], where the
+// next z is then stored.
 struct PcgVectors {
-    double *x, *r, *z, *p[2], *q;
+    double *x, *r, *q;
+    double2 *zp[2];
     const double *b;
     double *partials;
     unsigned int *counter;
