@@ -173,6 +173,28 @@ long mc_flow_launch_count(mc_flow *flow);
 const char *mc_flow_last_error(mc_flow *flow);
 const char *mc_status_string(int status);
 
+/* Allocation-free solve.  No counterpart in the reference: it is offered to
+ * callers that must not allocate device memory -- code that issues work while
+ * a CUDA stream capture is in progress (cudaMalloc is not permitted then) and
+ * hosts whose device memory is owned by their own pool or budget.
+ *
+ * Solves A x = b with the BiCGStab kernels the temperature stage uses (zero
+ * initial guess, ||b - A x|| <= rtol ||b||), on a 7-point system the caller
+ * owns on the current device, given in the ELL layout of this library:
+ * diag[n], off[6][n], col[6][n] (an unused slot has col = its row, off = 0).
+ * All pointers are device pointers; x receives the solution.  Work goes on
+ * `stream` (a cudaStream_t, may be NULL); the call returns when it is done.
+ * Nothing is allocated: the Krylov vectors, partial sums and status live in
+ * one file-scope device array sized for MC_SOLVE_NOALLOC_MAX_ROWS rows (about
+ * 16 MB, held by every device that loads the library until the process
+ * exits).  n above that limit returns MC_ERR_ARG.  All calls share the array,
+ * so calls that overlap on the GPU race.  The first call on a device looks up
+ * the array's address (cudaGetSymbolAddress, once per device); make that call
+ * before any stream capture.  iterations (may be NULL) receives the count. */
+#define MC_SOLVE_NOALLOC_MAX_ROWS 262144
+int mc_solve_bicgstab_noalloc(int n, const double *diag, const double *off, const int *col, const double *b,
+                              double *x, double rtol, int max_iters, void *stream, int *iterations);
+
 /* Box mesh in the reference layout: load_mesh for one flow rank
  * (src/examples/mesh_examples.cpp:120-571), x-min inlet, x-max outlet, walls
  * elsewhere.  Arrays are allocated by the library; release them with

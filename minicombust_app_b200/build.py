@@ -27,6 +27,7 @@ CUDA_SOURCES = [
     ("flow_kernels.cu", ["-fmad=false"]),
     ("krylov.cu", []),
     ("flow_api.cu", []),
+    ("solve_noalloc.cu", []),
 ]
 CXX_SOURCES = [("mesh_setup.cpp", ["-ffp-contract=off", "-fno-fast-math"])]
 

@@ -107,6 +107,8 @@ _SIGNATURES = {
     "mc_flow_launch_count": (c_long, [c_vp]),
     "mc_flow_last_error": (ctypes.c_char_p, [c_vp]),
     "mc_status_string": (ctypes.c_char_p, [c_int]),
+    "mc_solve_bicgstab_noalloc": (c_int, [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_dbl, c_int, c_vp,
+                                          ctypes.POINTER(c_int)]),
     "mc_mesh_box_create": (c_int, [c_u64, c_u64, c_u64, c_dbl, c_dbl, c_dbl, ctypes.POINTER(MeshView)]),
     "mc_mesh_box_destroy": (None, [ctypes.POINTER(MeshView)]),
 }
