@@ -100,6 +100,9 @@ typedef struct mc_flow_params {
     int precision;            /* MC_PRECISION_* */
     int initial_guess;        /* MC_GUESS_* for the pressure correction */
     int device;               /* CUDA device ordinal */
+    int amg_sweeps;           /* MC_PSOLVER_PCG_AMG: damped-Jacobi sweeps before and after the coarse correction */
+    double amg_omega;         /* Jacobi damping */
+    double amg_alpha;         /* coarse-correction scaling */
 } mc_flow_params;
 
 /* Per-pass statistics. */

@@ -26,6 +26,7 @@ NVCC_COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "
 CUDA_SOURCES = [
     ("flow_kernels.cu", ["-fmad=false"]),
     ("krylov.cu", []),
+    ("amg.cu", []),
     ("flow_api.cu", []),
     ("solve_noalloc.cu", []),
 ]

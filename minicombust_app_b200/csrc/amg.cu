@@ -1,0 +1,347 @@
+// Aggregation AMG for the pressure-correction system (see amg.h).
+#include "amg.h"
+
+#include <algorithm>
+#include <cstring>
+
+#include "krylov.cuh"
+#include "mc_reduce.cuh"
+
+namespace mcb {
+
+// ---------------------------------------------------------------- host setup
+
+int amg_build_host(int N, const std::vector<int> &col0, const std::vector<int> &dn0, std::vector<AmgHostLevel> &out,
+                   std::string &err)
+{
+    out.clear();
+    AmgHostLevel L0;
+    L0.n = N;
+    L0.k = 6;
+    L0.col = col0;
+    out.push_back(std::move(L0));
+    std::vector<int> dn = dn0;  // directional neighbours of the current level [6][n]
+    for (int guard = 0; guard < AMG_MAX_LEVELS; guard++) {
+        AmgHostLevel &cur = out.back();
+        const int n = cur.n;
+        if (n <= AMG_COARSEST_MAX) return 0;
+        if ((int)out.size() == AMG_MAX_LEVELS) break;
+        auto nb = [&](int d, int c) { return c < 0 ? -1 : dn[(size_t)d * n + c]; };
+        // 2 x 2 x 2 aggregates anchored at the first unaggregated cell (+x: slot 3, +y: 5, +z: 1)
+        std::vector<int> agg(n, -1), anchor;
+        int nagg = 0;
+        for (int c = 0; c < n; c++) {
+            if (agg[c] >= 0) continue;
+            const int A = nagg++;
+            anchor.push_back(c);
+            agg[c] = A;
+            const int x1 = nb(3, c), y1 = nb(5, c), z1 = nb(1, c);
+            const int xy = x1 >= 0 ? nb(5, x1) : nb(3, y1);
+            const int xz = x1 >= 0 ? nb(1, x1) : nb(3, z1);
+            const int yz = y1 >= 0 ? nb(1, y1) : nb(5, z1);
+            const int xyz = xy >= 0 ? nb(1, xy) : (xz >= 0 ? nb(5, xz) : nb(3, yz));
+            for (int cand : {x1, y1, xy, z1, xz, yz, xyz})
+                if (cand >= 0 && agg[cand] < 0) agg[cand] = A;
+        }
+        if (nagg * 2 > n) {
+            err = "AMG aggregation stalled (mesh without directional neighbours)";
+            return -1;
+        }
+        cur.agg = agg;
+        cur.mptr.assign(nagg + 1, 0);
+        for (int c = 0; c < n; c++) cur.mptr[agg[c] + 1]++;
+        for (int a = 0; a < nagg; a++) cur.mptr[a + 1] += cur.mptr[a];
+        cur.mlist.assign(n, 0);
+        {
+            std::vector<int> fill(cur.mptr.begin(), cur.mptr.end() - 1);
+            for (int c = 0; c < n; c++) cur.mlist[fill[agg[c]]++] = c;
+        }
+        // coarse directional neighbours: walk from the anchor until leaving the aggregate
+        std::vector<int> dnc((size_t)6 * nagg, -1);
+        for (int A = 0; A < nagg; A++)
+            for (int d = 0; d < 6; d++) {
+                int c = nb(d, anchor[A]);
+                for (int steps = 0; c >= 0 && agg[c] == A && steps < 4; steps++) c = nb(d, c);
+                dnc[(size_t)d * nagg + A] = (c >= 0 && agg[c] != A) ? agg[c] : -1;
+            }
+        // coarse pattern (sorted columns) and Galerkin lists
+        AmgHostLevel nxt;
+        nxt.n = nagg;
+        std::vector<std::vector<int>> cols(nagg);
+        int kmax = 0;
+        for (int A = 0; A < nagg; A++) {
+            std::vector<int> &cs = cols[A];
+            for (int t = cur.mptr[A]; t < cur.mptr[A + 1]; t++) {
+                const int i = cur.mlist[t];
+                for (int s = 0; s < cur.k; s++) {
+                    const int j = cur.col[(size_t)s * n + i];
+                    if (j == i) continue;
+                    const int J = agg[j];
+                    if (J != A && std::find(cs.begin(), cs.end(), J) == cs.end()) cs.push_back(J);
+                }
+            }
+            std::sort(cs.begin(), cs.end());
+            kmax = std::max(kmax, (int)cs.size());
+        }
+        nxt.k = std::max(kmax, 1);
+        const int kc = nxt.k;
+        nxt.col.assign((size_t)kc * nagg, 0);
+        for (int A = 0; A < nagg; A++)
+            for (int s = 0; s < kc; s++) nxt.col[(size_t)s * nagg + A] = s < (int)cols[A].size() ? cols[A][s] : A;
+        std::vector<int> count((size_t)nagg * (kc + 1) + 1, 0);
+        struct Contrib { int entry, id; };
+        std::vector<Contrib> contrib;
+        contrib.reserve((size_t)n * 7);
+        for (int A = 0; A < nagg; A++) {
+            for (int t = cur.mptr[A]; t < cur.mptr[A + 1]; t++) {
+                const int i = cur.mlist[t];
+                contrib.push_back({A * (kc + 1), i});
+                for (int s = 0; s < cur.k; s++) {
+                    const int j = cur.col[(size_t)s * n + i];
+                    if (j == i) continue;
+                    const int J = agg[j];
+                    int slot = 0;
+                    if (J != A) slot = 1 + (int)(std::lower_bound(cols[A].begin(), cols[A].end(), J) - cols[A].begin());
+                    contrib.push_back({A * (kc + 1) + slot, n + s * n + i});
+                }
+            }
+        }
+        for (const Contrib &c : contrib) count[c.entry + 1]++;
+        for (size_t e = 0; e + 1 < count.size(); e++) count[e + 1] += count[e];
+        nxt.gptr = count;
+        nxt.gidx.assign(contrib.size(), 0);
+        {
+            std::vector<int> fill(count.begin(), count.end() - 1);
+            for (const Contrib &c : contrib) nxt.gidx[fill[c.entry]++] = c.id;
+        }
+        dn.swap(dnc);
+        out.push_back(std::move(nxt));
+    }
+    err = "AMG hierarchy did not reach the coarsest size";
+    return -1;
+}
+
+// ------------------------------------------------------------------ kernels
+
+namespace {
+
+__device__ __forceinline__ double row_apply(const AmgLevel &L, int i, const double *__restrict__ e)
+{
+    double s = L.diag[i] * e[i];
+    for (int q = 0; q < L.k; q++) s += L.off[(size_t)q * L.n + i] * e[L.col[(size_t)q * L.n + i]];
+    return s;
+}
+
+__device__ __forceinline__ double inv_or_zero(double d) { return d != 0.0 ? 1.0 / d : 0.0; }
+
+} // namespace
+
+__global__ void k_amg_galerkin(AmgLevel fine, AmgLevel coarse)
+{
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= coarse.n) return;
+    const int kc = coarse.k;
+    for (int slot = 0; slot <= kc; slot++) {
+        const int e = I * (kc + 1) + slot;
+        double s = 0.0;
+        for (int t = coarse.gptr[e]; t < coarse.gptr[e + 1]; t++) {
+            const int id = coarse.gidx[t];
+            s += (id < fine.n) ? fine.diag[id] : fine.off[id - fine.n];
+        }
+        if (slot == 0)
+            coarse.diag[I] = s;
+        else
+            coarse.off[(size_t)(slot - 1) * coarse.n + I] = s;
+    }
+}
+
+// Dense Cholesky of A + sigma 1 1^T (sigma = mean diagonal / n) on the
+// coarsest level, one block, factor stored lower-triangular row-major.
+__global__ void k_amg_dense_factor(AmgLevel L, double *dense)
+{
+    extern __shared__ double A[];
+    const int n = L.n, t = threadIdx.x;
+    __shared__ double sigma;
+    if (t == 0) {
+        double s = 0.0;
+        for (int i = 0; i < n; i++) s += L.diag[i];
+        sigma = (s / n) / n;
+    }
+    __syncthreads();
+    for (int idx = t; idx < n * n; idx += blockDim.x) A[idx] = sigma;
+    __syncthreads();
+    if (t < n) {
+        A[t * n + t] += L.diag[t];
+        for (int q = 0; q < L.k; q++) {
+            const int j = L.col[(size_t)q * n + t];
+            if (j != t) A[t * n + j] += L.off[(size_t)q * n + t];
+        }
+    }
+    __syncthreads();
+    for (int j = 0; j < n; j++) {
+        if (t == 0) {
+            const double d = A[j * n + j];
+            A[j * n + j] = d > 0.0 ? sqrt(d) : 1.0;
+        }
+        __syncthreads();
+        if (t > j && t < n) A[t * n + j] /= A[j * n + j];
+        __syncthreads();
+        if (t > j && t < n)
+            for (int c = j + 1; c <= t; c++) A[t * n + c] -= A[t * n + j] * A[c * n + j];
+        __syncthreads();
+    }
+    for (int idx = t; idx < n * n; idx += blockDim.x) dense[idx] = A[idx];
+}
+
+__global__ void k_amg_dense_solve(AmgLevel L, const double *__restrict__ dense, const PcgState *st)
+{
+    if (st->done) return;
+    extern __shared__ double F[];
+    __shared__ double y[AMG_COARSEST_MAX];
+    const int n = L.n, t = threadIdx.x;
+    for (int idx = t; idx < n * n; idx += blockDim.x) F[idx] = dense[idx];
+    if (t < n) y[t] = L.r[t];
+    __syncthreads();
+    for (int j = 0; j < n; j++) {  // L y = r
+        if (t == j) y[j] /= F[j * n + j];
+        __syncthreads();
+        if (t > j && t < n) y[t] -= F[t * n + j] * y[j];
+        __syncthreads();
+    }
+    for (int j = n - 1; j >= 0; j--) {  // L^T x = y
+        if (t == j) y[j] /= F[j * n + j];
+        __syncthreads();
+        if (t < j) y[t] -= F[j * n + t] * y[j];
+        __syncthreads();
+    }
+    if (t < n) L.e[0][t] = y[t];
+}
+
+__global__ void k_amg_smooth_first(AmgLevel L, double omega, double *__restrict__ e, const PcgState *st)
+{
+    if (st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.n) return;
+    e[i] = omega * L.r[i] * inv_or_zero(L.diag[i]);
+}
+
+__global__ void k_amg_jacobi(AmgLevel L, double omega, const double *__restrict__ ein, double *__restrict__ eout,
+                             const PcgState *st)
+{
+    if (st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.n) return;
+    eout[i] = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
+}
+
+__global__ void k_amg_restrict(AmgLevel fine, AmgLevel coarse, const double *__restrict__ e, const PcgState *st)
+{
+    if (st->done) return;
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= coarse.n) return;
+    double s = 0.0;
+    for (int t = fine.mptr[I]; t < fine.mptr[I + 1]; t++) {
+        const int i = fine.mlist[t];
+        s += fine.r[i] - row_apply(fine, i, e);
+    }
+    coarse.r[I] = s;
+}
+
+__global__ void k_amg_prolong(AmgLevel fine, double alpha, const double *__restrict__ ec, double *__restrict__ e,
+                              const PcgState *st)
+{
+    if (st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= fine.n) return;
+    e[i] += alpha * ec[fine.agg[i]];
+}
+
+// Last post-smoothing sweep on level 0: z into zp[i].x and the PCG's r . z.
+__global__ void __launch_bounds__(MCB_THREADS) k_amg_final(AmgLevel L, double omega, const double *__restrict__ ein,
+                                                           double2 *__restrict__ zp, PcgState *st, double *partials,
+                                                           unsigned int *counter, int is_init)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    if (st->done) return;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x) {
+        const double z = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
+        zp[i].x = z;
+        acc[0] += L.r[i] * z;
+    }
+    if (publish_partials<1>(acc, partials, counter, sh)) {
+        double tot[1];
+        reduce_partials<1>(tot, partials, counter, sh);
+        if (threadIdx.x == 0) {
+            st->rz_old = is_init ? 1.0 : st->rz;
+            st->rz = tot[0];
+            if (!isfinite(tot[0])) {
+                st->done = 1;
+                st->status = KRYLOV_NONFINITE;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ drivers
+
+namespace {
+inline int blocks(int n) { return std::max(1, (n + MCB_THREADS - 1) / MCB_THREADS); }
+inline size_t dense_smem(int n) { return (size_t)n * n * sizeof(double); }
+} // namespace
+
+void amg_setup_values(cudaStream_t s, const AmgHierarchy &H, double * /*partials*/)
+{
+    for (int l = 1; l < H.levels; l++)
+        k_amg_galerkin<<<blocks(H.lv[l].n), MCB_THREADS, 0, s>>>(H.lv[l - 1], H.lv[l]);
+    const AmgLevel &C = H.lv[H.levels - 1];
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_amg_dense_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dense_smem(AMG_COARSEST_MAX));
+        cudaFuncSetAttribute(k_amg_dense_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dense_smem(AMG_COARSEST_MAX));
+        attr = true;
+    }
+    k_amg_dense_factor<<<1, AMG_COARSEST_MAX, dense_smem(C.n), s>>>(C, H.dense);
+}
+
+int amg_kernels_per_vcycle(const AmgHierarchy &H) { return (H.levels - 1) * (2 * H.sweeps + 2) + 1; }
+
+void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const double *r0, double2 *zp_out, PcgState *st,
+                double *partials, unsigned int *counter, int is_init)
+{
+    const int L = H.levels;
+    int cur[AMG_MAX_LEVELS] = {0};
+    AmgLevel lv[AMG_MAX_LEVELS];
+    for (int l = 0; l < L; l++) lv[l] = H.lv[l];
+    lv[0].r = const_cast<double *>(r0);
+    for (int l = 0; l + 1 < L; l++) {
+        k_amg_smooth_first<<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], H.omega, lv[l].e[0], st);
+        int c = 0;
+        for (int sw = 1; sw < H.sweeps; sw++) {
+            k_amg_jacobi<<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], H.omega, lv[l].e[c], lv[l].e[c ^ 1], st);
+            c ^= 1;
+        }
+        cur[l] = c;
+        k_amg_restrict<<<blocks(lv[l + 1].n), MCB_THREADS, 0, s>>>(lv[l], lv[l + 1], lv[l].e[c], st);
+    }
+    k_amg_dense_solve<<<1, AMG_COARSEST_MAX, dense_smem(lv[L - 1].n), s>>>(lv[L - 1], H.dense, st);
+    cur[L - 1] = 0;
+    for (int l = L - 2; l >= 0; l--) {
+        int c = cur[l];
+        k_amg_prolong<<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], H.alpha, lv[l + 1].e[cur[l + 1]], lv[l].e[c], st);
+        for (int sw = 1; sw <= H.sweeps; sw++) {
+            if (l == 0 && sw == H.sweeps) {
+                k_amg_final<<<krylov_grid(lv[0].n), MCB_THREADS, 0, s>>>(lv[0], H.omega, lv[0].e[c], zp_out, st,
+                                                                        partials, counter, is_init);
+            } else {
+                k_amg_jacobi<<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], H.omega, lv[l].e[c], lv[l].e[c ^ 1], st);
+                c ^= 1;
+            }
+        }
+        cur[l] = c;
+    }
+}
+
+} // namespace mcb

@@ -1,0 +1,88 @@
+// Aggregation AMG for the pressure-correction system.
+//
+// Hierarchy (built once per mesh on the host, from the matrix graph only):
+// level 0 is the pressure-correction matrix (7-point ELL); each coarser level
+// groups up to 2 x 2 x 2 cells of the level below into one aggregate, found
+// by walking the cells' directional neighbours (+x, +y, +z from the first
+// unaggregated cell), so that on a box every coarse level is again a 7-point
+// box operator.  Coarse matrices are Galerkin products A_c = P^T A P with the
+// piecewise-constant prolongation P; their values are recomputed on the GPU
+// whenever the fine values change, by summing precomputed lists of fine
+// entries (a gather, deterministic).  The coarsest level (<= 128 rows) is
+// solved exactly with a dense Cholesky factor of A_c + sigma 1 1^T, which for
+// the singular pure-Neumann system gives the minimum-norm solution of a
+// consistent right-hand side.
+//
+// Preconditioner: one symmetric V-cycle -- nu damped-Jacobi sweeps before and
+// after the coarse correction (scaled by alpha) on every level -- so PCG
+// sees a fixed symmetric operator.
+#pragma once
+
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+namespace mcb {
+
+constexpr int AMG_MAX_LEVELS = 16;
+constexpr int AMG_COARSEST_MAX = 128;
+
+// Device view of one level.
+struct AmgLevel {
+    int n;          // rows
+    int k;          // off-diagonal slots (ELL width)
+    double *diag;   // [n]
+    double *off;    // [k][n]
+    const int *col; // [k][n], unused slots point at their own row
+    // restriction to the next level: members of coarse row I are mlist[mptr[I] .. mptr[I+1])
+    const int *agg;   // [n] aggregate (next-level row) of each row
+    const int *mptr;  // [n_next + 1]
+    const int *mlist; // [n]
+    // Galerkin lists building THIS level's values from the level below:
+    // entry e = row * (k + 1) + slot (slot 0 = diagonal, s + 1 = off slot s)
+    // sums fine values gidx[gptr[e] .. gptr[e+1]) (fine diag id < n_fine,
+    // fine off id = n_fine + s * n_fine + row).
+    const int *gptr;
+    const int *gidx;
+    double *r;      // right-hand side of the level
+    double *e[2];   // ping-pong iterates
+};
+
+struct AmgHierarchy {
+    int levels = 0;
+    AmgLevel lv[AMG_MAX_LEVELS];
+    double *dense = nullptr;    // coarsest Cholesky factor [n][n] (row-major, lower)
+    int sweeps = 2;
+    double omega = 0.6667;
+    double alpha = 1.0;
+};
+
+// Host-side construction of the pattern data.  Inputs: level-0 ELL columns
+// (col0[6][N], boundary slots = own row) and directional neighbours dn0[6][N]
+// in cell_faces slot order (FRONT -z, BACK +z, LEFT -x, RIGHT +x, DOWN -y,
+// UP +y; -1 on the boundary).
+struct AmgHostLevel {
+    int n = 0, k = 0;
+    std::vector<int> col;               // [k][n]
+    std::vector<int> agg, mptr, mlist;  // restriction to the next level
+    std::vector<int> gptr, gidx;        // Galerkin lists for this level (levels >= 1)
+};
+
+int amg_build_host(int N, const std::vector<int> &col0, const std::vector<int> &dn0, std::vector<AmgHostLevel> &out,
+                   std::string &err);
+
+// Device work, all asynchronous on stream s.
+// Galerkin values of levels 1..L-1 and the coarsest dense factor.
+void amg_setup_values(cudaStream_t s, const AmgHierarchy &H, double *partials);
+// z = V-cycle(r0) for level 0; the result is written to zp[i].x (the PCG
+// interleaved buffer) and the partial sums of r0 . z go through the PCG
+// reduction (see krylov.cuh).  Kernels are no-ops once *done is set.
+struct PcgState;
+void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const double *r0, double2 *zp_out, PcgState *st,
+                double *partials, unsigned int *counter, int is_init);
+int amg_kernels_per_vcycle(const AmgHierarchy &H);
+
+} // namespace mcb

@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "amg.h"
 #include "flow_kernels.cuh"
 #include "krylov.cuh"
 #include "mc_internal.h"
@@ -27,7 +28,7 @@ enum KernelId {
     K_GRAD5, K_GRAD1, K_PRECOMP_AU, K_MOMENTUM, K_MASS_FLUX, K_OUTLET_FIX, K_PRESSURE_ROWS, K_PP_FACES,
     K_PP_CELLS, K_P_BOUNDARY, K_PP_MAX, K_TEMPERATURE, K_IMBALANCE, K_PCG_MEAN, K_PCG_INIT, K_PCG_ITER1,
     K_PCG_ITER2, K_PCG_XMEAN, K_PCG_SUBMEAN, K_BICG3_INIT, K_BICG3_1, K_BICG3_2, K_BICG3_3, K_BICG1_INIT,
-    K_BICG1_1, K_BICG1_2, K_BICG1_3, K_COUNT
+    K_BICG1_1, K_BICG1_2, K_BICG1_3, K_AMG_SETUP, K_PCG_INIT_AMG, K_PCG_ITER2_AMG, K_AMG_VCYCLE, K_COUNT
 };
 
 const char *kKernelNames[K_COUNT] = {
@@ -35,9 +36,11 @@ const char *kKernelNames[K_COUNT] = {
     "outlet_fix", "pressure_rows", "pp_correct_faces", "pp_correct_cells", "update_p_boundary", "pp_max",
     "temperature_assemble", "mass_imbalance", "pcg_mean", "pcg_init", "pcg_iter1_spmv", "pcg_iter2_update",
     "pcg_xmean", "pcg_sub_xmean", "bicg3_init", "bicg3_1_spmv", "bicg3_2_spmv", "bicg3_3_update",
-    "bicg1_init", "bicg1_1_spmv", "bicg1_2_spmv", "bicg1_3_update"};
+    "bicg1_init", "bicg1_1_spmv", "bicg1_2_spmv", "bicg1_3_update", "amg_setup_galerkin_factor",
+    "pcg_init_amg", "pcg_iter2_amg_update", "amg_vcycle"};
 
 constexpr int PCG_BATCH = 16;   // iterations per status read (even: ping-pong buffers)
+constexpr int PCG_AMG_BATCH = 4;
 constexpr int BICG_BATCH = 8;
 
 // One cudaMalloc carved into aligned sub-buffers.
@@ -98,7 +101,11 @@ struct mc_flow {
     BicgState<3> *h_b3 = nullptr;      // pinned
     BicgState<1> *h_b1 = nullptr;      // pinned
     double *h_scalars = nullptr;       // pinned
-    cudaGraphExec_t g_pcg = nullptr, g_b3 = nullptr, g_b1 = nullptr;
+    cudaGraphExec_t g_pcg = nullptr, g_b3 = nullptr, g_b1 = nullptr, g_pcg_amg = nullptr;
+    // aggregation AMG (pressure_solver == MC_PSOLVER_PCG_AMG)
+    bool use_amg = false;
+    AmgHierarchy amg;
+    char *amg_mem = nullptr;
 
     // state of the reference's control flow
     int first_pressure = 1;
@@ -225,23 +232,40 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
 {
     const Ell A = pressure_matrix(h);
     PcgVectors v = h->pv;
+    const bool amg = h->use_amg;
     launch(h, K_PCG_MEAN, [&] { pcg_mean(h->stream, A, v); });
-    launch(h, K_PCG_INIT, [&] { pcg_init(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, 0, 1); });
+    if (amg) {
+        launch(h, K_PCG_INIT_AMG, [&] { pcg_init_amg(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, 1); });
+        launch(h, K_AMG_VCYCLE, [&] { amg_vcycle(h->stream, h->amg, v.r, v.zp[0], v.st, v.partials, v.counter, 1); });
+        h->launches += amg_kernels_per_vcycle(h->amg) - 1;
+    } else {
+        launch(h, K_PCG_INIT, [&] { pcg_init(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, 0, 1); });
+    }
     int rc = check_launch(h);
     if (rc) return rc;
     // The device marks the solve done at max_iters; the host bound is a second guard.
-    const long max_batches = h->prm.max_iters / PCG_BATCH + 2;
+    const int batch_iters = amg ? PCG_AMG_BATCH : PCG_BATCH;
+    const long max_batches = h->prm.max_iters / batch_iters + 2;
+    const int per_iter = amg ? 2 + amg_kernels_per_vcycle(h->amg) : PCG_KERNELS_PER_ITER;
     for (long batch = 0;; batch++) {
         CUDA_TRY(h, cudaMemcpyAsync(h->h_pcg, v.st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
         flush_timing(h);
         if (h->h_pcg->done) break;
         if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "pressure solve state did not advance");
-        rc = run_batch(h, &h->g_pcg, PCG_BATCH * PCG_KERNELS_PER_ITER, [&] {
-            for (int it = 0; it < PCG_BATCH; it++) {
+        rc = run_batch(h, amg ? &h->g_pcg_amg : &h->g_pcg, batch_iters * per_iter, [&] {
+            for (int it = 0; it < batch_iters; it++) {
                 const int pin = it & 1;
                 launch(h, K_PCG_ITER1, [&] { pcg_iter1(h->stream, A, v, pin); });
-                launch(h, K_PCG_ITER2, [&] { pcg_iter2(h->stream, A, v, pin ^ 1); });
+                if (amg) {
+                    launch(h, K_PCG_ITER2_AMG, [&] { pcg_iter2_amg(h->stream, A, v, pin ^ 1); });
+                    launch(h, K_AMG_VCYCLE, [&] {
+                        amg_vcycle(h->stream, h->amg, v.r, v.zp[pin ^ 1], v.st, v.partials, v.counter, 0);
+                    });
+                    h->launches += amg_kernels_per_vcycle(h->amg) - 1;
+                } else {
+                    launch(h, K_PCG_ITER2, [&] { pcg_iter2(h->stream, A, v, pin ^ 1); });
+                }
             }
         });
         if (rc) return rc;
@@ -410,6 +434,10 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
         launch(h, K_PRESSURE_ROWS, [&] {
             k_pressure_rows<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a);
         });
+        if (h->use_amg) {
+            launch(h, K_AMG_SETUP, [&] { amg_setup_values(h->stream, h->amg, h->partials); });
+            h->launches += h->amg.levels - 1;
+        }
     }
     int rc = check_launch(h);
     if (rc) return rc;
@@ -606,6 +634,94 @@ int initial_fields(mc_flow *h, const int btype[6])
     return rc;
 }
 
+// Aggregation hierarchy for the pressure-correction system: pattern data on
+// the host (amg.cu), one extra device allocation for all levels.
+int build_amg(mc_flow *h, const HostMesh &hm)
+{
+    const int N = hm.N;
+    std::vector<int> dn((size_t)6 * N);
+    for (size_t i = 0; i < dn.size(); i++) dn[i] = hm.nbr[i] >= 0 ? hm.nbr[i] : -1;
+    std::vector<AmgHostLevel> lv;
+    std::string err;
+    if (amg_build_host(N, hm.col, dn, lv, err) != 0) return fail(h, MC_ERR_MESH, err);
+    const int L = (int)lv.size();
+    if (L < 2) {  // the whole system is already at the coarsest size: plain Jacobi PCG
+        h->use_amg = false;
+        return MC_OK;
+    }
+    Arena ar;
+    struct Item { void **p; size_t bytes; };
+    std::vector<Item> items;
+    auto add = [&](void *pp, size_t bytes) { items.push_back({(void **)pp, std::max<size_t>(bytes, 8)}); };
+    AmgHierarchy &H = h->amg;
+    H.levels = L;
+    H.sweeps = h->prm.amg_sweeps;
+    H.omega = h->prm.amg_omega;
+    H.alpha = h->prm.amg_alpha;
+    std::vector<int *> d_col(L), d_agg(L), d_mptr(L), d_mlist(L), d_gptr(L), d_gidx(L);
+    for (int l = 0; l < L; l++) {
+        const AmgHostLevel &a = lv[l];
+        AmgLevel &d = H.lv[l];
+        d.n = a.n;
+        d.k = a.k;
+        if (l > 0) {
+            add(&d.diag, (size_t)a.n * 8);
+            add(&d.off, (size_t)a.k * a.n * 8);
+            add(&d_col[l], a.col.size() * 4);
+            add(&d.r, (size_t)a.n * 8);
+            add(&d_gptr[l], a.gptr.size() * 4);
+            add(&d_gidx[l], a.gidx.size() * 4);
+        }
+        add(&d.e[0], (size_t)a.n * 8);
+        add(&d.e[1], (size_t)a.n * 8);
+        if (l + 1 < L) {
+            add(&d_agg[l], a.agg.size() * 4);
+            add(&d_mptr[l], a.mptr.size() * 4);
+            add(&d_mlist[l], a.mlist.size() * 4);
+        }
+    }
+    const int nc = lv[L - 1].n;
+    add(&H.dense, (size_t)nc * nc * 8);
+    std::vector<size_t> offs;
+    for (auto &it : items) offs.push_back(ar.reserve(it.bytes));
+    cudaError_t e = cudaMalloc((void **)&h->amg_mem, ar.used);
+    if (e != cudaSuccess) return fail(h, MC_ERR_NOMEM, std::string("cudaMalloc (AMG): ") + cudaGetErrorString(e));
+    CUDA_TRY(h, cudaMemset(h->amg_mem, 0, ar.used));
+    for (size_t i = 0; i < items.size(); i++) *items[i].p = h->amg_mem + offs[i];
+    auto put = [&](int *dst, const std::vector<int> &src) -> int {
+        if (!src.empty()) CUDA_TRY(h, cudaMemcpy(dst, src.data(), src.size() * 4, cudaMemcpyHostToDevice));
+        return MC_OK;
+    };
+    for (int l = 0; l < L; l++) {
+        AmgLevel &d = H.lv[l];
+        if (l == 0) {
+            d.diag = h->diag_p;
+            d.off = h->off_p;
+            d.col = h->col;
+            d.r = h->pv.r;
+        } else {
+            int rc = put(d_col[l], lv[l].col);
+            rc = rc ? rc : put(d_gptr[l], lv[l].gptr);
+            rc = rc ? rc : put(d_gidx[l], lv[l].gidx);
+            if (rc) return rc;
+            d.col = d_col[l];
+            d.gptr = d_gptr[l];
+            d.gidx = d_gidx[l];
+        }
+        if (l + 1 < L) {
+            int rc = put(d_agg[l], lv[l].agg);
+            rc = rc ? rc : put(d_mptr[l], lv[l].mptr);
+            rc = rc ? rc : put(d_mlist[l], lv[l].mlist);
+            if (rc) return rc;
+            d.agg = d_agg[l];
+            d.mptr = d_mptr[l];
+            d.mlist = d_mlist[l];
+        }
+    }
+    h->use_amg = true;
+    return MC_OK;
+}
+
 } // namespace
 
 // =================================================================== C ABI
@@ -627,6 +743,9 @@ void mc_flow_default_params(mc_flow_params *p, int mode)
     p->pressure_solver = MC_PSOLVER_PCG_JACOBI;
     p->precision = MC_PRECISION_FP64;
     p->initial_guess = MC_GUESS_ZERO;
+    p->amg_sweeps = 2;
+    p->amg_omega = 0.6667;
+    p->amg_alpha = 1.8;
     if (mode == MC_MODE_COMPAT) {
         p->viscosity = 0.000014;
         p->temperature0 = 2000.0;
@@ -649,9 +768,12 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
     if (!mesh || !params || !out) return MC_ERR_ARG;
     *out = nullptr;
     if (params->mode != MC_MODE_COMPAT && params->mode != MC_MODE_SIMPLE) return MC_ERR_ARG;
-    if (params->pressure_solver != MC_PSOLVER_PCG_JACOBI || params->precision != MC_PRECISION_FP64 ||
-        params->initial_guess != MC_GUESS_ZERO)
+    if ((params->pressure_solver != MC_PSOLVER_PCG_JACOBI && params->pressure_solver != MC_PSOLVER_PCG_AMG) ||
+        params->precision != MC_PRECISION_FP64 || params->initial_guess != MC_GUESS_ZERO)
         return MC_ERR_UNSUPPORTED;
+    if (params->pressure_solver == MC_PSOLVER_PCG_AMG &&
+        (params->amg_sweeps < 1 || !(params->amg_omega > 0) || !(params->amg_alpha > 0)))
+        return MC_ERR_ARG;
     if (!(params->delta > 0) || !(params->urf_momentum > 0) || !(params->urf_temperature > 0) ||
         !(params->u_rtol > 0) || !(params->p_rtol > 0) || params->max_iters <= 0)
         return MC_ERR_ARG;
@@ -698,6 +820,7 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
             rc = rc ? rc : upload3(h, h->xf, h->yf, h->zf, hm.xf, F);
             rc = rc ? rc : upload3(h, h->xc, h->yc, h->zc, hm.xc, N);
             rc = rc ? rc : initial_fields(h, hm.btype);
+            if (!rc && params->pressure_solver == MC_PSOLVER_PCG_AMG) rc = build_amg(h, hm);
         }
         if (!rc) {
             h->hcol.assign((size_t)6 * hm.N, -1);
@@ -750,8 +873,9 @@ int mc_flow_destroy(mc_flow *h)
 {
     if (!h) return MC_ERR_ARG;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    for (cudaGraphExec_t g : {h->g_pcg, h->g_b3, h->g_b1})
+    for (cudaGraphExec_t g : {h->g_pcg, h->g_b3, h->g_b1, h->g_pcg_amg})
         if (g) cudaGraphExecDestroy(g);
+    if (h->amg_mem) cudaFree(h->amg_mem);
     for (cudaEvent_t e : h->timing.ev) cudaEventDestroy(e);
     if (h->arena.base) cudaFree(h->arena.base);
     if (h->h_pcg) cudaFreeHost(h->h_pcg);

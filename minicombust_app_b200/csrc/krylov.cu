@@ -196,6 +196,82 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2(Ell A, PcgVectors v, 
     }
 }
 
+// Initialisation for the AMG-preconditioned PCG: r = b - mean(b), x = 0;
+// z comes from the first V-cycle (amg.cu), which also sets r . z.
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_init_amg(Ell A, PcgVectors v, double rtol, double abs_floor,
+                                                              int max_iters, int project)
+{
+    __shared__ double sh[2][MCB_THREADS];
+    const int N = A.N;
+    const double mean = project ? v.st->mean : 0.0;
+    double acc[2] = {0.0, 0.0};  // b.b, r.r
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double bi = v.b[i] - mean;
+        v.x[i] = 0.0;
+        v.r[i] = bi;
+        v.zp[0][i] = make_double2(0.0, 0.0);
+        v.zp[1][i] = make_double2(0.0, 0.0);
+        acc[0] += bi * bi;
+        acc[1] += bi * bi;
+    }
+    if (publish_partials<2>(acc, v.partials, v.counter, sh)) {
+        double tot[2];
+        reduce_partials<2>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) {
+            PcgState *st = v.st;
+            st->bb = tot[0];
+            st->rr = tot[1];
+            st->rz = 0.0;
+            st->rz_old = 1.0;
+            const double t = fmax(rtol * sqrt(tot[0]), abs_floor);
+            st->tol2 = t * t;
+            st->iter = 0;
+            st->max_iters = max_iters;
+            st->status = KRYLOV_OK;
+            st->done = (tot[0] == 0.0 || tot[1] <= st->tol2) ? 1 : 0;
+            if (!finite(tot[0])) {
+                st->done = 1;
+                st->status = KRYLOV_NONFINITE;
+            }
+        }
+    }
+}
+
+// x += alpha p; r -= alpha q; convergence on ||r||.  z follows from the V-cycle.
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2_amg(Ell A, PcgVectors v, const double2 *__restrict__ Y)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    const PcgState *st = v.st;
+    if (st->done) return;
+    const int N = A.N;
+    const double alpha = st->alpha;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        v.x[i] += alpha * Y[i].y;
+        const double ri = v.r[i] - alpha * v.q[i];
+        v.r[i] = ri;
+        acc[0] += ri * ri;
+    }
+    if (publish_partials<1>(acc, v.partials, v.counter, sh)) {
+        double tot[1];
+        reduce_partials<1>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) {
+            PcgState *s = v.st;
+            s->rr = tot[0];
+            s->iter += 1;
+            if (!finite(tot[0])) {
+                s->done = 1;
+                s->status = KRYLOV_NONFINITE;
+            } else if (tot[0] <= s->tol2) {
+                s->done = 1;
+            } else if (s->iter >= s->max_iters) {
+                s->done = 1;
+                s->status = KRYLOV_NOT_CONVERGED;
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(MCB_THREADS) k_pcg_xmean(int N, PcgVectors v)
 {
     __shared__ double sh[1][MCB_THREADS];
@@ -230,6 +306,15 @@ void pcg_iter1(cudaStream_t s, const Ell &A, const PcgVectors &v, int pin)
 void pcg_iter2(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew)
 {
     k_pcg_iter2<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.zp[pnew]);
+}
+void pcg_init_amg(cudaStream_t s, const Ell &A, const PcgVectors &v, double rtol, double abs_floor, int max_iters,
+                  int project)
+{
+    k_pcg_init_amg<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, abs_floor, max_iters, project);
+}
+void pcg_iter2_amg(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew)
+{
+    k_pcg_iter2_amg<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.zp[pnew]);
 }
 void pcg_xmean(cudaStream_t s, int N, const PcgVectors &v) { k_pcg_xmean<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, v); }
 void pcg_sub_xmean(cudaStream_t s, int N, const PcgVectors &v)

@@ -69,6 +69,11 @@ void pcg_init(cudaStream_t s, const Ell &A, const PcgVectors &v, double rtol, do
               int use_x0, int project);
 void pcg_iter1(cudaStream_t s, const Ell &A, const PcgVectors &v, int pin);
 void pcg_iter2(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew);
+// AMG-preconditioned variant: init without z, update without z (amg.cu
+// computes z and r . z after each update).
+void pcg_init_amg(cudaStream_t s, const Ell &A, const PcgVectors &v, double rtol, double abs_floor, int max_iters,
+                  int project);
+void pcg_iter2_amg(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew);
 void pcg_xmean(cudaStream_t s, int N, const PcgVectors &v);
 void pcg_sub_xmean(cudaStream_t s, int N, const PcgVectors &v);
 
