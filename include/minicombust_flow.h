@@ -103,6 +103,7 @@ typedef struct mc_flow_params {
     int amg_sweeps;           /* MC_PSOLVER_PCG_AMG: damped-Jacobi sweeps before and after the coarse correction */
     double amg_omega;         /* Jacobi damping */
     double amg_alpha;         /* coarse-correction scaling */
+    double ir_inner_rtol;     /* MC_PRECISION_FP32_REFINED: relative tolerance of each inner FP32 solve */
 } mc_flow_params;
 
 /* Per-pass statistics. */

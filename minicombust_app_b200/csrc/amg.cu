@@ -125,18 +125,35 @@ int amg_build_host(int N, const std::vector<int> &col0, const std::vector<int> &
 
 namespace {
 
-__device__ __forceinline__ double row_apply(const AmgLevel &L, int i, const double *__restrict__ e)
+template <typename T>
+__device__ __forceinline__ T row_apply(const AmgLevelT<T> &L, int i, const T *__restrict__ e)
 {
-    double s = L.diag[i] * e[i];
+    T s = L.diag[i] * e[i];
     for (int q = 0; q < L.k; q++) s += L.off[(size_t)q * L.n + i] * e[L.col[(size_t)q * L.n + i]];
     return s;
 }
 
-__device__ __forceinline__ double inv_or_zero(double d) { return d != 0.0 ? 1.0 / d : 0.0; }
+template <typename T>
+__device__ __forceinline__ T inv_or_zero(T d)
+{
+    return d != (T)0 ? (T)1 / d : (T)0;
+}
 
 } // namespace
 
-__global__ void k_amg_galerkin(AmgLevel fine, AmgLevel coarse)
+// FP32 copy of the level-0 values.
+__global__ void k_amg_round_level0(int n, const double *__restrict__ diag, const double *__restrict__ off,
+                                   float *__restrict__ diag32, float *__restrict__ off32)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    diag32[i] = (float)diag[i];
+#pragma unroll
+    for (int q = 0; q < 6; q++) off32[(size_t)q * n + i] = (float)off[(size_t)q * n + i];
+}
+
+template <typename T>
+__global__ void k_amg_galerkin(AmgLevelT<T> fine, AmgLevelT<T> coarse)
 {
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= coarse.n) return;
@@ -146,35 +163,36 @@ __global__ void k_amg_galerkin(AmgLevel fine, AmgLevel coarse)
         double s = 0.0;
         for (int t = coarse.gptr[e]; t < coarse.gptr[e + 1]; t++) {
             const int id = coarse.gidx[t];
-            s += (id < fine.n) ? fine.diag[id] : fine.off[id - fine.n];
+            s += (double)((id < fine.n) ? fine.diag[id] : fine.off[id - fine.n]);
         }
         if (slot == 0)
-            coarse.diag[I] = s;
+            coarse.diag[I] = (T)s;
         else
-            coarse.off[(size_t)(slot - 1) * coarse.n + I] = s;
+            coarse.off[(size_t)(slot - 1) * coarse.n + I] = (T)s;
     }
 }
 
 // Dense Cholesky of A + sigma 1 1^T (sigma = mean diagonal / n) on the
-// coarsest level, one block, factor stored lower-triangular row-major.
-__global__ void k_amg_dense_factor(AmgLevel L, double *dense)
+// coarsest level, one block, FP64, factor stored lower-triangular row-major.
+template <typename T>
+__global__ void k_amg_dense_factor(AmgLevelT<T> L, double *dense)
 {
     extern __shared__ double A[];
     const int n = L.n, t = threadIdx.x;
     __shared__ double sigma;
     if (t == 0) {
         double s = 0.0;
-        for (int i = 0; i < n; i++) s += L.diag[i];
+        for (int i = 0; i < n; i++) s += (double)L.diag[i];
         sigma = (s / n) / n;
     }
     __syncthreads();
     for (int idx = t; idx < n * n; idx += blockDim.x) A[idx] = sigma;
     __syncthreads();
     if (t < n) {
-        A[t * n + t] += L.diag[t];
+        A[t * n + t] += (double)L.diag[t];
         for (int q = 0; q < L.k; q++) {
             const int j = L.col[(size_t)q * n + t];
-            if (j != t) A[t * n + j] += L.off[(size_t)q * n + t];
+            if (j != t) A[t * n + j] += (double)L.off[(size_t)q * n + t];
         }
     }
     __syncthreads();
@@ -193,14 +211,15 @@ __global__ void k_amg_dense_factor(AmgLevel L, double *dense)
     for (int idx = t; idx < n * n; idx += blockDim.x) dense[idx] = A[idx];
 }
 
-__global__ void k_amg_dense_solve(AmgLevel L, const double *__restrict__ dense, const PcgState *st)
+template <typename T>
+__global__ void k_amg_dense_solve(AmgLevelT<T> L, const double *__restrict__ dense, const PcgState *st)
 {
     if (st->done) return;
     extern __shared__ double F[];
     __shared__ double y[AMG_COARSEST_MAX];
     const int n = L.n, t = threadIdx.x;
     for (int idx = t; idx < n * n; idx += blockDim.x) F[idx] = dense[idx];
-    if (t < n) y[t] = L.r[t];
+    if (t < n) y[t] = (double)L.r[t];
     __syncthreads();
     for (int j = 0; j < n; j++) {  // L y = r
         if (t == j) y[j] /= F[j * n + j];
@@ -214,10 +233,11 @@ __global__ void k_amg_dense_solve(AmgLevel L, const double *__restrict__ dense, 
         if (t < j) y[t] -= F[j * n + t] * y[j];
         __syncthreads();
     }
-    if (t < n) L.e[0][t] = y[t];
+    if (t < n) L.e[0][t] = (T)y[t];
 }
 
-__global__ void k_amg_smooth_first(AmgLevel L, double omega, double *__restrict__ e, const PcgState *st)
+template <typename T>
+__global__ void k_amg_smooth_first(AmgLevelT<T> L, T omega, T *__restrict__ e, const PcgState *st)
 {
     if (st->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -225,7 +245,8 @@ __global__ void k_amg_smooth_first(AmgLevel L, double omega, double *__restrict_
     e[i] = omega * L.r[i] * inv_or_zero(L.diag[i]);
 }
 
-__global__ void k_amg_jacobi(AmgLevel L, double omega, const double *__restrict__ ein, double *__restrict__ eout,
+template <typename T>
+__global__ void k_amg_jacobi(AmgLevelT<T> L, T omega, const T *__restrict__ ein, T *__restrict__ eout,
                              const PcgState *st)
 {
     if (st->done) return;
@@ -234,12 +255,13 @@ __global__ void k_amg_jacobi(AmgLevel L, double omega, const double *__restrict_
     eout[i] = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
 }
 
-__global__ void k_amg_restrict(AmgLevel fine, AmgLevel coarse, const double *__restrict__ e, const PcgState *st)
+template <typename T>
+__global__ void k_amg_restrict(AmgLevelT<T> fine, AmgLevelT<T> coarse, const T *__restrict__ e, const PcgState *st)
 {
     if (st->done) return;
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= coarse.n) return;
-    double s = 0.0;
+    T s = (T)0;
     for (int t = fine.mptr[I]; t < fine.mptr[I + 1]; t++) {
         const int i = fine.mlist[t];
         s += fine.r[i] - row_apply(fine, i, e);
@@ -247,7 +269,8 @@ __global__ void k_amg_restrict(AmgLevel fine, AmgLevel coarse, const double *__r
     coarse.r[I] = s;
 }
 
-__global__ void k_amg_prolong(AmgLevel fine, double alpha, const double *__restrict__ ec, double *__restrict__ e,
+template <typename T>
+__global__ void k_amg_prolong(AmgLevelT<T> fine, T alpha, const T *__restrict__ ec, T *__restrict__ e,
                               const PcgState *st)
 {
     if (st->done) return;
@@ -256,18 +279,19 @@ __global__ void k_amg_prolong(AmgLevel fine, double alpha, const double *__restr
     e[i] += alpha * ec[fine.agg[i]];
 }
 
-// Last post-smoothing sweep on level 0: z into zp[i].x and the PCG's r . z.
-__global__ void __launch_bounds__(MCB_THREADS) k_amg_final(AmgLevel L, double omega, const double *__restrict__ ein,
-                                                           double2 *__restrict__ zp, PcgState *st, double *partials,
-                                                           unsigned int *counter, int is_init)
+// Last post-smoothing sweep on level 0: z into zp[i].x and the PCG's r . z (FP64 sum).
+template <typename T>
+__global__ void __launch_bounds__(MCB_THREADS) k_amg_final(AmgLevelT<T> L, T omega, const T *__restrict__ ein,
+                                                           typename Pair<T>::type *__restrict__ zp, PcgState *st,
+                                                           double *partials, unsigned int *counter, int is_init)
 {
     __shared__ double sh[1][MCB_THREADS];
     if (st->done) return;
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x) {
-        const double z = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
+        const T z = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
         zp[i].x = z;
-        acc[0] += L.r[i] * z;
+        acc[0] += (double)L.r[i] * (double)z;
     }
     if (publish_partials<1>(acc, partials, counter, sh)) {
         double tot[1];
@@ -288,60 +312,90 @@ __global__ void __launch_bounds__(MCB_THREADS) k_amg_final(AmgLevel L, double om
 namespace {
 inline int blocks(int n) { return std::max(1, (n + MCB_THREADS - 1) / MCB_THREADS); }
 inline size_t dense_smem(int n) { return (size_t)n * n * sizeof(double); }
+
+template <typename T>
+const AmgLevelT<T> *levels_of(const AmgHierarchy &H);
+template <>
+const AmgLevelT<double> *levels_of<double>(const AmgHierarchy &H) { return H.lv; }
+template <>
+const AmgLevelT<float> *levels_of<float>(const AmgHierarchy &H) { return H.lv32; }
+
+template <typename T>
+void set_dense_attributes()
+{
+    static bool done = false;
+    if (done) return;
+    cudaFuncSetAttribute(k_amg_dense_factor<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)dense_smem(AMG_COARSEST_MAX));
+    cudaFuncSetAttribute(k_amg_dense_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)dense_smem(AMG_COARSEST_MAX));
+    done = true;
+}
 } // namespace
 
-void amg_setup_values(cudaStream_t s, const AmgHierarchy &H, double * /*partials*/)
+template <typename T>
+void amg_setup_values(cudaStream_t s, const AmgHierarchy &H)
 {
-    for (int l = 1; l < H.levels; l++)
-        k_amg_galerkin<<<blocks(H.lv[l].n), MCB_THREADS, 0, s>>>(H.lv[l - 1], H.lv[l]);
-    const AmgLevel &C = H.lv[H.levels - 1];
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_amg_dense_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dense_smem(AMG_COARSEST_MAX));
-        cudaFuncSetAttribute(k_amg_dense_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dense_smem(AMG_COARSEST_MAX));
-        attr = true;
-    }
-    k_amg_dense_factor<<<1, AMG_COARSEST_MAX, dense_smem(C.n), s>>>(C, H.dense);
+    const AmgLevelT<T> *lv = levels_of<T>(H);
+    if (sizeof(T) == sizeof(float))
+        k_amg_round_level0<<<blocks(H.lv[0].n), MCB_THREADS, 0, s>>>(H.lv[0].n, H.lv[0].diag, H.lv[0].off,
+                                                                     (float *)lv[0].diag, (float *)lv[0].off);
+    for (int l = 1; l < H.levels; l++) k_amg_galerkin<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l - 1], lv[l]);
+    set_dense_attributes<T>();
+    const AmgLevelT<T> &C = lv[H.levels - 1];
+    k_amg_dense_factor<T><<<1, AMG_COARSEST_MAX, dense_smem(C.n), s>>>(C, H.dense);
 }
 
 int amg_kernels_per_vcycle(const AmgHierarchy &H) { return (H.levels - 1) * (2 * H.sweeps + 2) + 1; }
 
-void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const double *r0, double2 *zp_out, PcgState *st,
-                double *partials, unsigned int *counter, int is_init)
+template <typename T>
+void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out_v, PcgState *st, double *partials,
+                unsigned int *counter, int is_init)
 {
+    using T2 = typename Pair<T>::type;
+    T2 *zp_out = (T2 *)zp_out_v;
     const int L = H.levels;
+    const T omega = (T)H.omega, alpha = (T)H.alpha;
     int cur[AMG_MAX_LEVELS] = {0};
-    AmgLevel lv[AMG_MAX_LEVELS];
-    for (int l = 0; l < L; l++) lv[l] = H.lv[l];
-    lv[0].r = const_cast<double *>(r0);
+    AmgLevelT<T> lv[AMG_MAX_LEVELS];
+    const AmgLevelT<T> *src = levels_of<T>(H);
+    for (int l = 0; l < L; l++) lv[l] = src[l];
+    lv[0].r = const_cast<T *>(r0);
+    set_dense_attributes<T>();
     for (int l = 0; l + 1 < L; l++) {
-        k_amg_smooth_first<<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], H.omega, lv[l].e[0], st);
+        k_amg_smooth_first<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, lv[l].e[0], st);
         int c = 0;
         for (int sw = 1; sw < H.sweeps; sw++) {
-            k_amg_jacobi<<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], H.omega, lv[l].e[c], lv[l].e[c ^ 1], st);
+            k_amg_jacobi<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, lv[l].e[c], lv[l].e[c ^ 1], st);
             c ^= 1;
         }
         cur[l] = c;
-        k_amg_restrict<<<blocks(lv[l + 1].n), MCB_THREADS, 0, s>>>(lv[l], lv[l + 1], lv[l].e[c], st);
+        k_amg_restrict<T><<<blocks(lv[l + 1].n), MCB_THREADS, 0, s>>>(lv[l], lv[l + 1], lv[l].e[c], st);
     }
-    k_amg_dense_solve<<<1, AMG_COARSEST_MAX, dense_smem(lv[L - 1].n), s>>>(lv[L - 1], H.dense, st);
+    k_amg_dense_solve<T><<<1, AMG_COARSEST_MAX, dense_smem(lv[L - 1].n), s>>>(lv[L - 1], H.dense, st);
     cur[L - 1] = 0;
     for (int l = L - 2; l >= 0; l--) {
         int c = cur[l];
-        k_amg_prolong<<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], H.alpha, lv[l + 1].e[cur[l + 1]], lv[l].e[c], st);
+        k_amg_prolong<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], alpha, lv[l + 1].e[cur[l + 1]], lv[l].e[c], st);
         for (int sw = 1; sw <= H.sweeps; sw++) {
             if (l == 0 && sw == H.sweeps) {
-                k_amg_final<<<krylov_grid(lv[0].n), MCB_THREADS, 0, s>>>(lv[0], H.omega, lv[0].e[c], zp_out, st,
-                                                                        partials, counter, is_init);
+                k_amg_final<T><<<krylov_grid(lv[0].n), MCB_THREADS, 0, s>>>(lv[0], omega, lv[0].e[c], zp_out, st,
+                                                                           partials, counter, is_init);
             } else {
-                k_amg_jacobi<<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], H.omega, lv[l].e[c], lv[l].e[c ^ 1], st);
+                k_amg_jacobi<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, lv[l].e[c], lv[l].e[c ^ 1],
+                                                                       st);
                 c ^= 1;
             }
         }
         cur[l] = c;
     }
 }
+
+template void amg_setup_values<double>(cudaStream_t, const AmgHierarchy &);
+template void amg_setup_values<float>(cudaStream_t, const AmgHierarchy &);
+template void amg_vcycle<double>(cudaStream_t, const AmgHierarchy &, const double *, void *, PcgState *, double *,
+                                 unsigned int *, int);
+template void amg_vcycle<float>(cudaStream_t, const AmgHierarchy &, const float *, void *, PcgState *, double *,
+                                unsigned int *, int);
 
 } // namespace mcb

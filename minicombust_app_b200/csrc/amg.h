@@ -30,12 +30,13 @@ namespace mcb {
 constexpr int AMG_MAX_LEVELS = 16;
 constexpr int AMG_COARSEST_MAX = 128;
 
-// Device view of one level.
-struct AmgLevel {
+// Device view of one level; T is the storage type of values and vectors.
+template <typename T>
+struct AmgLevelT {
     int n;          // rows
     int k;          // off-diagonal slots (ELL width)
-    double *diag;   // [n]
-    double *off;    // [k][n]
+    T *diag;        // [n]
+    T *off;         // [k][n]
     const int *col; // [k][n], unused slots point at their own row
     // restriction to the next level: members of coarse row I are mlist[mptr[I] .. mptr[I+1])
     const int *agg;   // [n] aggregate (next-level row) of each row
@@ -47,14 +48,17 @@ struct AmgLevel {
     // fine off id = n_fine + s * n_fine + row).
     const int *gptr;
     const int *gidx;
-    double *r;      // right-hand side of the level
-    double *e[2];   // ping-pong iterates
+    T *r;           // right-hand side of the level
+    T *e[2];        // ping-pong iterates
 };
+using AmgLevel = AmgLevelT<double>;
 
 struct AmgHierarchy {
     int levels = 0;
-    AmgLevel lv[AMG_MAX_LEVELS];
-    double *dense = nullptr;    // coarsest Cholesky factor [n][n] (row-major, lower)
+    AmgLevelT<double> lv[AMG_MAX_LEVELS];    // FP64 values (level 0 = the pressure-correction matrix)
+    AmgLevelT<float> lv32[AMG_MAX_LEVELS];   // FP32 values, when the refined FP32 path is enabled
+    bool has32 = false;
+    double *dense = nullptr;    // coarsest Cholesky factor [n][n] (row-major, lower), FP64
     int sweeps = 2;
     double omega = 0.6667;
     double alpha = 1.0;
@@ -75,14 +79,18 @@ int amg_build_host(int N, const std::vector<int> &col0, const std::vector<int> &
                    std::string &err);
 
 // Device work, all asynchronous on stream s.
-// Galerkin values of levels 1..L-1 and the coarsest dense factor.
-void amg_setup_values(cudaStream_t s, const AmgHierarchy &H, double *partials);
-// z = V-cycle(r0) for level 0; the result is written to zp[i].x (the PCG
-// interleaved buffer) and the partial sums of r0 . z go through the PCG
-// reduction (see krylov.cuh).  Kernels are no-ops once *done is set.
+// Galerkin values of levels 1..L-1 and the coarsest dense factor, for the
+// FP64 (T = double) or the FP32 (T = float; level 0 rounded from FP64 first)
+// hierarchy.
+template <typename T>
+void amg_setup_values(cudaStream_t s, const AmgHierarchy &H);
+// z = V-cycle(r0) on level 0; z goes to zp[i].x (the PCG interleaved buffer)
+// and r0 . z (FP64 sum) into the PCG state.  Kernels are no-ops once
+// st->done is set.
 struct PcgState;
-void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const double *r0, double2 *zp_out, PcgState *st,
-                double *partials, unsigned int *counter, int is_init);
+template <typename T>
+void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out, PcgState *st, double *partials,
+                unsigned int *counter, int is_init);
 int amg_kernels_per_vcycle(const AmgHierarchy &H);
 
 } // namespace mcb

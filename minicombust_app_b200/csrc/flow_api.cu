@@ -28,7 +28,8 @@ enum KernelId {
     K_GRAD5, K_GRAD1, K_PRECOMP_AU, K_MOMENTUM, K_MASS_FLUX, K_OUTLET_FIX, K_PRESSURE_ROWS, K_PP_FACES,
     K_PP_CELLS, K_P_BOUNDARY, K_PP_MAX, K_TEMPERATURE, K_IMBALANCE, K_PCG_MEAN, K_PCG_INIT, K_PCG_ITER1,
     K_PCG_ITER2, K_PCG_XMEAN, K_PCG_SUBMEAN, K_BICG3_INIT, K_BICG3_1, K_BICG3_2, K_BICG3_3, K_BICG1_INIT,
-    K_BICG1_1, K_BICG1_2, K_BICG1_3, K_AMG_SETUP, K_PCG_INIT_AMG, K_PCG_ITER2_AMG, K_AMG_VCYCLE, K_COUNT
+    K_BICG1_1, K_BICG1_2, K_BICG1_3, K_AMG_SETUP, K_PCG_INIT_AMG, K_PCG_ITER2_AMG, K_AMG_VCYCLE,
+    K_IR, K_PCG_INIT_AMG32, K_PCG_ITER1_32, K_PCG_ITER2_AMG32, K_AMG_VCYCLE32, K_COUNT
 };
 
 const char *kKernelNames[K_COUNT] = {
@@ -37,7 +38,8 @@ const char *kKernelNames[K_COUNT] = {
     "temperature_assemble", "mass_imbalance", "pcg_mean", "pcg_init", "pcg_iter1_spmv", "pcg_iter2_update",
     "pcg_xmean", "pcg_sub_xmean", "bicg3_init", "bicg3_1_spmv", "bicg3_2_spmv", "bicg3_3_update",
     "bicg1_init", "bicg1_1_spmv", "bicg1_2_spmv", "bicg1_3_update", "amg_setup_galerkin_factor",
-    "pcg_init_amg", "pcg_iter2_amg_update", "amg_vcycle"};
+    "pcg_init_amg", "pcg_iter2_amg_update", "amg_vcycle", "ir_fp64_residual_update", "pcg32_init_amg",
+    "pcg32_iter1_spmv", "pcg32_iter2_amg_update", "amg32_vcycle"};
 
 constexpr int PCG_BATCH = 16;   // iterations per status read (even: ping-pong buffers)
 constexpr int PCG_AMG_BATCH = 4;
@@ -106,6 +108,12 @@ struct mc_flow {
     bool use_amg = false;
     AmgHierarchy amg;
     char *amg_mem = nullptr;
+    // FP32-refined pressure solve (precision == MC_PRECISION_FP32_REFINED)
+    bool refined = false;
+    PcgVectorsT<float> pv32{};   // inner FP32 PCG: x = correction, b = outer residual in FP32
+    float *r32 = nullptr;
+    PcgState *h_pcg_inner = nullptr;  // pinned
+    cudaGraphExec_t g_pcg_amg32 = nullptr;
 
     // state of the reference's control flow
     int first_pressure = 1;
@@ -236,7 +244,8 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
     launch(h, K_PCG_MEAN, [&] { pcg_mean(h->stream, A, v); });
     if (amg) {
         launch(h, K_PCG_INIT_AMG, [&] { pcg_init_amg(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, 1); });
-        launch(h, K_AMG_VCYCLE, [&] { amg_vcycle(h->stream, h->amg, v.r, v.zp[0], v.st, v.partials, v.counter, 1); });
+        launch(h, K_AMG_VCYCLE,
+               [&] { amg_vcycle<double>(h->stream, h->amg, v.r, v.zp[0], v.st, v.partials, v.counter, 1); });
         h->launches += amg_kernels_per_vcycle(h->amg) - 1;
     } else {
         launch(h, K_PCG_INIT, [&] { pcg_init(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, 0, 1); });
@@ -260,7 +269,7 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
                 if (amg) {
                     launch(h, K_PCG_ITER2_AMG, [&] { pcg_iter2_amg(h->stream, A, v, pin ^ 1); });
                     launch(h, K_AMG_VCYCLE, [&] {
-                        amg_vcycle(h->stream, h->amg, v.r, v.zp[pin ^ 1], v.st, v.partials, v.counter, 0);
+                        amg_vcycle<double>(h->stream, h->amg, v.r, v.zp[pin ^ 1], v.st, v.partials, v.counter, 0);
                     });
                     h->launches += amg_kernels_per_vcycle(h->amg) - 1;
                 } else {
@@ -279,6 +288,76 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
     *bnorm = std::sqrt(s.bb);
     *relres = s.bb > 0 ? std::sqrt(s.rr / s.bb) : 0.0;
     return krylov_status_to_mc(s.status);
+}
+
+// FP32-refined pressure solve: FP64 outer iterative refinement (true
+// residual, norms, solution accumulation) around inner PCG solves whose
+// matrix, vectors and AMG V-cycle are FP32 (dot products summed in FP64).
+int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *relres, double *bnorm)
+{
+    const Ell A = pressure_matrix(h);
+    const EllT<float> A32{h->N, h->amg.lv32[0].diag, h->amg.lv32[0].off, h->col};
+    PcgVectors o = h->pv;
+    PcgVectorsT<float> in = h->pv32;
+    constexpr int kMaxOuter = 50;
+    launch(h, K_PCG_MEAN, [&] { pcg_mean(h->stream, A, o); });
+    launch(h, K_IR, [&] {
+        ir_init(h->stream, A, o.b, o.x, o.r, h->r32, o.st, o.partials, o.counter, h->prm.p_rtol, abs_floor, kMaxOuter);
+    });
+    int rc = check_launch(h);
+    if (rc) return rc;
+    const int per_iter = 2 + amg_kernels_per_vcycle(h->amg);
+    const long max_batches = h->prm.max_iters / PCG_AMG_BATCH + 2;
+    int inner_total = 0, worst = MC_OK;
+    for (int outer = 0;; outer++) {
+        CUDA_TRY(h, cudaMemcpyAsync(h->h_pcg, o.st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        flush_timing(h);
+        if (h->h_pcg->done) break;
+        if (outer > kMaxOuter) return fail(h, MC_ERR_NOT_CONVERGED, "refinement state did not advance");
+        launch(h, K_PCG_INIT_AMG32,
+               [&] { pcg_init_amg<float>(h->stream, A32, in, h->prm.ir_inner_rtol, 0.0, h->prm.max_iters, 0); });
+        launch(h, K_AMG_VCYCLE32,
+               [&] { amg_vcycle<float>(h->stream, h->amg, in.r, in.zp[0], in.st, in.partials, in.counter, 1); });
+        h->launches += amg_kernels_per_vcycle(h->amg) - 1;
+        rc = check_launch(h);
+        if (rc) return rc;
+        for (long batch = 0;; batch++) {
+            CUDA_TRY(h, cudaMemcpyAsync(h->h_pcg_inner, in.st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
+            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+            flush_timing(h);
+            if (h->h_pcg_inner->done) break;
+            if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "inner solve state did not advance");
+            rc = run_batch(h, &h->g_pcg_amg32, PCG_AMG_BATCH * per_iter, [&] {
+                for (int it = 0; it < PCG_AMG_BATCH; it++) {
+                    const int pin = it & 1;
+                    launch(h, K_PCG_ITER1_32, [&] { pcg_iter1<float>(h->stream, A32, in, pin); });
+                    launch(h, K_PCG_ITER2_AMG32, [&] { pcg_iter2_amg<float>(h->stream, A32, in, pin ^ 1); });
+                    launch(h, K_AMG_VCYCLE32, [&] {
+                        amg_vcycle<float>(h->stream, h->amg, in.r, in.zp[pin ^ 1], in.st, in.partials, in.counter, 0);
+                    });
+                    h->launches += amg_kernels_per_vcycle(h->amg) - 1;
+                }
+            });
+            if (rc) return rc;
+        }
+        inner_total += h->h_pcg_inner->iter;
+        if (h->h_pcg_inner->status == KRYLOV_NONFINITE) return fail(h, MC_ERR_NONFINITE, "inner FP32 solve");
+        launch(h, K_IR, [&] { ir_add(h->stream, h->N, o.x, in.x, o.st); });
+        launch(h, K_IR, [&] { ir_residual(h->stream, A, o.b, o.x, o.r, h->r32, o.st, o.partials, o.counter); });
+        rc = check_launch(h);
+        if (rc) return rc;
+    }
+    launch(h, K_PCG_XMEAN, [&] { pcg_xmean(h->stream, h->N, o); });
+    launch(h, K_PCG_SUBMEAN, [&] { pcg_sub_xmean(h->stream, h->N, o); });
+    rc = check_launch(h);
+    if (rc) return rc;
+    const PcgState &st = *h->h_pcg;
+    *iters = inner_total;
+    *bnorm = std::sqrt(st.bb);
+    *relres = st.bb > 0 ? std::sqrt(st.rr / st.bb) : 0.0;
+    const int s = krylov_status_to_mc(st.status);
+    return s != MC_OK ? s : worst;
 }
 
 template <int R>
@@ -435,7 +514,12 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
             k_pressure_rows<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a);
         });
         if (h->use_amg) {
-            launch(h, K_AMG_SETUP, [&] { amg_setup_values(h->stream, h->amg, h->partials); });
+            launch(h, K_AMG_SETUP, [&] {
+                if (h->refined)
+                    amg_setup_values<float>(h->stream, h->amg);
+                else
+                    amg_setup_values<double>(h->stream, h->amg);
+            });
             h->launches += h->amg.levels - 1;
         }
     }
@@ -448,7 +532,8 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
         int its = 0;
         double relres = 0.0, bnorm = 0.0;
         const double floor = (simple && loop > 1) ? h->prm.p_rtol * h->p_bnorm_ref : 0.0;
-        rc = solve_pressure(h, floor, &its, &relres, &bnorm);
+        rc = h->refined ? solve_pressure_refined(h, floor, &its, &relres, &bnorm)
+                        : solve_pressure(h, floor, &its, &relres, &bnorm);
         if (rc == MC_ERR_CUDA) return rc;
         if (rc != MC_OK && worst == MC_OK) worst = rc;
         if (loop == 1) h->p_bnorm_ref = bnorm;
@@ -682,6 +767,25 @@ int build_amg(mc_flow *h, const HostMesh &hm)
     }
     const int nc = lv[L - 1].n;
     add(&H.dense, (size_t)nc * nc * 8);
+    const bool fp32 = h->prm.precision == MC_PRECISION_FP32_REFINED;
+    PcgState *inner_state = nullptr;
+    if (fp32) {
+        for (int l = 0; l < L; l++) {
+            AmgLevelT<float> &f = H.lv32[l];
+            add(&f.diag, (size_t)lv[l].n * 4);
+            add(&f.off, (size_t)lv[l].k * lv[l].n * 4);
+            add(&f.r, (size_t)lv[l].n * 4);
+            add(&f.e[0], (size_t)lv[l].n * 4);
+            add(&f.e[1], (size_t)lv[l].n * 4);
+        }
+        add(&h->pv32.x, (size_t)N * 4);
+        add(&h->pv32.r, (size_t)N * 4);
+        add(&h->pv32.q, (size_t)N * 4);
+        add(&h->pv32.zp[0], (size_t)N * 8);
+        add(&h->pv32.zp[1], (size_t)N * 8);
+        add(&h->r32, (size_t)N * 4);
+        add(&inner_state, sizeof(PcgState));
+    }
     std::vector<size_t> offs;
     for (auto &it : items) offs.push_back(ar.reserve(it.bytes));
     cudaError_t e = cudaMalloc((void **)&h->amg_mem, ar.used);
@@ -718,6 +822,27 @@ int build_amg(mc_flow *h, const HostMesh &hm)
             d.mlist = d_mlist[l];
         }
     }
+    if (fp32) {
+        for (int l = 0; l < L; l++) {
+            AmgLevelT<float> &f = H.lv32[l];
+            const AmgLevelT<double> &d = H.lv[l];
+            f.n = d.n;
+            f.k = d.k;
+            f.col = d.col;
+            f.agg = d.agg;
+            f.mptr = d.mptr;
+            f.mlist = d.mlist;
+            f.gptr = d.gptr;
+            f.gidx = d.gidx;
+        }
+        h->pv32.b = h->r32;
+        h->pv32.partials = h->partials;
+        h->pv32.counter = h->counter;
+        h->pv32.st = inner_state;
+        CUDA_TRY(h, cudaMallocHost((void **)&h->h_pcg_inner, sizeof(PcgState)));
+        H.has32 = true;
+        h->refined = true;
+    }
     h->use_amg = true;
     return MC_OK;
 }
@@ -746,6 +871,7 @@ void mc_flow_default_params(mc_flow_params *p, int mode)
     p->amg_sweeps = 2;
     p->amg_omega = 0.6667;
     p->amg_alpha = 1.8;
+    p->ir_inner_rtol = 1e-2;
     if (mode == MC_MODE_COMPAT) {
         p->viscosity = 0.000014;
         p->temperature0 = 2000.0;
@@ -769,7 +895,11 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
     *out = nullptr;
     if (params->mode != MC_MODE_COMPAT && params->mode != MC_MODE_SIMPLE) return MC_ERR_ARG;
     if ((params->pressure_solver != MC_PSOLVER_PCG_JACOBI && params->pressure_solver != MC_PSOLVER_PCG_AMG) ||
-        params->precision != MC_PRECISION_FP64 || params->initial_guess != MC_GUESS_ZERO)
+        (params->precision != MC_PRECISION_FP64 && params->precision != MC_PRECISION_FP32_REFINED) ||
+        params->initial_guess != MC_GUESS_ZERO)
+        return MC_ERR_UNSUPPORTED;
+    if (params->precision == MC_PRECISION_FP32_REFINED &&
+        (params->pressure_solver != MC_PSOLVER_PCG_AMG || !(params->ir_inner_rtol > 0) || params->ir_inner_rtol >= 1))
         return MC_ERR_UNSUPPORTED;
     if (params->pressure_solver == MC_PSOLVER_PCG_AMG &&
         (params->amg_sweeps < 1 || !(params->amg_omega > 0) || !(params->amg_alpha > 0)))
@@ -873,7 +1003,7 @@ int mc_flow_destroy(mc_flow *h)
 {
     if (!h) return MC_ERR_ARG;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    for (cudaGraphExec_t g : {h->g_pcg, h->g_b3, h->g_b1, h->g_pcg_amg})
+    for (cudaGraphExec_t g : {h->g_pcg, h->g_b3, h->g_b1, h->g_pcg_amg, h->g_pcg_amg32})
         if (g) cudaGraphExecDestroy(g);
     if (h->amg_mem) cudaFree(h->amg_mem);
     for (cudaEvent_t e : h->timing.ev) cudaEventDestroy(e);
@@ -882,6 +1012,7 @@ int mc_flow_destroy(mc_flow *h)
     if (h->h_b3) cudaFreeHost(h->h_b3);
     if (h->h_b1) cudaFreeHost(h->h_b1);
     if (h->h_scalars) cudaFreeHost(h->h_scalars);
+    if (h->h_pcg_inner) cudaFreeHost(h->h_pcg_inner);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return MC_OK;

@@ -98,9 +98,12 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_init(Ell A, PcgVectors v, d
 
 // p_new = z + beta p_old (own row and, on the fly, neighbour rows); q = A p_new.
 // Two rows per thread are kept in flight so that their gathers overlap.
-__global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(Ell A, PcgVectors v, const double2 *__restrict__ X,
-                                                           double2 *__restrict__ Y)
+template <typename T>
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(EllT<T> A, PcgVectorsT<T> v,
+                                                           const typename Pair<T>::type *__restrict__ X,
+                                                           typename Pair<T>::type *__restrict__ Y)
 {
+    using T2 = typename Pair<T>::type;
     __shared__ double sh[1][MCB_THREADS];
     const PcgState *st = v.st;
     if (st->done) return;
@@ -113,7 +116,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(Ell A, PcgVectors v, 
         const bool has1 = i1 < N;
         const int j1 = has1 ? i1 : i0;
         int ca[6], cb[6];
-        double oa[6], ob[6];
+        T oa[6], ob[6];
 #pragma unroll
         for (int k = 0; k < 6; k++) {
             ca[k] = A.col[(size_t)k * N + i0];
@@ -121,22 +124,23 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(Ell A, PcgVectors v, 
             oa[k] = A.off[(size_t)k * N + i0];
             ob[k] = A.off[(size_t)k * N + j1];
         }
-        const double2 sa = X[i0], sb = X[j1];
-        const double pa = sa.x + beta * sa.y, pb = sb.x + beta * sb.y;
-        double qa = A.diag[i0] * pa, qb = A.diag[j1] * pb;
+        const T2 sa = X[i0], sb = X[j1];
+        const T bt = (T)beta;
+        const T pa = sa.x + bt * sa.y, pb = sb.x + bt * sb.y;
+        T qa = A.diag[i0] * pa, qb = A.diag[j1] * pb;
 #pragma unroll
         for (int k = 0; k < 6; k++) {
-            const double2 ga = X[ca[k]], gb = X[cb[k]];
-            qa += oa[k] * (ga.x + beta * ga.y);
-            qb += ob[k] * (gb.x + beta * gb.y);
+            const T2 ga = X[ca[k]], gb = X[cb[k]];
+            qa += oa[k] * (ga.x + bt * ga.y);
+            qb += ob[k] * (gb.x + bt * gb.y);
         }
         Y[i0].y = pa;
         v.q[i0] = qa;
-        acc[0] += pa * qa;
+        acc[0] += (double)pa * (double)qa;
         if (has1) {
             Y[i1].y = pb;
             v.q[i1] = qb;
-            acc[0] += pb * qb;
+            acc[0] += (double)pb * (double)qb;
         }
     }
     if (publish_partials<1>(acc, v.partials, v.counter, sh)) {
@@ -198,21 +202,23 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2(Ell A, PcgVectors v, 
 
 // Initialisation for the AMG-preconditioned PCG: r = b - mean(b), x = 0;
 // z comes from the first V-cycle (amg.cu), which also sets r . z.
-__global__ void __launch_bounds__(MCB_THREADS) k_pcg_init_amg(Ell A, PcgVectors v, double rtol, double abs_floor,
-                                                              int max_iters, int project)
+template <typename T>
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_init_amg(EllT<T> A, PcgVectorsT<T> v, double rtol,
+                                                              double abs_floor, int max_iters, int project)
 {
+    using T2 = typename Pair<T>::type;
     __shared__ double sh[2][MCB_THREADS];
     const int N = A.N;
     const double mean = project ? v.st->mean : 0.0;
     double acc[2] = {0.0, 0.0};  // b.b, r.r
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const double bi = v.b[i] - mean;
-        v.x[i] = 0.0;
+        const T bi = (T)((double)v.b[i] - mean);
+        v.x[i] = (T)0;
         v.r[i] = bi;
-        v.zp[0][i] = make_double2(0.0, 0.0);
-        v.zp[1][i] = make_double2(0.0, 0.0);
-        acc[0] += bi * bi;
-        acc[1] += bi * bi;
+        v.zp[0][i] = T2{(T)0, (T)0};
+        v.zp[1][i] = T2{(T)0, (T)0};
+        acc[0] += (double)bi * (double)bi;
+        acc[1] += (double)bi * (double)bi;
     }
     if (publish_partials<2>(acc, v.partials, v.counter, sh)) {
         double tot[2];
@@ -238,19 +244,21 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_init_amg(Ell A, PcgVectors 
 }
 
 // x += alpha p; r -= alpha q; convergence on ||r||.  z follows from the V-cycle.
-__global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2_amg(Ell A, PcgVectors v, const double2 *__restrict__ Y)
+template <typename T>
+__global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2_amg(EllT<T> A, PcgVectorsT<T> v,
+                                                               const typename Pair<T>::type *__restrict__ Y)
 {
     __shared__ double sh[1][MCB_THREADS];
     const PcgState *st = v.st;
     if (st->done) return;
     const int N = A.N;
-    const double alpha = st->alpha;
+    const T alpha = (T)st->alpha;
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         v.x[i] += alpha * Y[i].y;
-        const double ri = v.r[i] - alpha * v.q[i];
+        const T ri = v.r[i] - alpha * v.q[i];
         v.r[i] = ri;
-        acc[0] += ri * ri;
+        acc[0] += (double)ri * (double)ri;
     }
     if (publish_partials<1>(acc, v.partials, v.counter, sh)) {
         double tot[1];
@@ -267,6 +275,92 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2_amg(Ell A, PcgVectors
             } else if (s->iter >= s->max_iters) {
                 s->done = 1;
                 s->status = KRYLOV_NOT_CONVERGED;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------ FP64 iterative refinement
+// Outer loop of the FP32-refined pressure solve: FP64 solution, FP64 true
+// residual r = b' - A x with b' = b - mean(b), FP64 norms; each inner FP32
+// solve gets r rounded to FP32 as its right-hand side.
+
+__global__ void __launch_bounds__(MCB_THREADS) k_ir_init(Ell A, const double *__restrict__ b, double *__restrict__ x,
+                                                         double *__restrict__ r, float *__restrict__ r32, PcgState *st,
+                                                         double *partials, unsigned int *counter, double rtol,
+                                                         double abs_floor, int max_outer)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    const int N = A.N;
+    const double mean = st->mean;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double bi = b[i] - mean;
+        x[i] = 0.0;
+        r[i] = bi;
+        r32[i] = (float)bi;
+        acc[0] += bi * bi;
+    }
+    if (publish_partials<1>(acc, partials, counter, sh)) {
+        double tot[1];
+        reduce_partials<1>(tot, partials, counter, sh);
+        if (threadIdx.x == 0) {
+            st->bb = tot[0];
+            st->rr = tot[0];
+            const double t = fmax(rtol * sqrt(tot[0]), abs_floor);
+            st->tol2 = t * t;
+            st->iter = 0;
+            st->max_iters = max_outer;
+            st->status = KRYLOV_OK;
+            st->done = (tot[0] == 0.0 || tot[0] <= st->tol2) ? 1 : 0;
+            if (!finite(tot[0])) {
+                st->done = 1;
+                st->status = KRYLOV_NONFINITE;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(MCB_THREADS) k_ir_add(int N, double *__restrict__ x, const float *__restrict__ e,
+                                                        const PcgState *st)
+{
+    if (st->done) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) x[i] += (double)e[i];
+}
+
+__global__ void __launch_bounds__(MCB_THREADS) k_ir_residual(Ell A, const double *__restrict__ b,
+                                                             const double *__restrict__ x, double *__restrict__ r,
+                                                             float *__restrict__ r32, PcgState *st, double *partials,
+                                                             unsigned int *counter)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    if (st->done) return;
+    const int N = A.N;
+    const double mean = st->mean;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        double ax = A.diag[i] * x[i];
+#pragma unroll
+        for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * x[A.col[(size_t)k * N + i]];
+        const double ri = (b[i] - mean) - ax;
+        r[i] = ri;
+        r32[i] = (float)ri;
+        acc[0] += ri * ri;
+    }
+    if (publish_partials<1>(acc, partials, counter, sh)) {
+        double tot[1];
+        reduce_partials<1>(tot, partials, counter, sh);
+        if (threadIdx.x == 0) {
+            st->rr = tot[0];
+            st->iter += 1;
+            if (!finite(tot[0])) {
+                st->done = 1;
+                st->status = KRYLOV_NONFINITE;
+            } else if (tot[0] <= st->tol2) {
+                st->done = 1;
+            } else if (st->iter >= st->max_iters) {
+                st->done = 1;
+                st->status = KRYLOV_NOT_CONVERGED;
             }
         }
     }
@@ -299,22 +393,47 @@ void pcg_init(cudaStream_t s, const Ell &A, const PcgVectors &v, double rtol, do
 {
     k_pcg_init<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, abs_floor, max_iters, use_x0, project);
 }
-void pcg_iter1(cudaStream_t s, const Ell &A, const PcgVectors &v, int pin)
+template <typename T>
+void pcg_iter1(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, int pin)
 {
-    k_pcg_iter1<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.zp[pin], v.zp[pin ^ 1]);
+    k_pcg_iter1<T><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.zp[pin], v.zp[pin ^ 1]);
 }
 void pcg_iter2(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew)
 {
     k_pcg_iter2<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.zp[pnew]);
 }
-void pcg_init_amg(cudaStream_t s, const Ell &A, const PcgVectors &v, double rtol, double abs_floor, int max_iters,
-                  int project)
+template <typename T>
+void pcg_init_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, double rtol, double abs_floor,
+                  int max_iters, int project)
 {
-    k_pcg_init_amg<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, abs_floor, max_iters, project);
+    k_pcg_init_amg<T><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, abs_floor, max_iters, project);
 }
-void pcg_iter2_amg(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew)
+template <typename T>
+void pcg_iter2_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, int pnew)
 {
-    k_pcg_iter2_amg<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.zp[pnew]);
+    k_pcg_iter2_amg<T><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.zp[pnew]);
+}
+#define MCB_INSTANTIATE_PCG(T)                                                                                  \
+    template void pcg_iter1<T>(cudaStream_t, const EllT<T> &, const PcgVectorsT<T> &, int);                   \
+    template void pcg_init_amg<T>(cudaStream_t, const EllT<T> &, const PcgVectorsT<T> &, double, double, int, \
+                                  int);                                                                       \
+    template void pcg_iter2_amg<T>(cudaStream_t, const EllT<T> &, const PcgVectorsT<T> &, int);
+MCB_INSTANTIATE_PCG(double)
+MCB_INSTANTIATE_PCG(float)
+void ir_init(cudaStream_t s, const Ell &A, const double *b, double *x, double *r, float *r32, PcgState *st,
+             double *partials, unsigned int *counter, double rtol, double abs_floor, int max_outer)
+{
+    k_ir_init<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, b, x, r, r32, st, partials, counter, rtol, abs_floor,
+                                                       max_outer);
+}
+void ir_add(cudaStream_t s, int N, double *x, const float *e, const PcgState *st)
+{
+    k_ir_add<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, x, e, st);
+}
+void ir_residual(cudaStream_t s, const Ell &A, const double *b, const double *x, double *r, float *r32, PcgState *st,
+                 double *partials, unsigned int *counter)
+{
+    k_ir_residual<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, b, x, r, r32, st, partials, counter);
 }
 void pcg_xmean(cudaStream_t s, int N, const PcgVectors &v) { k_pcg_xmean<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, v); }
 void pcg_sub_xmean(cudaStream_t s, int N, const PcgVectors &v)

@@ -13,12 +13,27 @@
 
 namespace mcb {
 
-struct Ell {
-    int N;
-    const double *diag;
-    const double *off;  // [6][N]
-    const int *col;     // [6][N]
+// Paired vector type for the interleaved (z, p) buffers.
+template <typename T>
+struct Pair;
+template <>
+struct Pair<double> {
+    using type = double2;
 };
+template <>
+struct Pair<float> {
+    using type = float2;
+};
+
+// 7-point system in ELL form; T is the storage type of the values.
+template <typename T>
+struct EllT {
+    int N;
+    const T *diag;
+    const T *off;   // [6][N]
+    const int *col; // [6][N]
+};
+using Ell = EllT<double>;
 
 struct PcgState {
     double rz, rz_old, alpha, pq, rr, bb, tol2, mean, xmean;
@@ -36,14 +51,18 @@ struct BicgState {
 // direction interleaved, so that a neighbour costs one 16-byte gather.
 // Iteration k reads zp[k & 1] and writes p into zp[(k & 1) ^ 1], where the
 // next z is then stored.
-struct PcgVectors {
-    double *x, *r, *q;
-    double2 *zp[2];
-    const double *b;
+// Storage type T (double, or float for the inner solve of the refined
+// pressure path); dot products and the scalars in PcgState stay FP64.
+template <typename T>
+struct PcgVectorsT {
+    T *x, *r, *q;
+    typename Pair<T>::type *zp[2];
+    const T *b;
     double *partials;
     unsigned int *counter;
     PcgState *st;
 };
+using PcgVectors = PcgVectorsT<double>;
 
 template <int R>
 struct BicgVectors {
@@ -67,13 +86,25 @@ int krylov_grid(int N);
 void pcg_mean(cudaStream_t s, const Ell &A, const PcgVectors &v);
 void pcg_init(cudaStream_t s, const Ell &A, const PcgVectors &v, double rtol, double abs_floor, int max_iters,
               int use_x0, int project);
-void pcg_iter1(cudaStream_t s, const Ell &A, const PcgVectors &v, int pin);
+template <typename T>
+void pcg_iter1(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, int pin);
 void pcg_iter2(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew);
 // AMG-preconditioned variant: init without z, update without z (amg.cu
 // computes z and r . z after each update).
-void pcg_init_amg(cudaStream_t s, const Ell &A, const PcgVectors &v, double rtol, double abs_floor, int max_iters,
-                  int project);
-void pcg_iter2_amg(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew);
+template <typename T>
+void pcg_init_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, double rtol, double abs_floor,
+                  int max_iters, int project);
+template <typename T>
+void pcg_iter2_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, int pnew);
+// FP64 iterative refinement around an FP32 inner solve: the state's mean
+// (from pcg_mean) defines b' = b - mean; ir_init sets x = 0, r = b', r32 =
+// (float) r and the tolerance; ir_add accumulates x += e in FP64; ir_residual
+// recomputes the FP64 true residual, its norm, r32, and the convergence flag.
+void ir_init(cudaStream_t s, const Ell &A, const double *b, double *x, double *r, float *r32, PcgState *st,
+             double *partials, unsigned int *counter, double rtol, double abs_floor, int max_outer);
+void ir_add(cudaStream_t s, int N, double *x, const float *e, const PcgState *st);
+void ir_residual(cudaStream_t s, const Ell &A, const double *b, const double *x, double *r, float *r32, PcgState *st,
+                 double *partials, unsigned int *counter);
 void pcg_xmean(cudaStream_t s, int N, const PcgVectors &v);
 void pcg_sub_xmean(cudaStream_t s, int N, const PcgVectors &v);
 

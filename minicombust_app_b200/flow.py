@@ -57,7 +57,7 @@ class FlowParams(ctypes.Structure):
                 ("urf_momentum", c_dbl), ("urf_pressure", c_dbl), ("urf_temperature", c_dbl),
                 ("flux_corr", c_dbl), ("u_rtol", c_dbl), ("p_rtol", c_dbl), ("max_iters", c_int),
                 ("pressure_solver", c_int), ("precision", c_int), ("initial_guess", c_int), ("device", c_int),
-                ("amg_sweeps", c_int), ("amg_omega", c_dbl), ("amg_alpha", c_dbl)]
+                ("amg_sweeps", c_int), ("amg_omega", c_dbl), ("amg_alpha", c_dbl), ("ir_inner_rtol", c_dbl)]
 
 
 class IterStats(ctypes.Structure):

@@ -214,3 +214,46 @@ def test_amg_pressure_solver_matches_oracle(gpu, dims):
         assert err <= PARITY, (name, err)
     if solver.N > 1000:
         assert solver.last_stats.pressure_iters_first * 3 < jac.last_stats.pressure_iters_first
+
+
+@pytest.mark.parametrize("dims", [(40, 20, 20), (7, 3, 5)])
+def test_fp32_refined_pressure_solver_matches_oracle(gpu, dims):
+    """FP64 iterative refinement around FP32 AMG-PCG inner solves reaches the
+    FP64 answer: the outer residual is the true FP64 residual, so with the
+    pressure tolerance at 1e-12 the fields meet the same 1e-9 gate as the
+    all-FP64 solvers."""
+    lengths = (0.2, 0.1, 0.1)
+    solver, orc = make_pair(dims, lengths, SIMPLE, u_rtol=1e-13, p_rtol=1e-12,
+                            pressure_solver=flow.PSOLVER_PCG_AMG, precision=flow.PRECISION_FP32_REFINED)
+    seed_both(solver, orc, BASE_SIMPLE, seed=3)
+    for p in range(5):
+        solver.simple_iteration()
+        assert orc.step() == 0
+        assert solver.last_stats.pressure_rel_residual <= 1e-12
+    for name in FIELDS:
+        err = rel_err(solver.field(name), orc.field(name))
+        assert err <= PARITY, (name, err)
+
+
+def test_fp32_refined_reaches_rtol_at_default_tolerance(gpu):
+    """At the default 1e-8 pressure tolerance the refined solve stops on the
+    FP64 true residual and lands within the solver tolerance of the FP64 AMG
+    solve."""
+    dims, lengths = (48, 24, 24), (0.2, 0.1, 0.1)
+    out = {}
+    for prec in (flow.PRECISION_FP64, flow.PRECISION_FP32_REFINED):
+        s = flow.FlowSolver(flow.Mesh.box(*dims, *lengths),
+                            params=flow.default_params(flow.MODE_SIMPLE, pressure_solver=flow.PSOLVER_PCG_AMG,
+                                                       precision=prec))
+        init = noisy_initial_fields(s.N, BASE_SIMPLE, 5)
+        for name, vals in init.items():
+            a = s.field(name)
+            a[:s.N] = vals
+            s.set_field(name, a)
+        for _ in range(3):
+            s.simple_iteration()
+            assert s.last_stats.pressure_rel_residual <= 1e-8
+        out[prec] = [s.field(n) for n in FIELDS]
+        s.close()
+    for name, a, b in zip(FIELDS, out[flow.PRECISION_FP32_REFINED], out[flow.PRECISION_FP64]):
+        assert rel_err(a, b) <= 1e-6, name
