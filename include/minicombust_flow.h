@@ -51,6 +51,10 @@ enum { MC_MODE_COMPAT = 0, MC_MODE_SIMPLE = 1 };
 enum { MC_PSOLVER_PCG_JACOBI = 0, MC_PSOLVER_PCG_AMG = 1 };
 enum { MC_PRECISION_FP64 = 0, MC_PRECISION_FP32_REFINED = 1 };
 enum { MC_GUESS_ZERO = 0, MC_GUESS_PREVIOUS = 1, MC_GUESS_LEARNED = 2 };
+/* Cell order inside the handle.  Inputs and outputs of every call stay in the
+ * caller's (reference) numbering; MC_REORDER_RCM renumbers cells by reverse
+ * Cuthill-McKee and faces by first touch in that order, on the device only. */
+enum { MC_REORDER_NONE = 0, MC_REORDER_RCM = 1 };
 
 /* Field ids: the member order of phi_vector<T> (utils.hpp:158-174). */
 enum {
@@ -104,6 +108,7 @@ typedef struct mc_flow_params {
     double amg_omega;         /* Jacobi damping */
     double amg_alpha;         /* coarse-correction scaling */
     double ir_inner_rtol;     /* MC_PRECISION_FP32_REFINED: relative tolerance of each inner FP32 solve */
+    int reorder;              /* MC_REORDER_* */
 } mc_flow_params;
 
 /* Per-pass statistics. */
@@ -140,6 +145,9 @@ int mc_flow_set_sources(mc_flow *flow, const double *host_particle_terms);
 /* Face arrays in reference face order.  which: 0 mass flux [faces], 1 area,
  * 2 lambda, 3 rlencos, 4 face_fields [faces][2], 5 normals [faces][3], 6 centres [faces][3]. */
 int mc_flow_get_face_array(mc_flow *flow, int which, double *host_values);
+/* The handle's cell order: cell_new_to_old[i] = caller's id of the handle's
+ * i-th cell (the identity without reordering).  No reference counterpart. */
+int mc_flow_get_cell_order(mc_flow *flow, int *cell_new_to_old);
 /* which: 0 A_phi.U (momentum diagonal after under-relaxation), 1 pressure
  * diagonal, 2 cell volumes, 3 cell densities; [cells]. */
 int mc_flow_get_cell_array(mc_flow *flow, int which, double *host_values);
@@ -205,6 +213,11 @@ int mc_solve_bicgstab_noalloc(int n, const double *diag, const double *off, cons
  * mc_mesh_box_destroy. */
 int mc_mesh_box_create(uint64_t ex, uint64_t ey, uint64_t ez, double lx, double ly, double lz, mc_mesh_view *out);
 void mc_mesh_box_destroy(mc_mesh_view *mesh);
+
+/* Validate a mesh and write the reverse Cuthill-McKee cell order that
+ * MC_REORDER_RCM uses (cell_new_to_old[i] = caller's id of the i-th cell).
+ * Host only.  No reference counterpart. */
+int mc_mesh_rcm_order(const mc_mesh_view *mesh, int *cell_new_to_old);
 
 #ifdef __cplusplus
 }

@@ -27,19 +27,30 @@ int amg_build_host(int N, const std::vector<int> &col0, const std::vector<int> &
         if (n <= AMG_COARSEST_MAX) return 0;
         if ((int)out.size() == AMG_MAX_LEVELS) break;
         auto nb = [&](int d, int c) { return c < 0 ? -1 : dn[(size_t)d * n + c]; };
-        // 2 x 2 x 2 aggregates anchored at the first unaggregated cell (+x: slot 3, +y: 5, +z: 1)
+        // 2 x 2 x 2 aggregates anchored at the first unaggregated cell.  Per
+        // axis the aggregate extends to the + side (x: slot 3, y: 5, z: 1)
+        // when that neighbour is free, else to the - side (2, 4, 0), so the
+        // blocks stay whole in any cell order (in x-fastest order the + side
+        // is always free).
         std::vector<int> agg(n, -1), anchor;
         int nagg = 0;
+        auto side = [&](int plus, int minus, int c) {
+            const int a = nb(plus, c);
+            if (a >= 0 && agg[a] < 0) return plus;
+            const int b = nb(minus, c);
+            return (b >= 0 && agg[b] < 0) ? minus : plus;
+        };
         for (int c = 0; c < n; c++) {
             if (agg[c] >= 0) continue;
             const int A = nagg++;
             anchor.push_back(c);
             agg[c] = A;
-            const int x1 = nb(3, c), y1 = nb(5, c), z1 = nb(1, c);
-            const int xy = x1 >= 0 ? nb(5, x1) : nb(3, y1);
-            const int xz = x1 >= 0 ? nb(1, x1) : nb(3, z1);
-            const int yz = y1 >= 0 ? nb(1, y1) : nb(5, z1);
-            const int xyz = xy >= 0 ? nb(1, xy) : (xz >= 0 ? nb(5, xz) : nb(3, yz));
+            const int dx = side(3, 2, c), dy = side(5, 4, c), dz = side(1, 0, c);
+            const int x1 = nb(dx, c), y1 = nb(dy, c), z1 = nb(dz, c);
+            const int xy = x1 >= 0 ? nb(dy, x1) : nb(dx, y1);
+            const int xz = x1 >= 0 ? nb(dz, x1) : nb(dx, z1);
+            const int yz = y1 >= 0 ? nb(dz, y1) : nb(dy, z1);
+            const int xyz = xy >= 0 ? nb(dz, xy) : (xz >= 0 ? nb(dy, xz) : nb(dx, yz));
             for (int cand : {x1, y1, xy, z1, xz, yz, xyz})
                 if (cand >= 0 && agg[cand] < 0) agg[cand] = A;
         }

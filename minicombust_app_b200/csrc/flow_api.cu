@@ -29,7 +29,7 @@ enum KernelId {
     K_PP_CELLS, K_P_BOUNDARY, K_PP_MAX, K_TEMPERATURE, K_IMBALANCE, K_PCG_MEAN, K_PCG_INIT, K_PCG_ITER1,
     K_PCG_ITER2, K_PCG_XMEAN, K_PCG_SUBMEAN, K_BICG3_INIT, K_BICG3_1, K_BICG3_2, K_BICG3_3, K_BICG1_INIT,
     K_BICG1_1, K_BICG1_2, K_BICG1_3, K_AMG_SETUP, K_PCG_INIT_AMG, K_PCG_ITER2_AMG, K_AMG_VCYCLE,
-    K_IR, K_PCG_INIT_AMG32, K_PCG_ITER1_32, K_PCG_ITER2_AMG32, K_AMG_VCYCLE32, K_COUNT
+    K_IR, K_PCG_INIT_AMG32, K_PCG_ITER1_32, K_PCG_ITER2_AMG32, K_AMG_VCYCLE32, K_PERMUTE, K_COUNT
 };
 
 const char *kKernelNames[K_COUNT] = {
@@ -39,7 +39,7 @@ const char *kKernelNames[K_COUNT] = {
     "pcg_xmean", "pcg_sub_xmean", "bicg3_init", "bicg3_1_spmv", "bicg3_2_spmv", "bicg3_3_update",
     "bicg1_init", "bicg1_1_spmv", "bicg1_2_spmv", "bicg1_3_update", "amg_setup_galerkin_factor",
     "pcg_init_amg", "pcg_iter2_amg_update", "amg_vcycle", "ir_fp64_residual_update", "pcg32_init_amg",
-    "pcg32_iter1_spmv", "pcg32_iter2_amg_update", "amg32_vcycle"};
+    "pcg32_iter1_spmv", "pcg32_iter2_amg_update", "amg32_vcycle", "permute"};
 
 constexpr int PCG_BATCH = 16;   // iterations per status read (even: ping-pong buffers)
 constexpr int PCG_AMG_BATCH = 4;
@@ -78,6 +78,11 @@ struct mc_flow {
     MeshArgs margs{};
     Arena arena;
     std::vector<int> hcol;   // ELL columns with -1 on boundary slots (CSR export)
+    // cell/face renumbering (reorder == MC_REORDER_RCM); host and device copies
+    bool reordered = false;
+    std::vector<int> cell_n2o, cell_o2n, face_o2n;
+    int *d_cell_n2o = nullptr, *d_cell_o2n = nullptr, *d_face_o2n = nullptr;
+    double *stage = nullptr;  // max(F, N + 6) doubles, staging for permuted copies
 
     // mesh
     int *fc0, *fc1, *nbr, *sface, *col, *outlet_faces;
@@ -544,7 +549,8 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
             st->pressure_rel_residual = relres;
         }
         launch(h, K_PP_MAX, [&] {
-            k_pp_max<<<krylov_grid(h->N), MCB_THREADS, 0, h->stream>>>(h->N, h->phi[G_PP], h->partials, h->counter,
+            k_pp_max<<<krylov_grid(h->N), MCB_THREADS, 0, h->stream>>>(h->N, h->ph.cell0, h->phi[G_PP], h->partials,
+                                                                       h->counter,
                                                                        h->scalars);
         });
         CUDA_TRY(h, cudaMemcpyAsync(h->h_scalars, h->scalars, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -612,6 +618,20 @@ int stage_temperature(mc_flow *h, mc_iter_stats *st)
 
 // ------------------------------------------------------------------ create
 
+// out[i] = in[idx[i]] for i < n, then `tail` values copied in place (the
+// six boundary slots of a field).
+__global__ void k_permute(int n, int tail, double *__restrict__ out, const double *__restrict__ in,
+                          const int *__restrict__ idx)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + tail; i += gridDim.x * blockDim.x)
+        out[i] = i < n ? in[idx[i]] : in[i];
+}
+
+void permute(mc_flow *h, double *out, const double *in, const int *idx, int n, int tail)
+{
+    launch(h, K_PERMUTE, [&] { k_permute<<<blocks_for(n + tail), MCB_THREADS, 0, h->stream>>>(n, tail, out, in, idx); });
+}
+
 int allocate(mc_flow *h)
 {
     const size_t N = (size_t)h->N, F = (size_t)h->F, NB = N + 6;
@@ -646,6 +666,12 @@ int allocate(mc_flow *h)
     for (int k = 0; k < 8; k++) add(&bic[k], 3 * N * 8);
     add(&h->b3.st, sizeof(BicgState<3>));
     add(&h->b1.st, sizeof(BicgState<1>));
+    if (h->reordered) {
+        add(&h->d_cell_n2o, N * 4);
+        add(&h->d_cell_o2n, N * 4);
+        add(&h->d_face_o2n, F * 4);
+        add(&h->stage, std::max(F, NB) * 8);
+    }
     size_t total = 0;
     std::vector<size_t> offs;
     for (auto &it : items) offs.push_back(A.reserve(it.bytes));
@@ -872,6 +898,7 @@ void mc_flow_default_params(mc_flow_params *p, int mode)
     p->amg_omega = 0.6667;
     p->amg_alpha = 1.8;
     p->ir_inner_rtol = 1e-2;
+    p->reorder = MC_REORDER_NONE;
     if (mode == MC_MODE_COMPAT) {
         p->viscosity = 0.000014;
         p->temperature0 = 2000.0;
@@ -898,6 +925,7 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
         (params->precision != MC_PRECISION_FP64 && params->precision != MC_PRECISION_FP32_REFINED) ||
         params->initial_guess != MC_GUESS_ZERO)
         return MC_ERR_UNSUPPORTED;
+    if (params->reorder != MC_REORDER_NONE && params->reorder != MC_REORDER_RCM) return MC_ERR_ARG;
     if (params->precision == MC_PRECISION_FP32_REFINED &&
         (params->pressure_solver != MC_PSOLVER_PCG_AMG || !(params->ir_inner_rtol > 0) || params->ir_inner_rtol >= 1))
         return MC_ERR_UNSUPPORTED;
@@ -916,6 +944,18 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
         std::string err;
         HostPhysics hp{params->density};
         rc = build_host_mesh(mesh, hp, hm, err);
+        if (!rc && params->reorder == MC_REORDER_RCM) {
+            std::vector<int> face_n2o;
+            rcm_cell_order(hm, h->cell_n2o);
+            rc = apply_reorder(hm, h->cell_n2o, face_n2o, err);
+            if (!rc) {
+                h->reordered = true;
+                h->cell_o2n.assign(hm.N, 0);
+                for (int n = 0; n < hm.N; n++) h->cell_o2n[h->cell_n2o[n]] = n;
+                h->face_o2n.assign(hm.F, 0);
+                for (int n = 0; n < hm.F; n++) h->face_o2n[face_n2o[n]] = n;
+            }
+        }
         if (rc) {
             h->err = err;
             mc_flow_destroy(h);
@@ -949,6 +989,12 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
             rc = rc ? rc : upload3(h, h->Sx, h->Sy, h->Sz, hm.S, F);
             rc = rc ? rc : upload3(h, h->xf, h->yf, h->zf, hm.xf, F);
             rc = rc ? rc : upload3(h, h->xc, h->yc, h->zc, hm.xc, N);
+            if (!rc && h->reordered) {
+                rc = upload(h, h->d_cell_n2o, h->cell_n2o.data(), N);
+                rc = rc ? rc : upload(h, h->d_cell_o2n, h->cell_o2n.data(), N);
+                rc = rc ? rc : upload(h, h->d_face_o2n, h->face_o2n.data(), F);
+                if (!rc) cudaStreamSynchronize(h->stream);
+            }
             rc = rc ? rc : initial_fields(h, hm.btype);
             if (!rc && params->pressure_solver == MC_PSOLVER_PCG_AMG) rc = build_amg(h, hm);
         }
@@ -962,6 +1008,7 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
             Physics &ph = h->ph;
             ph.N = hm.N;
             ph.mode = params->mode;
+            ph.cell0 = h->reordered ? h->cell_o2n[0] : 0;
             for (int s = 0; s < 6; s++) {
                 ph.btype[s] = hm.btype[s];
                 ph.last_bface[s] = hm.last_bface[s];
@@ -1023,7 +1070,13 @@ int mc_flow_set_field(mc_flow *h, int field, const double *vals)
     if (!h || !vals) return MC_ERR_ARG;
     const int g = grad_index(field);
     if (g < 0) return MC_ERR_UNSUPPORTED;
-    CUDA_TRY(h, cudaMemcpyAsync(h->phi[g], vals, ((size_t)h->N + 6) * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    const size_t NB = (size_t)h->N + 6;
+    if (h->reordered) {
+        CUDA_TRY(h, cudaMemcpyAsync(h->stage, vals, NB * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        permute(h, h->phi[g], h->stage, h->d_cell_n2o, h->N, 6);
+    } else {
+        CUDA_TRY(h, cudaMemcpyAsync(h->phi[g], vals, NB * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    }
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return MC_OK;
 }
@@ -1033,8 +1086,21 @@ int mc_flow_get_field(mc_flow *h, int field, double *vals)
     if (!h || !vals) return MC_ERR_ARG;
     const int g = grad_index(field);
     if (g < 0) return MC_ERR_UNSUPPORTED;
-    CUDA_TRY(h, cudaMemcpyAsync(vals, h->phi[g], ((size_t)h->N + 6) * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    const size_t NB = (size_t)h->N + 6;
+    const double *src = h->phi[g];
+    if (h->reordered) {
+        permute(h, h->stage, src, h->d_cell_o2n, h->N, 6);
+        src = h->stage;
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(vals, src, NB * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return MC_OK;
+}
+
+int mc_flow_get_cell_order(mc_flow *h, int *cell_new_to_old)
+{
+    if (!h || !cell_new_to_old) return MC_ERR_ARG;
+    for (int i = 0; i < h->N; i++) cell_new_to_old[i] = h->reordered ? h->cell_n2o[i] : i;
     return MC_OK;
 }
 
@@ -1045,7 +1111,12 @@ int mc_flow_get_gradient(mc_flow *h, int field, double *vals)
     if (g < 0) return MC_ERR_UNSUPPORTED;
     std::vector<double> tmp((size_t)h->N);
     for (int d = 0; d < 3; d++) {
-        CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), h->grad[g][d], (size_t)h->N * 8, cudaMemcpyDeviceToHost, h->stream));
+        const double *src = h->grad[g][d];
+        if (h->reordered) {
+            permute(h, h->stage, src, h->d_cell_o2n, h->N, 0);
+            src = h->stage;
+        }
+        CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), src, (size_t)h->N * 8, cudaMemcpyDeviceToHost, h->stream));
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
         for (int i = 0; i < h->N; i++) vals[3 * (size_t)i + d] = tmp[i];
     }
@@ -1059,7 +1130,8 @@ int mc_flow_set_sources(mc_flow *h, const double *terms)
     std::vector<double> soa(5 * N);
     double total = 0.0;
     for (size_t i = 0; i < N; i++) {
-        for (int k = 0; k < 5; k++) soa[k * N + i] = terms[5 * i + k];
+        const size_t j = h->reordered ? (size_t)h->cell_o2n[i] : i;
+        for (int k = 0; k < 5; k++) soa[k * N + j] = terms[5 * i + k];
         total += terms[5 * i + 4];
     }
     CUDA_TRY(h, cudaMemcpyAsync(h->src, soa.data(), 5 * N * 8, cudaMemcpyHostToDevice, h->stream));
@@ -1075,6 +1147,10 @@ int mc_flow_get_face_array(mc_flow *h, int which, double *vals)
     const size_t F = (size_t)h->F;
     auto get1 = [&](const double *d, int stride, int comp) -> int {
         std::vector<double> tmp(F);
+        if (h->reordered) {
+            permute(h, h->stage, d, h->d_face_o2n, h->F, 0);
+            d = h->stage;
+        }
         CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), d, F * 8, cudaMemcpyDeviceToHost, h->stream));
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
         for (size_t i = 0; i < F; i++) vals[stride * i + comp] = tmp[i];
@@ -1097,6 +1173,10 @@ int mc_flow_get_cell_array(mc_flow *h, int which, double *vals)
     if (!h || !vals) return MC_ERR_ARG;
     const double *src = which == 0 ? h->AU : which == 1 ? h->diag_p : which == 2 ? h->vol : which == 3 ? h->rho : nullptr;
     if (!src) return MC_ERR_ARG;
+    if (h->reordered) {
+        permute(h, h->stage, src, h->d_cell_o2n, h->N, 0);
+        src = h->stage;
+    }
     CUDA_TRY(h, cudaMemcpyAsync(vals, src, (size_t)h->N * 8, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return MC_OK;
@@ -1120,24 +1200,27 @@ int mc_flow_get_csr(mc_flow *h, int system, int *n, int *nnz, int *row_ptr, int 
     *n = (int)N;
     *nnz = (int)count;
     if (!row_ptr && !col && !val && !rhs) return MC_OK;
-    std::vector<double> diag(N), off(6 * N);
+    std::vector<double> diag(N), off(6 * N), b(N);
     CUDA_TRY(h, cudaMemcpyAsync(diag.data(), d_diag, N * 8, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(off.data(), d_off, 6 * N * 8, cudaMemcpyDeviceToHost, h->stream));
-    if (rhs) CUDA_TRY(h, cudaMemcpyAsync(rhs, d_rhs, N * 8, cudaMemcpyDeviceToHost, h->stream));
+    if (rhs) CUDA_TRY(h, cudaMemcpyAsync(b.data(), d_rhs, N * 8, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     size_t pos = 0;
     std::vector<std::pair<int, double>> row;
-    for (size_t i = 0; i < N; i++) {
+    // rows and columns in the caller's numbering
+    for (size_t o = 0; o < N; o++) {
+        const size_t i = h->reordered ? (size_t)h->cell_o2n[o] : o;
         row.clear();
-        row.push_back({(int)i, diag[i]});
+        row.push_back({(int)o, diag[i]});
+        if (rhs) rhs[o] = b[i];
         for (int k = 0; k < 6; k++) {
             const int c = h->hcol[k * N + i];
-            if (c >= 0) row.push_back({c, off[k * N + i]});
+            if (c >= 0) row.push_back({h->reordered ? h->cell_n2o[c] : c, off[k * N + i]});
         }
         std::sort(row.begin(), row.end(), [](const std::pair<int, double> &a, const std::pair<int, double> &b) {
             return a.first < b.first;
         });
-        if (row_ptr) row_ptr[i] = (int)pos;
+        if (row_ptr) row_ptr[o] = (int)pos;
         for (auto &e : row) {
             if (col) col[pos] = e.first;
             if (val) val[pos] = e.second;

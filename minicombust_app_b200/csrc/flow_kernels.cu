@@ -605,7 +605,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pp_correct_cells(Physics ph, Me
     const int N = ph.N;
     const int c = grid_stride_start();
     if (c < N) {
-        if (correct_all || (correct_cell0 && c == 0)) {
+        if (correct_all || (correct_cell0 && c == ph.cell0)) {
             const double A = a.AU[c];
             const double Ar = (A != 0.0) ? 1.0 / A : 0.0;
             const double fact = m.vol[c] * Ar;
@@ -653,13 +653,13 @@ __global__ void k_update_p_boundary(Physics ph, MeshArgs m, double *P, const dou
 }
 
 // Largest pressure correction, as the reference computes it (:2371-2378):
-// max(PP[0], max_{i >= 1} |PP[i]|).
-__global__ void __launch_bounds__(MCB_THREADS) k_pp_max(int N, const double *__restrict__ PP, double *partials,
+// max(PP[0], max_{i >= 1} |PP[i]|), cell 0 in the reference's numbering.
+__global__ void __launch_bounds__(MCB_THREADS) k_pp_max(int N, int cell0, const double *__restrict__ PP, double *partials,
                                                         unsigned int *counter, double *out)
 {
     __shared__ double sh[1][MCB_THREADS];
     double v[1] = {-1.0e308};
-    for (int i = grid_stride_start(); i < N; i += gridDim.x * blockDim.x) v[0] = fmax(v[0], i == 0 ? PP[0] : fabs(PP[i]));
+    for (int i = grid_stride_start(); i < N; i += gridDim.x * blockDim.x) v[0] = fmax(v[0], i == cell0 ? PP[i] : fabs(PP[i]));
     if (publish_partials<1, true>(v, partials, counter, sh)) {
         double tot[1];
         reduce_partials<1, true>(tot, partials, counter, sh);

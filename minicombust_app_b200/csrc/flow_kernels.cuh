@@ -87,7 +87,7 @@ __global__ void k_pp_correct_faces(Physics ph, MeshArgs m, CorrectArgs a);
 __global__ void k_pp_correct_cells(Physics ph, MeshArgs m, CorrectArgs a, int correct_all, int correct_cell0);
 __global__ void k_update_p_boundary(Physics ph, MeshArgs m, double *P, const double *gPx, const double *gPy,
                                     const double *gPz);
-__global__ void k_pp_max(int N, const double *PP, double *partials, unsigned int *counter, double *out);
+__global__ void k_pp_max(int N, int cell0, const double *PP, double *partials, unsigned int *counter, double *out);
 __global__ void k_mass_imbalance(Physics ph, MeshArgs m, const double *mdot, const double *src, double *partials,
                                  unsigned int *counter, double *out);
 

@@ -45,6 +45,7 @@ struct Physics {
     int mode;             // 0 compat, 1 simple
     int btype[6];
     int last_bface[6];    // last face (reference order) of each boundary side
+    int cell0;            // the handle's id of the reference's cell 0
     double mu, inlet_mu, u_in, rho_in, T_ref, rdelta;
     double urf_u, urf_T, urf_p, flux_corr;
 };

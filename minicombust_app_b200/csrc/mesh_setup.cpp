@@ -198,6 +198,168 @@ int build_host_mesh(const mc_mesh_view *mv, const HostPhysics &hp, HostMesh &hm,
     return MC_OK;
 }
 
+namespace {
+
+// Breadth-first levels from r over unvisited (global mark 0) cells; returns
+// the cells of the last level and the eccentricity.
+int bfs_last_level(const HostMesh &hm, const std::vector<int> &deg, int r, std::vector<int> &dist,
+                   std::vector<int> &touched, std::vector<int> &last)
+{
+    const int N = hm.N;
+    for (int t : touched) dist[t] = -1;
+    touched.clear();
+    dist[r] = 0;
+    touched.push_back(r);
+    int ecc = 0;
+    for (size_t head = 0; head < touched.size(); head++) {
+        const int u = touched[head];
+        ecc = dist[u];
+        for (int s = 0; s < 6; s++) {
+            const int v = hm.nbr[(size_t)s * N + u];
+            if (v >= 0 && dist[v] < 0) {
+                dist[v] = dist[u] + 1;
+                touched.push_back(v);
+            }
+        }
+    }
+    last.clear();
+    for (int t : touched)
+        if (dist[t] == ecc) last.push_back(t);
+    (void)deg;
+    return ecc;
+}
+
+} // namespace
+
+void rcm_cell_order(const HostMesh &hm, std::vector<int> &order)
+{
+    const int N = hm.N;
+    std::vector<int> deg(N, 0);
+    for (int c = 0; c < N; c++)
+        for (int s = 0; s < 6; s++) deg[c] += hm.nbr[(size_t)s * N + c] >= 0;
+    std::vector<int> by_deg(N);
+    for (int c = 0; c < N; c++) by_deg[c] = c;
+    std::stable_sort(by_deg.begin(), by_deg.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+    std::vector<char> seen(N, 0);
+    std::vector<int> dist(N, -1), touched, last, nb;
+    order.clear();
+    order.reserve(N);
+    size_t cand = 0;
+    while ((int)order.size() < N) {
+        while (seen[by_deg[cand]]) cand++;
+        // pseudo-peripheral start (George & Liu): move to a least-degree cell
+        // of the last BFS level while the eccentricity grows
+        int r = by_deg[cand];
+        int ecc = bfs_last_level(hm, deg, r, dist, touched, last);
+        for (int sweep = 0; sweep < 8; sweep++) {
+            int best = last[0];
+            for (int t : last)
+                if (deg[t] < deg[best] || (deg[t] == deg[best] && t < best)) best = t;
+            const int e2 = bfs_last_level(hm, deg, best, dist, touched, last);
+            if (e2 <= ecc) break;
+            r = best;
+            ecc = e2;
+        }
+        for (int t : touched) dist[t] = -1;
+        touched.clear();
+        // Cuthill-McKee sweep of the component
+        size_t head = order.size();
+        order.push_back(r);
+        seen[r] = 1;
+        for (; head < order.size(); head++) {
+            const int u = order[head];
+            nb.clear();
+            for (int s = 0; s < 6; s++) {
+                const int v = hm.nbr[(size_t)s * N + u];
+                if (v >= 0 && !seen[v]) {
+                    seen[v] = 1;
+                    nb.push_back(v);
+                }
+            }
+            std::sort(nb.begin(), nb.end(), [&](int a, int b) { return deg[a] != deg[b] ? deg[a] < deg[b] : a < b; });
+            order.insert(order.end(), nb.begin(), nb.end());
+        }
+    }
+    std::reverse(order.begin(), order.end());
+}
+
+int apply_reorder(HostMesh &hm, const std::vector<int> &cell_n2o, std::vector<int> &face_n2o, std::string &err)
+{
+    const int N = hm.N, F = hm.F;
+    if ((int)cell_n2o.size() != N) {
+        err = "cell permutation has the wrong length";
+        return MC_ERR_ARG;
+    }
+    std::vector<int> co2n(N, -1), fo2n(F, -1);
+    for (int n = 0; n < N; n++) {
+        const int o = cell_n2o[n];
+        if (o < 0 || o >= N || co2n[o] >= 0) {
+            err = "cell permutation is not a permutation";
+            return MC_ERR_ARG;
+        }
+        co2n[o] = n;
+    }
+    face_n2o.clear();
+    face_n2o.reserve(F);
+    for (int n = 0; n < N; n++)
+        for (int k = 0; k < 6; k++) {
+            const int f = hm.sface[(size_t)k * N + cell_n2o[n]];
+            if (fo2n[f] < 0) {
+                fo2n[f] = (int)face_n2o.size();
+                face_n2o.push_back(f);
+            }
+        }
+    if ((int)face_n2o.size() != F) {
+        err = "some faces belong to no cell";
+        return MC_ERR_MESH;
+    }
+    auto cell_id = [&](int c) { return c < N ? co2n[c] : c; };  // boundary slots N + side stay
+    std::vector<int> fc0(F), fc1(F);
+    std::vector<double> area(F), lam(F), rl(F), S(3 * (size_t)F), xf(3 * (size_t)F);
+    for (int n = 0; n < F; n++) {
+        const int o = face_n2o[n];
+        fc0[n] = cell_id(hm.fc0[o]);
+        fc1[n] = cell_id(hm.fc1[o]);
+        area[n] = hm.area[o];
+        lam[n] = hm.lam[o];
+        rl[n] = hm.rl[o];
+        for (int d = 0; d < 3; d++) {
+            S[3 * (size_t)n + d] = hm.S[3 * (size_t)o + d];
+            xf[3 * (size_t)n + d] = hm.xf[3 * (size_t)o + d];
+        }
+    }
+    std::vector<int> nbr((size_t)6 * N), sface((size_t)6 * N), col((size_t)6 * N);
+    std::vector<double> xc(3 * (size_t)N), vol(N), rho(N);
+    for (int n = 0; n < N; n++) {
+        const int o = cell_n2o[n];
+        for (int k = 0; k < 6; k++) {
+            const int v = hm.nbr[(size_t)k * N + o];
+            nbr[(size_t)k * N + n] = v >= 0 ? co2n[v] : -1 - fo2n[-1 - v];
+            sface[(size_t)k * N + n] = fo2n[hm.sface[(size_t)k * N + o]];
+            col[(size_t)k * N + n] = co2n[hm.col[(size_t)k * N + o]];
+        }
+        for (int d = 0; d < 3; d++) xc[3 * (size_t)n + d] = hm.xc[3 * (size_t)o + d];
+        vol[n] = hm.vol[o];
+        rho[n] = hm.rho[o];
+    }
+    for (int &f : hm.outlet_faces) f = fo2n[f];
+    for (int s = 0; s < 6; s++) hm.last_bface[s] = fo2n[hm.last_bface[s]];
+    hm.fc0.swap(fc0);
+    hm.fc1.swap(fc1);
+    hm.area.swap(area);
+    hm.lam.swap(lam);
+    hm.rl.swap(rl);
+    hm.S.swap(S);
+    hm.xf.swap(xf);
+    hm.nbr.swap(nbr);
+    hm.sface.swap(sface);
+    hm.col.swap(col);
+    hm.xc.swap(xc);
+    hm.vol.swap(vol);
+    hm.rho.swap(rho);
+    return MC_OK;
+}
+
 // Inlet effective viscosity (FlowSolver.hpp:421-422).
 double inlet_effective_viscosity(double mu, double u_in)
 {
@@ -319,4 +481,24 @@ extern "C" void mc_mesh_box_destroy(mc_mesh_view *m)
     delete[] m->cell_neighbours;
     delete[] m->cell_centers;
     memset(m, 0, sizeof(*m));
+}
+
+// Validate a mesh and return the reverse Cuthill-McKee cell order the
+// solver uses with MC_REORDER_RCM (host only, no device work).
+extern "C" int mc_mesh_rcm_order(const mc_mesh_view *mesh, int *cell_new_to_old)
+{
+    if (!mesh || !cell_new_to_old) return MC_ERR_ARG;
+    mcb::HostMesh hm;
+    std::string err;
+    int rc;
+    try {
+        rc = mcb::build_host_mesh(mesh, mcb::HostPhysics{1.0}, hm, err);
+        if (rc) return rc;
+        std::vector<int> order;
+        mcb::rcm_cell_order(hm, order);
+        std::copy(order.begin(), order.end(), cell_new_to_old);
+    } catch (const std::bad_alloc &) {
+        return MC_ERR_NOMEM;
+    }
+    return MC_OK;
 }

@@ -35,6 +35,7 @@ MC_ERR_UNSUPPORTED = -7
 MODE_COMPAT, MODE_SIMPLE = 0, 1
 PSOLVER_PCG_JACOBI, PSOLVER_PCG_AMG = 0, 1
 PRECISION_FP64, PRECISION_FP32_REFINED = 0, 1
+REORDER_NONE, REORDER_RCM = 0, 1
 GUESS_ZERO, GUESS_PREVIOUS, GUESS_LEARNED = 0, 1, 2
 SYSTEM_MOMENTUM, SYSTEM_PRESSURE, SYSTEM_TEMPERATURE, SYSTEM_MOMENTUM_V, SYSTEM_MOMENTUM_W = 0, 1, 2, 3, 4
 
@@ -57,7 +58,8 @@ class FlowParams(ctypes.Structure):
                 ("urf_momentum", c_dbl), ("urf_pressure", c_dbl), ("urf_temperature", c_dbl),
                 ("flux_corr", c_dbl), ("u_rtol", c_dbl), ("p_rtol", c_dbl), ("max_iters", c_int),
                 ("pressure_solver", c_int), ("precision", c_int), ("initial_guess", c_int), ("device", c_int),
-                ("amg_sweeps", c_int), ("amg_omega", c_dbl), ("amg_alpha", c_dbl), ("ir_inner_rtol", c_dbl)]
+                ("amg_sweeps", c_int), ("amg_omega", c_dbl), ("amg_alpha", c_dbl), ("ir_inner_rtol", c_dbl),
+                ("reorder", c_int)]
 
 
 class IterStats(ctypes.Structure):
@@ -90,6 +92,7 @@ _SIGNATURES = {
     "mc_flow_get_gradient": (c_int, [c_vp, c_int, c_vp]),
     "mc_flow_set_sources": (c_int, [c_vp, c_vp]),
     "mc_flow_get_face_array": (c_int, [c_vp, c_int, c_vp]),
+    "mc_flow_get_cell_order": (c_int, [c_vp, c_vp]),
     "mc_flow_get_cell_array": (c_int, [c_vp, c_int, c_vp]),
     "mc_flow_get_csr": (c_int, [c_vp, c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int), c_vp, c_vp, c_vp, c_vp]),
     "mc_flow_simple_iteration": (c_int, [c_vp, ctypes.POINTER(IterStats)]),
@@ -112,6 +115,7 @@ _SIGNATURES = {
                                           ctypes.POINTER(c_int)]),
     "mc_mesh_box_create": (c_int, [c_u64, c_u64, c_u64, c_dbl, c_dbl, c_dbl, ctypes.POINTER(MeshView)]),
     "mc_mesh_box_destroy": (None, [ctypes.POINTER(MeshView)]),
+    "mc_mesh_rcm_order": (c_int, [ctypes.POINTER(MeshView), c_vp]),
 }
 
 _lib = None
@@ -193,6 +197,32 @@ class Mesh:
         finally:
             L.mc_mesh_box_destroy(ctypes.byref(mv))
         return out
+
+    def rcm_order(self):
+        """Reverse Cuthill-McKee cell order (new-to-old) used by REORDER_RCM."""
+        out = np.empty(self.n_cells, dtype=np.int32)
+        mv = self.view()
+        _check(library().mc_mesh_rcm_order(ctypes.byref(mv), _ptr(out)), what="mc_mesh_rcm_order")
+        return out
+
+    def renumbered(self, cell_new_to_old):
+        """The same mesh with its cells renumbered (faces keep their order;
+        an internal face whose cells change order swaps its roles, as the
+        reference requires cell0 < cell1)."""
+        n2o = np.asarray(cell_new_to_old, dtype=np.int64)
+        N = self.n_cells
+        o2n = np.empty(N, dtype=np.int64)
+        o2n[n2o] = np.arange(N)
+        nb = self.cell_neighbours[n2o].copy()
+        internal = nb < N
+        nb[internal] = o2n[nb[internal].astype(np.int64)].astype(np.uint64)
+        fc = self.face_cells.astype(np.int64)
+        c0 = o2n[fc[:, 0]]
+        c1 = np.where(fc[:, 1] < N, o2n[np.minimum(fc[:, 1], N - 1)], fc[:, 1])
+        swap = (fc[:, 1] < N) & (c1 < c0)
+        fc_new = np.stack([np.where(swap, c1, c0), np.where(swap, c0, c1)], axis=1)
+        return Mesh(self.points, self.cell_nodes[n2o], fc_new.astype(np.uint64), self.cell_faces[n2o], nb,
+                    self.cell_centers[n2o], self.boundary_types)
 
     def view(self):
         mv = MeshView()
@@ -282,6 +312,12 @@ class FlowSolver:
         a = np.empty((self.F, width))
         _check(self.L.mc_flow_get_face_array(self.h, which, _ptr(a)), self.h, "get_face_array")
         return a if width > 1 else a[:, 0]
+
+    def cell_order(self):
+        """The handle's internal cell order: new-to-old ids (identity unless reordered)."""
+        a = np.empty(self.N, dtype=np.int32)
+        _check(self.L.mc_flow_get_cell_order(self.h, _ptr(a)), self.h, "get_cell_order")
+        return a
 
     def cell_array(self, which):
         a = np.empty(self.N)

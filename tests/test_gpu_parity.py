@@ -67,8 +67,9 @@ def blobs(n_cells, centers, k, seed, amplitude):
     return src
 
 
-def test_geometry_bitwise(gpu):
-    solver, orc = make_pair((8, 4, 4), (0.2, 0.1, 0.1))
+@pytest.mark.parametrize("reorder", [flow.REORDER_NONE, flow.REORDER_RCM], ids=["natural", "rcm"])
+def test_geometry_bitwise(gpu, reorder):
+    solver, orc = make_pair((8, 4, 4), (0.2, 0.1, 0.1), reorder=reorder)
     for w in (1, 2, 3, 5, 6):
         assert np.array_equal(solver.face_array(w), orc.face_array(w)), w
     assert np.array_equal(solver.cell_array(2), orc.cell_array(6))
@@ -76,8 +77,9 @@ def test_geometry_bitwise(gpu):
         assert np.array_equal(solver.field(name), orc.field(name)), name
 
 
-def test_assembly_stages_bitwise(gpu):
-    solver, orc = make_pair((9, 5, 4), (0.18, 0.1, 0.08))
+@pytest.mark.parametrize("reorder", [flow.REORDER_NONE, flow.REORDER_RCM], ids=["natural", "rcm"])
+def test_assembly_stages_bitwise(gpu, reorder):
+    solver, orc = make_pair((9, 5, 4), (0.18, 0.1, 0.08), reorder=reorder)
     seed_both(solver, orc, BASE_COMPAT, seed=11)
     solver.stage("gradients")
     orc.L.mco_stage_gradients(orc.h)
@@ -115,11 +117,14 @@ def test_assembly_stages_bitwise(gpu):
     assert rel_err(solver.field("TEM"), orc.field("TEM")) < 1e-12
 
 
-def test_compat_ten_passes_match_reference_golden(gpu):
+@pytest.mark.parametrize("reorder", [flow.REORDER_NONE, flow.REORDER_RCM], ids=["natural", "rcm"])
+def test_compat_ten_passes_match_reference_golden(gpu, reorder):
     """The parity gate: 16,000 cells, 10 SIMPLE passes, against the reference's own output."""
     g = np.load(os.path.join(GOLDEN, "ref_cfg1_10passes.npz"))
     dims, L = tuple(int(x) for x in g["dims"]), tuple(float(x) for x in g["lengths"])
-    solver = flow.FlowSolver(flow.Mesh.box(*dims, *L), params=flow.default_params(flow.MODE_COMPAT))
+    solver = flow.FlowSolver(flow.Mesh.box(*dims, *L), params=flow.default_params(flow.MODE_COMPAT, reorder=reorder))
+    if reorder == flow.REORDER_RCM:
+        assert not np.array_equal(solver.cell_order(), np.arange(solver.N))
     init = noisy_initial_fields(solver.N, BASE_COMPAT, 0)
     for name, vals in init.items():
         a = solver.field(name)
@@ -134,8 +139,9 @@ def test_compat_ten_passes_match_reference_golden(gpu):
     assert np.array_equal(rp, g["pressure_rowptr"]) and np.array_equal(col, g["pressure_col"])
 
 
-def test_compat_passes_match_oracle(gpu):
-    solver, orc = make_pair((8, 4, 4), (0.2, 0.1, 0.1))
+@pytest.mark.parametrize("reorder", [flow.REORDER_NONE, flow.REORDER_RCM], ids=["natural", "rcm"])
+def test_compat_passes_match_oracle(gpu, reorder):
+    solver, orc = make_pair((8, 4, 4), (0.2, 0.1, 0.1), reorder=reorder)
     seed_both(solver, orc, BASE_COMPAT, seed=2)
     for p in range(10):
         solver.simple_iteration()
@@ -192,14 +198,15 @@ def test_deterministic(gpu):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("dims", [(40, 20, 20), (20, 10, 10), (7, 3, 5)])
-def test_amg_pressure_solver_matches_oracle(gpu, dims):
+@pytest.mark.parametrize("dims,reorder", [((40, 20, 20), flow.REORDER_NONE), ((20, 10, 10), flow.REORDER_NONE),
+                                          ((7, 3, 5), flow.REORDER_NONE), ((40, 20, 20), flow.REORDER_RCM)])
+def test_amg_pressure_solver_matches_oracle(gpu, dims, reorder):
     """PCG with the aggregation-AMG V-cycle reaches the same solution as the
     oracle's conjugate gradients (both to 1e-13), in far fewer iterations than
     PCG with Jacobi."""
     lengths = (0.2, 0.1, 0.1)
     solver, orc = make_pair(dims, lengths, SIMPLE, u_rtol=1e-13, p_rtol=1e-13,
-                            pressure_solver=flow.PSOLVER_PCG_AMG)
+                            pressure_solver=flow.PSOLVER_PCG_AMG, reorder=reorder)
     jac = flow.FlowSolver(flow.Mesh.box(*dims, *lengths),
                           params=flow.default_params(flow.MODE_SIMPLE, u_rtol=1e-13, p_rtol=1e-13))
     seed_both(solver, orc, BASE_SIMPLE, seed=1)
