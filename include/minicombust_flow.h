@@ -121,6 +121,9 @@ typedef struct mc_iter_stats {
     double pressure_correction_max_first;
     double pressure_rel_residual;    /* last pressure solve, ||r|| / ||b|| */
     double mass_imbalance;           /* max over cells |div(mdot) - mass source| after the pass */
+    int guess_choice_first;          /* initial guess of the first pressure solve: -1 zero, 0 previous
+                                        correction, 1 learned (MC_GUESS_PREVIOUS / MC_GUESS_LEARNED) */
+    double guess_rel_residual_first; /* ||b - A x0|| / ||b|| of that guess (1 for zero) */
 } mc_iter_stats;
 
 typedef struct mc_flow mc_flow;
@@ -148,6 +151,22 @@ int mc_flow_get_face_array(mc_flow *flow, int which, double *host_values);
 /* The handle's cell order: cell_new_to_old[i] = caller's id of the handle's
  * i-th cell (the identity without reordering).  No reference counterpart. */
 int mc_flow_get_cell_order(mc_flow *flow, int *cell_new_to_old);
+
+/* Parameters of the learned pressure-correction guess (MC_GUESS_LEARNED);
+ * the layout is that of mc_gnn_get_params (minicombust_gnn.h).  Required
+ * before the first pass with MC_GUESS_LEARNED.  No reference counterpart. */
+int mc_flow_set_guess_params(mc_flow *flow, const float *params, int count);
+
+/* Snapshot dataset writer: after every pressure-correction solve, append one
+ * record of four float32 arrays of `cells` values in the caller's numbering
+ * -- the right-hand side projected to mean zero, the matrix diagonal, the
+ * previous converged correction and the converged correction -- to `path`,
+ * until max_records have been written.  File: a 64-byte header (magic
+ * "MCSNAP01", uint32 version 1, uint32 cells, uint32 fields 4, uint32 dtype 0
+ * = float32, uint64 records, zero padding), then the records.  The record
+ * count is written on close.  No reference counterpart. */
+int mc_flow_snapshot_open(mc_flow *flow, const char *path, int max_records);
+int mc_flow_snapshot_close(mc_flow *flow);
 /* which: 0 A_phi.U (momentum diagonal after under-relaxation), 1 pressure
  * diagonal, 2 cell volumes, 3 cell densities; [cells]. */
 int mc_flow_get_cell_array(mc_flow *flow, int which, double *host_values);

@@ -29,6 +29,8 @@ CUDA_SOURCES = [
     ("amg.cu", []),
     ("flow_api.cu", []),
     ("solve_noalloc.cu", []),
+    ("gnn.cu", []),
+    ("gnn_api.cu", []),
 ]
 CXX_SOURCES = [("mesh_setup.cpp", ["-ffp-contract=off", "-fno-fast-math"])]
 
@@ -60,6 +62,7 @@ def build(verbose=False, force=False):
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(ROOT, "include", "minicombust_flow.h"))
+    headers.append(os.path.join(ROOT, "include", "minicombust_gnn.h"))
     objs = []
     for src, flags in CUDA_SOURCES:
         s = os.path.join(CSRC, src)

@@ -14,6 +14,7 @@
 
 #include "amg.h"
 #include "flow_kernels.cuh"
+#include "gnn.cuh"
 #include "krylov.cuh"
 #include "mc_internal.h"
 #include "mc_reduce.cuh"
@@ -29,7 +30,8 @@ enum KernelId {
     K_PP_CELLS, K_P_BOUNDARY, K_PP_MAX, K_TEMPERATURE, K_IMBALANCE, K_PCG_MEAN, K_PCG_INIT, K_PCG_ITER1,
     K_PCG_ITER2, K_PCG_XMEAN, K_PCG_SUBMEAN, K_BICG3_INIT, K_BICG3_1, K_BICG3_2, K_BICG3_3, K_BICG1_INIT,
     K_BICG1_1, K_BICG1_2, K_BICG1_3, K_AMG_SETUP, K_PCG_INIT_AMG, K_PCG_ITER2_AMG, K_AMG_VCYCLE,
-    K_IR, K_PCG_INIT_AMG32, K_PCG_ITER1_32, K_PCG_ITER2_AMG32, K_AMG_VCYCLE32, K_PERMUTE, K_COUNT
+    K_IR, K_PCG_INIT_AMG32, K_PCG_ITER1_32, K_PCG_ITER2_AMG32, K_AMG_VCYCLE32, K_PERMUTE, K_GUESS, K_GNN,
+    K_SNAPSHOT, K_COUNT
 };
 
 const char *kKernelNames[K_COUNT] = {
@@ -39,7 +41,8 @@ const char *kKernelNames[K_COUNT] = {
     "pcg_xmean", "pcg_sub_xmean", "bicg3_init", "bicg3_1_spmv", "bicg3_2_spmv", "bicg3_3_update",
     "bicg1_init", "bicg1_1_spmv", "bicg1_2_spmv", "bicg1_3_update", "amg_setup_galerkin_factor",
     "pcg_init_amg", "pcg_iter2_amg_update", "amg_vcycle", "ir_fp64_residual_update", "pcg32_init_amg",
-    "pcg32_iter1_spmv", "pcg32_iter2_amg_update", "amg32_vcycle", "permute"};
+    "pcg32_iter1_spmv", "pcg32_iter2_amg_update", "amg32_vcycle", "permute", "guess_select", "gnn_forward",
+    "snapshot_pack"};
 
 constexpr int PCG_BATCH = 16;   // iterations per status read (even: ping-pong buffers)
 constexpr int PCG_AMG_BATCH = 4;
@@ -119,6 +122,25 @@ struct mc_flow {
     float *r32 = nullptr;
     PcgState *h_pcg_inner = nullptr;  // pinned
     cudaGraphExec_t g_pcg_amg32 = nullptr;
+    // initial guess of the pressure correction
+    double *pp_prev = nullptr;        // previous converged correction [N]
+    GuessState *gs = nullptr;
+    GuessState *h_gs = nullptr;       // pinned
+    double *x0_learned = nullptr;     // [N]
+    GnnGraph gnn_g{};
+    GnnWork gnn_w;
+    float *gnn_p = nullptr;
+    __nv_bfloat16 *gnn_pk = nullptr;
+    char *gnn_mem = nullptr;
+    bool gnn_loaded = false;
+    int guess_choice = -1;
+    double guess_rel = 1.0;
+    // snapshot dataset writer
+    FILE *snap = nullptr;
+    int snap_max = 0, snap_count = 0;
+    float *snap_dev = nullptr;        // [4][N] device staging (inside gnn_mem or its own allocation)
+    float *snap_host = nullptr;       // pinned [4][N]
+    char *snap_mem = nullptr;
 
     // state of the reference's control flow
     int first_pressure = 1;
@@ -241,19 +263,87 @@ int run_batch(mc_flow *h, cudaGraphExec_t *exec, int kernels_in_batch, Body &&bo
     return MC_OK;
 }
 
+// Snapshot record [4][N] float32 in the caller's numbering (idx = old -> new
+// or nullptr): b - mean, diagonal, previous correction, correction.
+__global__ void k_snapshot_pack(int N, const double *__restrict__ b, const PcgState *__restrict__ st,
+                                const double *__restrict__ diag, const double *__restrict__ prev,
+                                const double *__restrict__ x, const int *__restrict__ idx, float *__restrict__ out)
+{
+    const double mean = st->mean;
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < N; o += gridDim.x * blockDim.x) {
+        const int i = idx ? idx[o] : o;
+        out[o] = (float)(b[i] - mean);
+        out[(size_t)N + o] = (float)diag[i];
+        out[(size_t)2 * N + o] = (float)prev[i];
+        out[(size_t)3 * N + o] = (float)x[i];
+    }
+}
+
+// Initial guess of a pressure-correction solve (after pcg_mean): the
+// previous converged correction and, with MC_GUESS_LEARNED, the network's
+// prediction compete with the zero guess on ||b' - A x0||; the winner is
+// written into x.  Returns 1 when x holds the guess (0: start from zero).
+int select_guess(mc_flow *h, const Ell &A, const double *b, const PcgState *st, double *x)
+{
+    if (h->prm.initial_guess == MC_GUESS_ZERO) return 0;
+    const bool learned = h->prm.initial_guess == MC_GUESS_LEARNED;
+    if (learned) {
+        launch(h, K_GNN, [&] {
+            GnnInput<double> in{b, &st->mean, A.diag, h->pp_prev};
+            gnn_forward<double>(h->stream, h->gnn_g, in, h->gnn_p, h->gnn_pk, h->gnn_w, h->x0_learned);
+        });
+        h->launches += gnn_forward_launches() - 1;
+    }
+    launch(h, K_GUESS, [&] {
+        guess_residuals(h->stream, A, b, st, h->pp_prev, learned ? h->x0_learned : nullptr, h->gs, h->partials,
+                        h->counter);
+    });
+    launch(h, K_GUESS, [&] { guess_apply(h->stream, h->N, x, h->pp_prev, learned ? h->x0_learned : nullptr, h->gs); });
+    CUDA_TRY(h, cudaMemcpyAsync(h->h_gs, h->gs, sizeof(GuessState), cudaMemcpyDeviceToHost, h->stream));
+    return 1;
+}
+
+// After a solve: append a snapshot record, then keep the correction as the
+// next solve's previous correction.
+int after_pressure_solve(mc_flow *h)
+{
+    if (h->prm.initial_guess != MC_GUESS_ZERO) {
+        const GuessState &g = *h->h_gs;  // the copy was ordered before the solve's final synchronisation
+        h->guess_choice = g.choice;
+        h->guess_rel = g.bb > 0 ? std::sqrt((g.choice < 0 ? g.bb : g.rr[g.choice]) / g.bb) : 1.0;
+    }
+    if (h->snap && h->snap_count < h->snap_max) {
+        launch(h, K_SNAPSHOT, [&] {
+            k_snapshot_pack<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(
+                h->N, h->pv.b, h->pv.st, pressure_matrix(h).diag, h->pp_prev, h->phi[G_PP],
+                h->reordered ? h->d_cell_o2n : nullptr, h->snap_dev);
+        });
+        const size_t bytes = (size_t)4 * h->N * sizeof(float);
+        CUDA_TRY(h, cudaMemcpyAsync(h->snap_host, h->snap_dev, bytes, cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        if (std::fwrite(h->snap_host, 1, bytes, h->snap) != bytes) return fail(h, MC_ERR_ARG, "snapshot write failed");
+        h->snap_count++;
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(h->pp_prev, h->phi[G_PP], (size_t)h->N * 8, cudaMemcpyDeviceToDevice, h->stream));
+    return MC_OK;
+}
+
 int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, double *bnorm)
 {
     const Ell A = pressure_matrix(h);
     PcgVectors v = h->pv;
     const bool amg = h->use_amg;
     launch(h, K_PCG_MEAN, [&] { pcg_mean(h->stream, A, v); });
+    const int use_x0 = select_guess(h, A, v.b, v.st, v.x);
     if (amg) {
-        launch(h, K_PCG_INIT_AMG, [&] { pcg_init_amg(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, 1); });
+        launch(h, K_PCG_INIT_AMG,
+               [&] { pcg_init_amg(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, 1, use_x0); });
         launch(h, K_AMG_VCYCLE,
                [&] { amg_vcycle<double>(h->stream, h->amg, v.r, v.zp[0], v.st, v.partials, v.counter, 1); });
         h->launches += amg_kernels_per_vcycle(h->amg) - 1;
     } else {
-        launch(h, K_PCG_INIT, [&] { pcg_init(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, 0, 1); });
+        launch(h, K_PCG_INIT,
+               [&] { pcg_init(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, use_x0, 1); });
     }
     int rc = check_launch(h);
     if (rc) return rc;
@@ -306,8 +396,10 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
     PcgVectorsT<float> in = h->pv32;
     constexpr int kMaxOuter = 50;
     launch(h, K_PCG_MEAN, [&] { pcg_mean(h->stream, A, o); });
+    const int use_x0 = select_guess(h, A, o.b, o.st, o.x);
     launch(h, K_IR, [&] {
-        ir_init(h->stream, A, o.b, o.x, o.r, h->r32, o.st, o.partials, o.counter, h->prm.p_rtol, abs_floor, kMaxOuter);
+        ir_init(h->stream, A, o.b, o.x, o.r, h->r32, o.st, o.partials, o.counter, h->prm.p_rtol, abs_floor, kMaxOuter,
+                use_x0);
     });
     int rc = check_launch(h);
     if (rc) return rc;
@@ -504,6 +596,8 @@ int stage_momentum(mc_flow *h, mc_iter_stats *st)
 
 int stage_pressure(mc_flow *h, mc_iter_stats *st)
 {
+    if (h->prm.initial_guess == MC_GUESS_LEARNED && !h->gnn_loaded)
+        return fail(h, MC_ERR_ARG, "MC_GUESS_LEARNED needs mc_flow_set_guess_params first");
     const int simple = h->prm.mode == MC_MODE_SIMPLE;
     launch_mass_flux(h);
     if (simple || h->first_pressure) {
@@ -542,10 +636,18 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
         if (rc == MC_ERR_CUDA) return rc;
         if (rc != MC_OK && worst == MC_OK) worst = rc;
         if (loop == 1) h->p_bnorm_ref = bnorm;
+        {
+            const int rs = after_pressure_solve(h);
+            if (rs) return rs;
+        }
         if (st) {
             st->pressure_solves++;
             st->pressure_iters_total += its;
-            if (loop == 1) st->pressure_iters_first = its;
+            if (loop == 1) {
+                st->pressure_iters_first = its;
+                st->guess_choice_first = h->guess_choice;
+                st->guess_rel_residual_first = h->guess_rel;
+            }
             st->pressure_rel_residual = relres;
         }
         launch(h, K_PP_MAX, [&] {
@@ -666,6 +768,8 @@ int allocate(mc_flow *h)
     for (int k = 0; k < 8; k++) add(&bic[k], 3 * N * 8);
     add(&h->b3.st, sizeof(BicgState<3>));
     add(&h->b1.st, sizeof(BicgState<1>));
+    add(&h->pp_prev, N * 8);
+    add(&h->gs, sizeof(GuessState));
     if (h->reordered) {
         add(&h->d_cell_n2o, N * 4);
         add(&h->d_cell_o2n, N * 4);
@@ -743,6 +847,38 @@ int initial_fields(mc_flow *h, const int btype[6])
     rc = rc ? rc : put(G_PP, 0.0, 0.0, 0.0, 0.0);
     rc = rc ? rc : put(G_T, p.temperature0, p.temperature0, p.temperature0, p.temperature0);
     return rc;
+}
+
+// Guess state (pinned copy) and, for MC_GUESS_LEARNED, the network's graph,
+// parameters and inference scratch in one device allocation.
+int setup_guess(mc_flow *h, const HostMesh &hm)
+{
+    CUDA_TRY(h, cudaMallocHost((void **)&h->h_gs, sizeof(GuessState)));
+    memset(h->h_gs, 0, sizeof(GuessState));
+    if (h->prm.initial_guess != MC_GUESS_LEARNED) return MC_OK;
+    std::vector<int> col;
+    std::vector<uint32_t> edge;
+    std::vector<float> vhat;
+    gnn_graph_host(hm, col, edge, vhat);
+    const size_t N = (size_t)hm.N;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t eb = al(6 * N * 4), vb = al(N * 4), xb = al(N * 8), pb = al((size_t)GNN_NPARAM * 4),
+                 kb = al((size_t)GNN_NPACK * 2), wb = gnn_work_bytes(hm.N, false);
+    const cudaError_t e = cudaMalloc((void **)&h->gnn_mem, eb + vb + xb + pb + kb + wb);
+    if (e != cudaSuccess) return fail(h, MC_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    char *c = h->gnn_mem;
+    CUDA_TRY(h, cudaMemcpy(c, edge.data(), 6 * N * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(c + eb, vhat.data(), N * 4, cudaMemcpyHostToDevice));
+    h->gnn_g.n = hm.N;
+    h->gnn_g.col = h->col;
+    h->gnn_g.edge = reinterpret_cast<const __nv_bfloat162 *>(c);
+    h->gnn_g.vhat = reinterpret_cast<const float *>(c + eb);
+    h->x0_learned = reinterpret_cast<double *>(c + eb + vb);
+    h->gnn_p = reinterpret_cast<float *>(c + eb + vb + xb);
+    h->gnn_pk = reinterpret_cast<__nv_bfloat16 *>(c + eb + vb + xb + pb);
+    CUDA_TRY(h, cudaMemset(c + eb + vb + xb + pb + kb, 0, wb));
+    gnn_work_carve(h->gnn_w, c + eb + vb + xb + pb + kb, hm.N, false);
+    return MC_OK;
 }
 
 // Aggregation hierarchy for the pressure-correction system: pattern data on
@@ -922,9 +1058,11 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
     *out = nullptr;
     if (params->mode != MC_MODE_COMPAT && params->mode != MC_MODE_SIMPLE) return MC_ERR_ARG;
     if ((params->pressure_solver != MC_PSOLVER_PCG_JACOBI && params->pressure_solver != MC_PSOLVER_PCG_AMG) ||
-        (params->precision != MC_PRECISION_FP64 && params->precision != MC_PRECISION_FP32_REFINED) ||
-        params->initial_guess != MC_GUESS_ZERO)
+        (params->precision != MC_PRECISION_FP64 && params->precision != MC_PRECISION_FP32_REFINED))
         return MC_ERR_UNSUPPORTED;
+    if (params->initial_guess != MC_GUESS_ZERO && params->initial_guess != MC_GUESS_PREVIOUS &&
+        params->initial_guess != MC_GUESS_LEARNED)
+        return MC_ERR_ARG;
     if (params->reorder != MC_REORDER_NONE && params->reorder != MC_REORDER_RCM) return MC_ERR_ARG;
     if (params->precision == MC_PRECISION_FP32_REFINED &&
         (params->pressure_solver != MC_PSOLVER_PCG_AMG || !(params->ir_inner_rtol > 0) || params->ir_inner_rtol >= 1))
@@ -997,6 +1135,7 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
             }
             rc = rc ? rc : initial_fields(h, hm.btype);
             if (!rc && params->pressure_solver == MC_PSOLVER_PCG_AMG) rc = build_amg(h, hm);
+            if (!rc) rc = setup_guess(h, hm);
         }
         if (!rc) {
             h->hcol.assign((size_t)6 * hm.N, -1);
@@ -1060,6 +1199,9 @@ int mc_flow_destroy(mc_flow *h)
     if (h->h_b1) cudaFreeHost(h->h_b1);
     if (h->h_scalars) cudaFreeHost(h->h_scalars);
     if (h->h_pcg_inner) cudaFreeHost(h->h_pcg_inner);
+    if (h->snap) mc_flow_snapshot_close(h);
+    if (h->h_gs) cudaFreeHost(h->h_gs);
+    if (h->gnn_mem) cudaFree(h->gnn_mem);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return MC_OK;
@@ -1095,6 +1237,64 @@ int mc_flow_get_field(mc_flow *h, int field, double *vals)
     CUDA_TRY(h, cudaMemcpyAsync(vals, src, NB * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return MC_OK;
+}
+
+int mc_flow_set_guess_params(mc_flow *h, const float *params, int count)
+{
+    if (!h || !params || count != GNN_NPARAM) return MC_ERR_ARG;
+    if (h->prm.initial_guess != MC_GUESS_LEARNED) return fail(h, MC_ERR_ARG, "initial_guess is not MC_GUESS_LEARNED");
+    CUDA_TRY(h, cudaMemcpyAsync(h->gnn_p, params, (size_t)GNN_NPARAM * 4, cudaMemcpyHostToDevice, h->stream));
+    gnn_pack(h->stream, h->gnn_p, h->gnn_pk);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->gnn_loaded = true;
+    return MC_OK;
+}
+
+int mc_flow_snapshot_open(mc_flow *h, const char *path, int max_records)
+{
+    if (!h || !path || max_records <= 0) return MC_ERR_ARG;
+    if (h->snap) mc_flow_snapshot_close(h);
+    const size_t bytes = (size_t)4 * h->N * sizeof(float);
+    if (!h->snap_mem) {
+        CUDA_TRY(h, cudaMalloc((void **)&h->snap_mem, bytes));
+        CUDA_TRY(h, cudaMallocHost((void **)&h->snap_host, bytes));
+        h->snap_dev = reinterpret_cast<float *>(h->snap_mem);
+    }
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(h, MC_ERR_ARG, std::string("cannot open ") + path);
+    unsigned char head[64] = {0};
+    memcpy(head, "MCSNAP01", 8);
+    const uint32_t meta[4] = {1u, (uint32_t)h->N, 4u, 0u};
+    memcpy(head + 8, meta, sizeof(meta));
+    if (std::fwrite(head, 1, 64, f) != 64) {
+        std::fclose(f);
+        return fail(h, MC_ERR_ARG, "snapshot header write failed");
+    }
+    h->snap = f;
+    h->snap_max = max_records;
+    h->snap_count = 0;
+    return MC_OK;
+}
+
+int mc_flow_snapshot_close(mc_flow *h)
+{
+    if (!h) return MC_ERR_ARG;
+    int rc = MC_OK;
+    if (h->snap) {
+        const uint64_t count = (uint64_t)h->snap_count;
+        if (std::fseek(h->snap, 24, SEEK_SET) != 0 || std::fwrite(&count, 8, 1, h->snap) != 1) rc = MC_ERR_ARG;
+        if (std::fclose(h->snap) != 0) rc = MC_ERR_ARG;
+        h->snap = nullptr;
+    }
+    if (h->snap_mem) {
+        cudaFree(h->snap_mem);
+        cudaFreeHost(h->snap_host);
+        h->snap_mem = nullptr;
+        h->snap_host = nullptr;
+        h->snap_dev = nullptr;
+    }
+    return rc;
 }
 
 int mc_flow_get_cell_order(mc_flow *h, int *cell_new_to_old)

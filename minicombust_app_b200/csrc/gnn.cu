@@ -1,0 +1,863 @@
+// Learned initial guess: forward, backward and Adam kernels (see gnn.cuh).
+//
+// Every dense product is a block-level GEMM over a tile of 128 cells on the
+// tensor cores (mma.sync.m16n8k16, BF16 operands from shared memory, FP32
+// accumulators): with K = 32 or 64 and N = 32 the tiles are far below the
+// 128 x N minimum of a tcgen05 MMA, and the kernels are bound by the
+// activation traffic, not by the products.  Weight gradients are per-block
+// partial GEMMs (cells as the reduction dimension) summed afterwards in block
+// order, so training is deterministic.
+#include "gnn.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+#include "mc_reduce.cuh"
+
+namespace mcb {
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+using bf162 = __nv_bfloat162;
+
+constexpr int LDH = GNN_H + 8;        // row stride (elements) of [cell][32] tiles
+constexpr int LDU = 2 * GNN_H + 8;    // row stride of [cell][64] tiles
+constexpr int LDT = GNN_TILE + 8;     // row stride of transposed [channel][cell] tiles
+constexpr unsigned FULL = 0xffffffffu;
+
+int gnn_blocks(int n) { return (n + GNN_TILE - 1) / GNN_TILE; }
+int reduce_grid(int n) { return std::max(1, std::min((n + MCB_THREADS - 1) / MCB_THREADS, 148 * 4)); }
+
+__device__ __forceinline__ uint32_t ld32(const bf16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2])
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};\n"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// acc[MT][NT] += A[16 MT rows][16 KS] . W[8 NT rows][16 KS]^T for one warp.
+// A and W are row-major BF16 tiles in shared memory (strides lda, ldw, even).
+// Accumulator layout (m16n8): acc[.][.][0..1] = row g, cols 2t, 2t+1;
+// acc[.][.][2..3] = row g + 8; g = lane / 4, t = lane % 4.
+template <int MT, int NT, int KS>
+__device__ __forceinline__ void warp_gemm(float (&acc)[MT][NT][4], const bf16 *A, int lda, const bf16 *W, int ldw,
+                                          int lane)
+{
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int ks = 0; ks < KS; ks++) {
+        uint32_t a[MT][4], b[NT][2];
+#pragma unroll
+        for (int mt = 0; mt < MT; mt++) {
+            const bf16 *p = A + (mt * 16 + g) * lda + ks * 16 + 2 * t;
+            a[mt][0] = ld32(p);
+            a[mt][1] = ld32(p + 8 * lda);
+            a[mt][2] = ld32(p + 8);
+            a[mt][3] = ld32(p + 8 * lda + 8);
+        }
+#pragma unroll
+        for (int nt = 0; nt < NT; nt++) {
+            const bf16 *q = W + (nt * 8 + g) * ldw + ks * 16 + 2 * t;
+            b[nt][0] = ld32(q);
+            b[nt][1] = ld32(q + 8);
+        }
+#pragma unroll
+        for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+            for (int nt = 0; nt < NT; nt++) mma_bf16(acc[mt][nt], a[mt], b[nt]);
+    }
+}
+
+template <int MT, int NT>
+__device__ __forceinline__ void zero(float (&acc)[MT][NT][4])
+{
+#pragma unroll
+    for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+        for (int nt = 0; nt < NT; nt++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[mt][nt][e] = 0.f;
+}
+
+template <typename T>
+__device__ __forceinline__ float ldf(const T *p, int i)
+{
+    return (float)p[i];
+}
+
+// Per-lane staging of a warp's 32 cells: lane t holds the inputs of cell
+// base + t; shuffles broadcast them inside the per-cell loops.
+struct CellFeat {
+    float b, d, p, v;
+};
+
+template <typename T>
+__device__ __forceinline__ CellFeat load_features(const GnnGraph &g, const GnnInput<T> &in, const GnnScales &sc, int i)
+{
+    CellFeat f{0.f, 0.f, 0.f, 0.f};
+    if (i < g.n) {
+        const double rb = sc.sb > 0 ? 1.0 / sc.sb : 0.0, rd = sc.sd > 0 ? 1.0 / sc.sd : 0.0;
+        const double rx = sc.sx > 0 ? 1.0 / sc.sx : 0.0;
+        f.b = (float)(((double)in.b[i] - sc.shift) * rb);
+        f.d = (float)((double)in.diag[i] * rd);
+        f.p = in.prev ? (float)((double)in.prev[i] * rx) : 0.f;
+        f.v = g.vhat[i];
+    }
+    return f;
+}
+
+// Per-warp column sums of per-lane values `v` (lane = channel) are exact
+// already; this helper sums one value per (warp, channel) across the block
+// in warp order.  red: [4][32] shared.
+__device__ __forceinline__ float block_channel_sum(float v, float (*red)[GNN_H], int warp, int lane)
+{
+    __syncthreads();
+    red[warp][lane] = v;
+    __syncthreads();
+    float s = 0.f;
+    if (warp == 0) s = ((red[0][lane] + red[1][lane]) + red[2][lane]) + red[3][lane];
+    return s;
+}
+
+// Sum over the 8 row-groups (g) of an accumulator column pair held by lanes
+// with the same t; valid in lanes with g == 0.
+__device__ __forceinline__ float sum_over_g(float v)
+{
+    v += __shfl_xor_sync(FULL, v, 4);
+    v += __shfl_xor_sync(FULL, v, 8);
+    v += __shfl_xor_sync(FULL, v, 16);
+    return v;
+}
+
+// ------------------------------------------------------------------ kernels
+
+template <typename T>
+__global__ void __launch_bounds__(MCB_THREADS) k_gnn_scales(int n, GnnInput<T> in, double *partials,
+                                                            unsigned int *counter, GnnScales *out)
+{
+    __shared__ double sh[2][MCB_THREADS];
+    const double shift = in.shift ? *in.shift : 0.0;
+    double acc[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double b = (double)in.b[i] - shift;
+        acc[0] += b * b;
+        acc[1] += (double)in.diag[i];
+    }
+    if (publish_partials<2>(acc, partials, counter, sh)) {
+        double tot[2];
+        reduce_partials<2>(tot, partials, counter, sh);
+        if (threadIdx.x == 0) {
+            GnnScales s;
+            s.shift = shift;
+            s.sb = sqrt(tot[0] / n);
+            s.sd = tot[1] / n;
+            s.sx = (s.sd > 0 && isfinite(s.sb)) ? s.sb / s.sd : 0.0;
+            if (!(s.sb > 0) || !(s.sx > 0) || !isfinite(s.sx)) s.sb = s.sd = s.sx = 0.0;
+            *out = s;
+        }
+    }
+}
+
+// h0 = relu(We x + ce); lane = channel.
+template <typename T>
+__global__ void __launch_bounds__(GNN_TILE) k_gnn_encode(GnnGraph g, GnnInput<T> in, const float *__restrict__ p,
+                                                         const GnnScales *__restrict__ scp, bf16 *__restrict__ hout)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int base = blockIdx.x * GNN_TILE + warp * 32;
+    const GnnScales sc = *scp;
+    const CellFeat mine = load_features(g, in, sc, base + lane);
+    const float w0 = p[GP_WE + lane * GNN_IN], w1 = p[GP_WE + lane * GNN_IN + 1];
+    const float w2 = p[GP_WE + lane * GNN_IN + 2], w3 = p[GP_WE + lane * GNN_IN + 3], c = p[GP_CE + lane];
+    for (int r = 0; r < 32; r++) {
+        const float xb = __shfl_sync(FULL, mine.b, r), xd = __shfl_sync(FULL, mine.d, r);
+        const float xp = __shfl_sync(FULL, mine.p, r), xv = __shfl_sync(FULL, mine.v, r);
+        const int i = base + r;
+        if (i < g.n) hout[(size_t)i * GNN_H + lane] = __float2bfloat16(fmaxf(w0 * xb + w1 * xd + w2 * xp + w3 * xv + c, 0.f));
+    }
+}
+
+// Gather of one cell's message for channel `lane` (h is [n][H] BF16).
+struct SlotCache {
+    int col[6];
+    uint32_t edge[6];
+};
+
+__device__ __forceinline__ SlotCache load_slots(const GnnGraph &g, int i)
+{
+    SlotCache s;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        s.col[k] = i < g.n ? g.col[(size_t)k * g.n + i] : -1;
+        s.edge[k] = i < g.n ? *reinterpret_cast<const uint32_t *>(g.edge + (size_t)k * g.n + i) : 0u;
+    }
+    return s;
+}
+
+__device__ __forceinline__ float2 edge_of(uint32_t bits)
+{
+    bf162 e;
+    *reinterpret_cast<uint32_t *>(&e) = bits;
+    return __bfloat1622float2(e);
+}
+
+// One message-passing layer; TRAIN also stores relu(W1 u + c1).
+template <bool TRAIN>
+__global__ void __launch_bounds__(GNN_TILE) k_gnn_layer(GnnGraph g, const float *__restrict__ pl,
+                                                        const bf16 *__restrict__ pkl, const bf16 *__restrict__ hin,
+                                                        bf16 *__restrict__ hout, bf16 *__restrict__ asave)
+{
+    __shared__ __align__(16) bf16 sU[GNN_TILE * LDU];
+    __shared__ __align__(16) bf16 sW1[GNN_H * LDU];
+    __shared__ __align__(16) bf16 sW2[GNN_H * LDH];
+    __shared__ __align__(16) bf16 sA[GNN_TILE * LDH];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < GNN_H * 2 * GNN_H; e += GNN_TILE) sW1[(e >> 6) * LDU + (e & 63)] = pkl[GKL_W1 + e];
+    for (int e = tid; e < GNN_H * GNN_H; e += GNN_TILE) sW2[(e >> 5) * LDH + (e & 31)] = pkl[GKL_W2 + e];
+    const int n = g.n, base = blockIdx.x * GNN_TILE;
+    {
+        const float wg0 = pl[GPL_WG + 2 * lane], wg1 = pl[GPL_WG + 2 * lane + 1], cg = pl[GPL_CG + lane];
+        const SlotCache mine = load_slots(g, base + warp * 32 + lane);
+        for (int r = 0; r < 32; r++) {
+            const int row = warp * 32 + r, i = base + row;
+            bf16 hi = __float2bfloat16(0.f);
+            float m = 0.f;
+            if (i < n) {
+                hi = hin[(size_t)i * GNN_H + lane];
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    const int j = __shfl_sync(FULL, mine.col[k], r);
+                    const float2 e = edge_of(__shfl_sync(FULL, mine.edge[k], r));
+                    if (j != i) m += (wg0 * e.x + wg1 * e.y + cg) * __bfloat162float(hin[(size_t)j * GNN_H + lane]);
+                }
+            }
+            sU[row * LDU + lane] = hi;
+            sU[row * LDU + GNN_H + lane] = __float2bfloat16(m);
+        }
+    }
+    __syncthreads();
+    const int gq = lane >> 2, tq = lane & 3;
+    float acc[2][4][4];
+    zero(acc);
+    warp_gemm<2, 4, 4>(acc, sU + warp * 32 * LDU, LDU, sW1, LDU, lane);
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int hf = 0; hf < 2; hf++) {
+                const int row = warp * 32 + mt * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq;
+                const float z0 = acc[mt][nt][2 * hf] + pl[GPL_C1 + col];
+                const float z1 = acc[mt][nt][2 * hf + 1] + pl[GPL_C1 + col + 1];
+                const bf162 v = __floats2bfloat162_rn(fmaxf(z0, 0.f), fmaxf(z1, 0.f));
+                *reinterpret_cast<bf162 *>(sA + row * LDH + col) = v;
+                if (TRAIN && base + row < n) *reinterpret_cast<bf162 *>(asave + (size_t)(base + row) * GNN_H + col) = v;
+            }
+    __syncwarp();
+    zero(acc);
+    warp_gemm<2, 4, 2>(acc, sA + warp * 32 * LDH, LDH, sW2, LDH, lane);
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int hf = 0; hf < 2; hf++) {
+                const int row = warp * 32 + mt * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq, i = base + row;
+                if (i >= n) continue;
+                const float2 hv = __bfloat1622float2(*reinterpret_cast<const bf162 *>(sU + row * LDU + col));
+                const float o0 = hv.x + (acc[mt][nt][2 * hf] + pl[GPL_C2 + col]);
+                const float o1 = hv.y + (acc[mt][nt][2 * hf + 1] + pl[GPL_C2 + col + 1]);
+                *reinterpret_cast<bf162 *>(hout + (size_t)i * GNN_H + col) = __floats2bfloat162_rn(o0, o1);
+            }
+}
+
+// Load a [128][32] BF16 tile of rows base.. into shared memory (row stride LDH).
+__device__ __forceinline__ void load_tile(bf16 *s, const bf16 *__restrict__ h, int base, int n)
+{
+    for (int e = threadIdx.x; e < GNN_TILE * 4; e += GNN_TILE) {
+        const int row = e >> 2, part = e & 3, i = base + row;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (i < n) v = *reinterpret_cast<const uint4 *>(h + (size_t)i * GNN_H + part * 8);
+        *reinterpret_cast<uint4 *>(s + row * LDH + part * 8) = v;
+    }
+}
+
+// y = wo . relu(Wd h + cd) + co; x0 = s_x y.
+template <bool TRAIN>
+__global__ void __launch_bounds__(GNN_TILE) k_gnn_decode(GnnGraph g, const float *__restrict__ pd,
+                                                         const bf16 *__restrict__ pkd, const bf16 *__restrict__ hin,
+                                                         const GnnScales *__restrict__ scp, float *__restrict__ y,
+                                                         double *__restrict__ x0, bf16 *__restrict__ qsave)
+{
+    __shared__ __align__(16) bf16 sH[GNN_TILE * LDH];
+    __shared__ __align__(16) bf16 sW[GNN_H * LDH];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = g.n, base = blockIdx.x * GNN_TILE;
+    for (int e = tid; e < GNN_H * GNN_H; e += GNN_TILE) sW[(e >> 5) * LDH + (e & 31)] = pkd[e];
+    load_tile(sH, hin, base, n);
+    __syncthreads();
+    const int gq = lane >> 2, tq = lane & 3;
+    float acc[2][4][4];
+    zero(acc);
+    warp_gemm<2, 4, 2>(acc, sH + warp * 32 * LDH, LDH, sW, LDH, lane);
+    const double sx = scp->sx;
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int hf = 0; hf < 2; hf++) {
+            const int row = warp * 32 + mt * 16 + gq + 8 * hf, i = base + row;
+            float s = 0.f;
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++) {
+                const int col = nt * 8 + 2 * tq;
+                const float q0 = fmaxf(acc[mt][nt][2 * hf] + pd[GPD_CD + col], 0.f);
+                const float q1 = fmaxf(acc[mt][nt][2 * hf + 1] + pd[GPD_CD + col + 1], 0.f);
+                const bf162 qv = __floats2bfloat162_rn(q0, q1);
+                const float2 qr = __bfloat1622float2(qv);
+                s += pd[GPD_WO + col] * qr.x + pd[GPD_WO + col + 1] * qr.y;
+                if (TRAIN && i < n) *reinterpret_cast<bf162 *>(qsave + (size_t)i * GNN_H + col) = qv;
+            }
+            s += __shfl_xor_sync(FULL, s, 1);
+            s += __shfl_xor_sync(FULL, s, 2);
+            if (tq == 0 && i < n) {
+                const float yi = s + pd[GPD_CO];
+                y[i] = yi;
+                if (x0) x0[i] = sx * (double)yi;
+            }
+        }
+}
+
+// ---------------------------------------------------------------- training
+
+// Mean of (y - t / s_x) over the cells.
+__global__ void __launch_bounds__(MCB_THREADS) k_gnn_loss_mean(int n, const float *__restrict__ y,
+                                                               const float *__restrict__ t,
+                                                               const GnnScales *__restrict__ scp, double *partials,
+                                                               unsigned int *counter, double *loss)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    const double sx = scp->sx, rx = sx > 0 ? 1.0 / sx : 0.0;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        acc[0] += (double)y[i] - (double)t[i] * rx;
+    if (publish_partials<1>(acc, partials, counter, sh)) {
+        double tot[1];
+        reduce_partials<1>(tot, partials, counter, sh);
+        if (threadIdx.x == 0) loss[0] = tot[0] / n;
+    }
+}
+
+// dy = 2 weight (y - t / s_x - mean) / n; loss = mean of the squares.
+__global__ void __launch_bounds__(MCB_THREADS) k_gnn_loss_grad(int n, const float *__restrict__ y,
+                                                               const float *__restrict__ t,
+                                                               const GnnScales *__restrict__ scp, float weight,
+                                                               float *__restrict__ dy, double *partials,
+                                                               unsigned int *counter, double *loss)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    const double sx = scp->sx, rx = sx > 0 ? 1.0 / sx : 0.0, mu = loss[0];
+    const double k = 2.0 * (double)weight / n;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double d = (double)y[i] - (double)t[i] * rx - mu;
+        dy[i] = (float)(k * d);
+        acc[0] += d * d;
+    }
+    if (publish_partials<1>(acc, partials, counter, sh)) {
+        double tot[1];
+        reduce_partials<1>(tot, partials, counter, sh);
+        if (threadIdx.x == 0) loss[1] = tot[0] / n;
+    }
+}
+
+// Decoder backward: dh = Wd^T dq with dq = dy wo (.) [q > 0]; partial
+// gradients of Wd, cd, wo, co.
+__global__ void __launch_bounds__(GNN_TILE) k_gnn_decode_bwd(GnnGraph g, const float *__restrict__ pd,
+                                                             const bf16 *__restrict__ pkd,
+                                                             const bf16 *__restrict__ hin,
+                                                             const bf16 *__restrict__ q, const float *__restrict__ dy,
+                                                             float *__restrict__ dh, float *__restrict__ gpart)
+{
+    __shared__ __align__(16) bf16 sDQ[GNN_TILE * LDH];
+    __shared__ __align__(16) bf16 sDQT[GNN_H * LDT];
+    __shared__ __align__(16) bf16 sHT[GNN_H * LDT];
+    __shared__ __align__(16) bf16 sWT[GNN_H * LDH];
+    __shared__ float red[4][GNN_H];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = g.n, base = blockIdx.x * GNN_TILE;
+    for (int e = tid; e < GNN_H * GNN_H; e += GNN_TILE) sWT[(e & 31) * LDH + (e >> 5)] = pkd[e];  // [in][out]
+    const float wo = pd[GPD_WO + lane];
+    float s_dcd = 0.f, s_dwo = 0.f, s_dco = 0.f;
+    for (int r = 0; r < 32; r++) {
+        const int row = warp * 32 + r, i = base + row;
+        float dq = 0.f;
+        bf16 hv = __float2bfloat16(0.f);
+        if (i < n) {
+            const float qi = __bfloat162float(q[(size_t)i * GNN_H + lane]), d = dy[i];
+            dq = qi > 0.f ? d * wo : 0.f;
+            s_dwo += d * qi;
+            s_dco += d;
+            hv = hin[(size_t)i * GNN_H + lane];
+        }
+        s_dcd += dq;
+        const bf16 dqb = __float2bfloat16(dq);
+        sDQ[row * LDH + lane] = dqb;
+        sDQT[lane * LDT + row] = dqb;
+        sHT[lane * LDT + row] = hv;
+    }
+    __syncthreads();
+    const int gq = lane >> 2, tq = lane & 3;
+    {
+        float acc[2][4][4];
+        zero(acc);
+        warp_gemm<2, 4, 2>(acc, sDQ + warp * 32 * LDH, LDH, sWT, LDH, lane);
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+                for (int hf = 0; hf < 2; hf++) {
+                    const int row = warp * 32 + mt * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq, i = base + row;
+                    if (i < n)
+                        *reinterpret_cast<float2 *>(dh + (size_t)i * GNN_H + col) =
+                            make_float2(acc[mt][nt][2 * hf], acc[mt][nt][2 * hf + 1]);
+                }
+    }
+    float *gp = gpart + (size_t)blockIdx.x * GNN_NPARAM + GP_DEC;
+    {
+        // dWd[o][in] = sum_cells dq[cell][o] h[cell][in]: warp -> (m-tile warp / 2, n-tiles 2 (warp % 2) ..)
+        float acc[1][2][4];
+        zero(acc);
+        const int mt0 = warp >> 1, nt0 = (warp & 1) * 2;
+        warp_gemm<1, 2, 8>(acc, sDQT + mt0 * 16 * LDT, LDT, sHT + nt0 * 8 * LDT, LDT, lane);
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+            for (int hf = 0; hf < 2; hf++) {
+                const int o = mt0 * 16 + gq + 8 * hf, in = (nt0 + nt) * 8 + 2 * tq;
+                gp[GPD_WD + o * GNN_H + in] = acc[0][nt][2 * hf];
+                gp[GPD_WD + o * GNN_H + in + 1] = acc[0][nt][2 * hf + 1];
+            }
+    }
+    const float t_dcd = block_channel_sum(s_dcd, red, warp, lane);
+    if (warp == 0) gp[GPD_CD + lane] = t_dcd;
+    const float t_dwo = block_channel_sum(s_dwo, red, warp, lane);
+    if (warp == 0) gp[GPD_WO + lane] = t_dwo;
+    const float t_dco = block_channel_sum(lane == 0 ? s_dco : 0.f, red, warp, lane);
+    if (warp == 0 && lane == 0) gp[GPD_CO] = t_dco;
+}
+
+// Layer backward, dense part.  In: dho = dL/dh' (FP32), the layer input h and
+// the saved activation a.  Out: dhs = dL/dh through the residual and the
+// self half of u; dm = dL/dm; partial gradients of W1, c1, W2, c2.
+constexpr size_t BWD_SMEM = sizeof(bf16) * ((size_t)2 * GNN_H * LDT      // sUT
+                                            + (size_t)GNN_TILE * LDH     // sDH
+                                            + (size_t)GNN_H * LDT        // sDHT
+                                            + (size_t)GNN_H * LDT        // sAT
+                                            + (size_t)GNN_TILE * LDH     // sDZ
+                                            + (size_t)GNN_H * LDT        // sDZT
+                                            + (size_t)GNN_H * LDH        // sW2T
+                                            + (size_t)2 * GNN_H * LDH)   // sW1T
+                            + sizeof(float) * 4 * GNN_H;
+
+__global__ void __launch_bounds__(GNN_TILE) k_gnn_layer_bwd_mlp(GnnGraph g, const float *__restrict__ pl,
+                                                                const bf16 *__restrict__ pkl,
+                                                                const bf16 *__restrict__ hin,
+                                                                const bf16 *__restrict__ a,
+                                                                const float *__restrict__ dho,
+                                                                float *__restrict__ dhs, float *__restrict__ dm,
+                                                                float *__restrict__ gpart)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    bf16 *sUT = reinterpret_cast<bf16 *>(smem);
+    bf16 *sDH = sUT + 2 * GNN_H * LDT;
+    bf16 *sDHT = sDH + GNN_TILE * LDH;
+    bf16 *sAT = sDHT + GNN_H * LDT;
+    bf16 *sDZ = sAT + GNN_H * LDT;
+    bf16 *sDZT = sDZ + GNN_TILE * LDH;
+    bf16 *sW2T = sDZT + GNN_H * LDT;
+    bf16 *sW1T = sW2T + GNN_H * LDH;
+    float(*red)[GNN_H] = reinterpret_cast<float(*)[GNN_H]>(sW1T + 2 * GNN_H * LDH);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = g.n, base = blockIdx.x * GNN_TILE;
+    for (int e = tid; e < GNN_H * GNN_H; e += GNN_TILE) sW2T[(e & 31) * LDH + (e >> 5)] = pkl[GKL_W2 + e];
+    for (int e = tid; e < GNN_H * 2 * GNN_H; e += GNN_TILE) sW1T[(e & 63) * LDH + (e >> 6)] = pkl[GKL_W1 + e];
+    float s_dc2 = 0.f;
+    {
+        const float wg0 = pl[GPL_WG + 2 * lane], wg1 = pl[GPL_WG + 2 * lane + 1], cg = pl[GPL_CG + lane];
+        const SlotCache mine = load_slots(g, base + warp * 32 + lane);
+        for (int r = 0; r < 32; r++) {
+            const int row = warp * 32 + r, i = base + row;
+            bf16 hi = __float2bfloat16(0.f), ai = hi;
+            float m = 0.f, d = 0.f;
+            if (i < n) {
+                hi = hin[(size_t)i * GNN_H + lane];
+                ai = a[(size_t)i * GNN_H + lane];
+                d = dho[(size_t)i * GNN_H + lane];
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    const int j = __shfl_sync(FULL, mine.col[k], r);
+                    const float2 e = edge_of(__shfl_sync(FULL, mine.edge[k], r));
+                    if (j != i) m += (wg0 * e.x + wg1 * e.y + cg) * __bfloat162float(hin[(size_t)j * GNN_H + lane]);
+                }
+            }
+            s_dc2 += d;
+            sUT[lane * LDT + row] = hi;
+            sUT[(GNN_H + lane) * LDT + row] = __float2bfloat16(m);
+            sAT[lane * LDT + row] = ai;
+            const bf16 db = __float2bfloat16(d);
+            sDH[row * LDH + lane] = db;
+            sDHT[lane * LDT + row] = db;
+        }
+    }
+    __syncthreads();
+    const int gq = lane >> 2, tq = lane & 3;
+    float dc1[4][2];
+    {
+        float acc[2][4][4];
+        zero(acc);
+        warp_gemm<2, 4, 2>(acc, sDH + warp * 32 * LDH, LDH, sW2T, LDH, lane);
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) dc1[nt][0] = dc1[nt][1] = 0.f;
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+                for (int hf = 0; hf < 2; hf++) {
+                    const int row = warp * 32 + mt * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq;
+                    const float a0 = __bfloat162float(sAT[col * LDT + row]);
+                    const float a1 = __bfloat162float(sAT[(col + 1) * LDT + row]);
+                    const float z0 = a0 > 0.f ? acc[mt][nt][2 * hf] : 0.f;
+                    const float z1 = a1 > 0.f ? acc[mt][nt][2 * hf + 1] : 0.f;
+                    dc1[nt][0] += z0;
+                    dc1[nt][1] += z1;
+                    const bf162 zb = __floats2bfloat162_rn(z0, z1);
+                    *reinterpret_cast<bf162 *>(sDZ + row * LDH + col) = zb;
+                    sDZT[col * LDT + row] = zb.x;
+                    sDZT[(col + 1) * LDT + row] = zb.y;
+                }
+    }
+    __syncthreads();
+    {
+        float acc[2][8][4];
+        zero(acc);
+        warp_gemm<2, 8, 2>(acc, sDZ + warp * 32 * LDH, LDH, sW1T, LDH, lane);
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+            for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+                for (int hf = 0; hf < 2; hf++) {
+                    const int row = warp * 32 + mt * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq, i = base + row;
+                    if (i >= n) continue;
+                    if (nt < 4) {
+                        const float2 d = *reinterpret_cast<const float2 *>(dho + (size_t)i * GNN_H + col);
+                        *reinterpret_cast<float2 *>(dhs + (size_t)i * GNN_H + col) =
+                            make_float2(d.x + acc[mt][nt][2 * hf], d.y + acc[mt][nt][2 * hf + 1]);
+                    } else {
+                        *reinterpret_cast<float2 *>(dm + (size_t)i * GNN_H + col - GNN_H) =
+                            make_float2(acc[mt][nt][2 * hf], acc[mt][nt][2 * hf + 1]);
+                    }
+                }
+    }
+    float *gp = gpart + (size_t)blockIdx.x * GNN_NPARAM;
+    {
+        // dW2[o][in] = sum_cells dh'[cell][o] a[cell][in]
+        float acc[1][2][4];
+        zero(acc);
+        const int mt0 = warp >> 1, nt0 = (warp & 1) * 2;
+        warp_gemm<1, 2, 8>(acc, sDHT + mt0 * 16 * LDT, LDT, sAT + nt0 * 8 * LDT, LDT, lane);
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+            for (int hf = 0; hf < 2; hf++) {
+                const int o = mt0 * 16 + gq + 8 * hf, in = (nt0 + nt) * 8 + 2 * tq;
+                gp[GPL_W2 + o * GNN_H + in] = acc[0][nt][2 * hf];
+                gp[GPL_W2 + o * GNN_H + in + 1] = acc[0][nt][2 * hf + 1];
+            }
+    }
+    {
+        // dW1[o][k] = sum_cells dz[cell][o] u[cell][k]
+        float acc[1][4][4];
+        zero(acc);
+        const int mt0 = warp >> 1, nt0 = (warp & 1) * 4;
+        warp_gemm<1, 4, 8>(acc, sDZT + mt0 * 16 * LDT, LDT, sUT + nt0 * 8 * LDT, LDT, lane);
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int hf = 0; hf < 2; hf++) {
+                const int o = mt0 * 16 + gq + 8 * hf, k = (nt0 + nt) * 8 + 2 * tq;
+                gp[GPL_W1 + o * 2 * GNN_H + k] = acc[0][nt][2 * hf];
+                gp[GPL_W1 + o * 2 * GNN_H + k + 1] = acc[0][nt][2 * hf + 1];
+            }
+    }
+    // dc1: per-thread column sums -> over g lanes -> over warps
+    __syncthreads();
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const float v = sum_over_g(dc1[nt][e]);
+            if (gq == 0) red[warp][nt * 8 + 2 * tq + e] = v;
+        }
+    __syncthreads();
+    if (warp == 0) gp[GPL_C1 + lane] = ((red[0][lane] + red[1][lane]) + red[2][lane]) + red[3][lane];
+    const float t_dc2 = block_channel_sum(s_dc2, red, warp, lane);
+    if (warp == 0) gp[GPL_C2 + lane] = t_dc2;
+}
+
+// Layer backward, message part: dh_in_j = dhs_j + sum over j's internal
+// slots of g (.) dm_other; partial gradients of Wg, cg.
+__global__ void __launch_bounds__(GNN_TILE) k_gnn_layer_bwd_msg(GnnGraph g, const float *__restrict__ pl,
+                                                                const bf16 *__restrict__ hin,
+                                                                const float *__restrict__ dhs,
+                                                                const float *__restrict__ dm,
+                                                                float *__restrict__ dhi, float *__restrict__ gpart)
+{
+    __shared__ float red[4][GNN_H];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = g.n, base = blockIdx.x * GNN_TILE;
+    const float wg0 = pl[GPL_WG + 2 * lane], wg1 = pl[GPL_WG + 2 * lane + 1], cg = pl[GPL_CG + lane];
+    const SlotCache mine = load_slots(g, base + warp * 32 + lane);
+    float s0 = 0.f, s1 = 0.f, sc = 0.f;
+    for (int r = 0; r < 32; r++) {
+        const int i = base + warp * 32 + r;
+        if (i >= n) break;
+        const float dmi = dm[(size_t)i * GNN_H + lane];
+        float acc = dhs[(size_t)i * GNN_H + lane];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const int j = __shfl_sync(FULL, mine.col[k], r);
+            const float2 e = edge_of(__shfl_sync(FULL, mine.edge[k], r));
+            if (j != i) {
+                acc += (wg0 * e.x + wg1 * e.y + cg) * dm[(size_t)j * GNN_H + lane];
+                const float t = dmi * __bfloat162float(hin[(size_t)j * GNN_H + lane]);
+                s0 += t * e.x;
+                s1 += t * e.y;
+                sc += t;
+            }
+        }
+        dhi[(size_t)i * GNN_H + lane] = acc;
+    }
+    float *gp = gpart + (size_t)blockIdx.x * GNN_NPARAM;
+    const float t0 = block_channel_sum(s0, red, warp, lane);
+    if (warp == 0) gp[GPL_WG + 2 * lane] = t0;
+    const float t1 = block_channel_sum(s1, red, warp, lane);
+    if (warp == 0) gp[GPL_WG + 2 * lane + 1] = t1;
+    const float tc = block_channel_sum(sc, red, warp, lane);
+    if (warp == 0) gp[GPL_CG + lane] = tc;
+}
+
+// Encoder backward: partial gradients of We, ce.
+__global__ void __launch_bounds__(GNN_TILE) k_gnn_encode_bwd(GnnGraph g, GnnInput<float> in,
+                                                             const GnnScales *__restrict__ scp,
+                                                             const bf16 *__restrict__ h0,
+                                                             const float *__restrict__ dh0,
+                                                             float *__restrict__ gpart)
+{
+    __shared__ float red[4][GNN_H];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int base = blockIdx.x * GNN_TILE + warp * 32;
+    const GnnScales sc = *scp;
+    const CellFeat mine = load_features(g, in, sc, base + lane);
+    float s[GNN_IN + 1] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int r = 0; r < 32; r++) {
+        const float xb = __shfl_sync(FULL, mine.b, r), xd = __shfl_sync(FULL, mine.d, r);
+        const float xp = __shfl_sync(FULL, mine.p, r), xv = __shfl_sync(FULL, mine.v, r);
+        const int i = base + r;
+        if (i >= g.n) break;
+        const float h = __bfloat162float(h0[(size_t)i * GNN_H + lane]);
+        const float dz = h > 0.f ? dh0[(size_t)i * GNN_H + lane] : 0.f;
+        s[0] += dz * xb;
+        s[1] += dz * xd;
+        s[2] += dz * xp;
+        s[3] += dz * xv;
+        s[4] += dz;
+    }
+    float *gp = gpart + (size_t)blockIdx.x * GNN_NPARAM;
+    for (int f = 0; f < GNN_IN; f++) {
+        const float t = block_channel_sum(s[f], red, warp, lane);
+        if (warp == 0) gp[GP_WE + lane * GNN_IN + f] = t;
+    }
+    const float t = block_channel_sum(s[4], red, warp, lane);
+    if (warp == 0) gp[GP_CE + lane] = t;
+}
+
+// grad[p] += sum over blocks of gpart[block][p], in block order.
+__global__ void k_gnn_reduce(int nblocks, const float *__restrict__ gpart, float *__restrict__ grad)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < GNN_NPARAM; p += gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int b = 0; b < nblocks; b++) s += gpart[(size_t)b * GNN_NPARAM + p];
+        grad[p] += s;
+    }
+}
+
+__global__ void k_gnn_adam(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
+                           float *__restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < GNN_NPARAM; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+__global__ void k_gnn_pack(const float *__restrict__ p, bf16 *__restrict__ pk)
+{
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < GNN_NPACK; e += gridDim.x * blockDim.x) {
+        float v;
+        if (e < GK_WD) {
+            const int l = e / GKL_SIZE, r = e % GKL_SIZE;
+            v = r < GKL_W2 ? p[GP_LAYER0 + l * GPL_SIZE + GPL_W1 + r] : p[GP_LAYER0 + l * GPL_SIZE + GPL_W2 + r - GKL_W2];
+        } else {
+            v = p[GP_DEC + GPD_WD + e - GK_WD];
+        }
+        pk[e] = __float2bfloat16(v);
+    }
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+} // namespace
+
+// ------------------------------------------------------------------ host API
+
+size_t gnn_work_bytes(int n, bool train)
+{
+    GnnWork w;
+    gnn_work_carve(w, nullptr, n, train);
+    return (size_t)(reinterpret_cast<uintptr_t>(w.loss) + align256(2 * sizeof(double)));
+}
+
+void gnn_work_carve(GnnWork &w, char *base, int n, bool train)
+{
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char *p = base + off;
+        off += align256(bytes);
+        return p;
+    };
+    w.n = n;
+    w.nblocks = gnn_blocks(n);
+    w.train = train;
+    const size_t hb = (size_t)n * GNN_H * sizeof(bf16), fb = (size_t)n * GNN_H * sizeof(float);
+    const int nh = train ? GNN_L + 1 : 2;
+    for (int l = 0; l <= GNN_L; l++) w.h[l] = l < nh ? reinterpret_cast<bf16 *>(take(hb)) : nullptr;
+    for (int l = 0; l < GNN_L; l++) w.a[l] = train ? reinterpret_cast<bf16 *>(take(hb)) : nullptr;
+    w.q = train ? reinterpret_cast<bf16 *>(take(hb)) : nullptr;
+    w.y = reinterpret_cast<float *>(take((size_t)n * sizeof(float)));
+    w.dh[0] = train ? reinterpret_cast<float *>(take(fb)) : nullptr;
+    w.dh[1] = train ? reinterpret_cast<float *>(take(fb)) : nullptr;
+    w.dm = train ? reinterpret_cast<float *>(take(fb)) : nullptr;
+    w.dy = train ? reinterpret_cast<float *>(take((size_t)n * sizeof(float))) : nullptr;
+    w.gpart = train ? reinterpret_cast<float *>(take((size_t)w.nblocks * GNN_NPARAM * sizeof(float))) : nullptr;
+    w.partials = reinterpret_cast<double *>(take((size_t)reduce_grid(n) * 2 * sizeof(double)));
+    w.counter = reinterpret_cast<unsigned int *>(take(256));
+    w.scales = reinterpret_cast<GnnScales *>(take(sizeof(GnnScales)));
+    w.loss = reinterpret_cast<double *>(base + off);
+}
+
+void gnn_init_params(float *p, uint64_t seed)
+{
+    uint64_t state = seed;
+    auto next = [&]() {  // splitmix64
+        uint64_t z = (state += 0x9e3779b97f4a7c15ull);
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);  // [0, 1)
+    };
+    auto fill = [&](int off, int count, int fan_in, double gain) {
+        const double a = gain * std::sqrt(6.0 / fan_in);
+        for (int i = 0; i < count; i++) p[off + i] = (float)((2.0 * next() - 1.0) * a);
+    };
+    for (int i = 0; i < GNN_NPARAM; i++) p[i] = 0.f;
+    fill(GP_WE, GNN_H * GNN_IN, GNN_IN, 1.0);
+    for (int l = 0; l < GNN_L; l++) {
+        const int b = GP_LAYER0 + l * GPL_SIZE;
+        fill(b + GPL_WG, GNN_H * 2, 2, 0.5);
+        for (int c = 0; c < GNN_H; c++) p[b + GPL_CG + c] = 1.0f / 6.0f;
+        fill(b + GPL_W1, GNN_H * 2 * GNN_H, 2 * GNN_H, 1.0);
+        fill(b + GPL_W2, GNN_H * GNN_H, GNN_H, 0.2);
+    }
+    fill(GP_DEC + GPD_WD, GNN_H * GNN_H, GNN_H, 1.0);
+    fill(GP_DEC + GPD_WO, GNN_H, GNN_H, 0.5);
+}
+
+void gnn_pack(cudaStream_t s, const float *p, bf16 *pk) { k_gnn_pack<<<32, 256, 0, s>>>(p, pk); }
+
+template <typename T>
+static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &in, const float *p, const bf16 *pk,
+                         GnnWork &w, double *x0)
+{
+    const int nb = gnn_blocks(g.n);
+    k_gnn_scales<T><<<reduce_grid(g.n), MCB_THREADS, 0, s>>>(g.n, in, w.partials, w.counter, w.scales);
+    k_gnn_encode<T><<<nb, GNN_TILE, 0, s>>>(g, in, p, w.scales, w.h[0]);
+    for (int l = 0; l < GNN_L; l++) {
+        const float *pl = p + GP_LAYER0 + l * GPL_SIZE;
+        const bf16 *pkl = pk + GK_LAYER0 + l * GKL_SIZE;
+        if (w.train)
+            k_gnn_layer<true><<<nb, GNN_TILE, 0, s>>>(g, pl, pkl, w.h[l], w.h[l + 1], w.a[l]);
+        else
+            k_gnn_layer<false><<<nb, GNN_TILE, 0, s>>>(g, pl, pkl, w.h[l & 1], w.h[(l + 1) & 1], nullptr);
+    }
+    const bf16 *hl = w.train ? w.h[GNN_L] : w.h[GNN_L & 1];
+    if (w.train)
+        k_gnn_decode<true><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, w.q);
+    else
+        k_gnn_decode<false><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, nullptr);
+}
+
+template <typename T>
+void gnn_forward(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &in, const float *p, const bf16 *pk, GnnWork &w,
+                 double *x0)
+{
+    forward_impl<T>(s, g, in, p, pk, w, x0);
+}
+template void gnn_forward<double>(cudaStream_t, const GnnGraph &, const GnnInput<double> &, const float *,
+                                  const bf16 *, GnnWork &, double *);
+template void gnn_forward<float>(cudaStream_t, const GnnGraph &, const GnnInput<float> &, const float *, const bf16 *,
+                                 GnnWork &, double *);
+
+int gnn_forward_launches() { return 3 + GNN_L; }
+
+void gnn_loss_backward(cudaStream_t s, const GnnGraph &g, const GnnInput<float> &in, const float *target,
+                       const float *p, const bf16 *pk, GnnWork &w, float *grad, float weight)
+{
+    cudaFuncSetAttribute(k_gnn_layer_bwd_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BWD_SMEM);
+    const int nb = gnn_blocks(g.n), rg = reduce_grid(g.n);
+    forward_impl<float>(s, g, in, p, pk, w, nullptr);
+    k_gnn_loss_mean<<<rg, MCB_THREADS, 0, s>>>(g.n, w.y, target, w.scales, w.partials, w.counter, w.loss);
+    k_gnn_loss_grad<<<rg, MCB_THREADS, 0, s>>>(g.n, w.y, target, w.scales, weight, w.dy, w.partials, w.counter,
+                                               w.loss);
+    k_gnn_decode_bwd<<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, w.h[GNN_L], w.q, w.dy, w.dh[0], w.gpart);
+    int cur = 0;  // w.dh[cur] = dL/d(output of layer l)
+    for (int l = GNN_L - 1; l >= 0; l--) {
+        const float *pl = p + GP_LAYER0 + l * GPL_SIZE;
+        const bf16 *pkl = pk + GK_LAYER0 + l * GKL_SIZE;
+        float *gpl = w.gpart + GP_LAYER0 + l * GPL_SIZE;
+        k_gnn_layer_bwd_mlp<<<nb, GNN_TILE, BWD_SMEM, s>>>(g, pl, pkl, w.h[l], w.a[l], w.dh[cur], w.dh[cur ^ 1], w.dm,
+                                                           gpl);
+        k_gnn_layer_bwd_msg<<<nb, GNN_TILE, 0, s>>>(g, pl, w.h[l], w.dh[cur ^ 1], w.dm, w.dh[cur], gpl);
+    }
+    k_gnn_encode_bwd<<<nb, GNN_TILE, 0, s>>>(g, in, w.scales, w.h[0], w.dh[cur], w.gpart);
+    k_gnn_reduce<<<(GNN_NPARAM + 255) / 256, 256, 0, s>>>(nb, w.gpart, grad);
+}
+
+void gnn_adam(cudaStream_t s, float *p, const float *grad, float *m, float *v, float lr, float b1, float b2, float eps,
+              int t)
+{
+    const float c1 = 1.f - std::pow(b1, (float)t), c2 = 1.f - std::pow(b2, (float)t);
+    k_gnn_adam<<<(GNN_NPARAM + 255) / 256, 256, 0, s>>>(p, grad, m, v, lr, b1, b2, eps, c1, c2);
+}
+
+} // namespace mcb

@@ -204,7 +204,8 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2(Ell A, PcgVectors v, 
 // z comes from the first V-cycle (amg.cu), which also sets r . z.
 template <typename T>
 __global__ void __launch_bounds__(MCB_THREADS) k_pcg_init_amg(EllT<T> A, PcgVectorsT<T> v, double rtol,
-                                                              double abs_floor, int max_iters, int project)
+                                                              double abs_floor, int max_iters, int project,
+                                                              int use_x0)
 {
     using T2 = typename Pair<T>::type;
     __shared__ double sh[2][MCB_THREADS];
@@ -213,12 +214,20 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_init_amg(EllT<T> A, PcgVect
     double acc[2] = {0.0, 0.0};  // b.b, r.r
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const T bi = (T)((double)v.b[i] - mean);
-        v.x[i] = (T)0;
-        v.r[i] = bi;
+        T ri = bi;
+        if (use_x0) {
+            T ax = A.diag[i] * v.x[i];
+#pragma unroll
+            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * v.x[A.col[(size_t)k * N + i]];
+            ri = bi - ax;
+        } else {
+            v.x[i] = (T)0;
+        }
+        v.r[i] = ri;
         v.zp[0][i] = T2{(T)0, (T)0};
         v.zp[1][i] = T2{(T)0, (T)0};
         acc[0] += (double)bi * (double)bi;
-        acc[1] += (double)bi * (double)bi;
+        acc[1] += (double)ri * (double)ri;
     }
     if (publish_partials<2>(acc, v.partials, v.counter, sh)) {
         double tot[2];
@@ -288,37 +297,101 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2_amg(EllT<T> A, PcgVec
 __global__ void __launch_bounds__(MCB_THREADS) k_ir_init(Ell A, const double *__restrict__ b, double *__restrict__ x,
                                                          double *__restrict__ r, float *__restrict__ r32, PcgState *st,
                                                          double *partials, unsigned int *counter, double rtol,
-                                                         double abs_floor, int max_outer)
+                                                         double abs_floor, int max_outer, int use_x0)
 {
-    __shared__ double sh[1][MCB_THREADS];
+    __shared__ double sh[2][MCB_THREADS];
     const int N = A.N;
     const double mean = st->mean;
-    double acc[1] = {0.0};
+    double acc[2] = {0.0, 0.0};  // b'.b', r.r
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const double bi = b[i] - mean;
-        x[i] = 0.0;
-        r[i] = bi;
-        r32[i] = (float)bi;
+        double ri = bi;
+        if (use_x0) {
+            double ax = A.diag[i] * x[i];
+#pragma unroll
+            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * x[A.col[(size_t)k * N + i]];
+            ri = bi - ax;
+        } else {
+            x[i] = 0.0;
+        }
+        r[i] = ri;
+        r32[i] = (float)ri;
         acc[0] += bi * bi;
+        acc[1] += ri * ri;
     }
-    if (publish_partials<1>(acc, partials, counter, sh)) {
-        double tot[1];
-        reduce_partials<1>(tot, partials, counter, sh);
+    if (publish_partials<2>(acc, partials, counter, sh)) {
+        double tot[2];
+        reduce_partials<2>(tot, partials, counter, sh);
         if (threadIdx.x == 0) {
             st->bb = tot[0];
-            st->rr = tot[0];
+            st->rr = tot[1];
             const double t = fmax(rtol * sqrt(tot[0]), abs_floor);
             st->tol2 = t * t;
             st->iter = 0;
             st->max_iters = max_outer;
             st->status = KRYLOV_OK;
-            st->done = (tot[0] == 0.0 || tot[0] <= st->tol2) ? 1 : 0;
-            if (!finite(tot[0])) {
+            st->done = (tot[0] == 0.0 || tot[1] <= st->tol2) ? 1 : 0;
+            if (!finite(tot[0]) || !finite(tot[1])) {
                 st->done = 1;
                 st->status = KRYLOV_NONFINITE;
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(MCB_THREADS) k_guess_residuals(Ell A, const double *__restrict__ b,
+                                                                 const PcgState *__restrict__ st,
+                                                                 const double *__restrict__ xa,
+                                                                 const double *__restrict__ xb, GuessState *gs,
+                                                                 double *partials, unsigned int *counter)
+{
+    __shared__ double sh[3][MCB_THREADS];
+    const int N = A.N;
+    const double mean = st->mean;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double bi = b[i] - mean;
+        acc[0] += bi * bi;
+        if (xa) {
+            double ax = A.diag[i] * xa[i];
+#pragma unroll
+            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * xa[A.col[(size_t)k * N + i]];
+            acc[1] += (bi - ax) * (bi - ax);
+        }
+        if (xb) {
+            double ax = A.diag[i] * xb[i];
+#pragma unroll
+            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * xb[A.col[(size_t)k * N + i]];
+            acc[2] += (bi - ax) * (bi - ax);
+        }
+    }
+    if (publish_partials<3>(acc, partials, counter, sh)) {
+        double tot[3];
+        reduce_partials<3>(tot, partials, counter, sh);
+        if (threadIdx.x == 0) {
+            gs->bb = tot[0];
+            gs->rr[0] = xa ? tot[1] : -1.0;
+            gs->rr[1] = xb ? tot[2] : -1.0;
+            int choice = -1;
+            double best = tot[0];
+            if (xa && finite(tot[1]) && tot[1] < best) {
+                choice = 0;
+                best = tot[1];
+            }
+            if (xb && finite(tot[2]) && tot[2] < best) choice = 1;
+            gs->choice = choice;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(MCB_THREADS) k_guess_apply(int N, double *__restrict__ x,
+                                                             const double *__restrict__ xa,
+                                                             const double *__restrict__ xb,
+                                                             const GuessState *__restrict__ gs)
+{
+    const int c = gs->choice;
+    const double *src = c == 0 ? xa : (c == 1 ? xb : nullptr);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) x[i] = src ? src[i] : 0.0;
 }
 
 __global__ void __launch_bounds__(MCB_THREADS) k_ir_add(int N, double *__restrict__ x, const float *__restrict__ e,
@@ -404,9 +477,9 @@ void pcg_iter2(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew)
 }
 template <typename T>
 void pcg_init_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, double rtol, double abs_floor,
-                  int max_iters, int project)
+                  int max_iters, int project, int use_x0)
 {
-    k_pcg_init_amg<T><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, abs_floor, max_iters, project);
+    k_pcg_init_amg<T><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, abs_floor, max_iters, project, use_x0);
 }
 template <typename T>
 void pcg_iter2_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, int pnew)
@@ -416,15 +489,24 @@ void pcg_iter2_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, in
 #define MCB_INSTANTIATE_PCG(T)                                                                                  \
     template void pcg_iter1<T>(cudaStream_t, const EllT<T> &, const PcgVectorsT<T> &, int);                   \
     template void pcg_init_amg<T>(cudaStream_t, const EllT<T> &, const PcgVectorsT<T> &, double, double, int, \
-                                  int);                                                                       \
+                                  int, int);                                                                  \
     template void pcg_iter2_amg<T>(cudaStream_t, const EllT<T> &, const PcgVectorsT<T> &, int);
 MCB_INSTANTIATE_PCG(double)
 MCB_INSTANTIATE_PCG(float)
 void ir_init(cudaStream_t s, const Ell &A, const double *b, double *x, double *r, float *r32, PcgState *st,
-             double *partials, unsigned int *counter, double rtol, double abs_floor, int max_outer)
+             double *partials, unsigned int *counter, double rtol, double abs_floor, int max_outer, int use_x0)
 {
     k_ir_init<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, b, x, r, r32, st, partials, counter, rtol, abs_floor,
-                                                       max_outer);
+                                                       max_outer, use_x0);
+}
+void guess_residuals(cudaStream_t s, const Ell &A, const double *b, const PcgState *st, const double *xa,
+                     const double *xb, GuessState *gs, double *partials, unsigned int *counter)
+{
+    k_guess_residuals<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, b, st, xa, xb, gs, partials, counter);
+}
+void guess_apply(cudaStream_t s, int N, double *x, const double *xa, const double *xb, const GuessState *gs)
+{
+    k_guess_apply<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, x, xa, xb, gs);
 }
 void ir_add(cudaStream_t s, int N, double *x, const float *e, const PcgState *st)
 {

@@ -93,7 +93,7 @@ void pcg_iter2(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew);
 // computes z and r . z after each update).
 template <typename T>
 void pcg_init_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, double rtol, double abs_floor,
-                  int max_iters, int project);
+                  int max_iters, int project, int use_x0 = 0);
 template <typename T>
 void pcg_iter2_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, int pnew);
 // FP64 iterative refinement around an FP32 inner solve: the state's mean
@@ -101,7 +101,20 @@ void pcg_iter2_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, in
 // (float) r and the tolerance; ir_add accumulates x += e in FP64; ir_residual
 // recomputes the FP64 true residual, its norm, r32, and the convergence flag.
 void ir_init(cudaStream_t s, const Ell &A, const double *b, double *x, double *r, float *r32, PcgState *st,
-             double *partials, unsigned int *counter, double rtol, double abs_floor, int max_outer);
+             double *partials, unsigned int *counter, double rtol, double abs_floor, int max_outer, int use_x0 = 0);
+
+// Initial-guess selection for the pressure correction: the squared
+// residuals ||b' - A x_c||^2 of up to two candidates (b' = b - st->mean;
+// a null candidate is skipped) against ||b'||^2 of the zero guess; the
+// smallest wins.  guess_apply writes the winner into x.
+struct GuessState {
+    double bb, rr[2];
+    int choice;   // -1 zero, 0 candidate a, 1 candidate b
+    int pad;
+};
+void guess_residuals(cudaStream_t s, const Ell &A, const double *b, const PcgState *st, const double *xa,
+                     const double *xb, GuessState *gs, double *partials, unsigned int *counter);
+void guess_apply(cudaStream_t s, int N, double *x, const double *xa, const double *xb, const GuessState *gs);
 void ir_add(cudaStream_t s, int N, double *x, const float *e, const PcgState *st);
 void ir_residual(cudaStream_t s, const Ell &A, const double *b, const double *x, double *r, float *r32, PcgState *st,
                  double *partials, unsigned int *counter);

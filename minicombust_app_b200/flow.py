@@ -37,6 +37,21 @@ PSOLVER_PCG_JACOBI, PSOLVER_PCG_AMG = 0, 1
 PRECISION_FP64, PRECISION_FP32_REFINED = 0, 1
 REORDER_NONE, REORDER_RCM = 0, 1
 GUESS_ZERO, GUESS_PREVIOUS, GUESS_LEARNED = 0, 1, 2
+SNAPSHOT_MAGIC = b"MCSNAP01"
+
+
+def read_snapshots(path):
+    """Records of a snapshot file as a read-only array [records][4][cells]
+    (rhs projected to mean zero, diagonal, previous correction, correction)."""
+    with open(path, "rb") as f:
+        head = f.read(64)
+    if head[:8] != SNAPSHOT_MAGIC:
+        raise ValueError(f"{path}: not a snapshot file")
+    version, cells, fields, dtype = np.frombuffer(head[8:24], dtype=np.uint32)
+    records = int(np.frombuffer(head[24:32], dtype=np.uint64)[0])
+    if version != 1 or fields != 4 or dtype != 0:
+        raise ValueError(f"{path}: unsupported snapshot layout")
+    return np.memmap(path, dtype=np.float32, mode="r", offset=64, shape=(records, 4, int(cells)))
 SYSTEM_MOMENTUM, SYSTEM_PRESSURE, SYSTEM_TEMPERATURE, SYSTEM_MOMENTUM_V, SYSTEM_MOMENTUM_W = 0, 1, 2, 3, 4
 
 FIELDS = {"U": 0, "V": 1, "W": 2, "P": 3, "PP": 4, "TE": 5, "ED": 6, "TP": 7, "TEM": 8,
@@ -66,14 +81,16 @@ class IterStats(ctypes.Structure):
     _fields_ = [("momentum_iters", c_int * 3), ("temperature_iters", c_int), ("pressure_solves", c_int),
                 ("pressure_iters_total", c_int), ("pressure_iters_first", c_int),
                 ("pressure_correction_max_first", c_dbl), ("pressure_rel_residual", c_dbl),
-                ("mass_imbalance", c_dbl)]
+                ("mass_imbalance", c_dbl), ("guess_choice_first", c_int), ("guess_rel_residual_first", c_dbl)]
 
     def as_dict(self):
         return {"momentum_iters": list(self.momentum_iters), "temperature_iters": self.temperature_iters,
                 "pressure_solves": self.pressure_solves, "pressure_iters_total": self.pressure_iters_total,
                 "pressure_iters_first": self.pressure_iters_first,
                 "pressure_correction_max_first": self.pressure_correction_max_first,
-                "pressure_rel_residual": self.pressure_rel_residual, "mass_imbalance": self.mass_imbalance}
+                "pressure_rel_residual": self.pressure_rel_residual, "mass_imbalance": self.mass_imbalance,
+                "guess_choice_first": self.guess_choice_first,
+                "guess_rel_residual_first": self.guess_rel_residual_first}
 
 
 class FlowError(RuntimeError):
@@ -93,6 +110,9 @@ _SIGNATURES = {
     "mc_flow_set_sources": (c_int, [c_vp, c_vp]),
     "mc_flow_get_face_array": (c_int, [c_vp, c_int, c_vp]),
     "mc_flow_get_cell_order": (c_int, [c_vp, c_vp]),
+    "mc_flow_set_guess_params": (c_int, [c_vp, c_vp, c_int]),
+    "mc_flow_snapshot_open": (c_int, [c_vp, ctypes.c_char_p, c_int]),
+    "mc_flow_snapshot_close": (c_int, [c_vp]),
     "mc_flow_get_cell_array": (c_int, [c_vp, c_int, c_vp]),
     "mc_flow_get_csr": (c_int, [c_vp, c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int), c_vp, c_vp, c_vp, c_vp]),
     "mc_flow_simple_iteration": (c_int, [c_vp, ctypes.POINTER(IterStats)]),
@@ -312,6 +332,17 @@ class FlowSolver:
         a = np.empty((self.F, width))
         _check(self.L.mc_flow_get_face_array(self.h, which, _ptr(a)), self.h, "get_face_array")
         return a if width > 1 else a[:, 0]
+
+    def set_guess_params(self, params):
+        """Parameters of the learned guess (MC_GUESS_LEARNED), as from gnn.GuessNet.params()."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        _check(self.L.mc_flow_set_guess_params(self.h, _ptr(p), len(p)), self.h, "set_guess_params")
+
+    def snapshot_open(self, path, max_records):
+        _check(self.L.mc_flow_snapshot_open(self.h, os.fsencode(path), int(max_records)), self.h, "snapshot_open")
+
+    def snapshot_close(self):
+        _check(self.L.mc_flow_snapshot_close(self.h), self.h, "snapshot_close")
 
     def cell_order(self):
         """The handle's internal cell order: new-to-old ids (identity unless reordered)."""
