@@ -1,4 +1,6 @@
-"""Benchmark: SIMPLE iterations per second of the flow-solver pass on a B200.
+"""Benchmark: SIMPLE iterations per second of the flow-solver pass on a B200,
+learned initial guess + FP32-refined pressure solve against the plain FP64
+path, both to the same 1e-8 pressure residual.
 
 Workload (BASELINE metric configuration): box of 2*128 x 128 x 128 =
 4,194,304 hexahedral cells on a 0.2 x 0.1 x 0.1 m domain, inlet u = 50 m/s on
@@ -15,6 +17,13 @@ L2, so consecutive iterations stream from HBM.
 One step = one SIMPLE pass (gradients, momentum assembly and three solves,
 Rhie-Chow mass flux, pressure-correction assembly, PCG solve(s) and
 corrections, temperature assembly and solve).
+
+Two configurations run back to back from the same initial state:
+  headline ("value"): MC_GUESS_LEARNED (the committed trained parameters) +
+    MC_PRECISION_FP32_REFINED, pressure PCG-AMG;
+  plain ("plain_fp64"): zero guess, FP64 PCG-AMG.
+After the same number of passes the fields of the two are compared (max
+relative difference per field).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -37,7 +46,7 @@ sys.path.insert(0, ROOT)
 
 from minicombust_app_b200.workload import gaussian_blobs, noisy_fields  # noqa: E402
 
-METRIC = "SIMPLE iters/s at 4.2M cells"
+METRIC = "SIMPLE iters/s at 4.2M cells: learned+FP32-refined vs plain FP64, same 1e-8 residual"
 UNIT = "iters/s"
 
 
@@ -52,7 +61,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-roofline", action="store_true")
     ap.add_argument("--psolver", default="amg", choices=["amg", "jacobi"],
-                    help="pressure-correction preconditioner (aggregation AMG V-cycle or Jacobi)")
+                    help="pressure-correction preconditioner of the plain path (aggregation AMG or Jacobi)")
+    ap.add_argument("--config", default="both", choices=["both", "headline", "plain"],
+                    help="which configurations to time (default: both; value = headline)")
     return ap.parse_args()
 
 
@@ -118,6 +129,7 @@ def kernel_bytes(name, N, F, nnz_off):
     return {
         "pcg_iter1_spmv": 12 * nnz_off + 40 * N,   # diag, off+col, z, p_old -> p_new, q
         "pcg_iter2_update": 64 * N,                # x rw, r rw, p, q, diag -> z
+        "pcg32_iter1_spmv": 8 * nnz_off + 20 * N,  # FP32 values, int32 columns
         "bicg3_1_spmv": 12 * nnz_off + 8 * N + 3 * 48 * N,
         "bicg3_2_spmv": 12 * nnz_off + 8 * N + 3 * 32 * N,
         "bicg3_3_update": 3 * 56 * N,
@@ -195,6 +207,78 @@ def run_reference_arm(args, rank, world):
 
 # ------------------------------------------------------------------- main
 
+FIELD_NAMES = ("U", "V", "W", "P", "TEM")
+
+
+def make_solver(flow, mesh, dims, lengths, args, rank, local, headline):
+    """The benchmark solver of one configuration, seeded identically."""
+    if headline:
+        from minicombust_app_b200 import train_guess
+        params = flow.default_params(flow.MODE_SIMPLE, device=local, p_rtol=1e-8, u_rtol=1e-8,
+                                     pressure_solver=flow.PSOLVER_PCG_AMG, precision=flow.PRECISION_FP32_REFINED,
+                                     initial_guess=flow.GUESS_LEARNED)
+    else:
+        psolver = flow.PSOLVER_PCG_AMG if args.psolver == "amg" else flow.PSOLVER_PCG_JACOBI
+        params = flow.default_params(flow.MODE_SIMPLE, device=local, p_rtol=1e-8, u_rtol=1e-8,
+                                     pressure_solver=psolver)
+    solver = flow.FlowSolver(mesh, params=params)
+    if headline:
+        solver.set_guess_params(train_guess.load_params())
+    N = solver.N
+    for name, vals in noisy_fields(N, seed=rank).items():
+        a = solver.field(name)
+        a[:N] = vals
+        solver.set_field(name, a)
+    solver.set_sources(gaussian_blobs(dims, lengths, args.blobs, seed=rank))
+    return solver
+
+
+def timed_steps(torch, solver, stream, steps, barrier, max_over_ranks, local):
+    """Device-timed SIMPLE passes (CUDA events on the solver's stream,
+    barrier + synchronize on both sides, max over ranks), clocks sampled."""
+    stats = []
+    launches0 = solver.launch_count()
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        solver.simple_iteration()
+        stats.append(solver.last_stats.as_dict())
+    ev1.record(stream)
+    barrier()
+    clocks = sampler.stop()
+    t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    return t, stats, clocks, solver.launch_count() - launches0
+
+
+def roofline_of(solver, mesh, N):
+    """One instrumented pass: the dominant kernel with an algorithmic byte
+    model, its CUDA-event launch time and achieved bandwidth."""
+    solver.reset_kernel_times()
+    solver.set_timing(True)
+    solver.simple_iteration()
+    solver.set_timing(False)
+    kt = solver.kernel_times()
+    nnz_off = int(np.sum(mesh.face_cells[:, 1] < N)) * 2
+    total = sum(v[0] for v in kt.values())
+    ranked = sorted(((ms, name, cnt) for name, (ms, cnt) in kt.items() if cnt > 0), reverse=True)
+    peak, kind = measured_peaks()
+    roof = None
+    for ms, name, cnt in ranked:
+        b = kernel_bytes(name, N, mesh.n_faces, nnz_off)
+        if b is None:
+            continue
+        avg_s = ms / cnt / 1e3
+        achieved = b / avg_s / 1e9
+        roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": kind, "traffic": None, "bytes_per_launch": b,
+                "avg_launch_us": avg_s * 1e6, "launches_per_step": cnt, "share_of_step": ms / total}
+        break
+    return roof, {k: round(v[0], 4) for k, v in kt.items() if v[1] > 0}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -219,22 +303,6 @@ def main():
     if not os.path.exists(flow.LIB_PATH):
         mcbuild.build()
 
-    m = args.m
-    dims, lengths = (2 * m, m, m), (0.2, 0.1, 0.1)
-    mesh = flow.Mesh.box(*dims, *lengths)
-    psolver = flow.PSOLVER_PCG_AMG if args.psolver == "amg" else flow.PSOLVER_PCG_JACOBI
-    params = flow.default_params(flow.MODE_SIMPLE, device=local, p_rtol=1e-8, u_rtol=1e-8, pressure_solver=psolver)
-    solver = flow.FlowSolver(mesh, params=params)
-    N = solver.N
-    init = noisy_fields(N, seed=rank)
-    for name, vals in init.items():
-        a = solver.field(name)
-        a[:N] = vals
-        solver.set_field(name, a)
-    solver.set_sources(gaussian_blobs(dims, lengths, args.blobs, seed=rank))
-
-    stream = torch.cuda.ExternalStream(solver.stream(), device=torch.device("cuda", local))
-
     def barrier():
         torch.cuda.synchronize()
         if dist:
@@ -248,75 +316,49 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    for _ in range(args.warmup):
-        solver.simple_iteration()
-
-    # ---- device-resident throughput (value)
-    stats = []
-    launches0 = solver.launch_count()
-    sampler = ClockSampler(local)
-    barrier()
-    sampler.start()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        solver.simple_iteration()
-        stats.append(solver.last_stats.as_dict())
-    ev1.record(stream)
-    barrier()
-    clocks = sampler.stop()
-    launches = solver.launch_count() - launches0
-    t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
-    value = world * args.steps / t_dev
-
-    # ---- end to end through the C ABI with host buffers
-    names = ("U", "V", "W", "P", "TEM")
-    pinned = {n: torch.empty(N + 6, dtype=torch.float64, pin_memory=True) for n in names}
-    for n in names:
-        pinned[n].numpy()[:] = solver.field(n)
-    h2d = 5 * (N + 6) * 8
-    d2h = 5 * (N + 6) * 8
-    L = flow.library()
-    h = solver.h
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        for i, n in enumerate(names):
-            flow._check(L.mc_flow_set_field(h, flow.FIELDS[n], pinned[n].data_ptr()), h, "set_field")
-        solver.simple_iteration()
-        for n in names:
-            flow._check(L.mc_flow_get_field(h, flow.FIELDS[n], pinned[n].data_ptr()), h, "get_field")
-    e1.record(stream)
-    barrier()
-    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
-    e2e = world * args.steps / t_e2e
-
-    line = None
-    if rank == 0:
-        # ---- roofline of the dominant kernel (separate instrumented pass)
-        roof = None
-        kt = {}
-        if not args.no_roofline:
-            solver.reset_kernel_times()
-            solver.set_timing(True)
+    m = args.m
+    dims, lengths = (2 * m, m, m), (0.2, 0.1, 0.1)
+    mesh = flow.Mesh.box(*dims, *lengths)
+    N = mesh.n_cells
+    runs = {}
+    order = {"both": ("plain", "headline"), "headline": ("headline",), "plain": ("plain",)}[args.config]
+    for cfg in order:
+        solver = make_solver(flow, mesh, dims, lengths, args, rank, local, cfg == "headline")
+        stream = torch.cuda.ExternalStream(solver.stream(), device=torch.device("cuda", local))
+        for _ in range(args.warmup):
             solver.simple_iteration()
-            solver.set_timing(False)
-            kt = solver.kernel_times()
-            nnz_off = int(np.sum(mesh.face_cells[:, 1] < N)) * 2
-            ranked = sorted(((ms, name, cnt) for name, (ms, cnt) in kt.items() if cnt > 0), reverse=True)
-            for ms, name, cnt in ranked:
-                b = kernel_bytes(name, N, mesh.n_faces, nnz_off)
-                if b is None:
-                    continue
-                avg_s = ms / cnt / 1e3
-                peak, kind = measured_peaks()
-                achieved = b / avg_s / 1e9
-                roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "peak_source": kind, "traffic": None,
-                        "bytes_per_launch": b, "avg_launch_us": avg_s * 1e6, "launches_per_step": cnt,
-                        "share_of_step": ms / sum(v[0] for v in kt.values())}
-                break
+        t, stats, clocks, launches = timed_steps(torch, solver, stream, args.steps, barrier, max_over_ranks, local)
+        fields = {n: solver.field(n)[:N].copy() for n in FIELD_NAMES} if rank == 0 else None
+        r = {"t": t, "stats": stats, "clocks": clocks, "launches": launches, "fields": fields}
+        if cfg == order[-1]:
+            # end to end through the C ABI with pinned host buffers: every
+            # step uploads the five fields and reads them back
+            pinned = {n: torch.empty(N + 6, dtype=torch.float64, pin_memory=True) for n in FIELD_NAMES}
+            for n in FIELD_NAMES:
+                pinned[n].numpy()[:] = solver.field(n)
+            L, h = flow.library(), solver.h
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                for n in FIELD_NAMES:
+                    flow._check(L.mc_flow_set_field(h, flow.FIELDS[n], pinned[n].data_ptr()), h, "set_field")
+                solver.simple_iteration()
+                for n in FIELD_NAMES:
+                    flow._check(L.mc_flow_get_field(h, flow.FIELDS[n], pinned[n].data_ptr()), h, "get_field")
+            e1.record(stream)
+            barrier()
+            r["e2e"] = world * args.steps / max_over_ranks(e0.elapsed_time(e1) / 1e3)
+            r["e2e_bytes"] = 5 * (N + 6) * 8
+        if rank == 0 and not args.no_roofline:
+            r["roofline"], r["kernel_ms"] = roofline_of(solver, mesh, N)
+        runs[cfg] = r
+        solver.close()
+
+    if rank == 0:
+        main_cfg = order[-1]
+        R = runs[main_cfg]
+        value = world * args.steps / R["t"]
         cpu = None
         if not args.no_cpu_baseline:
             per_pass = reference_sample(32, 3)
@@ -325,26 +367,40 @@ def main():
                 cpu = {"value": 1.0 / (per_pass * scale), "unit": UNIT, "cores": 1, "kind": "reference",
                        "sample": f"3 SIMPLE passes of the reference CPU FlowSolver (its own physics) on 2*32^3 "
                                  f"cells, time per pass x {scale:.0f} (cell-count scaling)"}
-        pit = [s["pressure_iters_total"] for s in stats]
+        summary = {}
+        for cfg, r in runs.items():
+            pit = [st["pressure_iters_total"] for st in r["stats"]]
+            summary[cfg] = {"value": world * args.steps / r["t"], "ms_per_step": 1e3 * r["t"] / args.steps,
+                            "pressure_iters_per_step": float(np.mean(pit)),
+                            "guess_rel_residual": float(np.mean([st["guess_rel_residual_first"] for st in r["stats"]])),
+                            "momentum_iters": r["stats"][-1]["momentum_iters"],
+                            "temperature_iters": r["stats"][-1]["temperature_iters"],
+                            "pressure_rel_residual": max(st["pressure_rel_residual"] for st in r["stats"]),
+                            "mass_imbalance": r["stats"][-1]["mass_imbalance"], "gpu_launches": r["launches"],
+                            "roofline": r.get("roofline"), "kernel_ms_one_step": r.get("kernel_ms")}
+        field_err = None
+        if "plain" in runs and "headline" in runs:
+            field_err = {}
+            for n in FIELD_NAMES:
+                a, b = runs["headline"]["fields"][n], runs["plain"]["fields"][n]
+                field_err[n] = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+        desc = ("learned initial guess + FP32-refined pressure PCG-AMG (FP64 outer refinement)"
+                if main_cfg == "headline" else "plain FP64 path, pressure PCG-AMG")
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "warmup": args.warmup, "ms_per_step": 1e3 * R["t"] / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if main_cfg == "headline" else "f64",
+                "data": "synthetic",
                 "config": {"workload": f"simple-mode SIMPLE pass, box 2*{m}x{m}x{m} = {N} cells, {args.blobs} "
-                                       f"source blobs, plain FP64 path (PCG + {'aggregation-AMG V-cycle' if args.psolver == 'amg' else 'Jacobi'} "
-                                       "pressure, BiCGStab momentum/T, rtol 1e-8)",
+                                       f"source blobs, {desc}, BiCGStab momentum/T, rtol 1e-8",
                            "cells": N, "faces": mesh.n_faces, "l2": "inputs larger than L2 (~4.5 GB working set)",
                            "parallelism": "replicas" if world > 1 else "single GPU"},
-                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "gpu_launches": launches,
-                "clocks": clocks,
-                "roofline": roof,
-                "cpu_baseline": cpu,
-                "solver": {"pressure_iters_per_step": float(np.mean(pit)), "momentum_iters": stats[-1]["momentum_iters"],
-                           "temperature_iters": stats[-1]["temperature_iters"],
-                           "mass_imbalance": stats[-1]["mass_imbalance"]},
-                "kernel_ms_one_step": {k: round(v[0], 4) for k, v in kt.items() if v[1] > 0}}
+                "e2e": {"value": R["e2e"], "unit": UNIT, "h2d_bytes_per_step": R["e2e_bytes"],
+                        "d2h_bytes_per_step": R["e2e_bytes"]},
+                "gpu_launches": R["launches"], "clocks": R["clocks"], "roofline": R.get("roofline"),
+                "cpu_baseline": cpu, "configs": summary, "field_rel_diff_vs_plain_fp64": field_err}
+        if "plain" in runs and "headline" in runs:
+            line["speedup_vs_plain_fp64"] = summary["headline"]["value"] / summary["plain"]["value"]
         print(json.dumps(line))
-    solver.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

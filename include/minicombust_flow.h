@@ -121,8 +121,9 @@ typedef struct mc_iter_stats {
     double pressure_correction_max_first;
     double pressure_rel_residual;    /* last pressure solve, ||r|| / ||b|| */
     double mass_imbalance;           /* max over cells |div(mdot) - mass source| after the pass */
-    int guess_choice_first;          /* initial guess of the first pressure solve: -1 zero, 0 previous
-                                        correction, 1 learned (MC_GUESS_PREVIOUS / MC_GUESS_LEARNED) */
+    int guess_choice_first;          /* initial guess of the first pressure solve: -1 zero, 2 the
+                                        residual-minimising combination of the previous correction and
+                                        (MC_GUESS_LEARNED) the network's prediction */
     double guess_rel_residual_first; /* ||b - A x0|| / ||b|| of that guess (1 for zero) */
 } mc_iter_stats;
 

@@ -134,6 +134,7 @@ struct mc_flow {
     char *gnn_mem = nullptr;
     bool gnn_loaded = false;
     int guess_choice = -1;
+    int corrector = 1;                // pressure-correction solve within the pass (1 = first)
     double guess_rel = 1.0;
     // snapshot dataset writer
     FILE *snap = nullptr;
@@ -286,7 +287,9 @@ __global__ void k_snapshot_pack(int N, const double *__restrict__ b, const PcgSt
 int select_guess(mc_flow *h, const Ell &A, const double *b, const PcgState *st, double *x)
 {
     if (h->prm.initial_guess == MC_GUESS_ZERO) return 0;
-    const bool learned = h->prm.initial_guess == MC_GUESS_LEARNED;
+    // the network runs for the first corrector of a pass; the later ones, whose
+    // right-hand sides are already small, use the previous correction alone
+    const bool learned = h->prm.initial_guess == MC_GUESS_LEARNED && h->corrector == 1;
     if (learned) {
         launch(h, K_GNN, [&] {
             GnnInput<double> in{b, &st->mean, A.diag, h->pp_prev};
@@ -310,7 +313,7 @@ int after_pressure_solve(mc_flow *h)
     if (h->prm.initial_guess != MC_GUESS_ZERO) {
         const GuessState &g = *h->h_gs;  // the copy was ordered before the solve's final synchronisation
         h->guess_choice = g.choice;
-        h->guess_rel = g.bb > 0 ? std::sqrt((g.choice < 0 ? g.bb : g.rr[g.choice]) / g.bb) : 1.0;
+        h->guess_rel = g.bb > 0 ? std::sqrt((g.choice < 0 ? g.bb : g.rc) / g.bb) : 1.0;
     }
     if (h->snap && h->snap_count < h->snap_max) {
         launch(h, K_SNAPSHOT, [&] {
@@ -631,6 +634,7 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
         int its = 0;
         double relres = 0.0, bnorm = 0.0;
         const double floor = (simple && loop > 1) ? h->prm.p_rtol * h->p_bnorm_ref : 0.0;
+        h->corrector = loop;
         rc = h->refined ? solve_pressure_refined(h, floor, &its, &relres, &bnorm)
                         : solve_pressure(h, floor, &its, &relres, &bnorm);
         if (rc == MC_ERR_CUDA) return rc;
@@ -859,18 +863,23 @@ int setup_guess(mc_flow *h, const HostMesh &hm)
     std::vector<int> col;
     std::vector<uint32_t> edge;
     std::vector<float> vhat;
-    gnn_graph_host(hm, col, edge, vhat);
+    std::vector<uint8_t> mask;
+    GnnGraph aff{};
+    gnn_graph_host(hm, col, edge, vhat, aff, mask);
     const size_t N = (size_t)hm.N;
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t eb = al(6 * N * 4), vb = al(N * 4), xb = al(N * 8), pb = al((size_t)GNN_NPARAM * 4),
-                 kb = al((size_t)GNN_NPACK * 2), wb = gnn_work_bytes(hm.N, false);
-    const cudaError_t e = cudaMalloc((void **)&h->gnn_mem, eb + vb + xb + pb + kb + wb);
+                 kb = al((size_t)GNN_NPACK * 2), wb = gnn_work_bytes(hm.N, false), mb = al(mask.size()),
+                 cb = al(6 * N * 4);
+    const cudaError_t e = cudaMalloc((void **)&h->gnn_mem, eb + vb + xb + pb + kb + wb + mb + cb);
     if (e != cudaSuccess) return fail(h, MC_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     char *c = h->gnn_mem;
     CUDA_TRY(h, cudaMemcpy(c, edge.data(), 6 * N * 4, cudaMemcpyHostToDevice));
     CUDA_TRY(h, cudaMemcpy(c + eb, vhat.data(), N * 4, cudaMemcpyHostToDevice));
+    int *dcol = reinterpret_cast<int *>(c + eb + vb + xb + pb + kb + wb + mb);
+    CUDA_TRY(h, cudaMemcpy(dcol, col.data(), 6 * N * 4, cudaMemcpyHostToDevice));
     h->gnn_g.n = hm.N;
-    h->gnn_g.col = h->col;
+    h->gnn_g.col = dcol;
     h->gnn_g.edge = reinterpret_cast<const __nv_bfloat162 *>(c);
     h->gnn_g.vhat = reinterpret_cast<const float *>(c + eb);
     h->x0_learned = reinterpret_cast<double *>(c + eb + vb);
@@ -878,6 +887,17 @@ int setup_guess(mc_flow *h, const HostMesh &hm)
     h->gnn_pk = reinterpret_cast<__nv_bfloat16 *>(c + eb + vb + xb + pb);
     CUDA_TRY(h, cudaMemset(c + eb + vb + xb + pb + kb, 0, wb));
     gnn_work_carve(h->gnn_w, c + eb + vb + xb + pb + kb, hm.N, false);
+    h->gnn_g.affine = aff.affine;
+    for (int k = 0; k < 6; k++) {
+        h->gnn_g.doff[k] = aff.doff[k];
+        h->gnn_g.ebits[k] = aff.ebits[k];
+    }
+    h->gnn_g.mask = nullptr;
+    if (aff.affine) {
+        uint8_t *md = reinterpret_cast<uint8_t *>(c + eb + vb + xb + pb + kb + wb);
+        CUDA_TRY(h, cudaMemcpy(md, mask.data(), mask.size(), cudaMemcpyHostToDevice));
+        h->gnn_g.mask = md;
+    }
     return MC_OK;
 }
 

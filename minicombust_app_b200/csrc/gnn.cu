@@ -100,11 +100,9 @@ __device__ __forceinline__ CellFeat load_features(const GnnGraph &g, const GnnIn
 {
     CellFeat f{0.f, 0.f, 0.f, 0.f};
     if (i < g.n) {
-        const double rb = sc.sb > 0 ? 1.0 / sc.sb : 0.0, rd = sc.sd > 0 ? 1.0 / sc.sd : 0.0;
-        const double rx = sc.sx > 0 ? 1.0 / sc.sx : 0.0;
-        f.b = (float)(((double)in.b[i] - sc.shift) * rb);
-        f.d = (float)((double)in.diag[i] * rd);
-        f.p = in.prev ? (float)((double)in.prev[i] * rx) : 0.f;
+        f.b = (float)(((double)in.b[i] - sc.shift) * sc.rb);
+        f.d = (float)((double)in.diag[i] * sc.rd);
+        f.p = in.prev ? (float)((double)in.prev[i] * sc.rx) : 0.f;
         f.v = g.vhat[i];
     }
     return f;
@@ -157,27 +155,47 @@ __global__ void __launch_bounds__(MCB_THREADS) k_gnn_scales(int n, GnnInput<T> i
             s.sd = tot[1] / n;
             s.sx = (s.sd > 0 && isfinite(s.sb)) ? s.sb / s.sd : 0.0;
             if (!(s.sb > 0) || !(s.sx > 0) || !isfinite(s.sx)) s.sb = s.sd = s.sx = 0.0;
+            s.rb = s.sb > 0 ? 1.0 / s.sb : 0.0;
+            s.rd = s.sd > 0 ? 1.0 / s.sd : 0.0;
+            s.rx = s.sx > 0 ? 1.0 / s.sx : 0.0;
             *out = s;
         }
     }
 }
 
-// h0 = relu(We x + ce); lane = channel.
+// Eight consecutive BF16 channels as one 16-byte word.
+union Chunk8 {
+    uint4 u;
+    bf162 h[4];
+};
+
+// h0 = relu(We x + ce).  Thread = cell: one feature load, 32 channels from
+// the weights in shared memory, four 16-byte stores.
 template <typename T>
 __global__ void __launch_bounds__(GNN_TILE) k_gnn_encode(GnnGraph g, GnnInput<T> in, const float *__restrict__ p,
                                                          const GnnScales *__restrict__ scp, bf16 *__restrict__ hout)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int base = blockIdx.x * GNN_TILE + warp * 32;
-    const GnnScales sc = *scp;
-    const CellFeat mine = load_features(g, in, sc, base + lane);
-    const float w0 = p[GP_WE + lane * GNN_IN], w1 = p[GP_WE + lane * GNN_IN + 1];
-    const float w2 = p[GP_WE + lane * GNN_IN + 2], w3 = p[GP_WE + lane * GNN_IN + 3], c = p[GP_CE + lane];
-    for (int r = 0; r < 32; r++) {
-        const float xb = __shfl_sync(FULL, mine.b, r), xd = __shfl_sync(FULL, mine.d, r);
-        const float xp = __shfl_sync(FULL, mine.p, r), xv = __shfl_sync(FULL, mine.v, r);
-        const int i = base + r;
-        if (i < g.n) hout[(size_t)i * GNN_H + lane] = __float2bfloat16(fmaxf(w0 * xb + w1 * xd + w2 * xp + w3 * xv + c, 0.f));
+    __shared__ float sw[GNN_H * (GNN_IN + 1)];
+    for (int e = threadIdx.x; e < GNN_H * (GNN_IN + 1); e += GNN_TILE) sw[e] = p[GP_WE + e];  // We then ce
+    __syncthreads();
+    const int i = blockIdx.x * GNN_TILE + threadIdx.x;
+    if (i >= g.n) return;
+    const CellFeat x = load_features(g, in, *scp, i);
+#pragma unroll
+    for (int c4 = 0; c4 < 4; c4++) {
+        Chunk8 o;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            float z[2];
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int c = c4 * 8 + 2 * q + e;
+                const float *w = sw + c * GNN_IN;
+                z[e] = fmaxf(w[0] * x.b + w[1] * x.d + w[2] * x.p + w[3] * x.v + sw[GNN_H * GNN_IN + c], 0.f);
+            }
+            o.h[q] = __floats2bfloat162_rn(z[0], z[1]);
+        }
+        *reinterpret_cast<uint4 *>(hout + (size_t)i * GNN_H + c4 * 8) = o.u;
     }
 }
 
@@ -205,74 +223,193 @@ __device__ __forceinline__ float2 edge_of(uint32_t bits)
     return __bfloat1622float2(e);
 }
 
-// One message-passing layer; TRAIN also stores relu(W1 u + c1).
-template <bool TRAIN>
-__global__ void __launch_bounds__(GNN_TILE) k_gnn_layer(GnnGraph g, const float *__restrict__ pl,
-                                                        const bf16 *__restrict__ pkl, const bf16 *__restrict__ hin,
-                                                        bf16 *__restrict__ hout, bf16 *__restrict__ asave)
+// Asynchronous 16-byte global -> shared copy; src_bytes = 0 writes zeros.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes)
 {
-    __shared__ __align__(16) bf16 sU[GNN_TILE * LDU];
-    __shared__ __align__(16) bf16 sW1[GNN_H * LDU];
-    __shared__ __align__(16) bf16 sW2[GNN_H * LDH];
-    __shared__ __align__(16) bf16 sA[GNN_TILE * LDH];
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Shared memory of k_gnn_layer (bytes): own rows [128][LDH] (a GEMM operand),
+// the six neighbour rows [6][128][32] (zeros where a slot has no neighbour;
+// later reused for relu(W1 u + c1) and h'), messages [128][LDH].
+constexpr size_t LAYER_SMEM_H = sizeof(bf16) * GNN_TILE * LDH;
+constexpr size_t LAYER_SMEM_N = sizeof(bf16) * 6 * GNN_TILE * GNN_H;
+constexpr size_t LAYER_SMEM = 2 * LAYER_SMEM_H + LAYER_SMEM_N;
+
+// One message-passing layer on a tile of 128 cells, 256 threads; TRAIN also
+// stores relu(W1 u + c1).  Thread (row r, chunk c) handles rows r, r + 64
+// and channels 8c .. 8c + 7; all 14 row copies of a thread are in flight
+// together.  Warp w owns rows 16w .. 16w + 15 in the products.  The weight
+// fragments are read through L1 (the same 6 KB for every block).
+constexpr int LAYER_THREADS = 2 * GNN_TILE;
+
+template <bool TRAIN>
+__global__ void __launch_bounds__(LAYER_THREADS) k_gnn_layer(GnnGraph g, const float *__restrict__ pl,
+                                                             const bf16 *__restrict__ pkl,
+                                                             const bf16 *__restrict__ hin, bf16 *__restrict__ hout,
+                                                             bf16 *__restrict__ asave)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    bf16 *sH = reinterpret_cast<bf16 *>(smem);
+    bf16 *sN = reinterpret_cast<bf16 *>(smem + LAYER_SMEM_H);
+    bf16 *sM = reinterpret_cast<bf16 *>(smem + LAYER_SMEM_H + LAYER_SMEM_N);
+    bf16 *sA = sN;  // after the messages are formed
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int e = tid; e < GNN_H * 2 * GNN_H; e += GNN_TILE) sW1[(e >> 6) * LDU + (e & 63)] = pkl[GKL_W1 + e];
-    for (int e = tid; e < GNN_H * GNN_H; e += GNN_TILE) sW2[(e >> 5) * LDH + (e & 31)] = pkl[GKL_W2 + e];
+    const int c4 = tid & 3, r0 = tid >> 2;
     const int n = g.n, base = blockIdx.x * GNN_TILE;
-    {
-        const float wg0 = pl[GPL_WG + 2 * lane], wg1 = pl[GPL_WG + 2 * lane + 1], cg = pl[GPL_CG + lane];
-        const SlotCache mine = load_slots(g, base + warp * 32 + lane);
-        for (int r = 0; r < 32; r++) {
-            const int row = warp * 32 + r, i = base + row;
-            bf16 hi = __float2bfloat16(0.f);
-            float m = 0.f;
-            if (i < n) {
-                hi = hin[(size_t)i * GNN_H + lane];
+    // 1. stage own and neighbour rows
 #pragma unroll
-                for (int k = 0; k < 6; k++) {
-                    const int j = __shfl_sync(FULL, mine.col[k], r);
-                    const float2 e = edge_of(__shfl_sync(FULL, mine.edge[k], r));
-                    if (j != i) m += (wg0 * e.x + wg1 * e.y + cg) * __bfloat162float(hin[(size_t)j * GNN_H + lane]);
+    for (int q = 0; q < 2; q++) {
+        const int r = r0 + 64 * q, i = base + r;
+        const bool in = i < n;
+        cp_async16(sH + r * LDH + c4 * 8, hin + (size_t)(in ? i : 0) * GNN_H + c4 * 8, in ? 16 : 0);
+        const unsigned mk = (in && g.affine) ? g.mask[i] : 0u;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            int j;
+            bool ok;
+            if (g.affine) {
+                ok = (mk >> k) & 1u;
+                j = ok ? i + g.doff[k] : 0;
+            } else {
+                j = in ? g.col[(size_t)k * n + i] : 0;
+                ok = in && j != i;
+                j = ok ? j : 0;
+            }
+            cp_async16(sN + (k * GNN_TILE + r) * GNN_H + c4 * 8, hin + (size_t)j * GNN_H + c4 * 8, ok ? 16 : 0);
+        }
+    }
+    // gates while the copies are in flight
+    float wg0[8], wg1[8], cg[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        wg0[c] = pl[GPL_WG + 2 * (c4 * 8 + c)];
+        wg1[c] = pl[GPL_WG + 2 * (c4 * 8 + c) + 1];
+        cg[c] = pl[GPL_CG + c4 * 8 + c];
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // 2. messages (rows with no neighbour in a slot were staged as zeros)
+    if (g.affine) {
+        float gate[6][8];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const float2 e = edge_of(g.ebits[k]);
+#pragma unroll
+            for (int c = 0; c < 8; c++) gate[k][c] = wg0[c] * e.x + wg1[c] * e.y + cg[c];
+        }
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int r = r0 + 64 * q;
+            float m[8];
+#pragma unroll
+            for (int c = 0; c < 8; c++) m[c] = 0.f;
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                Chunk8 v;
+                v.u = *reinterpret_cast<const uint4 *>(sN + (k * GNN_TILE + r) * GNN_H + c4 * 8);
+#pragma unroll
+                for (int q2 = 0; q2 < 4; q2++) {
+                    const float2 h = __bfloat1622float2(v.h[q2]);
+                    m[2 * q2] += gate[k][2 * q2] * h.x;
+                    m[2 * q2 + 1] += gate[k][2 * q2 + 1] * h.y;
                 }
             }
-            sU[row * LDU + lane] = hi;
-            sU[row * LDU + GNN_H + lane] = __float2bfloat16(m);
+            Chunk8 mo;
+#pragma unroll
+            for (int q2 = 0; q2 < 4; q2++) mo.h[q2] = __floats2bfloat162_rn(m[2 * q2], m[2 * q2 + 1]);
+            *reinterpret_cast<uint4 *>(sM + r * LDH + c4 * 8) = mo.u;
+        }
+    } else {
+        // m = wg0 (.) sum e.x h_j + wg1 (.) sum e.y h_j + cg (.) sum h_j
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int r = r0 + 64 * q, i = base + r;
+            float s0[8], s1[8], s2[8];
+#pragma unroll
+            for (int c = 0; c < 8; c++) s0[c] = s1[c] = s2[c] = 0.f;
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                Chunk8 v;
+                v.u = *reinterpret_cast<const uint4 *>(sN + (k * GNN_TILE + r) * GNN_H + c4 * 8);
+                const float2 e =
+                    edge_of(i < n ? *reinterpret_cast<const uint32_t *>(g.edge + (size_t)k * n + i) : 0u);
+#pragma unroll
+                for (int q2 = 0; q2 < 4; q2++) {
+                    const float2 h = __bfloat1622float2(v.h[q2]);
+                    s0[2 * q2] += e.x * h.x;
+                    s0[2 * q2 + 1] += e.x * h.y;
+                    s1[2 * q2] += e.y * h.x;
+                    s1[2 * q2 + 1] += e.y * h.y;
+                    s2[2 * q2] += h.x;
+                    s2[2 * q2 + 1] += h.y;
+                }
+            }
+            Chunk8 mo;
+#pragma unroll
+            for (int q2 = 0; q2 < 4; q2++) {
+                const int c = 2 * q2;
+                mo.h[q2] = __floats2bfloat162_rn(wg0[c] * s0[c] + wg1[c] * s1[c] + cg[c] * s2[c],
+                                                 wg0[c + 1] * s0[c + 1] + wg1[c + 1] * s1[c + 1] + cg[c + 1] * s2[c + 1]);
+            }
+            *reinterpret_cast<uint4 *>(sM + r * LDH + c4 * 8) = mo.u;
         }
     }
     __syncthreads();
+    // 3. z = W1 [h; m] + c1 on the warp's 16 rows
     const int gq = lane >> 2, tq = lane & 3;
-    float acc[2][4][4];
+    float b1[4][2], b2[4][2];
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            b1[nt][e] = pl[GPL_C1 + nt * 8 + 2 * tq + e];
+            b2[nt][e] = pl[GPL_C2 + nt * 8 + 2 * tq + e];
+        }
+    float acc[1][4][4];
     zero(acc);
-    warp_gemm<2, 4, 4>(acc, sU + warp * 32 * LDU, LDU, sW1, LDU, lane);
+    warp_gemm<1, 4, 2>(acc, sH + warp * 16 * LDH, LDH, pkl + GKL_W1, 2 * GNN_H, lane);
+    warp_gemm<1, 4, 2>(acc, sM + warp * 16 * LDH, LDH, pkl + GKL_W1 + GNN_H, 2 * GNN_H, lane);
 #pragma unroll
-    for (int mt = 0; mt < 2; mt++)
+    for (int nt = 0; nt < 4; nt++)
 #pragma unroll
-        for (int nt = 0; nt < 4; nt++)
-#pragma unroll
-            for (int hf = 0; hf < 2; hf++) {
-                const int row = warp * 32 + mt * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq;
-                const float z0 = acc[mt][nt][2 * hf] + pl[GPL_C1 + col];
-                const float z1 = acc[mt][nt][2 * hf + 1] + pl[GPL_C1 + col + 1];
-                const bf162 v = __floats2bfloat162_rn(fmaxf(z0, 0.f), fmaxf(z1, 0.f));
-                *reinterpret_cast<bf162 *>(sA + row * LDH + col) = v;
-                if (TRAIN && base + row < n) *reinterpret_cast<bf162 *>(asave + (size_t)(base + row) * GNN_H + col) = v;
-            }
+        for (int hf = 0; hf < 2; hf++) {
+            const int row = warp * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq;
+            const bf162 v = __floats2bfloat162_rn(fmaxf(acc[0][nt][2 * hf] + b1[nt][0], 0.f),
+                                                  fmaxf(acc[0][nt][2 * hf + 1] + b1[nt][1], 0.f));
+            *reinterpret_cast<bf162 *>(sA + row * LDH + col) = v;
+            if (TRAIN && base + row < n) *reinterpret_cast<bf162 *>(asave + (size_t)(base + row) * GNN_H + col) = v;
+        }
     __syncwarp();
+    // 4. h' = h + W2 a + c2
     zero(acc);
-    warp_gemm<2, 4, 2>(acc, sA + warp * 32 * LDH, LDH, sW2, LDH, lane);
+    warp_gemm<1, 4, 2>(acc, sA + warp * 16 * LDH, LDH, pkl + GKL_W2, GNN_H, lane);
+    __syncwarp();  // the warp's reads of sA are done; its rows now take h'
 #pragma unroll
-    for (int mt = 0; mt < 2; mt++)
+    for (int nt = 0; nt < 4; nt++)
 #pragma unroll
-        for (int nt = 0; nt < 4; nt++)
+        for (int hf = 0; hf < 2; hf++) {
+            const int row = warp * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq;
+            const float2 hv = __bfloat1622float2(*reinterpret_cast<const bf162 *>(sH + row * LDH + col));
+            *reinterpret_cast<bf162 *>(sA + row * LDH + col) = __floats2bfloat162_rn(
+                hv.x + (acc[0][nt][2 * hf] + b2[nt][0]), hv.y + (acc[0][nt][2 * hf + 1] + b2[nt][1]));
+        }
+    __syncwarp();
+    // 5. coalesced store of the warp's 16 rows: 4 lanes per 64-byte row
 #pragma unroll
-            for (int hf = 0; hf < 2; hf++) {
-                const int row = warp * 32 + mt * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq, i = base + row;
-                if (i >= n) continue;
-                const float2 hv = __bfloat1622float2(*reinterpret_cast<const bf162 *>(sU + row * LDU + col));
-                const float o0 = hv.x + (acc[mt][nt][2 * hf] + pl[GPL_C2 + col]);
-                const float o1 = hv.y + (acc[mt][nt][2 * hf + 1] + pl[GPL_C2 + col + 1]);
-                *reinterpret_cast<bf162 *>(hout + (size_t)i * GNN_H + col) = __floats2bfloat162_rn(o0, o1);
-            }
+    for (int q = 0; q < 2; q++) {
+        const int row = warp * 16 + (lane >> 2) + 8 * q, i = base + row;
+        if (i < n)
+            *reinterpret_cast<uint4 *>(hout + (size_t)i * GNN_H + (lane & 3) * 8) =
+                *reinterpret_cast<const uint4 *>(sA + row * LDH + (lane & 3) * 8);
+    }
 }
 
 // Load a [128][32] BF16 tile of rows base.. into shared memory (row stride LDH).
@@ -802,13 +939,15 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
     const int nb = gnn_blocks(g.n);
     k_gnn_scales<T><<<reduce_grid(g.n), MCB_THREADS, 0, s>>>(g.n, in, w.partials, w.counter, w.scales);
     k_gnn_encode<T><<<nb, GNN_TILE, 0, s>>>(g, in, p, w.scales, w.h[0]);
+    cudaFuncSetAttribute(k_gnn_layer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LAYER_SMEM);
+    cudaFuncSetAttribute(k_gnn_layer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LAYER_SMEM);
     for (int l = 0; l < GNN_L; l++) {
         const float *pl = p + GP_LAYER0 + l * GPL_SIZE;
         const bf16 *pkl = pk + GK_LAYER0 + l * GKL_SIZE;
         if (w.train)
-            k_gnn_layer<true><<<nb, GNN_TILE, 0, s>>>(g, pl, pkl, w.h[l], w.h[l + 1], w.a[l]);
+            k_gnn_layer<true><<<nb, LAYER_THREADS, LAYER_SMEM, s>>>(g, pl, pkl, w.h[l], w.h[l + 1], w.a[l]);
         else
-            k_gnn_layer<false><<<nb, GNN_TILE, 0, s>>>(g, pl, pkl, w.h[l & 1], w.h[(l + 1) & 1], nullptr);
+            k_gnn_layer<false><<<nb, LAYER_THREADS, LAYER_SMEM, s>>>(g, pl, pkl, w.h[l & 1], w.h[(l + 1) & 1], nullptr);
     }
     const bf16 *hl = w.train ? w.h[GNN_L] : w.h[GNN_L & 1];
     if (w.train)

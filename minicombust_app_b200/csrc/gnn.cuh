@@ -20,8 +20,9 @@
 // difference (the pressure-correction system is singular in the constant).
 //
 // The dense products run on the tensor cores as mma.sync m16n8k16 BF16 tiles
-// of 128 cells per block; the gathers put one channel per lane so a
-// neighbour's 32-channel row is one 64-byte load.
+// of 128 cells per block.  The forward gather stages a tile's own and
+// neighbour rows in shared memory with asynchronous 16-byte copies, all in
+// flight at once; the backward gathers put one channel per lane.
 #pragma once
 
 #include <stdint.h>
@@ -67,15 +68,26 @@ constexpr int GNN_NPACK = GK_WD + GNN_H * GNN_H;
 
 struct GnnScales {
     double sb, sd, sx, shift;
+    double rb, rd, rx;   // reciprocals (0 where the scale is 0)
 };
 
-// Graph in the solver's cell order: 7-point ELL columns (unused slots hold
-// the row itself), per-slot face features, normalised volumes.
+// Graph in the solver's cell order.  Slot k is direction k of the
+// reference's cell_faces (FRONT, BACK, LEFT, RIGHT, DOWN, UP): col[k][i] is
+// the neighbour through it (the row itself on the boundary), edge[k][i] its
+// face features, vhat the normalised volumes.
+// Offset form (`affine`): every internal slot k of every cell i has the
+// neighbour i + doff[k] and the face features ebits[k] -- a uniform box in
+// x-fastest order; mask[i] bit k marks the internal slots.  The forward
+// kernels then need neither col nor edge.
 struct GnnGraph {
     int n;
     const int *col;                  // [6][n]
     const __nv_bfloat162 *edge;      // [6][n]
     const float *vhat;               // [n]
+    int affine;
+    int doff[6];
+    uint32_t ebits[6];
+    const uint8_t *mask;             // [n], nullptr unless affine
 };
 
 // One sample's raw inputs (device arrays of length n, type T).
@@ -127,10 +139,13 @@ int gnn_forward_launches();
 void gnn_loss_backward(cudaStream_t s, const GnnGraph &g, const GnnInput<float> &in, const float *target,
                        const float *p, const __nv_bfloat16 *pk, GnnWork &w, float *grad, float weight);
 
-// Host: graph arrays of a solver mesh (its own numbering): ELL columns, the
-// per-slot face features as BF16 pairs, normalised volumes.
+// Host: graph arrays of a solver mesh (its own numbering): direction-slot
+// columns, the per-slot face features as BF16 pairs, normalised volumes.
+// `aff` receives the offset form when it applies (aff.affine = 1, mask
+// filled), else aff.affine = 0 and mask is empty.
 struct HostMesh;
-void gnn_graph_host(const HostMesh &hm, std::vector<int> &col, std::vector<uint32_t> &edge, std::vector<float> &vhat);
+void gnn_graph_host(const HostMesh &hm, std::vector<int> &col, std::vector<uint32_t> &edge, std::vector<float> &vhat,
+                    GnnGraph &aff, std::vector<uint8_t> &mask);
 
 // Adam with bias correction; step t >= 1.
 void gnn_adam(cudaStream_t s, float *p, const float *grad, float *m, float *v, float lr, float b1, float b2, float eps,

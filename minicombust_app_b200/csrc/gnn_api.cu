@@ -1,5 +1,6 @@
 // C ABI of the learned guess network (include/minicombust_gnn.h).
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -12,7 +13,8 @@
 
 namespace mcb {
 
-void gnn_graph_host(const HostMesh &hm, std::vector<int> &col, std::vector<uint32_t> &edge, std::vector<float> &vhat)
+void gnn_graph_host(const HostMesh &hm, std::vector<int> &col, std::vector<uint32_t> &edge, std::vector<float> &vhat,
+                    GnnGraph &aff, std::vector<uint8_t> &mask)
 {
     const int N = hm.N;
     double asum = 0.0, rsum = 0.0;
@@ -24,12 +26,19 @@ void gnn_graph_host(const HostMesh &hm, std::vector<int> &col, std::vector<uint3
             cnt++;
         }
     const double ra = cnt && asum > 0 ? cnt / asum : 0.0, rr = cnt && rsum > 0 ? cnt / rsum : 0.0;
-    col = hm.col;
+    // slot k = direction k (the sum over neighbours does not depend on the
+    // slot order; a direction order makes the offsets of a box constant)
+    col.assign((size_t)6 * N, 0);
     edge.assign((size_t)6 * N, 0u);
     for (int k = 0; k < 6; k++)
         for (int i = 0; i < N; i++) {
-            const int f = hm.sface[(size_t)k * N + i];
-            if (hm.fc1[f] >= N) continue;
+            const int j = hm.nbr[(size_t)k * N + i];
+            col[(size_t)k * N + i] = j >= 0 ? j : i;
+            if (j < 0) continue;
+            int f = -1;
+            for (int s = 0; s < 6; s++)
+                if (hm.col[(size_t)s * N + i] == j) f = hm.sface[(size_t)s * N + i];
+            if (f < 0) continue;
             const __nv_bfloat162 e = __floats2bfloat162_rn((float)(hm.area[f] * ra), (float)(hm.rl[f] * rr));
             uint32_t bits;
             std::memcpy(&bits, &e, 4);
@@ -40,6 +49,35 @@ void gnn_graph_host(const HostMesh &hm, std::vector<int> &col, std::vector<uint3
     const double rv = vsum > 0 ? N / vsum : 0.0;
     vhat.resize(N);
     for (int i = 0; i < N; i++) vhat[i] = (float)(hm.vol[i] * rv);
+    // offset form
+    aff.affine = 0;
+    mask.clear();
+    bool ok = true, seen[6] = {false, false, false, false, false, false};
+    std::vector<uint8_t> mk(N, 0);
+    for (int k = 0; k < 6 && ok; k++)
+        for (int i = 0; i < N; i++) {
+            const int j = col[(size_t)k * N + i];
+            if (j == i) continue;
+            const uint32_t e = edge[(size_t)k * N + i];
+            if (!seen[k]) {
+                seen[k] = true;
+                aff.doff[k] = j - i;
+                aff.ebits[k] = e;
+            } else if (j - i != aff.doff[k] || e != aff.ebits[k]) {
+                ok = false;
+                break;
+            }
+            mk[i] |= (uint8_t)(1u << k);
+        }
+    if (ok) {
+        for (int k = 0; k < 6; k++)
+            if (!seen[k]) {
+                aff.doff[k] = 0;
+                aff.ebits[k] = 0u;
+            }
+        aff.affine = 1;
+        mask.swap(mk);
+    }
 }
 
 } // namespace mcb
@@ -65,6 +103,14 @@ struct mc_gnn_graph {
 };
 
 namespace {
+
+// MC_GNN_GENERAL_GATHER=1 keeps the general (column-list) gather even where
+// the offset form applies; the tests use it to check both paths.
+bool gnn_force_general()
+{
+    const char *v = std::getenv("MC_GNN_GENERAL_GATHER");
+    return v && v[0] == '1';
+}
 
 int cuda_status(cudaError_t e) { return e == cudaSuccess ? MC_OK : (e == cudaErrorMemoryAllocation ? MC_ERR_NOMEM : MC_ERR_CUDA); }
 
@@ -177,23 +223,26 @@ int mc_gnn_graph_create(mc_gnn *net, const mc_mesh_view *mesh, mc_gnn_graph **ou
     std::vector<int> col;
     std::vector<uint32_t> edge;
     std::vector<float> vhat;
+    std::vector<uint8_t> mask;
+    GnnGraph aff{};
     try {
         const int rc = build_host_mesh(mesh, HostPhysics{1.0}, hm, err);
         if (rc) return rc;
-        gnn_graph_host(hm, col, edge, vhat);
+        gnn_graph_host(hm, col, edge, vhat, aff, mask);
     } catch (const std::bad_alloc &) {
         return MC_ERR_NOMEM;
     }
     mc_gnn_graph *gr = new (std::nothrow) mc_gnn_graph();
     if (!gr) return MC_ERR_NOMEM;
     const int N = hm.N;
-    const size_t cb = (size_t)6 * N * 4, eb = (size_t)6 * N * 4, vb = (size_t)N * 4;
+    const size_t cb = (size_t)6 * N * 4, eb = (size_t)6 * N * 4, vb = (size_t)N * 4, mb = mask.size();
     gr->dev = net->dev;
     int rc = cuda_status(cudaSetDevice(net->dev));
-    if (!rc) rc = cuda_status(cudaMalloc((void **)&gr->mem, cb + eb + vb));
+    if (!rc) rc = cuda_status(cudaMalloc((void **)&gr->mem, cb + eb + vb + mb));
     if (!rc) rc = cuda_status(cudaMemcpy(gr->mem, col.data(), cb, cudaMemcpyHostToDevice));
     if (!rc) rc = cuda_status(cudaMemcpy(gr->mem + cb, edge.data(), eb, cudaMemcpyHostToDevice));
     if (!rc) rc = cuda_status(cudaMemcpy(gr->mem + cb + eb, vhat.data(), vb, cudaMemcpyHostToDevice));
+    if (!rc && mb) rc = cuda_status(cudaMemcpy(gr->mem + cb + eb + vb, mask.data(), mb, cudaMemcpyHostToDevice));
     if (rc) {
         mc_gnn_graph_destroy(gr);
         return rc;
@@ -202,6 +251,12 @@ int mc_gnn_graph_create(mc_gnn *net, const mc_mesh_view *mesh, mc_gnn_graph **ou
     gr->g.col = reinterpret_cast<const int *>(gr->mem);
     gr->g.edge = reinterpret_cast<const __nv_bfloat162 *>(gr->mem + cb);
     gr->g.vhat = reinterpret_cast<const float *>(gr->mem + cb + eb);
+    gr->g.affine = aff.affine && !gnn_force_general();
+    for (int k = 0; k < 6; k++) {
+        gr->g.doff[k] = aff.doff[k];
+        gr->g.ebits[k] = aff.ebits[k];
+    }
+    gr->g.mask = mb ? reinterpret_cast<const uint8_t *>(gr->mem + cb + eb + vb) : nullptr;
     *out = gr;
     return MC_OK;
 }

@@ -339,59 +339,86 @@ __global__ void __launch_bounds__(MCB_THREADS) k_ir_init(Ell A, const double *__
     }
 }
 
+__device__ __forceinline__ double ell_row(const Ell &A, const double *__restrict__ x, int i)
+{
+    double ax = A.diag[i] * x[i];
+#pragma unroll
+    for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * A.N + i] * x[A.col[(size_t)k * A.N + i]];
+    return ax;
+}
+
+// Dot products of b' = b - mean, u = A xa and w = A xb; the last block
+// solves the 2 x 2 least-squares problem min ||b' - alpha u - beta w||
+// (1 x 1 when a candidate is absent or the two are colinear).
 __global__ void __launch_bounds__(MCB_THREADS) k_guess_residuals(Ell A, const double *__restrict__ b,
                                                                  const PcgState *__restrict__ st,
                                                                  const double *__restrict__ xa,
                                                                  const double *__restrict__ xb, GuessState *gs,
                                                                  double *partials, unsigned int *counter)
 {
-    __shared__ double sh[3][MCB_THREADS];
+    __shared__ double sh[8][MCB_THREADS];
     const int N = A.N;
     const double mean = st->mean;
-    double acc[3] = {0.0, 0.0, 0.0};
+    // bb, bu, bw, uu, uw, ww, |b'-u|^2, |b'-w|^2
+    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const double bi = b[i] - mean;
+        const double u = xa ? ell_row(A, xa, i) : 0.0;
+        const double w = xb ? ell_row(A, xb, i) : 0.0;
         acc[0] += bi * bi;
-        if (xa) {
-            double ax = A.diag[i] * xa[i];
-#pragma unroll
-            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * xa[A.col[(size_t)k * N + i]];
-            acc[1] += (bi - ax) * (bi - ax);
-        }
-        if (xb) {
-            double ax = A.diag[i] * xb[i];
-#pragma unroll
-            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * xb[A.col[(size_t)k * N + i]];
-            acc[2] += (bi - ax) * (bi - ax);
-        }
+        acc[1] += bi * u;
+        acc[2] += bi * w;
+        acc[3] += u * u;
+        acc[4] += u * w;
+        acc[5] += w * w;
+        acc[6] += (bi - u) * (bi - u);
+        acc[7] += (bi - w) * (bi - w);
     }
-    if (publish_partials<3>(acc, partials, counter, sh)) {
-        double tot[3];
-        reduce_partials<3>(tot, partials, counter, sh);
+    if (publish_partials<8>(acc, partials, counter, sh)) {
+        double t[8];
+        reduce_partials<8>(t, partials, counter, sh);
         if (threadIdx.x == 0) {
-            gs->bb = tot[0];
-            gs->rr[0] = xa ? tot[1] : -1.0;
-            gs->rr[1] = xb ? tot[2] : -1.0;
-            int choice = -1;
-            double best = tot[0];
-            if (xa && finite(tot[1]) && tot[1] < best) {
-                choice = 0;
-                best = tot[1];
+            const double bb = t[0], bu = t[1], bw = t[2], uu = t[3], uw = t[4], ww = t[5];
+            gs->bb = bb;
+            gs->rr[0] = xa ? t[6] : -1.0;
+            gs->rr[1] = xb ? t[7] : -1.0;
+            double al = 0.0, be = 0.0;
+            const bool ha = xa && uu > 0 && finite(uu), hb = xb && ww > 0 && finite(ww);
+            const double det = uu * ww - uw * uw;
+            if (ha && hb && det > 1e-12 * uu * ww) {
+                al = (bu * ww - bw * uw) / det;
+                be = (bw * uu - bu * uw) / det;
+            } else if (hb) {
+                be = bw / ww;
+            } else if (ha) {
+                al = bu / uu;
             }
-            if (xb && finite(tot[2]) && tot[2] < best) choice = 1;
+            // residual of the combination: bb - 2 (al bu + be bw) + |al u + be w|^2
+            double rc = bb - 2.0 * (al * bu + be * bw) + (al * al * uu + 2.0 * al * be * uw + be * be * ww);
+            int choice = 2;
+            if (!finite(rc) || !(rc < bb) || !finite(al) || !finite(be)) {
+                choice = -1;
+                al = be = 0.0;
+                rc = bb;
+            }
+            gs->coef[0] = al;
+            gs->coef[1] = be;
+            gs->rc = fmax(rc, 0.0);
             gs->choice = choice;
         }
     }
 }
 
+// x = alpha xa + beta xb (zero for choice -1).
 __global__ void __launch_bounds__(MCB_THREADS) k_guess_apply(int N, double *__restrict__ x,
                                                              const double *__restrict__ xa,
                                                              const double *__restrict__ xb,
                                                              const GuessState *__restrict__ gs)
 {
-    const int c = gs->choice;
-    const double *src = c == 0 ? xa : (c == 1 ? xb : nullptr);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) x[i] = src ? src[i] : 0.0;
+    const double al = gs->coef[0], be = gs->coef[1];
+    const bool ua = xa && al != 0.0, ub = xb && be != 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+        x[i] = (ua ? al * xa[i] : 0.0) + (ub ? be * xb[i] : 0.0);
 }
 
 __global__ void __launch_bounds__(MCB_THREADS) k_ir_add(int N, double *__restrict__ x, const float *__restrict__ e,

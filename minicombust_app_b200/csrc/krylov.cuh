@@ -103,13 +103,15 @@ void pcg_iter2_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, in
 void ir_init(cudaStream_t s, const Ell &A, const double *b, double *x, double *r, float *r32, PcgState *st,
              double *partials, unsigned int *counter, double rtol, double abs_floor, int max_outer, int use_x0 = 0);
 
-// Initial-guess selection for the pressure correction: the squared
-// residuals ||b' - A x_c||^2 of up to two candidates (b' = b - st->mean;
-// a null candidate is skipped) against ||b'||^2 of the zero guess; the
-// smallest wins.  guess_apply writes the winner into x.
+// Initial guess of the pressure correction from up to two candidates xa, xb
+// (a null candidate is skipped): the combination x0 = alpha xa + beta xb
+// that minimises ||b' - A x0|| (b' = b - st->mean).  Zero lies in the span,
+// so the guess never starts from a larger residual than the zero guess; if
+// rounding says otherwise the zero guess is used.  rr[] are the residuals of
+// the single candidates, rc that of the combination.
 struct GuessState {
-    double bb, rr[2];
-    int choice;   // -1 zero, 0 candidate a, 1 candidate b
+    double bb, rr[2], coef[2], rc;
+    int choice;   // -1 zero, 2 combination
     int pad;
 };
 void guess_residuals(cudaStream_t s, const Ell &A, const double *b, const PcgState *st, const double *xa,

@@ -78,9 +78,13 @@ def test_graph_export_matches_the_mesh(gpu):
     assert abs(vhat.mean() - 1.0) < 1e-6
 
 
+@pytest.mark.parametrize("gather", ["offset", "general"])
 @pytest.mark.parametrize("dims", [(16, 8, 8), (9, 5, 3)])
-def test_forward_matches_oracle(gpu, dims):
+def test_forward_matches_oracle(gpu, dims, gather, monkeypatch):
+    """Both gathers: the constant-offset form of a box mesh and the general column list."""
     import torch
+    if gather == "general":
+        monkeypatch.setenv("MC_GNN_GENERAL_GATHER", "1")
     net, gr, graph, host, dev = setup(dims, seed=1)
     p = net.params().astype(np.float64)
     b, diag, prev, _ = host[0]
