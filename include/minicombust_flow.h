@@ -107,7 +107,9 @@ typedef struct mc_flow_params {
     int amg_sweeps;           /* MC_PSOLVER_PCG_AMG: damped-Jacobi sweeps before and after the coarse correction */
     double amg_omega;         /* Jacobi damping */
     double amg_alpha;         /* coarse-correction scaling */
-    double ir_inner_rtol;     /* MC_PRECISION_FP32_REFINED: relative tolerance of each inner FP32 solve */
+    double ir_inner_rtol;     /* MC_PRECISION_FP32_REFINED: each inner FP32 solve reduces its residual by
+                                 the factor still missing to p_rtol (with a margin of 2), but by no less
+                                 than this: the smallest relative tolerance asked of an FP32 solve */
     int reorder;              /* MC_REORDER_* */
 } mc_flow_params;
 

@@ -31,7 +31,8 @@ enum KernelId {
     K_PCG_ITER2, K_PCG_XMEAN, K_PCG_SUBMEAN, K_BICG3_INIT, K_BICG3_1, K_BICG3_2, K_BICG3_3, K_BICG1_INIT,
     K_BICG1_1, K_BICG1_2, K_BICG1_3, K_AMG_SETUP, K_PCG_INIT_AMG, K_PCG_ITER2_AMG, K_AMG_VCYCLE,
     K_IR, K_PCG_INIT_AMG32, K_PCG_ITER1_32, K_PCG_ITER2_AMG32, K_AMG_VCYCLE32, K_PERMUTE, K_GUESS, K_GNN,
-    K_SNAPSHOT, K_COUNT
+    K_SNAPSHOT, K_BIR, K_ROUND_ELL, K_BICG3_INIT32, K_BICG3_1_32, K_BICG3_2_32, K_BICG3_3_32, K_BICG1_INIT32,
+    K_BICG1_1_32, K_BICG1_2_32, K_BICG1_3_32, K_COUNT
 };
 
 const char *kKernelNames[K_COUNT] = {
@@ -42,7 +43,9 @@ const char *kKernelNames[K_COUNT] = {
     "bicg1_init", "bicg1_1_spmv", "bicg1_2_spmv", "bicg1_3_update", "amg_setup_galerkin_factor",
     "pcg_init_amg", "pcg_iter2_amg_update", "amg_vcycle", "ir_fp64_residual_update", "pcg32_init_amg",
     "pcg32_iter1_spmv", "pcg32_iter2_amg_update", "amg32_vcycle", "permute", "guess_select", "gnn_forward",
-    "snapshot_pack"};
+    "snapshot_pack", "bicg_refine_fp64_residual", "round_fp32", "bicg3_32_init", "bicg3_32_1_spmv",
+    "bicg3_32_2_spmv", "bicg3_32_3_update", "bicg1_32_init", "bicg1_32_1_spmv", "bicg1_32_2_spmv",
+    "bicg1_32_3_update"};
 
 constexpr int PCG_BATCH = 16;   // iterations per status read (even: ping-pong buffers)
 constexpr int PCG_AMG_BATCH = 4;
@@ -122,6 +125,18 @@ struct mc_flow {
     float *r32 = nullptr;
     PcgState *h_pcg_inner = nullptr;  // pinned
     cudaGraphExec_t g_pcg_amg32 = nullptr;
+    // FP32-refined momentum and temperature solves
+    float *m32_diag = nullptr, *m32_off = nullptr, *t32_diag = nullptr, *t32_off = nullptr;
+    BicgVectorsT<float, 3> bi3{};
+    BicgVectorsT<float, 1> bi1{};
+    BirVectors<3> bo3{};
+    BirVectors<1> bo1{};
+    BicgState<3> *h_bi3 = nullptr;   // pinned
+    BicgState<1> *h_bi1 = nullptr;
+    BirState<3> *h_bo3 = nullptr;
+    BirState<1> *h_bo1 = nullptr;
+    cudaGraphExec_t g_b3_32 = nullptr, g_b1_32 = nullptr;
+    char *bir_mem = nullptr;
     // initial guess of the pressure correction
     double *pp_prev = nullptr;        // previous converged correction [N]
     GuessState *gs = nullptr;
@@ -415,8 +430,13 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
         flush_timing(h);
         if (h->h_pcg->done) break;
         if (outer > kMaxOuter) return fail(h, MC_ERR_NOT_CONVERGED, "refinement state did not advance");
+        // each inner solve asks for the reduction still missing (with a
+        // margin of 2), but never for less than ir_inner_rtol
+        const PcgState &os = *h->h_pcg;
+        double inner_rtol = os.rr > 0 ? 0.5 * std::sqrt(os.tol2 / os.rr) : h->prm.ir_inner_rtol;
+        inner_rtol = std::min(0.5, std::max(h->prm.ir_inner_rtol, inner_rtol));
         launch(h, K_PCG_INIT_AMG32,
-               [&] { pcg_init_amg<float>(h->stream, A32, in, h->prm.ir_inner_rtol, 0.0, h->prm.max_iters, 0); });
+               [&] { pcg_init_amg<float>(h->stream, A32, in, inner_rtol, 0.0, h->prm.max_iters, 0); });
         launch(h, K_AMG_VCYCLE32,
                [&] { amg_vcycle<float>(h->stream, h->amg, in.r, in.zp[0], in.st, in.partials, in.counter, 1); });
         h->launches += amg_kernels_per_vcycle(h->amg) - 1;
@@ -489,6 +509,66 @@ int solve_bicg(mc_flow *h, const Ell &A, const BicgVectors<R> &v, BicgState<R> *
         iters_out[j] = hs->iter[j];
         const int s = krylov_status_to_mc(hs->status[j]);
         if (s == MC_ERR_NONFINITE || worst == MC_OK) worst = (s != MC_OK) ? s : worst;
+    }
+    return worst;
+}
+
+// FP64 iterative refinement around FP32 BiCGStab solves (momentum, R = 3;
+// temperature, R = 1): each inner solve asks for the reduction still missing
+// (margin 2, floor ir_inner_rtol); the outer loop stops on the FP64 true
+// residual, ||b - A x|| <= u_rtol ||b|| per system.
+template <int R>
+int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const BicgVectorsT<float, R> &in,
+                       const BirVectors<R> &out, BicgState<R> *hin, BirState<R> *hout, cudaGraphExec_t *exec,
+                       int kid_init32, int kid1_32, int iters_out[R])
+{
+    constexpr int kMaxOuter = 30;
+    launch(h, K_BIR, [&] { bir_init<R>(h->stream, A, out, h->prm.u_rtol, kMaxOuter); });
+    int rc = check_launch(h);
+    if (rc) return rc;
+    for (int j = 0; j < R; j++) iters_out[j] = 0;
+    const long max_batches = h->prm.max_iters / BICG_BATCH + 2;
+    for (int outer = 0;; outer++) {
+        CUDA_TRY(h, cudaMemcpyAsync(hout, out.st, sizeof(BirState<R>), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        flush_timing(h);
+        if (hout->all_done) break;
+        if (outer > kMaxOuter) return fail(h, MC_ERR_NOT_CONVERGED, "refinement state did not advance");
+        double inner_rtol = 0.5;
+        for (int j = 0; j < R; j++)
+            if (!hout->done[j] && hout->rr[j] > 0)
+                inner_rtol = std::min(inner_rtol, 0.5 * std::sqrt(hout->tol2[j] / hout->rr[j]));
+        inner_rtol = std::max(inner_rtol, h->prm.ir_inner_rtol);
+        launch(h, kid_init32, [&] { bicg_init_t<float, R>(h->stream, A32, in, inner_rtol, h->prm.max_iters); });
+        for (long batch = 0;; batch++) {
+            CUDA_TRY(h, cudaMemcpyAsync(hin, in.st, sizeof(BicgState<R>), cudaMemcpyDeviceToHost, h->stream));
+            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+            flush_timing(h);
+            if (hin->all_done) break;
+            if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "BiCGStab state did not advance");
+            rc = run_batch(h, exec, BICG_BATCH * BICG_KERNELS_PER_ITER, [&] {
+                for (int it = 0; it < BICG_BATCH; it++) {
+                    const int pin = it & 1;
+                    launch(h, kid1_32, [&] { bicg_1_t<float, R>(h->stream, A32, in, pin); });
+                    launch(h, kid1_32 + 1, [&] { bicg_2_t<float, R>(h->stream, A32, in, pin ^ 1); });
+                    launch(h, kid1_32 + 2, [&] { bicg_3_t<float, R>(h->stream, A32, in, pin ^ 1); });
+                }
+            });
+            if (rc) return rc;
+        }
+        for (int j = 0; j < R; j++) {
+            iters_out[j] += hin->iter[j];
+            if (hin->status[j] == KRYLOV_NONFINITE) return fail(h, MC_ERR_NONFINITE, "inner FP32 BiCGStab");
+        }
+        launch(h, K_BIR, [&] { bir_add<R>(h->stream, A.N, out); });
+        launch(h, K_BIR, [&] { bir_residual<R>(h->stream, A, out); });
+        rc = check_launch(h);
+        if (rc) return rc;
+    }
+    int worst = MC_OK;
+    for (int j = 0; j < R; j++) {
+        const int st = krylov_status_to_mc(hout->status[j]);
+        if (st == MC_ERR_NONFINITE || worst == MC_OK) worst = (st != MC_OK) ? st : worst;
     }
     return worst;
 }
@@ -591,7 +671,14 @@ int stage_momentum(mc_flow *h, mc_iter_stats *st)
     int rc = check_launch(h);
     if (rc) return rc;
     int its[3] = {0, 0, 0};
-    rc = solve_bicg<3>(h, momentum_matrix(h), h->b3, h->h_b3, &h->g_b3, K_BICG3_INIT, K_BICG3_1, its);
+    if (h->bir_mem) {
+        launch(h, K_ROUND_ELL, [&] { round_ell(h->stream, h->N, h->AU, h->off_m, h->m32_diag, h->m32_off); });
+        const EllT<float> A32{h->N, h->m32_diag, h->m32_off, h->col};
+        rc = solve_bicg_refined<3>(h, momentum_matrix(h), A32, h->bi3, h->bo3, h->h_bi3, h->h_bo3, &h->g_b3_32,
+                                   K_BICG3_INIT32, K_BICG3_1_32, its);
+    } else {
+        rc = solve_bicg<3>(h, momentum_matrix(h), h->b3, h->h_b3, &h->g_b3, K_BICG3_INIT, K_BICG3_1, its);
+    }
     if (st)
         for (int j = 0; j < 3; j++) st->momentum_iters[j] = its[j];
     return rc;
@@ -717,7 +804,14 @@ int stage_temperature(mc_flow *h, mc_iter_stats *st)
     int rc = check_launch(h);
     if (rc) return rc;
     int its[1] = {0};
-    rc = solve_bicg<1>(h, temperature_matrix(h), h->b1, h->h_b1, &h->g_b1, K_BICG1_INIT, K_BICG1_1, its);
+    if (h->bir_mem) {
+        launch(h, K_ROUND_ELL, [&] { round_ell(h->stream, h->N, h->diag_t, h->off_t, h->t32_diag, h->t32_off); });
+        const EllT<float> A32{h->N, h->t32_diag, h->t32_off, h->col};
+        rc = solve_bicg_refined<1>(h, temperature_matrix(h), A32, h->bi1, h->bo1, h->h_bi1, h->h_bo1, &h->g_b1_32,
+                                   K_BICG1_INIT32, K_BICG1_1_32, its);
+    } else {
+        rc = solve_bicg<1>(h, temperature_matrix(h), h->b1, h->h_b1, &h->g_b1, K_BICG1_INIT, K_BICG1_1, its);
+    }
     if (st) st->temperature_iters = its[0];
     return rc;
 }
@@ -851,6 +945,67 @@ int initial_fields(mc_flow *h, const int btype[6])
     rc = rc ? rc : put(G_PP, 0.0, 0.0, 0.0, 0.0);
     rc = rc ? rc : put(G_T, p.temperature0, p.temperature0, p.temperature0, p.temperature0);
     return rc;
+}
+
+// FP32-refined momentum and temperature solves: FP32 matrix copies, the
+// inner BiCGStab vectors (shared by the two solves, which never overlap) and
+// the refinement state, in one device allocation.
+int setup_bicg_refined(mc_flow *h)
+{
+    const size_t N = (size_t)h->N;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t m7 = al(7 * N * 4), v3 = al(3 * N * 4);
+    const size_t total = 2 * m7 + 11 * v3 + 4 * al(512);
+    const cudaError_t e = cudaMalloc((void **)&h->bir_mem, total);
+    if (e != cudaSuccess) return fail(h, MC_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    CUDA_TRY(h, cudaMemset(h->bir_mem, 0, total));
+    char *c = h->bir_mem;
+    auto take = [&](size_t b) { char *p = c; c += b; return p; };
+    h->m32_diag = reinterpret_cast<float *>(take(m7));
+    h->m32_off = h->m32_diag + N;
+    h->t32_diag = reinterpret_cast<float *>(take(m7));
+    h->t32_off = h->t32_diag + N;
+    float *vec[11];
+    for (int k = 0; k < 11; k++) vec[k] = reinterpret_cast<float *>(take(v3));
+    BicgState<3> *st3 = reinterpret_cast<BicgState<3> *>(take(al(512)));
+    BicgState<1> *st1 = reinterpret_cast<BicgState<1> *>(take(al(512)));
+    BirState<3> *bo3 = reinterpret_cast<BirState<3> *>(take(al(512)));
+    BirState<1> *bo1 = reinterpret_cast<BirState<1> *>(take(al(512)));
+    // vec: 0 e (inner solution), 1 r32 (inner right-hand side), 2 r, 3 r0, 4-5 p, 6-7 v, 8 s, 9 t
+    for (int j = 0; j < 3; j++) h->bi3.x[j] = vec[0] + j * N;
+    h->bi3.b = vec[1];
+    h->bi3.r = vec[2];
+    h->bi3.r0 = vec[3];
+    h->bi3.p[0] = vec[4];
+    h->bi3.p[1] = vec[5];
+    h->bi3.v[0] = vec[6];
+    h->bi3.v[1] = vec[7];
+    h->bi3.s = vec[8];
+    h->bi3.t = vec[9];
+    h->bi3.partials = h->partials;
+    h->bi3.counter = h->counter;
+    h->bi3.st = st3;
+    h->bi1.x[0] = vec[0];
+    h->bi1.b = vec[1];
+    h->bi1.r = vec[2];
+    h->bi1.r0 = vec[3];
+    h->bi1.p[0] = vec[4];
+    h->bi1.p[1] = vec[5];
+    h->bi1.v[0] = vec[6];
+    h->bi1.v[1] = vec[7];
+    h->bi1.s = vec[8];
+    h->bi1.t = vec[9];
+    h->bi1.partials = h->partials;
+    h->bi1.counter = h->counter;
+    h->bi1.st = st1;
+    h->bo3 = BirVectors<3>{{h->phi[G_U], h->phi[G_V], h->phi[G_W]}, h->b_m, vec[1], vec[0], h->partials, h->counter,
+                           bo3};
+    h->bo1 = BirVectors<1>{{h->phi[G_T]}, h->b_t, vec[1], vec[0], h->partials, h->counter, bo1};
+    CUDA_TRY(h, cudaMallocHost((void **)&h->h_bi3, sizeof(BicgState<3>)));
+    CUDA_TRY(h, cudaMallocHost((void **)&h->h_bi1, sizeof(BicgState<1>)));
+    CUDA_TRY(h, cudaMallocHost((void **)&h->h_bo3, sizeof(BirState<3>)));
+    CUDA_TRY(h, cudaMallocHost((void **)&h->h_bo1, sizeof(BirState<1>)));
+    return MC_OK;
 }
 
 // Guess state (pinned copy) and, for MC_GUESS_LEARNED, the network's graph,
@@ -1053,7 +1208,7 @@ void mc_flow_default_params(mc_flow_params *p, int mode)
     p->amg_sweeps = 2;
     p->amg_omega = 0.6667;
     p->amg_alpha = 1.8;
-    p->ir_inner_rtol = 1e-2;
+    p->ir_inner_rtol = 1e-4;
     p->reorder = MC_REORDER_NONE;
     if (mode == MC_MODE_COMPAT) {
         p->viscosity = 0.000014;
@@ -1156,6 +1311,7 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
             rc = rc ? rc : initial_fields(h, hm.btype);
             if (!rc && params->pressure_solver == MC_PSOLVER_PCG_AMG) rc = build_amg(h, hm);
             if (!rc) rc = setup_guess(h, hm);
+            if (!rc && params->precision == MC_PRECISION_FP32_REFINED) rc = setup_bicg_refined(h);
         }
         if (!rc) {
             h->hcol.assign((size_t)6 * hm.N, -1);
@@ -1209,7 +1365,7 @@ int mc_flow_destroy(mc_flow *h)
 {
     if (!h) return MC_ERR_ARG;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    for (cudaGraphExec_t g : {h->g_pcg, h->g_b3, h->g_b1, h->g_pcg_amg, h->g_pcg_amg32})
+    for (cudaGraphExec_t g : {h->g_pcg, h->g_b3, h->g_b1, h->g_pcg_amg, h->g_pcg_amg32, h->g_b3_32, h->g_b1_32})
         if (g) cudaGraphExecDestroy(g);
     if (h->amg_mem) cudaFree(h->amg_mem);
     for (cudaEvent_t e : h->timing.ev) cudaEventDestroy(e);
@@ -1222,6 +1378,9 @@ int mc_flow_destroy(mc_flow *h)
     if (h->snap) mc_flow_snapshot_close(h);
     if (h->h_gs) cudaFreeHost(h->h_gs);
     if (h->gnn_mem) cudaFree(h->gnn_mem);
+    if (h->bir_mem) cudaFree(h->bir_mem);
+    for (void *p : {(void *)h->h_bi3, (void *)h->h_bi1, (void *)h->h_bo3, (void *)h->h_bo1})
+        if (p) cudaFreeHost(p);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return MC_OK;

@@ -22,7 +22,6 @@ using bf16 = __nv_bfloat16;
 using bf162 = __nv_bfloat162;
 
 constexpr int LDH = GNN_H + 8;        // row stride (elements) of [cell][32] tiles
-constexpr int LDU = 2 * GNN_H + 8;    // row stride of [cell][64] tiles
 constexpr int LDT = GNN_TILE + 8;     // row stride of transposed [channel][cell] tiles
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -403,6 +402,120 @@ __global__ void __launch_bounds__(LAYER_THREADS) k_gnn_layer(GnnGraph g, const f
         }
     __syncwarp();
     // 5. coalesced store of the warp's 16 rows: 4 lanes per 64-byte row
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int row = warp * 16 + (lane >> 2) + 8 * q, i = base + row;
+        if (i < n)
+            *reinterpret_cast<uint4 *>(hout + (size_t)i * GNN_H + (lane & 3) * 8) =
+                *reinterpret_cast<const uint4 *>(sA + row * LDH + (lane & 3) * 8);
+    }
+}
+
+// Offset-form weights of every layer: slot 0 = W1 columns of h_i, slot 1 + k
+// = W1 columns of m with each input channel c scaled by the gate of
+// direction k, g_k[c] = Wg[c] . e_k + cg[c].  Row-major [out][in] per slot.
+__global__ void k_gnn_fold(const float *__restrict__ p, GnnGraph g, bf16 *__restrict__ fold)
+{
+    constexpr int PER_LAYER = 7 * GNN_H * GNN_H;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < GNN_L * PER_LAYER; e += gridDim.x * blockDim.x) {
+        const int l = e / PER_LAYER, r = e % PER_LAYER;
+        const int k = r / (GNN_H * GNN_H), o = (r / GNN_H) % GNN_H, c = r % GNN_H;
+        const float *pl = p + GP_LAYER0 + l * GPL_SIZE;
+        float v;
+        if (k == 0) {
+            v = pl[GPL_W1 + o * 2 * GNN_H + c];
+        } else {
+            const float2 ek = edge_of(g.ebits[k - 1]);
+            const float gate = pl[GPL_WG + 2 * c] * ek.x + pl[GPL_WG + 2 * c + 1] * ek.y + pl[GPL_CG + c];
+            v = pl[GPL_W1 + o * 2 * GNN_H + GNN_H + c] * gate;
+        }
+        fold[e] = __float2bfloat16(v);
+    }
+}
+
+// Shared memory of k_gnn_layer_fold: seven row tiles [7][128][LDH] -- the
+// cells' own rows and their neighbours through the six directions (zeros on
+// the boundary) -- then the layer's weights: the seven folded W1 slots
+// [7][32][LDH] and W2 [32][LDH].
+constexpr size_t FOLD_SMEM_T = sizeof(bf16) * 7 * GNN_TILE * LDH;
+constexpr size_t FOLD_SMEM = FOLD_SMEM_T + sizeof(bf16) * 8 * GNN_H * LDH;
+
+// One message-passing layer on a graph in offset form (inference).
+// z = sum_k T_k Wf_k^T over the seven staged tiles, a = relu(z + c1),
+// h' = h + W2 a + c2; 256 threads, warp w owns rows 16w .. 16w + 15.
+__global__ void __launch_bounds__(LAYER_THREADS) k_gnn_layer_fold(GnnGraph g, const float *__restrict__ pl,
+                                                                  const bf16 *__restrict__ wf,
+                                                                  const bf16 *__restrict__ pkl,
+                                                                  const bf16 *__restrict__ hin,
+                                                                  bf16 *__restrict__ hout)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    bf16 *sT = reinterpret_cast<bf16 *>(smem);
+    bf16 *sW = reinterpret_cast<bf16 *>(smem + FOLD_SMEM_T);  // [8][32][LDH]: 7 folded W1 slots, W2
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int c4 = tid & 3, r0 = tid >> 2;
+    const int n = g.n, base = blockIdx.x * GNN_TILE;
+    // weights: 8 x 32 rows of 64 bytes, 4 chunks per thread
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int e = tid + LAYER_THREADS * q, row = e >> 2, part = e & 3;  // row 0..255
+        const bf16 *src = row < 7 * GNN_H ? wf + (size_t)row * GNN_H : pkl + GKL_W2 + (size_t)(row - 7 * GNN_H) * GNN_H;
+        cp_async16(sW + row * LDH + part * 8, src + part * 8, 16);
+    }
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int r = r0 + 64 * q, i = base + r;
+        const bool in = i < n;
+        cp_async16(sT + r * LDH + c4 * 8, hin + (size_t)(in ? i : 0) * GNN_H + c4 * 8, in ? 16 : 0);
+        const unsigned mk = in ? g.mask[i] : 0u;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const bool ok = (mk >> k) & 1u;
+            const int j = ok ? i + g.doff[k] : 0;
+            cp_async16(sT + ((1 + k) * GNN_TILE + r) * LDH + c4 * 8, hin + (size_t)j * GNN_H + c4 * 8, ok ? 16 : 0);
+        }
+    }
+    const int gq = lane >> 2, tq = lane & 3;
+    float b1[4][2], b2[4][2];
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            b1[nt][e] = pl[GPL_C1 + nt * 8 + 2 * tq + e];
+            b2[nt][e] = pl[GPL_C2 + nt * 8 + 2 * tq + e];
+        }
+    cp_async_wait_all();
+    __syncthreads();
+    float acc[1][4][4];
+    zero(acc);
+#pragma unroll
+    for (int k = 0; k < 7; k++)
+        warp_gemm<1, 4, 2>(acc, sT + (k * GNN_TILE + warp * 16) * LDH, LDH, sW + k * GNN_H * LDH, LDH, lane);
+    __syncwarp();  // the warp's reads of its rows are done; tile 1 rows now take a, then h'
+    bf16 *sA = sT + GNN_TILE * LDH;
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+        for (int hf = 0; hf < 2; hf++) {
+            const int row = warp * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq;
+            *reinterpret_cast<bf162 *>(sA + row * LDH + col) =
+                __floats2bfloat162_rn(fmaxf(acc[0][nt][2 * hf] + b1[nt][0], 0.f),
+                                      fmaxf(acc[0][nt][2 * hf + 1] + b1[nt][1], 0.f));
+        }
+    __syncwarp();
+    zero(acc);
+    warp_gemm<1, 4, 2>(acc, sA + warp * 16 * LDH, LDH, sW + 7 * GNN_H * LDH, LDH, lane);
+    __syncwarp();
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+        for (int hf = 0; hf < 2; hf++) {
+            const int row = warp * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq;
+            const float2 hv = __bfloat1622float2(*reinterpret_cast<const bf162 *>(sT + row * LDH + col));
+            *reinterpret_cast<bf162 *>(sA + row * LDH + col) = __floats2bfloat162_rn(
+                hv.x + (acc[0][nt][2 * hf] + b2[nt][0]), hv.y + (acc[0][nt][2 * hf + 1] + b2[nt][1]));
+        }
+    __syncwarp();
 #pragma unroll
     for (int q = 0; q < 2; q++) {
         const int row = warp * 16 + (lane >> 2) + 8 * q, i = base + row;
@@ -892,6 +1005,7 @@ void gnn_work_carve(GnnWork &w, char *base, int n, bool train)
     for (int l = 0; l < GNN_L; l++) w.a[l] = train ? reinterpret_cast<bf16 *>(take(hb)) : nullptr;
     w.q = train ? reinterpret_cast<bf16 *>(take(hb)) : nullptr;
     w.y = reinterpret_cast<float *>(take((size_t)n * sizeof(float)));
+    w.fold = reinterpret_cast<bf16 *>(take((size_t)GNN_L * 7 * GNN_H * GNN_H * sizeof(bf16)));
     w.dh[0] = train ? reinterpret_cast<float *>(take(fb)) : nullptr;
     w.dh[1] = train ? reinterpret_cast<float *>(take(fb)) : nullptr;
     w.dm = train ? reinterpret_cast<float *>(take(fb)) : nullptr;
@@ -932,25 +1046,37 @@ void gnn_init_params(float *p, uint64_t seed)
 
 void gnn_pack(cudaStream_t s, const float *p, bf16 *pk) { k_gnn_pack<<<32, 256, 0, s>>>(p, pk); }
 
+// train: keep every layer's input and relu(W1 u + c1) for the backward pass
+// (needs a work area carved with train = true); inference ping-pongs h[0],
+// h[1] and uses the offset-form weights where the graph allows.
 template <typename T>
 static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &in, const float *p, const bf16 *pk,
-                         GnnWork &w, double *x0)
+                         GnnWork &w, double *x0, bool train)
 {
     const int nb = gnn_blocks(g.n);
     k_gnn_scales<T><<<reduce_grid(g.n), MCB_THREADS, 0, s>>>(g.n, in, w.partials, w.counter, w.scales);
     k_gnn_encode<T><<<nb, GNN_TILE, 0, s>>>(g, in, p, w.scales, w.h[0]);
-    cudaFuncSetAttribute(k_gnn_layer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LAYER_SMEM);
-    cudaFuncSetAttribute(k_gnn_layer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LAYER_SMEM);
+    const bool folded = !train && g.affine;
+    if (folded) {
+        k_gnn_fold<<<(GNN_L * 7 * GNN_H * GNN_H + 255) / 256, 256, 0, s>>>(p, g, w.fold);
+        cudaFuncSetAttribute(k_gnn_layer_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FOLD_SMEM);
+    } else {
+        cudaFuncSetAttribute(k_gnn_layer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LAYER_SMEM);
+        cudaFuncSetAttribute(k_gnn_layer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LAYER_SMEM);
+    }
     for (int l = 0; l < GNN_L; l++) {
         const float *pl = p + GP_LAYER0 + l * GPL_SIZE;
         const bf16 *pkl = pk + GK_LAYER0 + l * GKL_SIZE;
-        if (w.train)
+        if (train)
             k_gnn_layer<true><<<nb, LAYER_THREADS, LAYER_SMEM, s>>>(g, pl, pkl, w.h[l], w.h[l + 1], w.a[l]);
+        else if (folded)
+            k_gnn_layer_fold<<<nb, LAYER_THREADS, FOLD_SMEM, s>>>(g, pl, w.fold + (size_t)l * 7 * GNN_H * GNN_H, pkl,
+                                                                 w.h[l & 1], w.h[(l + 1) & 1]);
         else
             k_gnn_layer<false><<<nb, LAYER_THREADS, LAYER_SMEM, s>>>(g, pl, pkl, w.h[l & 1], w.h[(l + 1) & 1], nullptr);
     }
-    const bf16 *hl = w.train ? w.h[GNN_L] : w.h[GNN_L & 1];
-    if (w.train)
+    const bf16 *hl = train ? w.h[GNN_L] : w.h[GNN_L & 1];
+    if (train)
         k_gnn_decode<true><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, w.q);
     else
         k_gnn_decode<false><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, nullptr);
@@ -960,21 +1086,21 @@ template <typename T>
 void gnn_forward(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &in, const float *p, const bf16 *pk, GnnWork &w,
                  double *x0)
 {
-    forward_impl<T>(s, g, in, p, pk, w, x0);
+    forward_impl<T>(s, g, in, p, pk, w, x0, false);
 }
 template void gnn_forward<double>(cudaStream_t, const GnnGraph &, const GnnInput<double> &, const float *,
                                   const bf16 *, GnnWork &, double *);
 template void gnn_forward<float>(cudaStream_t, const GnnGraph &, const GnnInput<float> &, const float *, const bf16 *,
                                  GnnWork &, double *);
 
-int gnn_forward_launches() { return 3 + GNN_L; }
+int gnn_forward_launches() { return 4 + GNN_L; }
 
 void gnn_loss_backward(cudaStream_t s, const GnnGraph &g, const GnnInput<float> &in, const float *target,
                        const float *p, const bf16 *pk, GnnWork &w, float *grad, float weight)
 {
     cudaFuncSetAttribute(k_gnn_layer_bwd_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BWD_SMEM);
     const int nb = gnn_blocks(g.n), rg = reduce_grid(g.n);
-    forward_impl<float>(s, g, in, p, pk, w, nullptr);
+    forward_impl<float>(s, g, in, p, pk, w, nullptr, true);
     k_gnn_loss_mean<<<rg, MCB_THREADS, 0, s>>>(g.n, w.y, target, w.scales, w.partials, w.counter, w.loss);
     k_gnn_loss_grad<<<rg, MCB_THREADS, 0, s>>>(g.n, w.y, target, w.scales, weight, w.dy, w.partials, w.counter,
                                                w.loss);

@@ -115,6 +115,7 @@ struct GnnWork {
     unsigned int *counter = nullptr;
     GnnScales *scales = nullptr;
     double *loss = nullptr;              // [2]: mean offset, loss
+    __nv_bfloat16 *fold = nullptr;       // [L][7][H][H] offset-form weights (inference)
 };
 
 size_t gnn_work_bytes(int n, bool train);
@@ -126,8 +127,11 @@ void gnn_init_params(float *p, uint64_t seed);
 // Device: refresh the BF16 copies from the FP32 parameters.
 void gnn_pack(cudaStream_t s, const float *p, __nv_bfloat16 *pk);
 
-// Forward pass.  Writes y (units of s_x) and, when x0 is given, x0 = s_x y
-// in FP64 (the initial guess in the solver's units).
+// Forward pass (inference).  Writes y (units of s_x) and, when x0 is given,
+// x0 = s_x y in FP64 (the initial guess in the solver's units).  On a graph in
+// offset form the per-direction gates are folded into the first weight
+// matrix, [W1h | W1m diag(g_1) | ... | W1m diag(g_6)], so that each layer is
+// one tensor-core product over the seven staged row tiles.
 template <typename T>
 void gnn_forward(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &in, const float *p, const __nv_bfloat16 *pk,
                  GnnWork &w, double *x0);

@@ -551,9 +551,14 @@ void pcg_sub_xmean(cudaStream_t s, int N, const PcgVectors &v)
 }
 
 // ----------------------------------------------------------------- BiCGStab
+//
+// Templated on the storage type T; the scalars of an iteration are cast to
+// T once, so T = double is the plain FP64 solver and T = float keeps every
+// vector and matrix access in FP32 (dot products accumulate in FP64).
 
-template <int R>
-__global__ void __launch_bounds__(MCB_THREADS) k_bicg_init(Ell A, BicgVectors<R> v, double rtol, int max_iters)
+template <typename T, int R>
+__global__ void __launch_bounds__(MCB_THREADS) k_bicg_init(EllT<T> A, BicgVectorsT<T, R> v, double rtol,
+                                                           int max_iters)
 {
     __shared__ double sh[R][MCB_THREADS];
     const int N = A.N;
@@ -564,15 +569,15 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_init(Ell A, BicgVectors<R>
 #pragma unroll
         for (int j = 0; j < R; j++) {
             const size_t o = (size_t)j * N + i;
-            const double bi = v.b[o];
-            v.x[j][i] = 0.0;
+            const T bi = v.b[o];
+            v.x[j][i] = (T)0;
             v.r[o] = bi;
             v.r0[o] = bi;
-            v.p[0][o] = 0.0;
-            v.p[1][o] = 0.0;
-            v.v[0][o] = 0.0;
-            v.v[1][o] = 0.0;
-            acc[j] += bi * bi;
+            v.p[0][o] = (T)0;
+            v.p[1][o] = (T)0;
+            v.v[0][o] = (T)0;
+            v.v[1][o] = (T)0;
+            acc[j] += (double)bi * (double)bi;
         }
     }
     if (publish_partials<R>(acc, v.partials, v.counter, sh)) {
@@ -601,29 +606,29 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_init(Ell A, BicgVectors<R>
 }
 
 // p_new = r + beta (p_old - omega v_old); v_new = A p_new.
-template <int R>
-__global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(Ell A, BicgVectors<R> v, const double *__restrict__ po,
-                                                        const double *__restrict__ vo, double *__restrict__ pn,
-                                                        double *__restrict__ vn)
+template <typename T, int R>
+__global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ po,
+                                                        const T *__restrict__ vo, T *__restrict__ pn,
+                                                        T *__restrict__ vn)
 {
     __shared__ double sh[R][MCB_THREADS];
     const BicgState<R> *st = v.st;
     if (st->all_done) return;
     const int N = A.N;
-    double beta[R], omega[R];
+    T beta[R], omega[R];
     bool act[R];
 #pragma unroll
     for (int j = 0; j < R; j++) {
         act[j] = !st->done[j];
-        beta[j] = (st->rho_new[j] / st->rho[j]) * (st->alpha[j] / st->omega[j]);
-        omega[j] = st->omega[j];
+        beta[j] = (T)((st->rho_new[j] / st->rho[j]) * (st->alpha[j] / st->omega[j]));
+        omega[j] = (T)st->omega[j];
     }
     double acc[R];
 #pragma unroll
     for (int j = 0; j < R; j++) acc[j] = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const double d = A.diag[i];
-        double offk[6];
+        const T d = A.diag[i];
+        T offk[6];
         int colk[6];
 #pragma unroll
         for (int k = 0; k < 6; k++) {
@@ -634,8 +639,8 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(Ell A, BicgVectors<R> v,
         for (int j = 0; j < R; j++) {
             if (!act[j]) continue;
             const size_t base = (size_t)j * N;
-            const double pi = v.r[base + i] + beta[j] * (po[base + i] - omega[j] * vo[base + i]);
-            double vi = d * pi;
+            const T pi = v.r[base + i] + beta[j] * (po[base + i] - omega[j] * vo[base + i]);
+            T vi = d * pi;
 #pragma unroll
             for (int k = 0; k < 6; k++) {
                 const size_t q = base + colk[k];
@@ -643,7 +648,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(Ell A, BicgVectors<R> v,
             }
             pn[base + i] = pi;
             vn[base + i] = vi;
-            acc[j] += v.r0[base + i] * vi;
+            acc[j] += (double)v.r0[base + i] * (double)vi;
         }
     }
     if (publish_partials<R>(acc, v.partials, v.counter, sh)) {
@@ -664,26 +669,26 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(Ell A, BicgVectors<R> v,
 }
 
 // s = r - alpha v; t = A s.
-template <int R>
-__global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(Ell A, BicgVectors<R> v, const double *__restrict__ vv)
+template <typename T, int R>
+__global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ vv)
 {
     __shared__ double sh[2 * R][MCB_THREADS];
     const BicgState<R> *st = v.st;
     if (st->all_done) return;
     const int N = A.N;
-    double alpha[R];
+    T alpha[R];
     bool act[R];
 #pragma unroll
     for (int j = 0; j < R; j++) {
         act[j] = !st->done[j];
-        alpha[j] = st->alpha[j];
+        alpha[j] = (T)st->alpha[j];
     }
     double acc[2 * R];
 #pragma unroll
     for (int j = 0; j < 2 * R; j++) acc[j] = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const double d = A.diag[i];
-        double offk[6];
+        const T d = A.diag[i];
+        T offk[6];
         int colk[6];
 #pragma unroll
         for (int k = 0; k < 6; k++) {
@@ -694,8 +699,8 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(Ell A, BicgVectors<R> v,
         for (int j = 0; j < R; j++) {
             if (!act[j]) continue;
             const size_t base = (size_t)j * N;
-            const double si = v.r[base + i] - alpha[j] * vv[base + i];
-            double ti = d * si;
+            const T si = v.r[base + i] - alpha[j] * vv[base + i];
+            T ti = d * si;
 #pragma unroll
             for (int k = 0; k < 6; k++) {
                 const size_t q = base + colk[k];
@@ -703,8 +708,8 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(Ell A, BicgVectors<R> v,
             }
             v.s[base + i] = si;
             v.t[base + i] = ti;
-            acc[2 * j] += ti * si;
-            acc[2 * j + 1] += ti * ti;
+            acc[2 * j] += (double)ti * (double)si;
+            acc[2 * j + 1] += (double)ti * (double)ti;
         }
     }
     if (publish_partials<2 * R>(acc, v.partials, v.counter, sh)) {
@@ -722,20 +727,20 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(Ell A, BicgVectors<R> v,
 }
 
 // x += alpha p + omega s; r = s - omega t; convergence on ||r||.
-template <int R>
-__global__ void __launch_bounds__(MCB_THREADS) k_bicg_3(Ell A, BicgVectors<R> v, const double *__restrict__ p)
+template <typename T, int R>
+__global__ void __launch_bounds__(MCB_THREADS) k_bicg_3(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ p)
 {
     __shared__ double sh[2 * R][MCB_THREADS];
     const BicgState<R> *st = v.st;
     if (st->all_done) return;
     const int N = A.N;
-    double alpha[R], omega[R];
+    T alpha[R], omega[R];
     bool act[R];
 #pragma unroll
     for (int j = 0; j < R; j++) {
         act[j] = !st->done[j];
-        alpha[j] = st->alpha[j];
-        omega[j] = st->omega[j];
+        alpha[j] = (T)st->alpha[j];
+        omega[j] = (T)st->omega[j];
     }
     double acc[2 * R];
 #pragma unroll
@@ -745,12 +750,12 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_3(Ell A, BicgVectors<R> v,
         for (int j = 0; j < R; j++) {
             if (!act[j]) continue;
             const size_t o = (size_t)j * N + i;
-            const double si = v.s[o];
+            const T si = v.s[o];
             v.x[j][i] += alpha[j] * p[o] + omega[j] * si;
-            const double ri = si - omega[j] * v.t[o];
+            const T ri = si - omega[j] * v.t[o];
             v.r[o] = ri;
-            acc[2 * j] += v.r0[o] * ri;
-            acc[2 * j + 1] += ri * ri;
+            acc[2 * j] += (double)v.r0[o] * (double)ri;
+            acc[2 * j + 1] += (double)ri * (double)ri;
         }
     }
     if (publish_partials<2 * R>(acc, v.partials, v.counter, sh)) {
@@ -782,32 +787,215 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_3(Ell A, BicgVectors<R> v,
     }
 }
 
+// Refinement: x = 0, r32 = (float) b, norms and tolerances.
+template <int R>
+__global__ void __launch_bounds__(MCB_THREADS) k_bir_init(Ell A, BirVectors<R> v, double rtol, int max_outer)
+{
+    __shared__ double sh[R][MCB_THREADS];
+    const int N = A.N;
+    double acc[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) acc[j] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const double bi = v.b[(size_t)j * N + i];
+            v.x[j][i] = 0.0;
+            v.r32[(size_t)j * N + i] = (float)bi;
+            acc[j] += bi * bi;
+        }
+    }
+    if (publish_partials<R>(acc, v.partials, v.counter, sh)) {
+        double tot[R];
+        reduce_partials<R>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) {
+            BirState<R> *st = v.st;
+            int all = 1;
+            for (int j = 0; j < R; j++) {
+                st->bb[j] = tot[j];
+                st->rr[j] = tot[j];
+                st->tol2[j] = rtol * rtol * tot[j];
+                st->status[j] = finite(tot[j]) ? KRYLOV_OK : KRYLOV_NONFINITE;
+                st->done[j] = (tot[j] == 0.0 || !finite(tot[j])) ? 1 : 0;
+                all &= st->done[j];
+            }
+            st->iter = 0;
+            st->all_done = all;
+            st->max_outer = max_outer;
+        }
+    }
+}
+
+// x_j += e_j for the systems still open.
+template <int R>
+__global__ void __launch_bounds__(MCB_THREADS) k_bir_add(int N, BirVectors<R> v)
+{
+    const BirState<R> *st = v.st;
+    if (st->all_done) return;
+    bool act[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) act[j] = !st->done[j];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int j = 0; j < R; j++)
+            if (act[j]) v.x[j][i] += (double)v.e[(size_t)j * N + i];
+}
+
+// r = b - A x in FP64, r32 = (float) r (zero for closed systems), norms and
+// convergence.
+template <int R>
+__global__ void __launch_bounds__(MCB_THREADS) k_bir_residual(Ell A, BirVectors<R> v)
+{
+    __shared__ double sh[R][MCB_THREADS];
+    BirState<R> *st = v.st;
+    if (st->all_done) return;
+    const int N = A.N;
+    bool act[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) act[j] = !st->done[j];
+    double acc[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) acc[j] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double d = A.diag[i];
+        double offk[6];
+        int colk[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            offk[k] = A.off[(size_t)k * N + i];
+            colk[k] = A.col[(size_t)k * N + i];
+        }
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const size_t o = (size_t)j * N + i;
+            if (!act[j]) {
+                v.r32[o] = 0.f;
+                continue;
+            }
+            const double *x = v.x[j];
+            double ax = d * x[i];
+#pragma unroll
+            for (int k = 0; k < 6; k++) ax += offk[k] * x[colk[k]];
+            const double ri = v.b[o] - ax;
+            v.r32[o] = (float)ri;
+            acc[j] += ri * ri;
+        }
+    }
+    if (publish_partials<R>(acc, v.partials, v.counter, sh)) {
+        double tot[R];
+        reduce_partials<R>(tot, v.partials, v.counter, sh);
+        if (threadIdx.x == 0) {
+            int all = 1;
+            st->iter += 1;
+            for (int j = 0; j < R; j++) {
+                if (!st->done[j]) {
+                    st->rr[j] = tot[j];
+                    if (!finite(tot[j])) {
+                        st->done[j] = 1;
+                        st->status[j] = KRYLOV_NONFINITE;
+                    } else if (tot[j] <= st->tol2[j]) {
+                        st->done[j] = 1;
+                    } else if (st->iter >= st->max_outer) {
+                        st->done[j] = 1;
+                        st->status[j] = KRYLOV_NOT_CONVERGED;
+                    }
+                }
+                all &= st->done[j];
+            }
+            st->all_done = all;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(MCB_THREADS) k_round_ell(int N, const double *__restrict__ diag,
+                                                           const double *__restrict__ off, float *__restrict__ d32,
+                                                           float *__restrict__ o32)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        d32[i] = (float)diag[i];
+#pragma unroll
+        for (int k = 0; k < 6; k++) o32[(size_t)k * N + i] = (float)off[(size_t)k * N + i];
+    }
+}
+
+template <typename T, int R>
+void bicg_init_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, double rtol, int max_iters)
+{
+    k_bicg_init<T, R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, max_iters);
+}
+template <typename T, int R>
+void bicg_1_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int pin)
+{
+    k_bicg_1<T, R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.p[pin], v.v[pin], v.p[pin ^ 1], v.v[pin ^ 1]);
+}
+template <typename T, int R>
+void bicg_2_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int vnew)
+{
+    k_bicg_2<T, R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.v[vnew]);
+}
+template <typename T, int R>
+void bicg_3_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int pnew)
+{
+    k_bicg_3<T, R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.p[pnew]);
+}
 template <int R>
 void bicg_init(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, double rtol, int max_iters)
 {
-    k_bicg_init<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, max_iters);
+    bicg_init_t<double, R>(s, A, v, rtol, max_iters);
 }
 template <int R>
 void bicg_1(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, int pin)
 {
-    k_bicg_1<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.p[pin], v.v[pin], v.p[pin ^ 1], v.v[pin ^ 1]);
+    bicg_1_t<double, R>(s, A, v, pin);
 }
 template <int R>
 void bicg_2(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, int vnew)
 {
-    k_bicg_2<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.v[vnew]);
+    bicg_2_t<double, R>(s, A, v, vnew);
 }
 template <int R>
 void bicg_3(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, int pnew)
 {
-    k_bicg_3<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.p[pnew]);
+    bicg_3_t<double, R>(s, A, v, pnew);
 }
+template <int R>
+void bir_init(cudaStream_t s, const Ell &A, const BirVectors<R> &v, double rtol, int max_outer)
+{
+    k_bir_init<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, max_outer);
+}
+template <int R>
+void bir_add(cudaStream_t s, int N, const BirVectors<R> &v)
+{
+    k_bir_add<R><<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, v);
+}
+template <int R>
+void bir_residual(cudaStream_t s, const Ell &A, const BirVectors<R> &v)
+{
+    k_bir_residual<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v);
+}
+void round_ell(cudaStream_t s, int N, const double *diag, const double *off, float *diag32, float *off32)
+{
+    k_round_ell<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, diag, off, diag32, off32);
+}
+
+#define MCB_INSTANTIATE_BICG_T(T, R)                                                                          \
+    template void bicg_init_t<T, R>(cudaStream_t, const EllT<T> &, const BicgVectorsT<T, R> &, double, int); \
+    template void bicg_1_t<T, R>(cudaStream_t, const EllT<T> &, const BicgVectorsT<T, R> &, int);            \
+    template void bicg_2_t<T, R>(cudaStream_t, const EllT<T> &, const BicgVectorsT<T, R> &, int);            \
+    template void bicg_3_t<T, R>(cudaStream_t, const EllT<T> &, const BicgVectorsT<T, R> &, int);
+MCB_INSTANTIATE_BICG_T(double, 1)
+MCB_INSTANTIATE_BICG_T(double, 3)
+MCB_INSTANTIATE_BICG_T(float, 1)
+MCB_INSTANTIATE_BICG_T(float, 3)
 
 #define MCB_INSTANTIATE_BICG(R)                                                                  \
     template void bicg_init<R>(cudaStream_t, const Ell &, const BicgVectors<R> &, double, int); \
     template void bicg_1<R>(cudaStream_t, const Ell &, const BicgVectors<R> &, int);            \
     template void bicg_2<R>(cudaStream_t, const Ell &, const BicgVectors<R> &, int);            \
-    template void bicg_3<R>(cudaStream_t, const Ell &, const BicgVectors<R> &, int);
+    template void bicg_3<R>(cudaStream_t, const Ell &, const BicgVectors<R> &, int);            \
+    template void bir_init<R>(cudaStream_t, const Ell &, const BirVectors<R> &, double, int);   \
+    template void bir_add<R>(cudaStream_t, int, const BirVectors<R> &);                          \
+    template void bir_residual<R>(cudaStream_t, const Ell &, const BirVectors<R> &);
 MCB_INSTANTIATE_BICG(1)
 MCB_INSTANTIATE_BICG(3)
 

@@ -64,14 +64,39 @@ struct PcgVectorsT {
 };
 using PcgVectors = PcgVectorsT<double>;
 
-template <int R>
-struct BicgVectors {
-    double *x[R];
-    const double *b;          // [R][N]
-    double *r, *r0, *p[2], *v[2], *s, *t;  // each [R][N]
+// Storage type T (double, or float for the inner solves of the refined
+// path); dot products and the scalars in BicgState stay FP64.
+template <typename T, int R>
+struct BicgVectorsT {
+    T *x[R];
+    const T *b;          // [R][N]
+    T *r, *r0, *p[2], *v[2], *s, *t;  // each [R][N]
     double *partials;
     unsigned int *counter;
     BicgState<R> *st;
+};
+template <int R>
+using BicgVectors = BicgVectorsT<double, R>;
+
+// FP64 iterative refinement around FP32 BiCGStab solves of R systems with
+// one matrix (momentum: R = 3; temperature: R = 1): x (FP64) starts at zero,
+// r = b - A x in FP64, r32 = (float) r feeds the inner solve of A32 e = r32,
+// x += e; each system stops when ||r_j|| <= rtol ||b_j||.
+template <int R>
+struct BirState {
+    double bb[R], rr[R], tol2[R];
+    int done[R], status[R];
+    int iter, all_done, max_outer, pad;
+};
+template <int R>
+struct BirVectors {
+    double *x[R];
+    const double *b;     // [R][N]
+    float *r32;          // [R][N]
+    const float *e;      // [R][N] inner solution
+    double *partials;
+    unsigned int *counter;
+    BirState<R> *st;
 };
 
 enum { KRYLOV_OK = 0, KRYLOV_NOT_CONVERGED = 1, KRYLOV_NONFINITE = 2 };
@@ -122,6 +147,23 @@ void ir_residual(cudaStream_t s, const Ell &A, const double *b, const double *x,
                  double *partials, unsigned int *counter);
 void pcg_xmean(cudaStream_t s, int N, const PcgVectors &v);
 void pcg_sub_xmean(cudaStream_t s, int N, const PcgVectors &v);
+
+template <typename T, int R>
+void bicg_init_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, double rtol, int max_iters);
+template <typename T, int R>
+void bicg_1_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int pin);
+template <typename T, int R>
+void bicg_2_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int vnew);
+template <typename T, int R>
+void bicg_3_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int pnew);
+template <int R>
+void bir_init(cudaStream_t s, const Ell &A, const BirVectors<R> &v, double rtol, int max_outer);
+template <int R>
+void bir_add(cudaStream_t s, int N, const BirVectors<R> &v);
+template <int R>
+void bir_residual(cudaStream_t s, const Ell &A, const BirVectors<R> &v);
+// FP32 copy of a 7-point matrix's values.
+void round_ell(cudaStream_t s, int N, const double *diag, const double *off, float *diag32, float *off32);
 
 template <int R>
 void bicg_init(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, double rtol, int max_iters);
