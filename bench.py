@@ -22,8 +22,9 @@ Two configurations run back to back from the same initial state:
   headline ("value"): MC_GUESS_LEARNED (the committed trained parameters) +
     MC_PRECISION_FP32_REFINED, pressure PCG-AMG;
   plain ("plain_fp64"): zero guess, FP64 PCG-AMG.
-After the same number of passes the fields of the two are compared (max
-relative difference per field).
+After the same number of passes each configuration's fields are compared
+with an untimed FP64 run at tight tolerances (1e-12) from the same state:
+max relative difference per field ("error vs FP64 reference").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -62,6 +63,7 @@ def parse():
     ap.add_argument("--no-roofline", action="store_true")
     ap.add_argument("--psolver", default="amg", choices=["amg", "jacobi"],
                     help="pressure-correction preconditioner of the plain path (aggregation AMG or Jacobi)")
+    ap.add_argument("--no-field-check", action="store_true", help="skip the tight FP64 reference run")
     ap.add_argument("--config", default="both", choices=["both", "headline", "plain"],
                     help="which configurations to time (default: both; value = headline)")
     return ap.parse_args()
@@ -210,9 +212,12 @@ def run_reference_arm(args, rank, world):
 FIELD_NAMES = ("U", "V", "W", "P", "TEM")
 
 
-def make_solver(flow, mesh, dims, lengths, args, rank, local, headline):
+def make_solver(flow, mesh, dims, lengths, args, rank, local, headline, tight=False):
     """The benchmark solver of one configuration, seeded identically."""
-    if headline:
+    if tight:
+        params = flow.default_params(flow.MODE_SIMPLE, device=local, p_rtol=1e-12, u_rtol=1e-12,
+                                     pressure_solver=flow.PSOLVER_PCG_AMG)
+    elif headline:
         from minicombust_app_b200 import train_guess
         params = flow.default_params(flow.MODE_SIMPLE, device=local, p_rtol=1e-8, u_rtol=1e-8,
                                      pressure_solver=flow.PSOLVER_PCG_AMG, precision=flow.PRECISION_FP32_REFINED,
@@ -222,7 +227,7 @@ def make_solver(flow, mesh, dims, lengths, args, rank, local, headline):
         params = flow.default_params(flow.MODE_SIMPLE, device=local, p_rtol=1e-8, u_rtol=1e-8,
                                      pressure_solver=psolver)
     solver = flow.FlowSolver(mesh, params=params)
-    if headline:
+    if headline and not tight:
         solver.set_guess_params(train_guess.load_params())
     N = solver.N
     for name, vals in noisy_fields(N, seed=rank).items():
@@ -355,6 +360,14 @@ def main():
         runs[cfg] = r
         solver.close()
 
+    reference_fields = None
+    if rank == 0 and not args.no_field_check:
+        ref = make_solver(flow, mesh, dims, lengths, args, rank, local, False, tight=True)
+        for _ in range(args.warmup + args.steps):
+            ref.simple_iteration()
+        reference_fields = {n: ref.field(n)[:N].copy() for n in FIELD_NAMES}
+        ref.close()
+
     if rank == 0:
         main_cfg = order[-1]
         R = runs[main_cfg]
@@ -379,11 +392,11 @@ def main():
                             "mass_imbalance": r["stats"][-1]["mass_imbalance"], "gpu_launches": r["launches"],
                             "roofline": r.get("roofline"), "kernel_ms_one_step": r.get("kernel_ms")}
         field_err = None
-        if "plain" in runs and "headline" in runs:
+        if reference_fields is not None:
             field_err = {}
-            for n in FIELD_NAMES:
-                a, b = runs["headline"]["fields"][n], runs["plain"]["fields"][n]
-                field_err[n] = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+            for cfg, r in runs.items():
+                field_err[cfg] = {n: float(np.abs(r["fields"][n] - reference_fields[n]).max()
+                                           / max(np.abs(reference_fields[n]).max(), 1e-300)) for n in FIELD_NAMES}
         desc = ("learned initial guess + FP32-refined pressure PCG-AMG (FP64 outer refinement)"
                 if main_cfg == "headline" else "plain FP64 path, pressure PCG-AMG")
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -397,7 +410,8 @@ def main():
                 "e2e": {"value": R["e2e"], "unit": UNIT, "h2d_bytes_per_step": R["e2e_bytes"],
                         "d2h_bytes_per_step": R["e2e_bytes"]},
                 "gpu_launches": R["launches"], "clocks": R["clocks"], "roofline": R.get("roofline"),
-                "cpu_baseline": cpu, "configs": summary, "field_rel_diff_vs_plain_fp64": field_err}
+                "cpu_baseline": cpu, "configs": summary,
+                "field_rel_error_vs_fp64_reference": field_err}
         if "plain" in runs and "headline" in runs:
             line["speedup_vs_plain_fp64"] = summary["headline"]["value"] / summary["plain"]["value"]
         print(json.dumps(line))

@@ -140,7 +140,14 @@ template <typename T>
 __device__ __forceinline__ T row_apply(const AmgLevelT<T> &L, int i, const T *__restrict__ e)
 {
     T s = L.diag[i] * e[i];
-    for (int q = 0; q < L.k; q++) s += L.off[(size_t)q * L.n + i] * e[L.col[(size_t)q * L.n + i]];
+    if (L.dc.code) {
+        int c[6];
+        row_cols(L.dc, L.col, L.n, i, c);
+#pragma unroll
+        for (int q = 0; q < 6; q++) s += L.off[(size_t)q * L.n + i] * e[c[q]];
+    } else {
+        for (int q = 0; q < L.k; q++) s += L.off[(size_t)q * L.n + i] * e[L.col[(size_t)q * L.n + i]];
+    }
     return s;
 }
 

@@ -25,6 +25,8 @@
 
 #include <cuda_runtime.h>
 
+#include "krylov.cuh"
+
 namespace mcb {
 
 constexpr int AMG_MAX_LEVELS = 16;
@@ -38,6 +40,7 @@ struct AmgLevelT {
     T *diag;        // [n]
     T *off;         // [k][n]
     const int *col; // [k][n], unused slots point at their own row
+    DirCodes dc;    // level 0 of a structured box: columns from direction codes (k = 6)
     // restriction to the next level: members of coarse row I are mlist[mptr[I] .. mptr[I+1])
     const int *agg;   // [n] aggregate (next-level row) of each row
     const int *mptr;  // [n_next + 1]

@@ -7,9 +7,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "amg.h"
@@ -84,6 +86,8 @@ struct mc_flow {
     MeshArgs margs{};
     Arena arena;
     std::vector<int> hcol;   // ELL columns with -1 on boundary slots (CSR export)
+    uint32_t *dcode = nullptr;  // direction codes of the ELL columns (used when dc.code is set)
+    DirCodes dc;
     // cell/face renumbering (reorder == MC_REORDER_RCM); host and device copies
     bool reordered = false;
     std::vector<int> cell_n2o, cell_o2n, face_o2n;
@@ -245,9 +249,9 @@ int grad_index(int field)
     }
 }
 
-Ell momentum_matrix(mc_flow *h) { return Ell{h->N, h->AU, h->off_m, h->col}; }
-Ell pressure_matrix(mc_flow *h) { return Ell{h->N, h->diag_p, h->off_p, h->col}; }
-Ell temperature_matrix(mc_flow *h) { return Ell{h->N, h->diag_t, h->off_t, h->col}; }
+Ell momentum_matrix(mc_flow *h) { return Ell{h->N, h->AU, h->off_m, h->col, h->dc}; }
+Ell pressure_matrix(mc_flow *h) { return Ell{h->N, h->diag_p, h->off_p, h->col, h->dc}; }
+Ell temperature_matrix(mc_flow *h) { return Ell{h->N, h->diag_t, h->off_t, h->col, h->dc}; }
 
 // ------------------------------------------------------------ Krylov drivers
 
@@ -409,7 +413,7 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
 int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *relres, double *bnorm)
 {
     const Ell A = pressure_matrix(h);
-    const EllT<float> A32{h->N, h->amg.lv32[0].diag, h->amg.lv32[0].off, h->col};
+    const EllT<float> A32{h->N, h->amg.lv32[0].diag, h->amg.lv32[0].off, h->col, h->dc};
     PcgVectors o = h->pv;
     PcgVectorsT<float> in = h->pv32;
     constexpr int kMaxOuter = 50;
@@ -673,7 +677,7 @@ int stage_momentum(mc_flow *h, mc_iter_stats *st)
     int its[3] = {0, 0, 0};
     if (h->bir_mem) {
         launch(h, K_ROUND_ELL, [&] { round_ell(h->stream, h->N, h->AU, h->off_m, h->m32_diag, h->m32_off); });
-        const EllT<float> A32{h->N, h->m32_diag, h->m32_off, h->col};
+        const EllT<float> A32{h->N, h->m32_diag, h->m32_off, h->col, h->dc};
         rc = solve_bicg_refined<3>(h, momentum_matrix(h), A32, h->bi3, h->bo3, h->h_bi3, h->h_bo3, &h->g_b3_32,
                                    K_BICG3_INIT32, K_BICG3_1_32, its);
     } else {
@@ -806,7 +810,7 @@ int stage_temperature(mc_flow *h, mc_iter_stats *st)
     int its[1] = {0};
     if (h->bir_mem) {
         launch(h, K_ROUND_ELL, [&] { round_ell(h->stream, h->N, h->diag_t, h->off_t, h->t32_diag, h->t32_off); });
-        const EllT<float> A32{h->N, h->t32_diag, h->t32_off, h->col};
+        const EllT<float> A32{h->N, h->t32_diag, h->t32_off, h->col, h->dc};
         rc = solve_bicg_refined<1>(h, temperature_matrix(h), A32, h->bi1, h->bo1, h->h_bi1, h->h_bo1, &h->g_b1_32,
                                    K_BICG1_INIT32, K_BICG1_1_32, its);
     } else {
@@ -867,6 +871,7 @@ int allocate(mc_flow *h)
     add(&h->b3.st, sizeof(BicgState<3>));
     add(&h->b1.st, sizeof(BicgState<1>));
     add(&h->pp_prev, N * 8);
+    add(&h->dcode, N * 4);
     add(&h->gs, sizeof(GuessState));
     if (h->reordered) {
         add(&h->d_cell_n2o, N * 4);
@@ -1056,6 +1061,50 @@ int setup_guess(mc_flow *h, const HostMesh &hm)
     return MC_OK;
 }
 
+// MC_DIR_CODES=0 keeps the column lists even where direction codes apply
+// (the tests use it to check both forms).
+bool dir_codes_disabled()
+{
+    const char *v = std::getenv("MC_DIR_CODES");
+    return v && v[0] == '0';
+}
+
+// Direction codes of the ELL columns (DirCodes): slot k of row i holds the
+// direction d with nbr[d][i] == col[k][i] (7: unused slot).  Returns false
+// when some direction's neighbour offset is not the same for every row (RCM
+// order, irregular meshes): the kernels then read the column list.
+bool build_dir_codes(const HostMesh &hm, std::vector<uint32_t> &code, int doff[6])
+{
+    const int N = hm.N;
+    bool seen[6] = {false, false, false, false, false, false};
+    for (int d = 0; d < 6; d++) doff[d] = 0;
+    code.assign(N, 0u);
+    for (int i = 0; i < N; i++) {
+        uint32_t cw = 0;
+        for (int k = 0; k < 6; k++) {
+            const int j = hm.col[(size_t)k * N + i];
+            unsigned dsel = 7;
+            if (j != i) {
+                for (int d = 0; d < 6; d++)
+                    if (hm.nbr[(size_t)d * N + i] == j) {
+                        dsel = (unsigned)d;
+                        break;
+                    }
+                if (dsel == 7) return false;
+                if (!seen[dsel]) {
+                    seen[dsel] = true;
+                    doff[dsel] = j - i;
+                } else if (doff[dsel] != j - i) {
+                    return false;
+                }
+            }
+            cw |= dsel << (3 * k);
+        }
+        code[i] = cw;
+    }
+    return true;
+}
+
 // Aggregation hierarchy for the pressure-correction system: pattern data on
 // the host (amg.cu), one extra device allocation for all levels.
 int build_amg(mc_flow *h, const HostMesh &hm)
@@ -1139,6 +1188,7 @@ int build_amg(mc_flow *h, const HostMesh &hm)
             d.diag = h->diag_p;
             d.off = h->off_p;
             d.col = h->col;
+            d.dc = h->dc;
             d.r = h->pv.r;
         } else {
             int rc = put(d_col[l], lv[l].col);
@@ -1166,6 +1216,7 @@ int build_amg(mc_flow *h, const HostMesh &hm)
             f.n = d.n;
             f.k = d.k;
             f.col = d.col;
+            f.dc = d.dc;
             f.agg = d.agg;
             f.mptr = d.mptr;
             f.mlist = d.mlist;
@@ -1309,6 +1360,27 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
                 if (!rc) cudaStreamSynchronize(h->stream);
             }
             rc = rc ? rc : initial_fields(h, hm.btype);
+            if (!rc) {
+                std::vector<uint32_t> code;
+                int doff[6];
+                if (build_dir_codes(hm, code, doff) && !dir_codes_disabled()) {
+                    rc = upload(h, h->dcode, code.data(), N);
+                    if (!rc) cudaStreamSynchronize(h->stream);
+                    h->dc.code = h->dcode;
+                    for (int d = 0; d < 6; d++) h->dc.doff[d] = doff[d];
+                    // the most frequent code word and its per-slot offsets
+                    std::unordered_map<uint32_t, int> freq;
+                    for (uint32_t cw : code) freq[cw]++;
+                    uint32_t canon = code[0];
+                    for (const auto &f : freq)
+                        if (f.second > freq[canon]) canon = f.first;
+                    h->dc.canon = canon;
+                    for (int k = 0; k < 6; k++) {
+                        const unsigned d = (canon >> (3 * k)) & 7u;
+                        h->dc.coff[k] = d < 6 ? doff[d] : 0;
+                    }
+                }
+            }
             if (!rc && params->pressure_solver == MC_PSOLVER_PCG_AMG) rc = build_amg(h, hm);
             if (!rc) rc = setup_guess(h, hm);
             if (!rc && params->precision == MC_PRECISION_FP32_REFINED) rc = setup_bicg_refined(h);

@@ -58,8 +58,10 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_init(Ell A, PcgVectors v, d
         double ri = bi;
         if (use_x0) {
             double ax = A.diag[i] * v.x[i];
+            int c_[6];
+            row_cols(A, i, c_);
 #pragma unroll
-            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * v.x[A.col[(size_t)k * N + i]];
+            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * v.x[c_[k]];
             ri = bi - ax;
         } else {
             v.x[i] = 0.0;
@@ -117,10 +119,10 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(EllT<T> A, PcgVectors
         const int j1 = has1 ? i1 : i0;
         int ca[6], cb[6];
         T oa[6], ob[6];
+        row_cols(A, i0, ca);
+        row_cols(A, j1, cb);
 #pragma unroll
         for (int k = 0; k < 6; k++) {
-            ca[k] = A.col[(size_t)k * N + i0];
-            cb[k] = A.col[(size_t)k * N + j1];
             oa[k] = A.off[(size_t)k * N + i0];
             ob[k] = A.off[(size_t)k * N + j1];
         }
@@ -217,8 +219,10 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_init_amg(EllT<T> A, PcgVect
         T ri = bi;
         if (use_x0) {
             T ax = A.diag[i] * v.x[i];
+            int c_[6];
+            row_cols(A, i, c_);
 #pragma unroll
-            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * v.x[A.col[(size_t)k * N + i]];
+            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * v.x[c_[k]];
             ri = bi - ax;
         } else {
             v.x[i] = (T)0;
@@ -308,8 +312,10 @@ __global__ void __launch_bounds__(MCB_THREADS) k_ir_init(Ell A, const double *__
         double ri = bi;
         if (use_x0) {
             double ax = A.diag[i] * x[i];
+            int c_[6];
+            row_cols(A, i, c_);
 #pragma unroll
-            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * x[A.col[(size_t)k * N + i]];
+            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * x[c_[k]];
             ri = bi - ax;
         } else {
             x[i] = 0.0;
@@ -342,8 +348,10 @@ __global__ void __launch_bounds__(MCB_THREADS) k_ir_init(Ell A, const double *__
 __device__ __forceinline__ double ell_row(const Ell &A, const double *__restrict__ x, int i)
 {
     double ax = A.diag[i] * x[i];
+    int c_[6];
+    row_cols(A, i, c_);
 #pragma unroll
-    for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * A.N + i] * x[A.col[(size_t)k * A.N + i]];
+    for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * A.N + i] * x[c_[k]];
     return ax;
 }
 
@@ -440,8 +448,10 @@ __global__ void __launch_bounds__(MCB_THREADS) k_ir_residual(Ell A, const double
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         double ax = A.diag[i] * x[i];
+        int c_[6];
+        row_cols(A, i, c_);
 #pragma unroll
-        for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * x[A.col[(size_t)k * N + i]];
+        for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * x[c_[k]];
         const double ri = (b[i] - mean) - ax;
         r[i] = ri;
         r32[i] = (float)ri;
@@ -630,11 +640,9 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(EllT<T> A, BicgVectorsT<
         const T d = A.diag[i];
         T offk[6];
         int colk[6];
+        row_cols(A, i, colk);
 #pragma unroll
-        for (int k = 0; k < 6; k++) {
-            offk[k] = A.off[(size_t)k * N + i];
-            colk[k] = A.col[(size_t)k * N + i];
-        }
+        for (int k = 0; k < 6; k++) offk[k] = A.off[(size_t)k * N + i];
 #pragma unroll
         for (int j = 0; j < R; j++) {
             if (!act[j]) continue;
@@ -690,11 +698,9 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(EllT<T> A, BicgVectorsT<
         const T d = A.diag[i];
         T offk[6];
         int colk[6];
+        row_cols(A, i, colk);
 #pragma unroll
-        for (int k = 0; k < 6; k++) {
-            offk[k] = A.off[(size_t)k * N + i];
-            colk[k] = A.col[(size_t)k * N + i];
-        }
+        for (int k = 0; k < 6; k++) offk[k] = A.off[(size_t)k * N + i];
 #pragma unroll
         for (int j = 0; j < R; j++) {
             if (!act[j]) continue;
@@ -860,11 +866,9 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bir_residual(Ell A, BirVectors<
         const double d = A.diag[i];
         double offk[6];
         int colk[6];
+        row_cols(A, i, colk);
 #pragma unroll
-        for (int k = 0; k < 6; k++) {
-            offk[k] = A.off[(size_t)k * N + i];
-            colk[k] = A.col[(size_t)k * N + i];
-        }
+        for (int k = 0; k < 6; k++) offk[k] = A.off[(size_t)k * N + i];
 #pragma unroll
         for (int j = 0; j < R; j++) {
             const size_t o = (size_t)j * N + i;

@@ -9,6 +9,8 @@
 // the host polls a small status block between batches of iterations.
 #pragma once
 
+#include <stdint.h>
+
 #include <cuda_runtime.h>
 
 namespace mcb {
@@ -25,6 +27,44 @@ struct Pair<float> {
     using type = float2;
 };
 
+// Columns of the 7-point rows in direction-code form: on a structured box in
+// x-fastest order the neighbour through direction d is always row + doff[d],
+// so a row's six columns fit one 32-bit word (3 bits per slot: the direction
+// 0..5 of the slot, or 7 for an unused slot).  Kernels then read 4 bytes per
+// row instead of 24.
+// Most rows (all interior cells) share one code word, `canon`, whose
+// per-slot offsets are kept ready in coff.
+struct DirCodes {
+    const uint32_t *code = nullptr;  // [N]; nullptr: use the column list
+    int doff[6] = {0, 0, 0, 0, 0, 0};
+    uint32_t canon = 0;
+    int coff[6] = {0, 0, 0, 0, 0, 0};
+};
+
+// Column of each slot of row i (the row itself for an unused slot).
+__device__ __forceinline__ void row_cols(const DirCodes &dc, const int *__restrict__ col, int N, int i, int (&c)[6])
+{
+    if (dc.code) {
+        const uint32_t cw = dc.code[i];
+        if (cw == dc.canon) {
+#pragma unroll
+            for (int k = 0; k < 6; k++) c[k] = i + dc.coff[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                const unsigned d = (cw >> (3 * k)) & 7u;
+                int o = 0;
+#pragma unroll
+                for (int q = 0; q < 6; q++) o = (d == (unsigned)q) ? dc.doff[q] : o;
+                c[k] = i + o;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 6; k++) c[k] = col[(size_t)k * N + i];
+    }
+}
+
 // 7-point system in ELL form; T is the storage type of the values.
 template <typename T>
 struct EllT {
@@ -32,8 +72,15 @@ struct EllT {
     const T *diag;
     const T *off;   // [6][N]
     const int *col; // [6][N]
+    DirCodes dc{};
 };
 using Ell = EllT<double>;
+
+template <typename T>
+__device__ __forceinline__ void row_cols(const EllT<T> &A, int i, int (&c)[6])
+{
+    row_cols(A.dc, A.col, A.N, i, c);
+}
 
 struct PcgState {
     double rz, rz_old, alpha, pq, rr, bb, tol2, mean, xmean;
