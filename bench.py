@@ -45,6 +45,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from minicombust_app_b200 import replicas  # noqa: E402
 from minicombust_app_b200.workload import gaussian_blobs, noisy_fields  # noqa: E402
 
 METRIC = "SIMPLE iters/s at 4.2M cells: learned+FP32-refined vs plain FP64, same 1e-8 residual"
@@ -315,11 +316,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, dist, device="cuda")
 
     m = args.m
     dims, lengths = (2 * m, m, m), (0.2, 0.1, 0.1)
@@ -353,7 +350,7 @@ def main():
                     flow._check(L.mc_flow_get_field(h, flow.FIELDS[n], pinned[n].data_ptr()), h, "get_field")
             e1.record(stream)
             barrier()
-            r["e2e"] = world * args.steps / max_over_ranks(e0.elapsed_time(e1) / 1e3)
+            r["e2e"] = replicas.whole_job_rate(args.steps, max_over_ranks(e0.elapsed_time(e1) / 1e3), world)
             r["e2e_bytes"] = 5 * (N + 6) * 8
         if rank == 0 and not args.no_roofline:
             r["roofline"], r["kernel_ms"] = roofline_of(solver, mesh, N)
@@ -371,7 +368,7 @@ def main():
     if rank == 0:
         main_cfg = order[-1]
         R = runs[main_cfg]
-        value = world * args.steps / R["t"]
+        value = replicas.whole_job_rate(args.steps, R["t"], world)
         cpu = None
         if not args.no_cpu_baseline:
             per_pass = reference_sample(32, 3)
@@ -383,7 +380,8 @@ def main():
         summary = {}
         for cfg, r in runs.items():
             pit = [st["pressure_iters_total"] for st in r["stats"]]
-            summary[cfg] = {"value": world * args.steps / r["t"], "ms_per_step": 1e3 * r["t"] / args.steps,
+            summary[cfg] = {"value": replicas.whole_job_rate(args.steps, r["t"], world),
+                            "ms_per_step": 1e3 * r["t"] / args.steps,
                             "pressure_iters_per_step": float(np.mean(pit)),
                             "guess_rel_residual": float(np.mean([st["guess_rel_residual_first"] for st in r["stats"]])),
                             "momentum_iters": r["stats"][-1]["momentum_iters"],

@@ -1,6 +1,7 @@
 """The C-ABI library loads on a CPU-only machine, exports every entry point
-declared in include/minicombust_flow.h, and its host-only parts (parameter
-defaults, box mesh builder) agree with the reference/oracle."""
+declared in include/*.h (the flow solver and the guess network), and its
+host-only parts (parameter defaults, box mesh builder) agree with the
+reference/oracle."""
 import ctypes
 import os
 import re
@@ -13,10 +14,11 @@ from minicombust_app_b200 import flow
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "minicombust_flow.h")
+GNN_HEADER = os.path.join(ROOT, "include", "minicombust_gnn.h")
 
 
-def declared_symbols():
-    text = open(HEADER).read()
+def declared_symbols(header=HEADER):
+    text = open(header).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(mc_[a-z0-9_]+)\s*\(", text)))
 
@@ -28,6 +30,17 @@ def test_library_exports_every_declared_symbol():
     for n in names:
         assert hasattr(L, n), n
         assert n in flow._SIGNATURES, f"{n} has no ctypes signature"
+
+
+def test_library_exports_every_guess_network_symbol():
+    from minicombust_app_b200 import gnn
+    L = gnn.library()
+    names = declared_symbols(GNN_HEADER)
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(L, n), n
+        assert n in gnn._SIGNATURES, f"{n} has no ctypes signature"
+    assert L.mc_gnn_param_count() == 14177
 
 
 def test_default_params_are_reference_constants():
