@@ -191,7 +191,8 @@ __global__ void k_amg_galerkin(AmgLevelT<T> fine, AmgLevelT<T> coarse)
 }
 
 // Dense Cholesky of A + sigma 1 1^T (sigma = mean diagonal / n) on the
-// coarsest level, one block, FP64, factor stored lower-triangular row-major.
+// coarsest level, one block, FP64 (factor in shared memory), then its
+// explicit symmetric inverse, row-major in `dense` for the V-cycle's solve.
 template <typename T>
 __global__ void k_amg_dense_factor(AmgLevelT<T> L, double *dense)
 {
@@ -226,32 +227,47 @@ __global__ void k_amg_dense_factor(AmgLevelT<T> L, double *dense)
             for (int c = j + 1; c <= t; c++) A[t * n + c] -= A[t * n + j] * A[c * n + j];
         __syncthreads();
     }
-    for (int idx = t; idx < n * n; idx += blockDim.x) dense[idx] = A[idx];
+    // explicit inverse, column t by thread t: L y = e_t, then L^T x = y; the
+    // column is built in place in `dense` (this thread's column only)
+    if (t < n) {
+        for (int i = 0; i < t; i++) dense[i * n + t] = 0.0;  // L y = e_t: y_i = 0 above row t
+        for (int i = t; i < n; i++) {
+            double v = (i == t) ? 1.0 : 0.0;
+            for (int c = t; c < i; c++) v -= A[i * n + c] * dense[c * n + t];
+            dense[i * n + t] = v / A[i * n + i];
+        }
+        for (int i = n - 1; i >= 0; i--) {
+            double v = dense[i * n + t];
+            for (int c = i + 1; c < n; c++) v -= A[c * n + i] * dense[c * n + t];
+            dense[i * n + t] = v / A[i * n + i];
+        }
+    }
+    __syncthreads();
+    // symmetrise (the inverse of a symmetric matrix), pair (t, j > t) by thread t
+    if (t < n)
+        for (int j = t + 1; j < n; j++) {
+            const double m = 0.5 * (dense[t * n + j] + dense[j * n + t]);
+            dense[t * n + j] = m;
+            dense[j * n + t] = m;
+        }
 }
 
+// e = (A + sigma 1 1^T)^{-1} r on the coarsest level: one dense product with
+// the symmetric inverse formed at setup; thread t computes row t (the reads
+// dense[j][t] are coalesced across threads).
 template <typename T>
 __global__ void k_amg_dense_solve(AmgLevelT<T> L, const double *__restrict__ dense, const PcgState *st)
 {
     if (st->done) return;
-    extern __shared__ double F[];
-    __shared__ double y[AMG_COARSEST_MAX];
+    __shared__ double r[AMG_COARSEST_MAX];
     const int n = L.n, t = threadIdx.x;
-    for (int idx = t; idx < n * n; idx += blockDim.x) F[idx] = dense[idx];
-    if (t < n) y[t] = (double)L.r[t];
+    if (t < n) r[t] = (double)L.r[t];
     __syncthreads();
-    for (int j = 0; j < n; j++) {  // L y = r
-        if (t == j) y[j] /= F[j * n + j];
-        __syncthreads();
-        if (t > j && t < n) y[t] -= F[t * n + j] * y[j];
-        __syncthreads();
+    if (t < n) {
+        double y = 0.0;
+        for (int j = 0; j < n; j++) y += dense[(size_t)j * n + t] * r[j];
+        L.e[0][t] = (T)y;
     }
-    for (int j = n - 1; j >= 0; j--) {  // L^T x = y
-        if (t == j) y[j] /= F[j * n + j];
-        __syncthreads();
-        if (t < j) y[t] -= F[j * n + t] * y[j];
-        __syncthreads();
-    }
-    if (t < n) L.e[0][t] = (T)y[t];
 }
 
 template <typename T>
@@ -390,7 +406,7 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
         cur[l] = c;
         k_amg_restrict<T><<<blocks(lv[l + 1].n), MCB_THREADS, 0, s>>>(lv[l], lv[l + 1], lv[l].e[c], st);
     }
-    k_amg_dense_solve<T><<<1, AMG_COARSEST_MAX, dense_smem(lv[L - 1].n), s>>>(lv[L - 1], H.dense, st);
+    k_amg_dense_solve<T><<<1, AMG_COARSEST_MAX, 0, s>>>(lv[L - 1], H.dense, st);
     cur[L - 1] = 0;
     for (int l = L - 2; l >= 0; l--) {
         int c = cur[l];

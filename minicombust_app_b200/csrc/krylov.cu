@@ -617,7 +617,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_init(EllT<T> A, BicgVector
 
 // p_new = r + beta (p_old - omega v_old); v_new = A p_new.
 template <typename T, int R>
-__global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ po,
+__global__ void __launch_bounds__(MCB_THREADS, 4) k_bicg_1(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ po,
                                                         const T *__restrict__ vo, T *__restrict__ pn,
                                                         T *__restrict__ vn)
 {
@@ -678,7 +678,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_1(EllT<T> A, BicgVectorsT<
 
 // s = r - alpha v; t = A s.
 template <typename T, int R>
-__global__ void __launch_bounds__(MCB_THREADS) k_bicg_2(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ vv)
+__global__ void __launch_bounds__(MCB_THREADS, 4) k_bicg_2(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ vv)
 {
     __shared__ double sh[2 * R][MCB_THREADS];
     const BicgState<R> *st = v.st;
