@@ -858,7 +858,7 @@ int allocate(mc_flow *h)
     add(&h->off_p, 6 * N * 8); add(&h->diag_p, N * 8); add(&h->b_p, N * 8);
     add(&h->off_t, 6 * N * 8); add(&h->diag_t, N * 8); add(&h->b_t, N * 8);
     add(&h->src, 5 * N * 8);
-    add(&h->partials, (size_t)G * 8 * 8);
+    add(&h->partials, (size_t)G * 8 * 8 * 3);  // split BiCGStab launches use 3 x the blocks
     add(&h->counter, 256);
     add(&h->balance, sizeof(FluxBalance));
     add(&h->scalars, 8 * 8);

@@ -615,9 +615,42 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bicg_init(EllT<T> A, BicgVector
     }
 }
 
+// Row blocks and right-hand sides of a BiCGStab launch: fused (every block
+// works on all R systems) or split (block b works on system b % R of row
+// block b / R; the R blocks of a row block run together, so the matrix is
+// read from L2 R - 1 times out of R).  The split form keeps one system's state
+// per thread and runs at full occupancy; it is used for the FP32 inner solves.
+template <int R, bool SPLIT>
+struct BicgBlocks {
+    int j0, j1, b, nb;
+    __device__ BicgBlocks()
+    {
+        if (SPLIT) {
+            j0 = blockIdx.x % R;
+            j1 = j0 + 1;
+            b = blockIdx.x / R;
+            nb = gridDim.x / R;
+        } else {
+            j0 = 0;
+            j1 = R;
+            b = blockIdx.x;
+            nb = gridDim.x;
+        }
+    }
+};
+
+template <typename P, int R>
+__device__ __forceinline__ P pick(P const (&a)[R], int j)
+{
+    P r = a[0];
+#pragma unroll
+    for (int q = 1; q < R; q++) r = (j == q) ? a[q] : r;
+    return r;
+}
+
 // p_new = r + beta (p_old - omega v_old); v_new = A p_new.
-template <typename T, int R>
-__global__ void __launch_bounds__(MCB_THREADS, 4) k_bicg_1(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ po,
+template <typename T, int R, bool SPLIT>
+__global__ void __launch_bounds__(MCB_THREADS, SPLIT ? 8 : 4) k_bicg_1(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ po,
                                                         const T *__restrict__ vo, T *__restrict__ pn,
                                                         T *__restrict__ vn)
 {
@@ -625,38 +658,65 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_bicg_1(EllT<T> A, BicgVector
     const BicgState<R> *st = v.st;
     if (st->all_done) return;
     const int N = A.N;
-    T beta[R], omega[R];
-    bool act[R];
-#pragma unroll
-    for (int j = 0; j < R; j++) {
-        act[j] = !st->done[j];
-        beta[j] = (T)((st->rho_new[j] / st->rho[j]) * (st->alpha[j] / st->omega[j]));
-        omega[j] = (T)st->omega[j];
-    }
+    const BicgBlocks<R, SPLIT> bb;
     double acc[R];
 #pragma unroll
     for (int j = 0; j < R; j++) acc[j] = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const T d = A.diag[i];
-        T offk[6];
-        int colk[6];
-        row_cols(A, i, colk);
+    if (SPLIT) {
+        const int j = bb.j0;
+        if (!st->done[j]) {
+            const T beta = (T)((st->rho_new[j] / st->rho[j]) * (st->alpha[j] / st->omega[j]));
+            const T omega = (T)st->omega[j];
+            const size_t base = (size_t)j * N;
+            double a = 0.0;
+            for (int i = bb.b * blockDim.x + threadIdx.x; i < N; i += bb.nb * blockDim.x) {
+                int colk[6];
+                row_cols(A, i, colk);
+                const T pi = v.r[base + i] + beta * (po[base + i] - omega * vo[base + i]);
+                T vi = A.diag[i] * pi;
 #pragma unroll
-        for (int k = 0; k < 6; k++) offk[k] = A.off[(size_t)k * N + i];
+                for (int k = 0; k < 6; k++) {
+                    const size_t q = base + colk[k];
+                    vi += A.off[(size_t)k * N + i] * (v.r[q] + beta * (po[q] - omega * vo[q]));
+                }
+                pn[base + i] = pi;
+                vn[base + i] = vi;
+                a += (double)v.r0[base + i] * (double)vi;
+            }
+#pragma unroll
+            for (int q = 0; q < R; q++) acc[q] = (q == j) ? a : 0.0;
+        }
+    } else {
+        T beta[R], omega[R];
+        bool act[R];
 #pragma unroll
         for (int j = 0; j < R; j++) {
-            if (!act[j]) continue;
-            const size_t base = (size_t)j * N;
-            const T pi = v.r[base + i] + beta[j] * (po[base + i] - omega[j] * vo[base + i]);
-            T vi = d * pi;
+            act[j] = !st->done[j];
+            beta[j] = (T)((st->rho_new[j] / st->rho[j]) * (st->alpha[j] / st->omega[j]));
+            omega[j] = (T)st->omega[j];
+        }
+        for (int i = bb.b * blockDim.x + threadIdx.x; i < N; i += bb.nb * blockDim.x) {
+            const T d = A.diag[i];
+            T offk[6];
+            int colk[6];
+            row_cols(A, i, colk);
 #pragma unroll
-            for (int k = 0; k < 6; k++) {
-                const size_t q = base + colk[k];
-                vi += offk[k] * (v.r[q] + beta[j] * (po[q] - omega[j] * vo[q]));
+            for (int k = 0; k < 6; k++) offk[k] = A.off[(size_t)k * N + i];
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                if (!act[j]) continue;
+                const size_t base = (size_t)j * N;
+                const T pi = v.r[base + i] + beta[j] * (po[base + i] - omega[j] * vo[base + i]);
+                T vi = d * pi;
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    const size_t q = base + colk[k];
+                    vi += offk[k] * (v.r[q] + beta[j] * (po[q] - omega[j] * vo[q]));
+                }
+                pn[base + i] = pi;
+                vn[base + i] = vi;
+                acc[j] += (double)v.r0[base + i] * (double)vi;
             }
-            pn[base + i] = pi;
-            vn[base + i] = vi;
-            acc[j] += (double)v.r0[base + i] * (double)vi;
         }
     }
     if (publish_partials<R>(acc, v.partials, v.counter, sh)) {
@@ -677,45 +737,75 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_bicg_1(EllT<T> A, BicgVector
 }
 
 // s = r - alpha v; t = A s.
-template <typename T, int R>
-__global__ void __launch_bounds__(MCB_THREADS, 4) k_bicg_2(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ vv)
+template <typename T, int R, bool SPLIT>
+__global__ void __launch_bounds__(MCB_THREADS, SPLIT ? 8 : 4) k_bicg_2(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ vv)
 {
     __shared__ double sh[2 * R][MCB_THREADS];
     const BicgState<R> *st = v.st;
     if (st->all_done) return;
     const int N = A.N;
-    T alpha[R];
-    bool act[R];
-#pragma unroll
-    for (int j = 0; j < R; j++) {
-        act[j] = !st->done[j];
-        alpha[j] = (T)st->alpha[j];
-    }
+    const BicgBlocks<R, SPLIT> bb;
     double acc[2 * R];
 #pragma unroll
     for (int j = 0; j < 2 * R; j++) acc[j] = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const T d = A.diag[i];
-        T offk[6];
-        int colk[6];
-        row_cols(A, i, colk);
+    if (SPLIT) {
+        const int j = bb.j0;
+        if (!st->done[j]) {
+            const T alpha = (T)st->alpha[j];
+            const size_t base = (size_t)j * N;
+            double ts = 0.0, tt = 0.0;
+            for (int i = bb.b * blockDim.x + threadIdx.x; i < N; i += bb.nb * blockDim.x) {
+                int colk[6];
+                row_cols(A, i, colk);
+                const T si = v.r[base + i] - alpha * vv[base + i];
+                T ti = A.diag[i] * si;
 #pragma unroll
-        for (int k = 0; k < 6; k++) offk[k] = A.off[(size_t)k * N + i];
+                for (int k = 0; k < 6; k++) {
+                    const size_t q = base + colk[k];
+                    ti += A.off[(size_t)k * N + i] * (v.r[q] - alpha * vv[q]);
+                }
+                v.s[base + i] = si;
+                v.t[base + i] = ti;
+                ts += (double)ti * (double)si;
+                tt += (double)ti * (double)ti;
+            }
+#pragma unroll
+            for (int q = 0; q < R; q++) {
+                acc[2 * q] = (q == j) ? ts : 0.0;
+                acc[2 * q + 1] = (q == j) ? tt : 0.0;
+            }
+        }
+    } else {
+        T alpha[R];
+        bool act[R];
 #pragma unroll
         for (int j = 0; j < R; j++) {
-            if (!act[j]) continue;
-            const size_t base = (size_t)j * N;
-            const T si = v.r[base + i] - alpha[j] * vv[base + i];
-            T ti = d * si;
+            act[j] = !st->done[j];
+            alpha[j] = (T)st->alpha[j];
+        }
+        for (int i = bb.b * blockDim.x + threadIdx.x; i < N; i += bb.nb * blockDim.x) {
+            const T d = A.diag[i];
+            T offk[6];
+            int colk[6];
+            row_cols(A, i, colk);
 #pragma unroll
-            for (int k = 0; k < 6; k++) {
-                const size_t q = base + colk[k];
-                ti += offk[k] * (v.r[q] - alpha[j] * vv[q]);
+            for (int k = 0; k < 6; k++) offk[k] = A.off[(size_t)k * N + i];
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                if (!act[j]) continue;
+                const size_t base = (size_t)j * N;
+                const T si = v.r[base + i] - alpha[j] * vv[base + i];
+                T ti = d * si;
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    const size_t q = base + colk[k];
+                    ti += offk[k] * (v.r[q] - alpha[j] * vv[q]);
+                }
+                v.s[base + i] = si;
+                v.t[base + i] = ti;
+                acc[2 * j] += (double)ti * (double)si;
+                acc[2 * j + 1] += (double)ti * (double)ti;
             }
-            v.s[base + i] = si;
-            v.t[base + i] = ti;
-            acc[2 * j] += (double)ti * (double)si;
-            acc[2 * j + 1] += (double)ti * (double)ti;
         }
     }
     if (publish_partials<2 * R>(acc, v.partials, v.counter, sh)) {
@@ -733,35 +823,60 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_bicg_2(EllT<T> A, BicgVector
 }
 
 // x += alpha p + omega s; r = s - omega t; convergence on ||r||.
-template <typename T, int R>
-__global__ void __launch_bounds__(MCB_THREADS) k_bicg_3(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ p)
+template <typename T, int R, bool SPLIT>
+__global__ void __launch_bounds__(MCB_THREADS, SPLIT ? 8 : 1) k_bicg_3(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ p)
 {
     __shared__ double sh[2 * R][MCB_THREADS];
     const BicgState<R> *st = v.st;
     if (st->all_done) return;
     const int N = A.N;
-    T alpha[R], omega[R];
-    bool act[R];
-#pragma unroll
-    for (int j = 0; j < R; j++) {
-        act[j] = !st->done[j];
-        alpha[j] = (T)st->alpha[j];
-        omega[j] = (T)st->omega[j];
-    }
+    const BicgBlocks<R, SPLIT> bb;
     double acc[2 * R];
 #pragma unroll
     for (int j = 0; j < 2 * R; j++) acc[j] = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    if (SPLIT) {
+        const int j = bb.j0;
+        if (!st->done[j]) {
+            const T alpha = (T)st->alpha[j], omega = (T)st->omega[j];
+            T *x = pick(v.x, j);
+            const size_t base = (size_t)j * N;
+            double rr0 = 0.0, rr = 0.0;
+            for (int i = bb.b * blockDim.x + threadIdx.x; i < N; i += bb.nb * blockDim.x) {
+                const size_t o = base + i;
+                const T si = v.s[o];
+                x[i] += alpha * p[o] + omega * si;
+                const T ri = si - omega * v.t[o];
+                v.r[o] = ri;
+                rr0 += (double)v.r0[o] * (double)ri;
+                rr += (double)ri * (double)ri;
+            }
+#pragma unroll
+            for (int q = 0; q < R; q++) {
+                acc[2 * q] = (q == j) ? rr0 : 0.0;
+                acc[2 * q + 1] = (q == j) ? rr : 0.0;
+            }
+        }
+    } else {
+        T alpha[R], omega[R];
+        bool act[R];
 #pragma unroll
         for (int j = 0; j < R; j++) {
-            if (!act[j]) continue;
-            const size_t o = (size_t)j * N + i;
-            const T si = v.s[o];
-            v.x[j][i] += alpha[j] * p[o] + omega[j] * si;
-            const T ri = si - omega[j] * v.t[o];
-            v.r[o] = ri;
-            acc[2 * j] += (double)v.r0[o] * (double)ri;
-            acc[2 * j + 1] += (double)ri * (double)ri;
+            act[j] = !st->done[j];
+            alpha[j] = (T)st->alpha[j];
+            omega[j] = (T)st->omega[j];
+        }
+        for (int i = bb.b * blockDim.x + threadIdx.x; i < N; i += bb.nb * blockDim.x) {
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                if (!act[j]) continue;
+                const size_t o = (size_t)j * N + i;
+                const T si = v.s[o];
+                v.x[j][i] += alpha[j] * p[o] + omega[j] * si;
+                const T ri = si - omega[j] * v.t[o];
+                v.r[o] = ri;
+                acc[2 * j] += (double)v.r0[o] * (double)ri;
+                acc[2 * j + 1] += (double)ri * (double)ri;
+            }
         }
     }
     if (publish_partials<2 * R>(acc, v.partials, v.counter, sh)) {
@@ -927,20 +1042,28 @@ void bicg_init_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, 
 {
     k_bicg_init<T, R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, max_iters);
 }
+// FP32 systems with several right-hand sides use the split form.
+template <typename T, int R>
+constexpr bool bicg_split() { return sizeof(T) == 4 && R > 1; }
+
 template <typename T, int R>
 void bicg_1_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int pin)
 {
-    k_bicg_1<T, R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.p[pin], v.v[pin], v.p[pin ^ 1], v.v[pin ^ 1]);
+    constexpr bool S = bicg_split<T, R>();
+    k_bicg_1<T, R, S><<<krylov_grid(A.N) * (S ? R : 1), MCB_THREADS, 0, s>>>(A, v, v.p[pin], v.v[pin], v.p[pin ^ 1],
+                                                                            v.v[pin ^ 1]);
 }
 template <typename T, int R>
 void bicg_2_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int vnew)
 {
-    k_bicg_2<T, R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.v[vnew]);
+    constexpr bool S = bicg_split<T, R>();
+    k_bicg_2<T, R, S><<<krylov_grid(A.N) * (S ? R : 1), MCB_THREADS, 0, s>>>(A, v, v.v[vnew]);
 }
 template <typename T, int R>
 void bicg_3_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int pnew)
 {
-    k_bicg_3<T, R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.p[pnew]);
+    constexpr bool S = bicg_split<T, R>();
+    k_bicg_3<T, R, S><<<krylov_grid(A.N) * (S ? R : 1), MCB_THREADS, 0, s>>>(A, v, v.p[pnew]);
 }
 template <int R>
 void bicg_init(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, double rtol, int max_iters)
