@@ -1256,9 +1256,9 @@ void mc_flow_default_params(mc_flow_params *p, int mode)
     p->pressure_solver = MC_PSOLVER_PCG_JACOBI;
     p->precision = MC_PRECISION_FP64;
     p->initial_guess = MC_GUESS_ZERO;
-    p->amg_sweeps = 2;
+    p->amg_sweeps = 3;
     p->amg_omega = 0.6667;
-    p->amg_alpha = 1.8;
+    p->amg_alpha = 2.0;
     p->ir_inner_rtol = 1e-4;
     p->reorder = MC_REORDER_NONE;
     if (mode == MC_MODE_COMPAT) {
