@@ -26,6 +26,15 @@ constexpr int LDT = GNN_TILE + 8;     // row stride of transposed [channel][cell
 constexpr unsigned FULL = 0xffffffffu;
 
 int gnn_blocks(int n) { return (n + GNN_TILE - 1) / GNN_TILE; }
+
+// Multiprocessors of the current device (persistent launches: one block each).
+int sm_count()
+{
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    return n;
+}
 int reduce_grid(int n) { return std::max(1, std::min((n + MCB_THREADS - 1) / MCB_THREADS, 148 * 4)); }
 
 __device__ __forceinline__ uint32_t ld32(const bf16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
@@ -68,6 +77,67 @@ __device__ __forceinline__ void warp_gemm(float (&acc)[MT][NT][4], const bf16 *A
         for (int mt = 0; mt < MT; mt++)
 #pragma unroll
             for (int nt = 0; nt < NT; nt++) mma_bf16(acc[mt][nt], a[mt], b[nt]);
+    }
+}
+
+// Four 8x8 BF16 matrices from shared memory in the mma.m16n8k16 fragment
+// layout (lanes 8m .. 8m + 7 give the row addresses of matrix m).
+__device__ __forceinline__ void ldm_x4(uint32_t (&r)[4], const bf16 *p)
+{
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
+// acc (16 rows x 32 columns) += A[16][16 KS] . W[32][16 KS]^T for one warp,
+// A and W row-major BF16 in shared memory (row strides multiples of 8).
+template <int KS>
+__device__ __forceinline__ void warp_gemm16x32(float (&acc)[1][4][4], const bf16 *A, int lda, const bf16 *W, int ldw,
+                                               int lane)
+{
+#pragma unroll
+    for (int ks = 0; ks < KS; ks++) {
+        uint32_t a[4];
+        ldm_x4(a, A + (lane & 15) * lda + ks * 16 + (lane >> 4) * 8);
+#pragma unroll
+        for (int np = 0; np < 2; np++) {
+            uint32_t b[4];
+            ldm_x4(b, W + (np * 16 + (lane & 7) + ((lane >> 4) << 3)) * ldw + ks * 16 + ((lane >> 3) & 1) * 8);
+            const uint32_t b0[2] = {b[0], b[1]}, b1[2] = {b[2], b[3]};
+            mma_bf16(acc[0][2 * np], a, b0);
+            mma_bf16(acc[0][2 * np + 1], a, b1);
+        }
+    }
+}
+
+// B fragments of a [32][16 KS] row-major tile (W-form) for warp_gemm16x32r:
+// fr[ks][np] holds n-tiles 2 np, 2 np + 1 of k-step ks.
+template <int KS>
+__device__ __forceinline__ void load_bfrags(uint32_t (&fr)[KS][2][4], const bf16 *W, int ldw, int lane)
+{
+#pragma unroll
+    for (int ks = 0; ks < KS; ks++)
+#pragma unroll
+        for (int np = 0; np < 2; np++)
+            ldm_x4(fr[ks][np], W + (np * 16 + (lane & 7) + ((lane >> 4) << 3)) * ldw + ks * 16 + ((lane >> 3) & 1) * 8);
+}
+
+// acc (16 x 32) += A[16][16 KS] . W^T with W's fragments in registers.
+template <int KS>
+__device__ __forceinline__ void warp_gemm16x32r(float (&acc)[1][4][4], const bf16 *A, int lda,
+                                                const uint32_t (&fr)[KS][2][4], int lane)
+{
+#pragma unroll
+    for (int ks = 0; ks < KS; ks++) {
+        uint32_t a[4];
+        ldm_x4(a, A + (lane & 15) * lda + ks * 16 + (lane >> 4) * 8);
+#pragma unroll
+        for (int np = 0; np < 2; np++) {
+            const uint32_t b0[2] = {fr[ks][np][0], fr[ks][np][1]}, b1[2] = {fr[ks][np][2], fr[ks][np][3]};
+            mma_bf16(acc[0][2 * np], a, b0);
+            mma_bf16(acc[0][2 * np + 1], a, b1);
+        }
     }
 }
 
@@ -433,41 +503,37 @@ __global__ void k_gnn_fold(const float *__restrict__ p, GnnGraph g, bf16 *__rest
     }
 }
 
-// Shared memory of k_gnn_layer_fold: seven row tiles [7][128][LDH] -- the
-// cells' own rows and their neighbours through the six directions (zeros on
-// the boundary) -- then the layer's weights: the seven folded W1 slots
-// [7][32][LDH] and W2 [32][LDH].
+// Shared memory of k_gnn_layer_fold: the layer's weights -- the seven folded
+// W1 slots [7][32][LDH] and W2 [32][LDH] -- then two buffers of seven row
+// tiles [7][128][LDH] (the cells' own rows and their neighbours through the
+// six directions, zeros on the boundary).
+constexpr size_t FOLD_SMEM_W = sizeof(bf16) * 8 * GNN_H * LDH;
 constexpr size_t FOLD_SMEM_T = sizeof(bf16) * 7 * GNN_TILE * LDH;
-constexpr size_t FOLD_SMEM = FOLD_SMEM_T + sizeof(bf16) * 8 * GNN_H * LDH;
+constexpr size_t FOLD_SMEM = FOLD_SMEM_W + 2 * FOLD_SMEM_T;
 
-// One message-passing layer on a graph in offset form (inference).
-// z = sum_k T_k Wf_k^T over the seven staged tiles, a = relu(z + c1),
-// h' = h + W2 a + c2; 256 threads, warp w owns rows 16w .. 16w + 15.
-__global__ void __launch_bounds__(LAYER_THREADS) k_gnn_layer_fold(GnnGraph g, const float *__restrict__ pl,
-                                                                  const bf16 *__restrict__ wf,
-                                                                  const bf16 *__restrict__ pkl,
-                                                                  const bf16 *__restrict__ hin,
-                                                                  bf16 *__restrict__ hout)
+// Mask bytes of this thread's two rows of a tile (0 beyond the last cell).
+__device__ __forceinline__ void load_fold_masks(const GnnGraph &g, int base, unsigned (&mk)[2])
 {
-    extern __shared__ __align__(16) unsigned char smem[];
-    bf16 *sT = reinterpret_cast<bf16 *>(smem);
-    bf16 *sW = reinterpret_cast<bf16 *>(smem + FOLD_SMEM_T);  // [8][32][LDH]: 7 folded W1 slots, W2
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int c4 = tid & 3, r0 = tid >> 2;
-    const int n = g.n, base = blockIdx.x * GNN_TILE;
-    // weights: 8 x 32 rows of 64 bytes, 4 chunks per thread
+    const int r0 = threadIdx.x >> 2;
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int e = tid + LAYER_THREADS * q, row = e >> 2, part = e & 3;  // row 0..255
-        const bf16 *src = row < 7 * GNN_H ? wf + (size_t)row * GNN_H : pkl + GKL_W2 + (size_t)(row - 7 * GNN_H) * GNN_H;
-        cp_async16(sW + row * LDH + part * 8, src + part * 8, 16);
+    for (int q = 0; q < 2; q++) {
+        const int i = base + r0 + 64 * q;
+        mk[q] = i < g.n ? g.mask[i] : 0u;
     }
+}
+
+// Asynchronous copies of one tile's seven row tiles (thread = chunk of 8
+// channels x rows r, r + 64), with the rows' masks already in registers.
+__device__ __forceinline__ void stage_fold_tile(const GnnGraph &g, const bf16 *__restrict__ hin, bf16 *sT, int base,
+                                                const unsigned (&mks)[2])
+{
+    const int c4 = threadIdx.x & 3, r0 = threadIdx.x >> 2, n = g.n;
 #pragma unroll
     for (int q = 0; q < 2; q++) {
         const int r = r0 + 64 * q, i = base + r;
         const bool in = i < n;
         cp_async16(sT + r * LDH + c4 * 8, hin + (size_t)(in ? i : 0) * GNN_H + c4 * 8, in ? 16 : 0);
-        const unsigned mk = in ? g.mask[i] : 0u;
+        const unsigned mk = mks[q];
 #pragma unroll
         for (int k = 0; k < 6; k++) {
             const bool ok = (mk >> k) & 1u;
@@ -475,6 +541,43 @@ __global__ void __launch_bounds__(LAYER_THREADS) k_gnn_layer_fold(GnnGraph g, co
             cp_async16(sT + ((1 + k) * GNN_TILE + r) * LDH + c4 * 8, hin + (size_t)j * GNN_H + c4 * 8, ok ? 16 : 0);
         }
     }
+}
+
+// One message-passing layer on a graph in offset form (inference),
+// persistent: one block per SM keeps the weights, prefetches the next tile
+// while computing the current one.  Per tile: z = sum_k T_k Wf_k^T over the
+// seven staged tiles, a = relu(z + c1), h' = h + W2 a + c2; warp w owns rows
+// 16w .. 16w + 15.
+__global__ void __launch_bounds__(LAYER_THREADS, 1) k_gnn_layer_fold(GnnGraph g, const float *__restrict__ pl,
+                                                                     const bf16 *__restrict__ wf,
+                                                                     const bf16 *__restrict__ pkl,
+                                                                     const bf16 *__restrict__ hin,
+                                                                     bf16 *__restrict__ hout, int ntiles)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    bf16 *sW = reinterpret_cast<bf16 *>(smem);  // [8][32][LDH]: 7 folded W1 slots, W2
+    auto tile_buf = [&](int b) { return reinterpret_cast<bf16 *>(smem + FOLD_SMEM_W + (size_t)b * FOLD_SMEM_T); };
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = g.n;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {  // 8 x 32 weight rows of 64 bytes, 4 chunks per thread
+        const int e = tid + LAYER_THREADS * q, row = e >> 2, part = e & 3;
+        const bf16 *src = row < 7 * GNN_H ? wf + (size_t)row * GNN_H : pkl + GKL_W2 + (size_t)(row - 7 * GNN_H) * GNN_H;
+        cp_async16(sW + row * LDH + part * 8, src + part * 8, 16);
+    }
+    int tile = blockIdx.x;
+    unsigned mk[2];
+    load_fold_masks(g, tile * GNN_TILE, mk);
+    if (tile < ntiles) stage_fold_tile(g, hin, tile_buf(0), tile * GNN_TILE, mk);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    load_fold_masks(g, (tile + gridDim.x) * GNN_TILE, mk);  // one tile ahead of the copies
+    // the layer's weight fragments stay in registers for the whole launch
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    uint32_t w1f[7][2][2][4], w2f[2][2][4];
+#pragma unroll
+    for (int k = 0; k < 7; k++) load_bfrags<2>(w1f[k], sW + k * GNN_H * LDH, LDH, lane);
+    load_bfrags<2>(w2f, sW + 7 * GNN_H * LDH, LDH, lane);
     const int gq = lane >> 2, tq = lane & 3;
     float b1[4][2], b2[4][2];
 #pragma unroll
@@ -484,45 +587,61 @@ __global__ void __launch_bounds__(LAYER_THREADS) k_gnn_layer_fold(GnnGraph g, co
             b1[nt][e] = pl[GPL_C1 + nt * 8 + 2 * tq + e];
             b2[nt][e] = pl[GPL_C2 + nt * 8 + 2 * tq + e];
         }
-    cp_async_wait_all();
-    __syncthreads();
-    float acc[1][4][4];
-    zero(acc);
+    for (int buf = 0; tile < ntiles; tile += gridDim.x, buf ^= 1) {
+        const int next = tile + gridDim.x;
+        if (next < ntiles) stage_fold_tile(g, hin, tile_buf(buf ^ 1), next * GNN_TILE, mk);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        load_fold_masks(g, (next + gridDim.x) * GNN_TILE, mk);  // lands while this tile computes
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this tile (and the weights) landed
+        __syncthreads();
+        bf16 *sT = tile_buf(buf);
+        const int base = tile * GNN_TILE;
+        float acc[1][4][4], acc2[1][4][4];  // even and odd slots: two independent accumulation chains
+        zero(acc);
+        zero(acc2);
 #pragma unroll
-    for (int k = 0; k < 7; k++)
-        warp_gemm<1, 4, 2>(acc, sT + (k * GNN_TILE + warp * 16) * LDH, LDH, sW + k * GNN_H * LDH, LDH, lane);
-    __syncwarp();  // the warp's reads of its rows are done; tile 1 rows now take a, then h'
-    bf16 *sA = sT + GNN_TILE * LDH;
+        for (int k = 0; k < 7; k += 2) warp_gemm16x32r<2>(acc, sT + (k * GNN_TILE + warp * 16) * LDH, LDH, w1f[k], lane);
 #pragma unroll
-    for (int nt = 0; nt < 4; nt++)
+        for (int k = 1; k < 7; k += 2) warp_gemm16x32r<2>(acc2, sT + (k * GNN_TILE + warp * 16) * LDH, LDH, w1f[k], lane);
 #pragma unroll
-        for (int hf = 0; hf < 2; hf++) {
-            const int row = warp * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq;
-            *reinterpret_cast<bf162 *>(sA + row * LDH + col) =
-                __floats2bfloat162_rn(fmaxf(acc[0][nt][2 * hf] + b1[nt][0], 0.f),
-                                      fmaxf(acc[0][nt][2 * hf + 1] + b1[nt][1], 0.f));
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[0][nt][e] += acc2[0][nt][e];
+        __syncwarp();  // the warp's reads of its rows are done; tile 1 rows now take a, then h'
+        bf16 *sA = sT + GNN_TILE * LDH;
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int hf = 0; hf < 2; hf++) {
+                const int row = warp * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq;
+                *reinterpret_cast<bf162 *>(sA + row * LDH + col) =
+                    __floats2bfloat162_rn(fmaxf(acc[0][nt][2 * hf] + b1[nt][0], 0.f),
+                                          fmaxf(acc[0][nt][2 * hf + 1] + b1[nt][1], 0.f));
+            }
+        __syncwarp();
+        zero(acc);
+        warp_gemm16x32r<2>(acc, sA + warp * 16 * LDH, LDH, w2f, lane);
+        __syncwarp();
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int hf = 0; hf < 2; hf++) {
+                const int row = warp * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq;
+                const float2 hv = __bfloat1622float2(*reinterpret_cast<const bf162 *>(sT + row * LDH + col));
+                *reinterpret_cast<bf162 *>(sA + row * LDH + col) = __floats2bfloat162_rn(
+                    hv.x + (acc[0][nt][2 * hf] + b2[nt][0]), hv.y + (acc[0][nt][2 * hf + 1] + b2[nt][1]));
+            }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int row = warp * 16 + (lane >> 2) + 8 * q, i = base + row;
+            if (i < n)
+                *reinterpret_cast<uint4 *>(hout + (size_t)i * GNN_H + (lane & 3) * 8) =
+                    *reinterpret_cast<const uint4 *>(sA + row * LDH + (lane & 3) * 8);
         }
-    __syncwarp();
-    zero(acc);
-    warp_gemm<1, 4, 2>(acc, sA + warp * 16 * LDH, LDH, sW + 7 * GNN_H * LDH, LDH, lane);
-    __syncwarp();
-#pragma unroll
-    for (int nt = 0; nt < 4; nt++)
-#pragma unroll
-        for (int hf = 0; hf < 2; hf++) {
-            const int row = warp * 16 + gq + 8 * hf, col = nt * 8 + 2 * tq;
-            const float2 hv = __bfloat1622float2(*reinterpret_cast<const bf162 *>(sT + row * LDH + col));
-            *reinterpret_cast<bf162 *>(sA + row * LDH + col) = __floats2bfloat162_rn(
-                hv.x + (acc[0][nt][2 * hf] + b2[nt][0]), hv.y + (acc[0][nt][2 * hf + 1] + b2[nt][1]));
-        }
-    __syncwarp();
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-        const int row = warp * 16 + (lane >> 2) + 8 * q, i = base + row;
-        if (i < n)
-            *reinterpret_cast<uint4 *>(hout + (size_t)i * GNN_H + (lane & 3) * 8) =
-                *reinterpret_cast<const uint4 *>(sA + row * LDH + (lane & 3) * 8);
+        __syncthreads();  // every warp is done with this buffer before it is refilled
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // Load a [128][32] BF16 tile of rows base.. into shared memory (row stride LDH).
@@ -1070,8 +1189,8 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
         if (train)
             k_gnn_layer<true><<<nb, LAYER_THREADS, LAYER_SMEM, s>>>(g, pl, pkl, w.h[l], w.h[l + 1], w.a[l]);
         else if (folded)
-            k_gnn_layer_fold<<<nb, LAYER_THREADS, FOLD_SMEM, s>>>(g, pl, w.fold + (size_t)l * 7 * GNN_H * GNN_H, pkl,
-                                                                 w.h[l & 1], w.h[(l + 1) & 1]);
+            k_gnn_layer_fold<<<std::min(nb, sm_count()), LAYER_THREADS, FOLD_SMEM, s>>>(
+                g, pl, w.fold + (size_t)l * 7 * GNN_H * GNN_H, pkl, w.h[l & 1], w.h[(l + 1) & 1], nb);
         else
             k_gnn_layer<false><<<nb, LAYER_THREADS, LAYER_SMEM, s>>>(g, pl, pkl, w.h[l & 1], w.h[(l + 1) & 1], nullptr);
     }
