@@ -191,82 +191,112 @@ __global__ void k_amg_galerkin(AmgLevelT<T> fine, AmgLevelT<T> coarse)
 }
 
 // Dense Cholesky of A + sigma 1 1^T (sigma = mean diagonal / n) on the
-// coarsest level, one block, FP64 (factor in shared memory), then its
-// explicit symmetric inverse, row-major in `dense` for the V-cycle's solve.
+// coarsest level, one block of DENSE_THREADS, FP64 (factor in shared memory),
+// then its explicit symmetric inverse, row-major in `dense` for the V-cycle's
+// solve.  The trailing updates run one warp per row (lanes over columns);
+// the inverse one warp per column, with warp-reduced inner products.
+constexpr int DENSE_THREADS = 1024;
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 template <typename T>
-__global__ void k_amg_dense_factor(AmgLevelT<T> L, double *dense)
+__global__ void __launch_bounds__(DENSE_THREADS) k_amg_dense_factor(AmgLevelT<T> L, double *dense)
 {
     extern __shared__ double A[];
-    const int n = L.n, t = threadIdx.x;
-    __shared__ double sigma;
-    if (t == 0) {
-        double s = 0.0;
-        for (int i = 0; i < n; i++) s += (double)L.diag[i];
-        sigma = (s / n) / n;
+    // A: [n][ld] in shared memory, ld = n + 1 so that column accesses spread over the banks
+    const int n = L.n, ld = n + 1, t = threadIdx.x, lane = t & 31, warp = t >> 5, nwarps = blockDim.x >> 5;
+    __shared__ double sigma, wsum[DENSE_THREADS / 32];
+    {
+        double s = warp_sum(t < n ? (double)L.diag[t] : 0.0);
+        if (lane == 0) wsum[warp] = s;
+        __syncthreads();
+        if (t == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < nwarps; w++) tot += wsum[w];
+            sigma = (tot / n) / n;
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    for (int idx = t; idx < n * n; idx += blockDim.x) A[idx] = sigma;
+    for (int idx = t; idx < n * ld; idx += blockDim.x) A[idx] = sigma;
     __syncthreads();
     if (t < n) {
-        A[t * n + t] += (double)L.diag[t];
+        A[t * ld + t] += (double)L.diag[t];
         for (int q = 0; q < L.k; q++) {
             const int j = L.col[(size_t)q * n + t];
-            if (j != t) A[t * n + j] += (double)L.off[(size_t)q * n + t];
+            if (j != t) A[t * ld + j] += (double)L.off[(size_t)q * n + t];
         }
     }
     __syncthreads();
     for (int j = 0; j < n; j++) {
-        if (t == 0) {
-            const double d = A[j * n + j];
-            A[j * n + j] = d > 0.0 ? sqrt(d) : 1.0;
+        // column j below the pivot divided by sqrt(pivot); the pivot itself is
+        // replaced only after the trailing update, which does not read it
+        const double d = A[j * ld + j], sq = d > 0.0 ? sqrt(d) : 1.0;
+        if (t > j && t < n) A[t * ld + j] /= sq;
+        __syncthreads();
+        for (int r = j + 1 + warp; r < n; r += nwarps) {
+            const double lrj = A[r * ld + j];
+            for (int c = j + 1 + lane; c <= r; c += 32) A[r * ld + c] -= lrj * A[c * ld + j];
         }
-        __syncthreads();
-        if (t > j && t < n) A[t * n + j] /= A[j * n + j];
-        __syncthreads();
-        if (t > j && t < n)
-            for (int c = j + 1; c <= t; c++) A[t * n + c] -= A[t * n + j] * A[c * n + j];
+        if (t == j) A[j * ld + j] = sq;
         __syncthreads();
     }
-    // explicit inverse, column t by thread t: L y = e_t, then L^T x = y; the
-    // column is built in place in `dense` (this thread's column only)
-    if (t < n) {
-        for (int i = 0; i < t; i++) dense[i * n + t] = 0.0;  // L y = e_t: y_i = 0 above row t
-        for (int i = t; i < n; i++) {
-            double v = (i == t) ? 1.0 : 0.0;
-            for (int c = t; c < i; c++) v -= A[i * n + c] * dense[c * n + t];
-            dense[i * n + t] = v / A[i * n + i];
+    // L^{-1} in place, columns from the last to the first: for i > j,
+    // Linv[i][j] = -(sum_{k=j+1..i} Linv[i][k] L[k][j]) / L[j][j] uses the
+    // finished columns k > j and the still original column j.
+    __shared__ double colj[AMG_COARSEST_MAX];
+    for (int j = n - 1; j >= 0; j--) {
+        for (int i = j + 1 + warp; i < n; i += nwarps) {
+            double p = 0.0;
+            for (int k = j + 1 + lane; k <= i; k += 32) p += A[i * ld + k] * A[k * ld + j];
+            p = warp_sum(p);
+            if (lane == 0) colj[i] = -p / A[j * ld + j];
         }
-        for (int i = n - 1; i >= 0; i--) {
-            double v = dense[i * n + t];
-            for (int c = i + 1; c < n; c++) v -= A[c * n + i] * dense[c * n + t];
-            dense[i * n + t] = v / A[i * n + i];
-        }
+        __syncthreads();
+        if (t > j && t < n) A[t * ld + j] = colj[t];
+        if (t == j) A[j * ld + j] = 1.0 / A[j * ld + j];
+        __syncthreads();
     }
-    __syncthreads();
-    // symmetrise (the inverse of a symmetric matrix), pair (t, j > t) by thread t
-    if (t < n)
-        for (int j = t + 1; j < n; j++) {
-            const double m = 0.5 * (dense[t * n + j] + dense[j * n + t]);
-            dense[t * n + j] = m;
-            dense[j * n + t] = m;
-        }
+    // (A + sigma 1 1^T)^{-1} = L^{-T} L^{-1}: entry (i, j) = sum_{k >= max(i, j)} Linv[k][i] Linv[k][j],
+    // the same sum in the same order for (j, i), so the result is exactly symmetric
+    for (int idx = t; idx < n * n; idx += blockDim.x) {
+        const int i = idx / n, j = idx % n;
+        double p = 0.0;
+        for (int k = max(i, j); k < n; k++) p += A[k * ld + i] * A[k * ld + j];
+        dense[idx] = p;
+    }
 }
 
 // e = (A + sigma 1 1^T)^{-1} r on the coarsest level: one dense product with
 // the symmetric inverse formed at setup; thread t computes row t (the reads
 // dense[j][t] are coalesced across threads).
+constexpr int DENSE_SOLVE_PARTS = 8;  // threads per row of the dense product
+
 template <typename T>
-__global__ void k_amg_dense_solve(AmgLevelT<T> L, const double *__restrict__ dense, const PcgState *st)
+__global__ void __launch_bounds__(AMG_COARSEST_MAX * DENSE_SOLVE_PARTS)
+    k_amg_dense_solve(AmgLevelT<T> L, const double *__restrict__ dense, const PcgState *st)
 {
     if (st->done) return;
     __shared__ double r[AMG_COARSEST_MAX];
-    const int n = L.n, t = threadIdx.x;
+    __shared__ double part[DENSE_SOLVE_PARTS][AMG_COARSEST_MAX];
+    const int n = L.n, t = threadIdx.x, row = t % AMG_COARSEST_MAX, q = t / AMG_COARSEST_MAX;
     if (t < n) r[t] = (double)L.r[t];
     __syncthreads();
+    const int chunk = (n + DENSE_SOLVE_PARTS - 1) / DENSE_SOLVE_PARTS;
+    double y = 0.0;
+    if (row < n)
+        for (int j = q * chunk; j < min(n, (q + 1) * chunk); j++) y += dense[(size_t)j * n + row] * r[j];
+    part[q][row] = y;
+    __syncthreads();
     if (t < n) {
-        double y = 0.0;
-        for (int j = 0; j < n; j++) y += dense[(size_t)j * n + t] * r[j];
-        L.e[0][t] = (T)y;
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < DENSE_SOLVE_PARTS; k++) s += part[k][t];
+        L.e[0][t] = (T)s;
     }
 }
 
@@ -345,7 +375,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_amg_final(AmgLevelT<T> L, T ome
 
 namespace {
 inline int blocks(int n) { return std::max(1, (n + MCB_THREADS - 1) / MCB_THREADS); }
-inline size_t dense_smem(int n) { return (size_t)n * n * sizeof(double); }
+inline size_t dense_smem(int n) { return (size_t)n * (n + 1) * sizeof(double); }
 
 template <typename T>
 const AmgLevelT<T> *levels_of(const AmgHierarchy &H);
@@ -377,7 +407,7 @@ void amg_setup_values(cudaStream_t s, const AmgHierarchy &H)
     for (int l = 1; l < H.levels; l++) k_amg_galerkin<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l - 1], lv[l]);
     set_dense_attributes<T>();
     const AmgLevelT<T> &C = lv[H.levels - 1];
-    k_amg_dense_factor<T><<<1, AMG_COARSEST_MAX, dense_smem(C.n), s>>>(C, H.dense);
+    k_amg_dense_factor<T><<<1, DENSE_THREADS, dense_smem(C.n), s>>>(C, H.dense);
 }
 
 int amg_kernels_per_vcycle(const AmgHierarchy &H) { return (H.levels - 1) * (2 * H.sweeps + 2) + 1; }
@@ -406,7 +436,7 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
         cur[l] = c;
         k_amg_restrict<T><<<blocks(lv[l + 1].n), MCB_THREADS, 0, s>>>(lv[l], lv[l + 1], lv[l].e[c], st);
     }
-    k_amg_dense_solve<T><<<1, AMG_COARSEST_MAX, 0, s>>>(lv[L - 1], H.dense, st);
+    k_amg_dense_solve<T><<<1, AMG_COARSEST_MAX * DENSE_SOLVE_PARTS, 0, s>>>(lv[L - 1], H.dense, st);
     cur[L - 1] = 0;
     for (int l = L - 2; l >= 0; l--) {
         int c = cur[l];
