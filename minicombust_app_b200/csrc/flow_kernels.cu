@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_precomp_au(Physics ph, MeshArgs
 // calculate_UVW (:1689-1729) and setup/update_sparse_matrix (:1186-1339) for
 // the three velocity components at once.  The U, V and W systems share the
 // off-diagonal coefficients and, bit for bit, the diagonal.
-__global__ void __launch_bounds__(MCB_THREADS) k_momentum_assemble(Physics ph, MeshArgs m, MomentumArgs a)
+__global__ void __launch_bounds__(MCB_THREADS, 4) k_momentum_assemble(Physics ph, MeshArgs m, MomentumArgs a)
 {
     const int N = ph.N;
     const int c = grid_stride_start();
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_momentum_assemble(Physics ph, M
 // ------------------------------------------------------------- temperature
 // FluxScalar(TEMP) (FlowSolver.inl:2516-2744), unsteady term and
 // setup_sparse_matrix of Scalar_solve (:2885-2953).
-__global__ void __launch_bounds__(MCB_THREADS) k_temperature_assemble(Physics ph, MeshArgs m, ScalarArgs a)
+__global__ void __launch_bounds__(MCB_THREADS, 4) k_temperature_assemble(Physics ph, MeshArgs m, ScalarArgs a)
 {
     const int N = ph.N;
     const int c = grid_stride_start();
@@ -399,7 +399,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_temperature_assemble(Physics ph
 // calculate_mass_flux face loop (FlowSolver.inl:1885-2007): Rhie-Chow flux
 // and -ApV on internal faces; inlet, outlet and wall fluxes; partial sums
 // of the boundary balance (:2010-2034), finished by the last block.
-__global__ void __launch_bounds__(MCB_THREADS) k_mass_flux(Physics ph, MeshArgs m, MassFluxArgs a)
+__global__ void __launch_bounds__(MCB_THREADS, 4) k_mass_flux(Physics ph, MeshArgs m, MassFluxArgs a)
 {
     __shared__ double sh[3][MCB_THREADS];
     const int N = ph.N, F = m.F;
@@ -512,7 +512,7 @@ __global__ void k_outlet_fix(Physics ph, MeshArgs m, double *__restrict__ mdot, 
 
 // Pressure-correction rows (the S_U accumulation of calculate_mass_flux,
 // :1964 and :2101, and setup_pressure_matrix, :2139-2189).
-__global__ void __launch_bounds__(MCB_THREADS) k_pressure_rows(Physics ph, MeshArgs m, PressureRowArgs a)
+__global__ void __launch_bounds__(MCB_THREADS, 4) k_pressure_rows(Physics ph, MeshArgs m, PressureRowArgs a)
 {
     const int N = ph.N;
     const int c = grid_stride_start();
@@ -560,7 +560,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pressure_rows(Physics ph, MeshA
 // ------------------------------------------------------- corrector updates
 // Face part of one corrector pass of calculate_pressure: mass flux += a_f
 // (PP_N - PP_P) (:2402-2412) then update_mass_flux (:1812-1878).
-__global__ void __launch_bounds__(MCB_THREADS) k_pp_correct_faces(Physics ph, MeshArgs m, CorrectArgs a)
+__global__ void __launch_bounds__(MCB_THREADS, 4) k_pp_correct_faces(Physics ph, MeshArgs m, CorrectArgs a)
 {
     const int N = ph.N, F = m.F;
     for (int face = grid_stride_start(); face < F; face += gridDim.x * blockDim.x) {
@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pp_correct_faces(Physics ph, Me
 // simple mode, only cell 0 on the first call in compat mode), the next
 // corrector's right-hand side from the non-orthogonal flux corrections
 // (:1875-1876, simple mode), and PP = 0 (:2447-2450).
-__global__ void __launch_bounds__(MCB_THREADS) k_pp_correct_cells(Physics ph, MeshArgs m, CorrectArgs a,
+__global__ void __launch_bounds__(MCB_THREADS, 4) k_pp_correct_cells(Physics ph, MeshArgs m, CorrectArgs a,
                                                                   int correct_all, int correct_cell0)
 {
     const int N = ph.N;
