@@ -128,20 +128,33 @@ class ClockSampler:
 
 def kernel_bytes(name, N, F, nnz_off):
     """Algorithmic (unique-touch) bytes of one launch: each stored input
-    element read once, each output written once, at its stored type."""
+    element read once, each output written once, at its stored type.  The
+    solver kernels read a 4-byte direction code per row instead of the six
+    int32 columns (structured box); ELL values include the boundary padding."""
     return {
-        "pcg_iter1_spmv": 12 * nnz_off + 40 * N,   # diag, off+col, z, p_old -> p_new, q
-        "pcg_iter2_update": 64 * N,                # x rw, r rw, p, q, diag -> z
-        "pcg32_iter1_spmv": 8 * nnz_off + 20 * N,  # FP32 values, int32 columns
-        "bicg3_1_spmv": 12 * nnz_off + 8 * N + 3 * 48 * N,
-        "bicg3_2_spmv": 12 * nnz_off + 8 * N + 3 * 32 * N,
-        "bicg3_3_update": 3 * 56 * N,
+        "pcg_iter1_spmv": 92 * N,      # diag, 6 off, code, (z, p) pair -> p, q
+        "pcg32_iter1_spmv": 48 * N,    # the same in FP32
+        "pcg_iter2_update": 64 * N,    # x rw, r rw, p, q, diag -> z (Jacobi path)
+        "bicg3_1_spmv": 204 * N,       # matrix 60 + 3 x (r, p, v gathered; r0; p, v out)
+        "bicg3_2_spmv": 156 * N,       # matrix 60 + 3 x (r, v gathered; s, t out)
+        "bicg3_3_update": 168 * N,     # 3 x (s, p, t, r0, x rw, r out)
+        "bicg3_32_1_spmv": 104 * N,    # FP32, split per right-hand side
+        "bicg3_32_2_spmv": 80 * N,
+        "bicg3_32_3_update": 84 * N,
         "lsq_gradients_uvwpt": 208 * N,
         "momentum_assemble": 56 * F + 296 * N,
         "mass_flux": 88 * F + 176 * N,
         "pressure_rows": 24 * F + 120 * N,
         "temperature_assemble": 40 * F + 168 * N,
     }.get(name)
+
+
+# DRAM bytes per row (read + write) of one launch, measured with ncu on the
+# 2 x 96^3 case (a full capture of the 2 x 128^3 case is too large); scaled by
+# rows to the bench size for the roofline's `traffic`.
+NCU_DRAM_BYTES_PER_ROW = {
+    "pcg_iter1_spmv": 101.7, "pcg32_iter1_spmv": 43.0, "bicg3_1_spmv": 211.9, "bicg3_32_1_spmv": 102.5,
+}
 
 
 def measured_peaks():
@@ -278,8 +291,12 @@ def roofline_of(solver, mesh, N):
             continue
         avg_s = ms / cnt / 1e3
         achieved = b / avg_s / 1e9
+        per_row = NCU_DRAM_BYTES_PER_ROW.get(name)
         roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": kind, "traffic": None, "bytes_per_launch": b,
+                "frac": achieved / peak, "peak_source": kind,
+                "traffic": per_row * N if per_row else None,
+                "traffic_source": "ncu dram__bytes_read+write on 2x96^3, scaled by rows" if per_row else None,
+                "bytes_per_launch": b,
                 "avg_launch_us": avg_s * 1e6, "launches_per_step": cnt, "share_of_step": ms / total}
         break
     return roof, {k: round(v[0], 4) for k, v in kt.items() if v[1] > 0}
