@@ -44,7 +44,8 @@ typedef enum mc_status {
     MC_ERR_NONFINITE = -4,      /* a residual or reduction became NaN/Inf */
     MC_ERR_MESH = -5,           /* mesh arrays inconsistent */
     MC_ERR_NOMEM = -6,          /* device or host allocation failed */
-    MC_ERR_UNSUPPORTED = -7     /* option not available in this build */
+    MC_ERR_UNSUPPORTED = -7,    /* option not available in this build */
+    MC_ERR_TIMEOUT = -8         /* a bounded device-side wait gave up (tensor-core kernels) */
 } mc_status;
 
 enum { MC_MODE_COMPAT = 0, MC_MODE_SIMPLE = 1 };

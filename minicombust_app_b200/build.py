@@ -30,6 +30,7 @@ CUDA_SOURCES = [
     ("flow_api.cu", []),
     ("solve_noalloc.cu", []),
     ("gnn.cu", []),
+    ("gnn_umma.cu", []),
     ("gnn_api.cu", []),
 ]
 CXX_SOURCES = [("mesh_setup.cpp", ["-ffp-contract=off", "-fno-fast-math"])]

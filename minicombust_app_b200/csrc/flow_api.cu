@@ -314,6 +314,8 @@ int select_guess(mc_flow *h, const Ell &A, const double *b, const PcgState *st, 
             GnnInput<double> in{b, &st->mean, A.diag, h->pp_prev};
             gnn_forward<double>(h->stream, h->gnn_g, in, h->gnn_p, h->gnn_pk, h->gnn_w, h->x0_learned);
         });
+        CUDA_TRY(h, cudaMemcpyAsync(&h->gs->net_status, h->gnn_w.status, sizeof(int), cudaMemcpyDeviceToDevice,
+                                    h->stream));
         h->launches += gnn_forward_launches() - 1;
     }
     launch(h, K_GUESS, [&] {
@@ -331,6 +333,8 @@ int after_pressure_solve(mc_flow *h)
 {
     if (h->prm.initial_guess != MC_GUESS_ZERO) {
         const GuessState &g = *h->h_gs;  // the copy was ordered before the solve's final synchronisation
+        if (h->corrector == 1 && h->prm.initial_guess == MC_GUESS_LEARNED && g.net_status)
+            return fail(h, MC_ERR_TIMEOUT, "learned-guess layer kernel gave up waiting (prediction zeroed)");
         h->guess_choice = g.choice;
         h->guess_rel = g.bb > 0 ? std::sqrt((g.choice < 0 ? g.bb : g.rc) / g.bb) : 1.0;
     }
@@ -1827,6 +1831,7 @@ const char *mc_status_string(int s)
     case MC_ERR_MESH: return "inconsistent mesh";
     case MC_ERR_NOMEM: return "out of memory";
     case MC_ERR_UNSUPPORTED: return "unsupported option";
+    case MC_ERR_TIMEOUT: return "device-side wait timed out";
     default: return "unknown status";
     }
 }

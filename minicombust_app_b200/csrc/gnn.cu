@@ -1,9 +1,10 @@
 // Learned initial guess: forward, backward and Adam kernels (see gnn.cuh).
 //
-// Every dense product is a block-level GEMM over a tile of 128 cells on the
-// tensor cores (mma.sync.m16n8k16, BF16 operands from shared memory, FP32
-// accumulators): with K = 32 or 64 and N = 32 the tiles are far below the
-// 128 x N minimum of a tcgen05 MMA, and the kernels are bound by the
+// Inference on a graph in offset form runs each layer as one tcgen05 kernel
+// (gnn_umma.cu).  The other dense products -- training, the general-graph
+// layer, encoder and decoder -- are block-level GEMMs over a tile of 128
+// cells with mma.sync.m16n8k16 (BF16 operands from shared memory, FP32
+// accumulators); with K = 32 or 64 and N = 32 they are bound by the
 // activation traffic, not by the products.  Weight gradients are per-block
 // partial GEMMs (cells as the reduction dimension) summed afterwards in block
 // order, so training is deterministic.
@@ -242,7 +243,8 @@ union Chunk8 {
 // the weights in shared memory, four 16-byte stores.
 template <typename T>
 __global__ void __launch_bounds__(GNN_TILE) k_gnn_encode(GnnGraph g, GnnInput<T> in, const float *__restrict__ p,
-                                                         const GnnScales *__restrict__ scp, bf16 *__restrict__ hout)
+                                                         const GnnScales *__restrict__ scp, bf16 *__restrict__ hout,
+                                                         int planar)
 {
     __shared__ float sw[GNN_H * (GNN_IN + 1)];
     for (int e = threadIdx.x; e < GNN_H * (GNN_IN + 1); e += GNN_TILE) sw[e] = p[GP_WE + e];  // We then ce
@@ -264,7 +266,8 @@ __global__ void __launch_bounds__(GNN_TILE) k_gnn_encode(GnnGraph g, GnnInput<T>
             }
             o.h[q] = __floats2bfloat162_rn(z[0], z[1]);
         }
-        *reinterpret_cast<uint4 *>(hout + (size_t)i * GNN_H + c4 * 8) = o.u;
+        bf16 *dst = planar ? hout + ((size_t)c4 * g.n + i) * 8 : hout + (size_t)i * GNN_H + c4 * 8;
+        *reinterpret_cast<uint4 *>(dst) = o.u;
     }
 }
 
@@ -644,13 +647,15 @@ __global__ void __launch_bounds__(LAYER_THREADS, 1) k_gnn_layer_fold(GnnGraph g,
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Load a [128][32] BF16 tile of rows base.. into shared memory (row stride LDH).
-__device__ __forceinline__ void load_tile(bf16 *s, const bf16 *__restrict__ h, int base, int n)
+// Load a [128][32] BF16 tile of rows base.. into shared memory (row stride
+// LDH) from row-major or channel-planar activations.
+__device__ __forceinline__ void load_tile(bf16 *s, const bf16 *__restrict__ h, int base, int n, int planar = 0)
 {
     for (int e = threadIdx.x; e < GNN_TILE * 4; e += GNN_TILE) {
         const int row = e >> 2, part = e & 3, i = base + row;
         uint4 v = make_uint4(0, 0, 0, 0);
-        if (i < n) v = *reinterpret_cast<const uint4 *>(h + (size_t)i * GNN_H + part * 8);
+        if (i < n)
+            v = *reinterpret_cast<const uint4 *>(planar ? h + ((size_t)part * n + i) * 8 : h + (size_t)i * GNN_H + part * 8);
         *reinterpret_cast<uint4 *>(s + row * LDH + part * 8) = v;
     }
 }
@@ -660,14 +665,15 @@ template <bool TRAIN>
 __global__ void __launch_bounds__(GNN_TILE) k_gnn_decode(GnnGraph g, const float *__restrict__ pd,
                                                          const bf16 *__restrict__ pkd, const bf16 *__restrict__ hin,
                                                          const GnnScales *__restrict__ scp, float *__restrict__ y,
-                                                         double *__restrict__ x0, bf16 *__restrict__ qsave)
+                                                         double *__restrict__ x0, bf16 *__restrict__ qsave,
+                                                         const int *__restrict__ status, int planar)
 {
     __shared__ __align__(16) bf16 sH[GNN_TILE * LDH];
     __shared__ __align__(16) bf16 sW[GNN_H * LDH];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = g.n, base = blockIdx.x * GNN_TILE;
     for (int e = tid; e < GNN_H * GNN_H; e += GNN_TILE) sW[(e >> 5) * LDH + (e & 31)] = pkd[e];
-    load_tile(sH, hin, base, n);
+    load_tile(sH, hin, base, n, planar);
     __syncthreads();
     const int gq = lane >> 2, tq = lane & 3;
     float acc[2][4][4];
@@ -693,7 +699,7 @@ __global__ void __launch_bounds__(GNN_TILE) k_gnn_decode(GnnGraph g, const float
             s += __shfl_xor_sync(FULL, s, 1);
             s += __shfl_xor_sync(FULL, s, 2);
             if (tq == 0 && i < n) {
-                const float yi = s + pd[GPD_CO];
+                const float yi = *status ? 0.f : s + pd[GPD_CO];
                 y[i] = yi;
                 if (x0) x0[i] = sx * (double)yi;
             }
@@ -1133,6 +1139,7 @@ void gnn_work_carve(GnnWork &w, char *base, int n, bool train)
     w.partials = reinterpret_cast<double *>(take((size_t)reduce_grid(n) * 2 * sizeof(double)));
     w.counter = reinterpret_cast<unsigned int *>(take(256));
     w.scales = reinterpret_cast<GnnScales *>(take(sizeof(GnnScales)));
+    w.status = reinterpret_cast<int *>(take(sizeof(int)));
     w.loss = reinterpret_cast<double *>(base + off);
 }
 
@@ -1173,9 +1180,13 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
                          GnnWork &w, double *x0, bool train)
 {
     const int nb = gnn_blocks(g.n);
-    k_gnn_scales<T><<<reduce_grid(g.n), MCB_THREADS, 0, s>>>(g.n, in, w.partials, w.counter, w.scales);
-    k_gnn_encode<T><<<nb, GNN_TILE, 0, s>>>(g, in, p, w.scales, w.h[0]);
     const bool folded = !train && g.affine;
+    const GnnLayerPath path = gnn_layer_path();
+    const bool umma = folded && path != GnnLayerPath::Mma && gnn_umma_ready();
+    cudaMemsetAsync(w.status, 0, sizeof(int), s);
+    if (folded && !umma && path == GnnLayerPath::UmmaRequired) cudaMemsetAsync(w.status, 0x7f, sizeof(int), s);
+    k_gnn_scales<T><<<reduce_grid(g.n), MCB_THREADS, 0, s>>>(g.n, in, w.partials, w.counter, w.scales);
+    k_gnn_encode<T><<<nb, GNN_TILE, 0, s>>>(g, in, p, w.scales, w.h[0], umma ? 1 : 0);
     if (folded) {
         k_gnn_fold<<<(GNN_L * 7 * GNN_H * GNN_H + 255) / 256, 256, 0, s>>>(p, g, w.fold);
         cudaFuncSetAttribute(k_gnn_layer_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FOLD_SMEM);
@@ -1188,17 +1199,23 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
         const bf16 *pkl = pk + GK_LAYER0 + l * GKL_SIZE;
         if (train)
             k_gnn_layer<true><<<nb, LAYER_THREADS, LAYER_SMEM, s>>>(g, pl, pkl, w.h[l], w.h[l + 1], w.a[l]);
-        else if (folded)
-            k_gnn_layer_fold<<<std::min(nb, sm_count()), LAYER_THREADS, FOLD_SMEM, s>>>(
-                g, pl, w.fold + (size_t)l * 7 * GNN_H * GNN_H, pkl, w.h[l & 1], w.h[(l + 1) & 1], nb);
-        else
+        else if (folded) {
+            const bf16 *wf = w.fold + (size_t)l * 7 * GNN_H * GNN_H;
+            if (umma)
+                gnn_layer_umma(s, g, pl, wf, pkl, w.h[l & 1], w.h[(l + 1) & 1], w.status, sm_count());
+            else
+                k_gnn_layer_fold<<<std::min(nb, sm_count()), LAYER_THREADS, FOLD_SMEM, s>>>(
+                    g, pl, wf, pkl, w.h[l & 1], w.h[(l + 1) & 1], nb);
+        } else
             k_gnn_layer<false><<<nb, LAYER_THREADS, LAYER_SMEM, s>>>(g, pl, pkl, w.h[l & 1], w.h[(l + 1) & 1], nullptr);
     }
     const bf16 *hl = train ? w.h[GNN_L] : w.h[GNN_L & 1];
     if (train)
-        k_gnn_decode<true><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, w.q);
+        k_gnn_decode<true><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, w.q, w.status,
+                                                   0);
     else
-        k_gnn_decode<false><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, nullptr);
+        k_gnn_decode<false><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, nullptr,
+                                                    w.status, umma ? 1 : 0);
 }
 
 template <typename T>

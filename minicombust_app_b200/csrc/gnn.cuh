@@ -116,6 +116,7 @@ struct GnnWork {
     GnnScales *scales = nullptr;
     double *loss = nullptr;              // [2]: mean offset, loss
     __nv_bfloat16 *fold = nullptr;       // [L][7][H][H] offset-form weights (inference)
+    int *status = nullptr;               // nonzero: a tensor-core layer gave up waiting (prediction zeroed)
 };
 
 size_t gnn_work_bytes(int n, bool train);
@@ -136,6 +137,23 @@ template <typename T>
 void gnn_forward(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &in, const float *p, const __nv_bfloat16 *pk,
                  GnnWork &w, double *x0);
 int gnn_forward_launches();
+
+// Layer kernel of the offset form: the tcgen05 kernel (default), the same
+// kernel with no fall-back (MC_GNN_LAYER=umma), or the mma.sync kernel
+// (MC_GNN_LAYER=mma).
+enum class GnnLayerPath { Umma, UmmaRequired, Mma };
+GnnLayerPath gnn_layer_path();
+
+// The tcgen05 path keeps the activations channel-planar: h[c][i][e] =
+// channel 8 c + e of cell i (four planes of n x 16 bytes), so that a tile of
+// 128 rows is four contiguous 2 KB runs and lands in shared memory directly
+// in the tensor core's K-major core-matrix layout.
+// Launch attributes of the layer kernel (false: the kernel cannot run).
+bool gnn_umma_ready();
+// One offset-form layer on the tcgen05 tensor cores, `grid` persistent
+// blocks, planar activations hin -> hout.
+void gnn_layer_umma(cudaStream_t s, const GnnGraph &g, const float *pl, const __nv_bfloat16 *wf,
+                    const __nv_bfloat16 *pkl, const __nv_bfloat16 *hin, __nv_bfloat16 *hout, int *status, int grid);
 
 // Training: forward, loss against `target` (units of the solution), backward;
 // adds this sample's gradient, scaled by `weight`, into grad[NPARAM] and

@@ -291,8 +291,10 @@ int mc_gnn_predict(mc_gnn *net, const mc_gnn_graph *gr, const mc_gnn_sample *s, 
     gnn_forward<float>(net->stream, gr->g, input_of(*s), net->p, net->pk, net->work, x0);
     if (y) GNN_TRY(cudaMemcpyAsync(y, net->work.y, (size_t)gr->g.n * 4, cudaMemcpyDeviceToDevice, net->stream));
     GNN_TRY(cudaGetLastError());
+    int status = 0;
+    GNN_TRY(cudaMemcpyAsync(&status, net->work.status, sizeof(int), cudaMemcpyDeviceToHost, net->stream));
     GNN_TRY(cudaStreamSynchronize(net->stream));
-    return MC_OK;
+    return status ? MC_ERR_TIMEOUT : MC_OK;
 }
 
 int mc_gnn_loss_grad(mc_gnn *net, const mc_gnn_graph *gr, int batch, const mc_gnn_sample *samples, double *loss,

@@ -183,8 +183,8 @@ void ir_init(cudaStream_t s, const Ell &A, const double *b, double *x, double *r
 // the single candidates, rc that of the combination.
 struct GuessState {
     double bb, rr[2], coef[2], rc;
-    int choice;   // -1 zero, 2 combination
-    int pad;
+    int choice;      // -1 zero, 2 combination
+    int net_status;  // copy of the network's status (nonzero: its prediction was zeroed)
 };
 void guess_residuals(cudaStream_t s, const Ell &A, const double *b, const PcgState *st, const double *xa,
                      const double *xb, GuessState *gs, double *partials, unsigned int *counter);

@@ -31,6 +31,7 @@ MC_ERR_NONFINITE = -4
 MC_ERR_MESH = -5
 MC_ERR_NOMEM = -6
 MC_ERR_UNSUPPORTED = -7
+MC_ERR_TIMEOUT = -8
 
 MODE_COMPAT, MODE_SIMPLE = 0, 1
 PSOLVER_PCG_JACOBI, PSOLVER_PCG_AMG = 0, 1

@@ -131,3 +131,39 @@ def test_adam_training_reduces_the_loss(gpu):
     for _ in range(60):
         net2.train_step(gr2, dev2, 2e-3)
     assert np.array_equal(net.params(), net2.params())
+
+
+@pytest.mark.parametrize("layer", ["umma", "mma"])
+@pytest.mark.parametrize("dims", [(16, 8, 8), (9, 5, 3)])
+def test_offset_layer_kernels_match_oracle(gpu, dims, layer, monkeypatch):
+    """Both offset-form layer kernels -- tcgen05 (TMA tiles, TMEM accumulators)
+    and mma.sync -- explicitly selected, against the BF16-emulating oracle."""
+    import torch
+    monkeypatch.setenv("MC_GNN_LAYER", layer)
+    net, gr, graph, host, dev = setup(dims, seed=4)
+    p = net.params().astype(np.float64)
+    b, diag, prev, _ = host[0]
+    y = torch.empty(len(b), device="cuda")
+    net.predict(gr, dev[0][0], dev[0][1], dev[0][2], y=y)
+    y_bf, _ = G.forward(p, graph, b, diag, prev, bf16=True)
+    assert rel(y.cpu().numpy(), y_bf) <= 1e-2
+
+
+def test_tensor_core_layer_matches_mma_layer_on_many_tiles(gpu, monkeypatch):
+    """65,536 cells = 512 tiles: every persistent block runs several tiles, so
+    the three copy stages and both epilogue groups wrap their barrier phases."""
+    import torch
+    net, gr, graph, host, dev = setup((64, 32, 32), seed=5, nsamples=1)
+    rng = np.random.default_rng(9)
+    net.set_params((net.params() + 0.05 * rng.standard_normal(G.NPARAM)).astype(np.float32))
+    n = len(host[0][0])
+    ys = {}
+    for layer in ("umma", "mma"):
+        monkeypatch.setenv("MC_GNN_LAYER", layer)
+        y = torch.empty(n, device="cuda")
+        net.predict(gr, dev[0][0], dev[0][1], dev[0][2], y=y)
+        ys[layer] = y.cpu().numpy().astype(np.float64)
+    # same BF16 operands, FP32 accumulation in a different order: the layer
+    # outputs differ only where a BF16 rounding falls the other way
+    assert rel(ys["umma"], ys["mma"]) <= 1e-2
+    assert np.mean(np.abs(ys["umma"] - ys["mma"]) <= 1e-2 * np.abs(ys["mma"]).max()) > 0.99
