@@ -119,6 +119,10 @@ struct mc_flow {
     BicgState<1> *h_b1 = nullptr;      // pinned
     double *h_scalars = nullptr;       // pinned
     cudaGraphExec_t g_pcg = nullptr, g_b3 = nullptr, g_b1 = nullptr, g_pcg_amg = nullptr;
+    // device-side loops (conditional WHILE graphs) of the same solves
+    cudaGraphExec_t l_pcg = nullptr, l_b3 = nullptr, l_b1 = nullptr, l_pcg_amg = nullptr;
+    cudaGraphExec_t l_pcg_amg32 = nullptr, l_b3_32 = nullptr, l_b1_32 = nullptr;
+    bool loops_failed = false;   // a loop graph could not be built: host-driven batches
     // aggregation AMG (pressure_solver == MC_PSOLVER_PCG_AMG)
     bool use_amg = false;
     AmgHierarchy amg;
@@ -283,6 +287,95 @@ int run_batch(mc_flow *h, cudaGraphExec_t *exec, int kernels_in_batch, Body &&bo
     return MC_OK;
 }
 
+// Device side of a loop graph: repeat the body while the solve is not done.
+__global__ void k_loop_continue(cudaGraphConditionalHandle hc, const int *__restrict__ done)
+{
+    cudaGraphSetConditional(hc, *done ? 0u : 1u);
+}
+
+// MC_LOOP_GRAPHS=0 keeps the host-driven batches.
+bool loop_graphs_enabled()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = std::getenv("MC_LOOP_GRAPHS");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
+bool use_loops(const mc_flow *h) { return !h->timing.on && !h->loops_failed && loop_graphs_enabled(); }
+
+constexpr int LOOP_ITERS = 2;  // iterations per loop body (even: ping-pong buffers)
+
+// A whole solve as one graph launch: a kernel tests *done, a conditional
+// WHILE node repeats `body` (LOOP_ITERS iterations whose kernels return
+// early once *done is set) and the body ends with the same test, so the
+// iterations run back to back on the device with no status read between
+// them.  The device ends the loop at the solve's max_iters.  Returns false
+// (nothing launched) when the graph cannot be built.
+template <typename Body>
+bool run_loop(mc_flow *h, cudaGraphExec_t *exec, const int *done, Body &&body)
+{
+    if (!*exec) {
+        cudaGraph_t g = nullptr;
+        bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
+        cudaGraphConditionalHandle hc{};
+        ok = ok && cudaGraphConditionalHandleCreate(&hc, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+        cudaGraphNode_t test = nullptr, loop = nullptr;
+        if (ok) {
+            void *args[] = {&hc, &done};
+            cudaKernelNodeParams kp{};
+            kp.func = reinterpret_cast<void *>(k_loop_continue);
+            kp.gridDim = dim3(1);
+            kp.blockDim = dim3(1);
+            kp.kernelParams = args;
+            ok = cudaGraphAddKernelNode(&test, g, nullptr, 0, &kp) == cudaSuccess;
+        }
+        cudaGraphNodeParams cp{};
+        if (ok) {
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = hc;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            ok = cudaGraphAddNode(&loop, g, &test, 1, &cp) == cudaSuccess;
+        }
+        if (ok) {
+            ok = cudaStreamBeginCaptureToGraph(h->stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                const long before = h->launches;
+                body();
+                k_loop_continue<<<1, 1, 0, h->stream>>>(hc, done);
+                h->launches = before;
+                cudaGraph_t captured = nullptr;
+                ok = cudaStreamEndCapture(h->stream, &captured) == cudaSuccess;
+            }
+        }
+        ok = ok && cudaGraphInstantiate(exec, g, 0) == cudaSuccess;
+        if (g) cudaGraphDestroy(g);
+        if (!ok) {
+            *exec = nullptr;
+            cudaGetLastError();
+            h->loops_failed = true;
+            return false;
+        }
+    }
+    if (cudaGraphLaunch(*exec, h->stream) != cudaSuccess) {
+        cudaGetLastError();
+        h->loops_failed = true;
+        return false;
+    }
+    return true;
+}
+
+// Kernels a loop graph launched for `iters` iterations of `per_iter` kernels.
+long loop_launches(int iters, int per_iter)
+{
+    const long bodies = (iters + LOOP_ITERS - 1) / LOOP_ITERS;
+    return 1 + bodies * (LOOP_ITERS * per_iter + 1);
+}
+
 // Snapshot record [4][N] float32 in the caller's numbering (idx = old -> new
 // or nullptr): b - mean, diagonal, previous correction, correction.
 __global__ void k_snapshot_pack(int N, const double *__restrict__ b, const PcgState *__restrict__ st,
@@ -377,29 +470,34 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
     const int batch_iters = amg ? PCG_AMG_BATCH : PCG_BATCH;
     const long max_batches = h->prm.max_iters / batch_iters + 2;
     const int per_iter = amg ? 2 + amg_kernels_per_vcycle(h->amg) : PCG_KERNELS_PER_ITER;
+    auto iterations = [&](int count) {
+        for (int it = 0; it < count; it++) {
+            const int pin = it & 1;
+            launch(h, K_PCG_ITER1, [&] { pcg_iter1(h->stream, A, v, pin); });
+            if (amg) {
+                launch(h, K_PCG_ITER2_AMG, [&] { pcg_iter2_amg(h->stream, A, v, pin ^ 1); });
+                launch(h, K_AMG_VCYCLE, [&] {
+                    amg_vcycle<double>(h->stream, h->amg, v.r, v.zp[pin ^ 1], v.st, v.partials, v.counter, 0);
+                });
+                h->launches += amg_kernels_per_vcycle(h->amg) - 1;
+            } else {
+                launch(h, K_PCG_ITER2, [&] { pcg_iter2(h->stream, A, v, pin ^ 1); });
+            }
+        }
+    };
+    const bool looped = use_loops(h) &&
+                        run_loop(h, amg ? &h->l_pcg_amg : &h->l_pcg, &v.st->done, [&] { iterations(LOOP_ITERS); });
     for (long batch = 0;; batch++) {
         CUDA_TRY(h, cudaMemcpyAsync(h->h_pcg, v.st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
         flush_timing(h);
         if (h->h_pcg->done) break;
+        if (looped) return fail(h, MC_ERR_CUDA, "pressure solve loop ended before convergence");
         if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "pressure solve state did not advance");
-        rc = run_batch(h, amg ? &h->g_pcg_amg : &h->g_pcg, batch_iters * per_iter, [&] {
-            for (int it = 0; it < batch_iters; it++) {
-                const int pin = it & 1;
-                launch(h, K_PCG_ITER1, [&] { pcg_iter1(h->stream, A, v, pin); });
-                if (amg) {
-                    launch(h, K_PCG_ITER2_AMG, [&] { pcg_iter2_amg(h->stream, A, v, pin ^ 1); });
-                    launch(h, K_AMG_VCYCLE, [&] {
-                        amg_vcycle<double>(h->stream, h->amg, v.r, v.zp[pin ^ 1], v.st, v.partials, v.counter, 0);
-                    });
-                    h->launches += amg_kernels_per_vcycle(h->amg) - 1;
-                } else {
-                    launch(h, K_PCG_ITER2, [&] { pcg_iter2(h->stream, A, v, pin ^ 1); });
-                }
-            }
-        });
+        rc = run_batch(h, amg ? &h->g_pcg_amg : &h->g_pcg, batch_iters * per_iter, [&] { iterations(batch_iters); });
         if (rc) return rc;
     }
+    if (looped) h->launches += loop_launches(h->h_pcg->iter, per_iter);
     launch(h, K_PCG_XMEAN, [&] { pcg_xmean(h->stream, h->N, v); });
     launch(h, K_PCG_SUBMEAN, [&] { pcg_sub_xmean(h->stream, h->N, v); });
     rc = check_launch(h);
@@ -450,25 +548,30 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
         h->launches += amg_kernels_per_vcycle(h->amg) - 1;
         rc = check_launch(h);
         if (rc) return rc;
+        auto iterations = [&](int count) {
+            for (int it = 0; it < count; it++) {
+                const int pin = it & 1;
+                launch(h, K_PCG_ITER1_32, [&] { pcg_iter1<float>(h->stream, A32, in, pin); });
+                launch(h, K_PCG_ITER2_AMG32, [&] { pcg_iter2_amg<float>(h->stream, A32, in, pin ^ 1); });
+                launch(h, K_AMG_VCYCLE32, [&] {
+                    amg_vcycle<float>(h->stream, h->amg, in.r, in.zp[pin ^ 1], in.st, in.partials, in.counter, 0);
+                });
+                h->launches += amg_kernels_per_vcycle(h->amg) - 1;
+            }
+        };
+        const bool looped =
+            use_loops(h) && run_loop(h, &h->l_pcg_amg32, &in.st->done, [&] { iterations(LOOP_ITERS); });
         for (long batch = 0;; batch++) {
             CUDA_TRY(h, cudaMemcpyAsync(h->h_pcg_inner, in.st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
             CUDA_TRY(h, cudaStreamSynchronize(h->stream));
             flush_timing(h);
             if (h->h_pcg_inner->done) break;
+            if (looped) return fail(h, MC_ERR_CUDA, "inner solve loop ended before convergence");
             if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "inner solve state did not advance");
-            rc = run_batch(h, &h->g_pcg_amg32, PCG_AMG_BATCH * per_iter, [&] {
-                for (int it = 0; it < PCG_AMG_BATCH; it++) {
-                    const int pin = it & 1;
-                    launch(h, K_PCG_ITER1_32, [&] { pcg_iter1<float>(h->stream, A32, in, pin); });
-                    launch(h, K_PCG_ITER2_AMG32, [&] { pcg_iter2_amg<float>(h->stream, A32, in, pin ^ 1); });
-                    launch(h, K_AMG_VCYCLE32, [&] {
-                        amg_vcycle<float>(h->stream, h->amg, in.r, in.zp[pin ^ 1], in.st, in.partials, in.counter, 0);
-                    });
-                    h->launches += amg_kernels_per_vcycle(h->amg) - 1;
-                }
-            });
+            rc = run_batch(h, &h->g_pcg_amg32, PCG_AMG_BATCH * per_iter, [&] { iterations(PCG_AMG_BATCH); });
             if (rc) return rc;
         }
+        if (looped) h->launches += loop_launches(h->h_pcg_inner->iter, per_iter);
         inner_total += h->h_pcg_inner->iter;
         if (h->h_pcg_inner->status == KRYLOV_NONFINITE) return fail(h, MC_ERR_NONFINITE, "inner FP32 solve");
         launch(h, K_IR, [&] { ir_add(h->stream, h->N, o.x, in.x, o.st); });
@@ -490,28 +593,32 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
 
 template <int R>
 int solve_bicg(mc_flow *h, const Ell &A, const BicgVectors<R> &v, BicgState<R> *hs, cudaGraphExec_t *exec,
-               int kid_init, int kid1, int iters_out[R])
+               cudaGraphExec_t *loop, int kid_init, int kid1, int iters_out[R])
 {
     launch(h, kid_init, [&] { bicg_init<R>(h->stream, A, v, h->prm.u_rtol, h->prm.max_iters); });
     int rc = check_launch(h);
     if (rc) return rc;
     const long max_batches = h->prm.max_iters / BICG_BATCH + 2;
+    auto iterations = [&](int count) {
+        for (int it = 0; it < count; it++) {
+            const int pin = it & 1;
+            launch(h, kid1, [&] { bicg_1<R>(h->stream, A, v, pin); });
+            launch(h, kid1 + 1, [&] { bicg_2<R>(h->stream, A, v, pin ^ 1); });
+            launch(h, kid1 + 2, [&] { bicg_3<R>(h->stream, A, v, pin ^ 1); });
+        }
+    };
+    const bool looped = use_loops(h) && run_loop(h, loop, &v.st->all_done, [&] { iterations(LOOP_ITERS); });
     for (long batch = 0;; batch++) {
         CUDA_TRY(h, cudaMemcpyAsync(hs, v.st, sizeof(BicgState<R>), cudaMemcpyDeviceToHost, h->stream));
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
         flush_timing(h);
         if (hs->all_done) break;
+        if (looped) return fail(h, MC_ERR_CUDA, "BiCGStab loop ended before convergence");
         if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "BiCGStab state did not advance");
-        rc = run_batch(h, exec, BICG_BATCH * BICG_KERNELS_PER_ITER, [&] {
-            for (int it = 0; it < BICG_BATCH; it++) {
-                const int pin = it & 1;
-                launch(h, kid1, [&] { bicg_1<R>(h->stream, A, v, pin); });
-                launch(h, kid1 + 1, [&] { bicg_2<R>(h->stream, A, v, pin ^ 1); });
-                launch(h, kid1 + 2, [&] { bicg_3<R>(h->stream, A, v, pin ^ 1); });
-            }
-        });
+        rc = run_batch(h, exec, BICG_BATCH * BICG_KERNELS_PER_ITER, [&] { iterations(BICG_BATCH); });
         if (rc) return rc;
     }
+    if (looped) h->launches += loop_launches(*std::max_element(hs->iter, hs->iter + R), BICG_KERNELS_PER_ITER);
     int worst = MC_OK;
     for (int j = 0; j < R; j++) {
         iters_out[j] = hs->iter[j];
@@ -528,7 +635,7 @@ int solve_bicg(mc_flow *h, const Ell &A, const BicgVectors<R> &v, BicgState<R> *
 template <int R>
 int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const BicgVectorsT<float, R> &in,
                        const BirVectors<R> &out, BicgState<R> *hin, BirState<R> *hout, cudaGraphExec_t *exec,
-                       int kid_init32, int kid1_32, int iters_out[R])
+                       cudaGraphExec_t *loop, int kid_init32, int kid1_32, int iters_out[R])
 {
     constexpr int kMaxOuter = 30;
     launch(h, K_BIR, [&] { bir_init<R>(h->stream, A, out, h->prm.u_rtol, kMaxOuter); });
@@ -548,22 +655,26 @@ int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const B
                 inner_rtol = std::min(inner_rtol, 0.5 * std::sqrt(hout->tol2[j] / hout->rr[j]));
         inner_rtol = std::max(inner_rtol, h->prm.ir_inner_rtol);
         launch(h, kid_init32, [&] { bicg_init_t<float, R>(h->stream, A32, in, inner_rtol, h->prm.max_iters); });
+        auto iterations = [&](int count) {
+            for (int it = 0; it < count; it++) {
+                const int pin = it & 1;
+                launch(h, kid1_32, [&] { bicg_1_t<float, R>(h->stream, A32, in, pin); });
+                launch(h, kid1_32 + 1, [&] { bicg_2_t<float, R>(h->stream, A32, in, pin ^ 1); });
+                launch(h, kid1_32 + 2, [&] { bicg_3_t<float, R>(h->stream, A32, in, pin ^ 1); });
+            }
+        };
+        const bool looped = use_loops(h) && run_loop(h, loop, &in.st->all_done, [&] { iterations(LOOP_ITERS); });
         for (long batch = 0;; batch++) {
             CUDA_TRY(h, cudaMemcpyAsync(hin, in.st, sizeof(BicgState<R>), cudaMemcpyDeviceToHost, h->stream));
             CUDA_TRY(h, cudaStreamSynchronize(h->stream));
             flush_timing(h);
             if (hin->all_done) break;
+            if (looped) return fail(h, MC_ERR_CUDA, "BiCGStab loop ended before convergence");
             if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "BiCGStab state did not advance");
-            rc = run_batch(h, exec, BICG_BATCH * BICG_KERNELS_PER_ITER, [&] {
-                for (int it = 0; it < BICG_BATCH; it++) {
-                    const int pin = it & 1;
-                    launch(h, kid1_32, [&] { bicg_1_t<float, R>(h->stream, A32, in, pin); });
-                    launch(h, kid1_32 + 1, [&] { bicg_2_t<float, R>(h->stream, A32, in, pin ^ 1); });
-                    launch(h, kid1_32 + 2, [&] { bicg_3_t<float, R>(h->stream, A32, in, pin ^ 1); });
-                }
-            });
+            rc = run_batch(h, exec, BICG_BATCH * BICG_KERNELS_PER_ITER, [&] { iterations(BICG_BATCH); });
             if (rc) return rc;
         }
+        if (looped) h->launches += loop_launches(*std::max_element(hin->iter, hin->iter + R), BICG_KERNELS_PER_ITER);
         for (int j = 0; j < R; j++) {
             iters_out[j] += hin->iter[j];
             if (hin->status[j] == KRYLOV_NONFINITE) return fail(h, MC_ERR_NONFINITE, "inner FP32 BiCGStab");
@@ -683,9 +794,9 @@ int stage_momentum(mc_flow *h, mc_iter_stats *st)
         launch(h, K_ROUND_ELL, [&] { round_ell(h->stream, h->N, h->AU, h->off_m, h->m32_diag, h->m32_off); });
         const EllT<float> A32{h->N, h->m32_diag, h->m32_off, h->col, h->dc};
         rc = solve_bicg_refined<3>(h, momentum_matrix(h), A32, h->bi3, h->bo3, h->h_bi3, h->h_bo3, &h->g_b3_32,
-                                   K_BICG3_INIT32, K_BICG3_1_32, its);
+                                   &h->l_b3_32, K_BICG3_INIT32, K_BICG3_1_32, its);
     } else {
-        rc = solve_bicg<3>(h, momentum_matrix(h), h->b3, h->h_b3, &h->g_b3, K_BICG3_INIT, K_BICG3_1, its);
+        rc = solve_bicg<3>(h, momentum_matrix(h), h->b3, h->h_b3, &h->g_b3, &h->l_b3, K_BICG3_INIT, K_BICG3_1, its);
     }
     if (st)
         for (int j = 0; j < 3; j++) st->momentum_iters[j] = its[j];
@@ -816,9 +927,9 @@ int stage_temperature(mc_flow *h, mc_iter_stats *st)
         launch(h, K_ROUND_ELL, [&] { round_ell(h->stream, h->N, h->diag_t, h->off_t, h->t32_diag, h->t32_off); });
         const EllT<float> A32{h->N, h->t32_diag, h->t32_off, h->col, h->dc};
         rc = solve_bicg_refined<1>(h, temperature_matrix(h), A32, h->bi1, h->bo1, h->h_bi1, h->h_bo1, &h->g_b1_32,
-                                   K_BICG1_INIT32, K_BICG1_1_32, its);
+                                   &h->l_b1_32, K_BICG1_INIT32, K_BICG1_1_32, its);
     } else {
-        rc = solve_bicg<1>(h, temperature_matrix(h), h->b1, h->h_b1, &h->g_b1, K_BICG1_INIT, K_BICG1_1, its);
+        rc = solve_bicg<1>(h, temperature_matrix(h), h->b1, h->h_b1, &h->g_b1, &h->l_b1, K_BICG1_INIT, K_BICG1_1, its);
     }
     if (st) st->temperature_iters = its[0];
     return rc;
@@ -1441,7 +1552,8 @@ int mc_flow_destroy(mc_flow *h)
 {
     if (!h) return MC_ERR_ARG;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    for (cudaGraphExec_t g : {h->g_pcg, h->g_b3, h->g_b1, h->g_pcg_amg, h->g_pcg_amg32, h->g_b3_32, h->g_b1_32})
+    for (cudaGraphExec_t g : {h->g_pcg, h->g_b3, h->g_b1, h->g_pcg_amg, h->g_pcg_amg32, h->g_b3_32, h->g_b1_32,
+                              h->l_pcg, h->l_b3, h->l_b1, h->l_pcg_amg, h->l_pcg_amg32, h->l_b3_32, h->l_b1_32})
         if (g) cudaGraphExecDestroy(g);
     if (h->amg_mem) cudaFree(h->amg_mem);
     for (cudaEvent_t e : h->timing.ev) cudaEventDestroy(e);
