@@ -139,15 +139,17 @@ namespace {
 template <typename T>
 __device__ __forceinline__ T row_apply(const AmgLevelT<T> &L, int i, const T *__restrict__ e)
 {
-    T s = L.diag[i] * e[i];
+    const T s0 = L.diag[i] * e[i];
     if (L.dc.code) {
-        int c[6];
-        row_cols(L.dc, L.col, L.n, i, c);
+        return with_row_cols(L.dc, L.col, L.n, i, [&](const int(&c)[6]) {
+            T s = s0;
 #pragma unroll
-        for (int q = 0; q < 6; q++) s += L.off[(size_t)q * L.n + i] * e[c[q]];
-    } else {
-        for (int q = 0; q < L.k; q++) s += L.off[(size_t)q * L.n + i] * e[L.col[(size_t)q * L.n + i]];
+            for (int q = 0; q < 6; q++) s += L.off[(size_t)q * L.n + i] * e[c[q]];
+            return s;
+        });
     }
+    T s = s0;
+    for (int q = 0; q < L.k; q++) s += L.off[(size_t)q * L.n + i] * e[L.col[(size_t)q * L.n + i]];
     return s;
 }
 
@@ -159,19 +161,26 @@ __device__ __forceinline__ T inv_or_zero(T d)
 
 } // namespace
 
-// FP32 copy of the level-0 values.
+// FP32 copy of the level-0 values (in direction order when the level has
+// direction codes).
 __global__ void k_amg_round_level0(int n, const double *__restrict__ diag, const double *__restrict__ off,
-                                   float *__restrict__ diag32, float *__restrict__ off32)
+                                   const uint32_t *__restrict__ code, float *__restrict__ diag32,
+                                   float *__restrict__ off32)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     diag32[i] = (float)diag[i];
+    float o[6];
+    round_row_by_direction(off, code, n, i, o);
 #pragma unroll
-    for (int q = 0; q < 6; q++) off32[(size_t)q * n + i] = (float)off[(size_t)q * n + i];
+    for (int q = 0; q < 6; q++) off32[(size_t)q * n + i] = o[q];
 }
 
-template <typename T>
-__global__ void k_amg_galerkin(AmgLevelT<T> fine, AmgLevelT<T> coarse)
+// Coarse values as sums of fine values (the Galerkin lists index the fine
+// level's slot-ordered values: level 1 of the FP32 hierarchy is summed from
+// the FP64 level 0).
+template <typename TF, typename T>
+__global__ void k_amg_galerkin(AmgLevelT<TF> fine, AmgLevelT<T> coarse)
 {
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= coarse.n) return;
@@ -403,8 +412,11 @@ void amg_setup_values(cudaStream_t s, const AmgHierarchy &H)
     const AmgLevelT<T> *lv = levels_of<T>(H);
     if (sizeof(T) == sizeof(float))
         k_amg_round_level0<<<blocks(H.lv[0].n), MCB_THREADS, 0, s>>>(H.lv[0].n, H.lv[0].diag, H.lv[0].off,
+                                                                     lv[0].dc.dia ? H.lv[0].dc.code : nullptr,
                                                                      (float *)lv[0].diag, (float *)lv[0].off);
-    for (int l = 1; l < H.levels; l++) k_amg_galerkin<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l - 1], lv[l]);
+    if (H.levels > 1) k_amg_galerkin<double, T><<<blocks(lv[1].n), MCB_THREADS, 0, s>>>(H.lv[0], lv[1]);
+    for (int l = 2; l < H.levels; l++)
+        k_amg_galerkin<T, T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l - 1], lv[l]);
     set_dense_attributes<T>();
     const AmgLevelT<T> &C = lv[H.levels - 1];
     k_amg_dense_factor<T><<<1, DENSE_THREADS, dense_smem(C.n), s>>>(C, H.dense);

@@ -515,7 +515,7 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
 int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *relres, double *bnorm)
 {
     const Ell A = pressure_matrix(h);
-    const EllT<float> A32{h->N, h->amg.lv32[0].diag, h->amg.lv32[0].off, h->col, h->dc};
+    const EllT<float> A32{h->N, h->amg.lv32[0].diag, h->amg.lv32[0].off, h->col, h->amg.lv32[0].dc};
     PcgVectors o = h->pv;
     PcgVectorsT<float> in = h->pv32;
     constexpr int kMaxOuter = 50;
@@ -791,8 +791,9 @@ int stage_momentum(mc_flow *h, mc_iter_stats *st)
     if (rc) return rc;
     int its[3] = {0, 0, 0};
     if (h->bir_mem) {
-        launch(h, K_ROUND_ELL, [&] { round_ell(h->stream, h->N, h->AU, h->off_m, h->m32_diag, h->m32_off); });
-        const EllT<float> A32{h->N, h->m32_diag, h->m32_off, h->col, h->dc};
+        launch(h, K_ROUND_ELL,
+               [&] { round_ell(h->stream, h->N, h->AU, h->off_m, h->dc.code, h->m32_diag, h->m32_off); });
+        const EllT<float> A32{h->N, h->m32_diag, h->m32_off, h->col, by_direction(h->dc)};
         rc = solve_bicg_refined<3>(h, momentum_matrix(h), A32, h->bi3, h->bo3, h->h_bi3, h->h_bo3, &h->g_b3_32,
                                    &h->l_b3_32, K_BICG3_INIT32, K_BICG3_1_32, its);
     } else {
@@ -924,8 +925,9 @@ int stage_temperature(mc_flow *h, mc_iter_stats *st)
     if (rc) return rc;
     int its[1] = {0};
     if (h->bir_mem) {
-        launch(h, K_ROUND_ELL, [&] { round_ell(h->stream, h->N, h->diag_t, h->off_t, h->t32_diag, h->t32_off); });
-        const EllT<float> A32{h->N, h->t32_diag, h->t32_off, h->col, h->dc};
+        launch(h, K_ROUND_ELL,
+               [&] { round_ell(h->stream, h->N, h->diag_t, h->off_t, h->dc.code, h->t32_diag, h->t32_off); });
+        const EllT<float> A32{h->N, h->t32_diag, h->t32_off, h->col, by_direction(h->dc)};
         rc = solve_bicg_refined<1>(h, temperature_matrix(h), A32, h->bi1, h->bo1, h->h_bi1, h->h_bo1, &h->g_b1_32,
                                    &h->l_b1_32, K_BICG1_INIT32, K_BICG1_1_32, its);
     } else {
@@ -1331,7 +1333,7 @@ int build_amg(mc_flow *h, const HostMesh &hm)
             f.n = d.n;
             f.k = d.k;
             f.col = d.col;
-            f.dc = d.dc;
+            f.dc = l == 0 ? by_direction(d.dc) : d.dc;  // FP32 level 0 values are stored by direction
             f.agg = d.agg;
             f.mptr = d.mptr;
             f.mlist = d.mlist;

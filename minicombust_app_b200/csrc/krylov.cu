@@ -117,25 +117,21 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(EllT<T> A, PcgVectors
         const int i1 = i0 + stride;
         const bool has1 = i1 < N;
         const int j1 = has1 ? i1 : i0;
-        int ca[6], cb[6];
-        T oa[6], ob[6];
-        row_cols(A, i0, ca);
-        row_cols(A, j1, cb);
-#pragma unroll
-        for (int k = 0; k < 6; k++) {
-            oa[k] = A.off[(size_t)k * N + i0];
-            ob[k] = A.off[(size_t)k * N + j1];
-        }
         const T2 sa = X[i0], sb = X[j1];
         const T bt = (T)beta;
         const T pa = sa.x + bt * sa.y, pb = sb.x + bt * sb.y;
-        T qa = A.diag[i0] * pa, qb = A.diag[j1] * pb;
+        auto apply = [&](int i, T p) {
+            return with_row_cols(A.dc, A.col, N, i, [&](const int(&c)[6]) {
+                T q = A.diag[i] * p;
 #pragma unroll
-        for (int k = 0; k < 6; k++) {
-            const T2 ga = X[ca[k]], gb = X[cb[k]];
-            qa += oa[k] * (ga.x + bt * ga.y);
-            qb += ob[k] * (gb.x + bt * gb.y);
-        }
+                for (int k = 0; k < 6; k++) {
+                    const T2 g = X[c[k]];
+                    q += A.off[(size_t)k * N + i] * (g.x + bt * g.y);
+                }
+                return q;
+            });
+        };
+        const T qa = apply(i0, pa), qb = apply(j1, pb);
         Y[i0].y = pa;
         v.q[i0] = qa;
         acc[0] += (double)pa * (double)qa;
@@ -447,11 +443,12 @@ __global__ void __launch_bounds__(MCB_THREADS) k_ir_residual(Ell A, const double
     const double mean = st->mean;
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        double ax = A.diag[i] * x[i];
-        int c_[6];
-        row_cols(A, i, c_);
+        const double ax = with_row_cols(A.dc, A.col, N, i, [&](const int(&c)[6]) {
+            double s = A.diag[i] * x[i];
 #pragma unroll
-        for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * x[c_[k]];
+            for (int k = 0; k < 6; k++) s += A.off[(size_t)k * N + i] * x[c[k]];
+            return s;
+        });
         const double ri = (b[i] - mean) - ax;
         r[i] = ri;
         r32[i] = (float)ri;
@@ -1027,13 +1024,15 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bir_residual(Ell A, BirVectors<
 }
 
 __global__ void __launch_bounds__(MCB_THREADS) k_round_ell(int N, const double *__restrict__ diag,
-                                                           const double *__restrict__ off, float *__restrict__ d32,
-                                                           float *__restrict__ o32)
+                                                           const double *__restrict__ off, const uint32_t *__restrict__ code,
+                                                           float *__restrict__ d32, float *__restrict__ o32)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         d32[i] = (float)diag[i];
+        float o[6];
+        round_row_by_direction(off, code, N, i, o);
 #pragma unroll
-        for (int k = 0; k < 6; k++) o32[(size_t)k * N + i] = (float)off[(size_t)k * N + i];
+        for (int k = 0; k < 6; k++) o32[(size_t)k * N + i] = o[k];
     }
 }
 
@@ -1100,9 +1099,10 @@ void bir_residual(cudaStream_t s, const Ell &A, const BirVectors<R> &v)
 {
     k_bir_residual<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v);
 }
-void round_ell(cudaStream_t s, int N, const double *diag, const double *off, float *diag32, float *off32)
+void round_ell(cudaStream_t s, int N, const double *diag, const double *off, const uint32_t *code, float *diag32,
+               float *off32)
 {
-    k_round_ell<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, diag, off, diag32, off32);
+    k_round_ell<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, diag, off, code, diag32, off32);
 }
 
 #define MCB_INSTANTIATE_BICG_T(T, R)                                                                          \

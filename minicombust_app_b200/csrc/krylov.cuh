@@ -34,34 +34,112 @@ struct Pair<float> {
 // row instead of 24.
 // Most rows (all interior cells) share one code word, `canon`, whose
 // per-slot offsets are kept ready in coff.
+// `dia` marks a copy of the values stored by direction instead of by slot
+// (slot d = direction d, zero where the row has no neighbour that way): its
+// columns are row + doff[d] (clamped into [0, N), where the value is 0), so
+// the kernels read no column data at all.
 struct DirCodes {
     const uint32_t *code = nullptr;  // [N]; nullptr: use the column list
     int doff[6] = {0, 0, 0, 0, 0, 0};
     uint32_t canon = 0;
     int coff[6] = {0, 0, 0, 0, 0, 0};
+    int dia = 0;
 };
 
+// The same codes for a copy of the values in direction order (see `dia`).
+inline DirCodes by_direction(DirCodes dc)
+{
+    dc.dia = dc.code ? 1 : 0;
+    return dc;
+}
+
+__device__ __forceinline__ void dia_cols(const DirCodes &dc, int N, int i, int (&c)[6])
+{
+#pragma unroll
+    for (int k = 0; k < 6; k++) c[k] = min(max(i + dc.doff[k], 0), N - 1);
+}
+
 // Column of each slot of row i (the row itself for an unused slot).
+// Columns of a row from its code word (six 3-bit direction indices).
+__device__ __forceinline__ void decode_cols(const DirCodes &dc, uint32_t cw, int i, int (&c)[6])
+{
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        const unsigned d = (cw >> (3 * k)) & 7u;
+        int o = 0;
+#pragma unroll
+        for (int q = 0; q < 6; q++) o = (d == (unsigned)q) ? dc.doff[q] : o;
+        c[k] = i + o;
+    }
+}
+
 __device__ __forceinline__ void row_cols(const DirCodes &dc, const int *__restrict__ col, int N, int i, int (&c)[6])
 {
-    if (dc.code) {
+    if (dc.dia) {
+        dia_cols(dc, N, i, c);
+    } else if (dc.code) {
         const uint32_t cw = dc.code[i];
         if (cw == dc.canon) {
 #pragma unroll
             for (int k = 0; k < 6; k++) c[k] = i + dc.coff[k];
         } else {
-#pragma unroll
-            for (int k = 0; k < 6; k++) {
-                const unsigned d = (cw >> (3 * k)) & 7u;
-                int o = 0;
-#pragma unroll
-                for (int q = 0; q < 6; q++) o = (d == (unsigned)q) ? dc.doff[q] : o;
-                c[k] = i + o;
-            }
+            decode_cols(dc, cw, i, c);
         }
     } else {
 #pragma unroll
         for (int k = 0; k < 6; k++) c[k] = col[(size_t)k * N + i];
+    }
+}
+
+// Evaluate f(columns) for row i.  With direction codes f first runs on the
+// canonical columns (clamped into [0, N)) while the row's code word is still
+// in flight, so its neighbour loads do not wait for the code; only rows whose
+// code differs (the boundary rows of a box) run f again with their decoded
+// columns.  f must have no side effects; its result for a canonical row is
+// the same as with the columns of row_cols.
+template <typename F>
+__device__ __forceinline__ auto with_row_cols(const DirCodes &dc, const int *__restrict__ col, int N, int i, F &&f)
+{
+    int c[6];
+    if (dc.dia) {
+        dia_cols(dc, N, i, c);
+        return f(c);
+    }
+    if (dc.code) {
+        const uint32_t cw = dc.code[i];
+#pragma unroll
+        for (int k = 0; k < 6; k++) c[k] = min(max(i + dc.coff[k], 0), N - 1);
+        auto r = f(c);
+        if (cw != dc.canon) {
+            decode_cols(dc, cw, i, c);
+            r = f(c);
+        }
+        return r;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; k++) c[k] = col[(size_t)k * N + i];
+    return f(c);
+}
+
+// FP32 values of row i; with codes in direction order (slot d = direction d,
+// zero for a direction the row lacks), else in the original slot order.
+__device__ __forceinline__ void round_row_by_direction(const double *__restrict__ off, const uint32_t *__restrict__ code,
+                                                       int N, int i, float (&o)[6])
+{
+    if (code) {
+        const uint32_t cw = code[i];
+#pragma unroll
+        for (int d = 0; d < 6; d++) o[d] = 0.f;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const unsigned d = (cw >> (3 * k)) & 7u;
+            const float v = (float)off[(size_t)k * N + i];
+#pragma unroll
+            for (int q = 0; q < 6; q++) o[q] = (d == (unsigned)q) ? v : o[q];
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 6; k++) o[k] = (float)off[(size_t)k * N + i];
     }
 }
 
@@ -209,8 +287,10 @@ template <int R>
 void bir_add(cudaStream_t s, int N, const BirVectors<R> &v);
 template <int R>
 void bir_residual(cudaStream_t s, const Ell &A, const BirVectors<R> &v);
-// FP32 copy of a 7-point matrix's values.
-void round_ell(cudaStream_t s, int N, const double *diag, const double *off, float *diag32, float *off32);
+// FP32 copy of a 7-point matrix's values, by direction when `code` is given
+// (see DirCodes::dia), else in slot order.
+void round_ell(cudaStream_t s, int N, const double *diag, const double *off, const uint32_t *code, float *diag32,
+               float *off32);
 
 template <int R>
 void bicg_init(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, double rtol, int max_iters);
