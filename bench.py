@@ -129,18 +129,21 @@ class ClockSampler:
 def kernel_bytes(name, N, F, nnz_off):
     """Algorithmic (unique-touch) bytes of one launch: each stored input
     element read once, each output written once, at its stored type.  The
-    solver kernels read a 4-byte direction code per row instead of the six
-    int32 columns (structured box); ELL values include the boundary padding."""
+    FP64 solver kernels read a 4-byte direction code per row instead of the
+    six int32 columns (structured box); the FP32 copies are stored by
+    direction and read no column data.  ELL values include the boundary
+    padding."""
     return {
         "pcg_iter1_spmv": 92 * N,      # diag, 6 off, code, (z, p) pair -> p, q
-        "pcg32_iter1_spmv": 48 * N,    # the same in FP32
+        "pcg32_iter1_spmv": 44 * N,    # the same in FP32, no code
         "pcg_iter2_update": 64 * N,    # x rw, r rw, p, q, diag -> z (Jacobi path)
         "bicg3_1_spmv": 204 * N,       # matrix 60 + 3 x (r, p, v gathered; r0; p, v out)
         "bicg3_2_spmv": 156 * N,       # matrix 60 + 3 x (r, v gathered; s, t out)
         "bicg3_3_update": 168 * N,     # 3 x (s, p, t, r0, x rw, r out)
-        "bicg3_32_1_spmv": 104 * N,    # FP32, split per right-hand side
-        "bicg3_32_2_spmv": 80 * N,
+        "bicg3_32_1_spmv": 100 * N,    # FP32: matrix 28 + 3 x 24
+        "bicg3_32_2_spmv": 76 * N,     # FP32: matrix 28 + 3 x 16
         "bicg3_32_3_update": 84 * N,
+        "gnn_forward": 708 * N,        # inputs 24 + vhat 4, h0 out 64, 4 layers x (h in 64 + h out 64 + mask 1), decode 64 in + y, x0 out 12
         "lsq_gradients_uvwpt": 208 * N,
         "momentum_assemble": 56 * F + 296 * N,
         "mass_flux": 88 * F + 176 * N,

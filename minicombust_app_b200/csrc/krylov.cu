@@ -2,9 +2,10 @@
 // iteration streams the 7-point matrix (12 bytes per entry) and a handful of
 // vectors.
 #include "krylov.cuh"
-#include "mc_reduce.cuh"
 
 #include <algorithm>
+
+#include "mc_reduce.cuh"
 
 // Resident blocks per SM the grid-stride Krylov kernels are sized for.
 #ifndef MCB_KRYLOV_BLOCKS_PER_SM
@@ -1041,7 +1042,8 @@ void bicg_init_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, 
 {
     k_bicg_init<T, R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, max_iters);
 }
-// FP32 systems with several right-hand sides use the split form.
+// FP32 systems with several right-hand sides run the first product and the
+// update in the split form (one block range per right-hand side).
 template <typename T, int R>
 constexpr bool bicg_split() { return sizeof(T) == 4 && R > 1; }
 
@@ -1052,11 +1054,12 @@ void bicg_1_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int
     k_bicg_1<T, R, S><<<krylov_grid(A.N) * (S ? R : 1), MCB_THREADS, 0, s>>>(A, v, v.p[pin], v.v[pin], v.p[pin ^ 1],
                                                                             v.v[pin ^ 1]);
 }
+// The second product gathers two vectors per right-hand side: one pass over
+// the matrix for all of them is faster than the split form here.
 template <typename T, int R>
 void bicg_2_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int vnew)
 {
-    constexpr bool S = bicg_split<T, R>();
-    k_bicg_2<T, R, S><<<krylov_grid(A.N) * (S ? R : 1), MCB_THREADS, 0, s>>>(A, v, v.v[vnew]);
+    k_bicg_2<T, R, false><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.v[vnew]);
 }
 template <typename T, int R>
 void bicg_3_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int pnew)
