@@ -243,8 +243,7 @@ union Chunk8 {
 // the weights in shared memory, four 16-byte stores.
 template <typename T>
 __global__ void __launch_bounds__(GNN_TILE) k_gnn_encode(GnnGraph g, GnnInput<T> in, const float *__restrict__ p,
-                                                         const GnnScales *__restrict__ scp, bf16 *__restrict__ hout,
-                                                         int planar)
+                                                         const GnnScales *__restrict__ scp, bf16 *__restrict__ hout)
 {
     __shared__ float sw[GNN_H * (GNN_IN + 1)];
     for (int e = threadIdx.x; e < GNN_H * (GNN_IN + 1); e += GNN_TILE) sw[e] = p[GP_WE + e];  // We then ce
@@ -266,8 +265,7 @@ __global__ void __launch_bounds__(GNN_TILE) k_gnn_encode(GnnGraph g, GnnInput<T>
             }
             o.h[q] = __floats2bfloat162_rn(z[0], z[1]);
         }
-        bf16 *dst = planar ? hout + ((size_t)c4 * g.n + i) * 8 : hout + (size_t)i * GNN_H + c4 * 8;
-        *reinterpret_cast<uint4 *>(dst) = o.u;
+        *reinterpret_cast<uint4 *>(hout + (size_t)i * GNN_H + c4 * 8) = o.u;
     }
 }
 
@@ -647,15 +645,13 @@ __global__ void __launch_bounds__(LAYER_THREADS, 1) k_gnn_layer_fold(GnnGraph g,
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Load a [128][32] BF16 tile of rows base.. into shared memory (row stride
-// LDH) from row-major or channel-planar activations.
-__device__ __forceinline__ void load_tile(bf16 *s, const bf16 *__restrict__ h, int base, int n, int planar = 0)
+// Load a [128][32] BF16 tile of rows base.. into shared memory (row stride LDH).
+__device__ __forceinline__ void load_tile(bf16 *s, const bf16 *__restrict__ h, int base, int n)
 {
     for (int e = threadIdx.x; e < GNN_TILE * 4; e += GNN_TILE) {
         const int row = e >> 2, part = e & 3, i = base + row;
         uint4 v = make_uint4(0, 0, 0, 0);
-        if (i < n)
-            v = *reinterpret_cast<const uint4 *>(planar ? h + ((size_t)part * n + i) * 8 : h + (size_t)i * GNN_H + part * 8);
+        if (i < n) v = *reinterpret_cast<const uint4 *>(h + (size_t)i * GNN_H + part * 8);
         *reinterpret_cast<uint4 *>(s + row * LDH + part * 8) = v;
     }
 }
@@ -666,14 +662,14 @@ __global__ void __launch_bounds__(GNN_TILE) k_gnn_decode(GnnGraph g, const float
                                                          const bf16 *__restrict__ pkd, const bf16 *__restrict__ hin,
                                                          const GnnScales *__restrict__ scp, float *__restrict__ y,
                                                          double *__restrict__ x0, bf16 *__restrict__ qsave,
-                                                         const int *__restrict__ status, int planar)
+                                                         const int *__restrict__ status)
 {
     __shared__ __align__(16) bf16 sH[GNN_TILE * LDH];
     __shared__ __align__(16) bf16 sW[GNN_H * LDH];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = g.n, base = blockIdx.x * GNN_TILE;
     for (int e = tid; e < GNN_H * GNN_H; e += GNN_TILE) sW[(e >> 5) * LDH + (e & 31)] = pkd[e];
-    load_tile(sH, hin, base, n, planar);
+    load_tile(sH, hin, base, n);
     __syncthreads();
     const int gq = lane >> 2, tq = lane & 3;
     float acc[2][4][4];
@@ -1182,11 +1178,13 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
     const int nb = gnn_blocks(g.n);
     const bool folded = !train && g.affine;
     const GnnLayerPath path = gnn_layer_path();
-    const bool umma = folded && path != GnnLayerPath::Mma && gnn_umma_ready();
+    GnnTmaMap maps[2];
+    const bool umma = folded && path != GnnLayerPath::Mma && gnn_umma_map(&maps[0], w.h[0], g.n) &&
+                      gnn_umma_map(&maps[1], w.h[1], g.n) && gnn_umma_ready();
     cudaMemsetAsync(w.status, 0, sizeof(int), s);
     if (folded && !umma && path == GnnLayerPath::UmmaRequired) cudaMemsetAsync(w.status, 0x7f, sizeof(int), s);
     k_gnn_scales<T><<<reduce_grid(g.n), MCB_THREADS, 0, s>>>(g.n, in, w.partials, w.counter, w.scales);
-    k_gnn_encode<T><<<nb, GNN_TILE, 0, s>>>(g, in, p, w.scales, w.h[0], umma ? 1 : 0);
+    k_gnn_encode<T><<<nb, GNN_TILE, 0, s>>>(g, in, p, w.scales, w.h[0]);
     if (folded) {
         k_gnn_fold<<<(GNN_L * 7 * GNN_H * GNN_H + 255) / 256, 256, 0, s>>>(p, g, w.fold);
         cudaFuncSetAttribute(k_gnn_layer_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FOLD_SMEM);
@@ -1202,7 +1200,7 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
         else if (folded) {
             const bf16 *wf = w.fold + (size_t)l * 7 * GNN_H * GNN_H;
             if (umma)
-                gnn_layer_umma(s, g, pl, wf, pkl, w.h[l & 1], w.h[(l + 1) & 1], w.status, sm_count());
+                gnn_layer_umma(s, g, maps[l & 1], pl, wf, pkl, w.h[l & 1], w.h[(l + 1) & 1], w.status, sm_count());
             else
                 k_gnn_layer_fold<<<std::min(nb, sm_count()), LAYER_THREADS, FOLD_SMEM, s>>>(
                     g, pl, wf, pkl, w.h[l & 1], w.h[(l + 1) & 1], nb);
@@ -1211,11 +1209,10 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
     }
     const bf16 *hl = train ? w.h[GNN_L] : w.h[GNN_L & 1];
     if (train)
-        k_gnn_decode<true><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, w.q, w.status,
-                                                   0);
+        k_gnn_decode<true><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, w.q, w.status);
     else
         k_gnn_decode<false><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, nullptr,
-                                                    w.status, umma ? 1 : 0);
+                                                    w.status);
 }
 
 template <typename T>

@@ -144,16 +144,19 @@ int gnn_forward_launches();
 enum class GnnLayerPath { Umma, UmmaRequired, Mma };
 GnnLayerPath gnn_layer_path();
 
-// The tcgen05 path keeps the activations channel-planar: h[c][i][e] =
-// channel 8 c + e of cell i (four planes of n x 16 bytes), so that a tile of
-// 128 rows is four contiguous 2 KB runs and lands in shared memory directly
-// in the tensor core's K-major core-matrix layout.
+// TMA descriptor of the activations h ([n][32] BF16) in tiles of 128 rows
+// with the 64-byte swizzle (an opaque CUtensorMap).
+struct alignas(64) GnnTmaMap {
+    unsigned char raw[128];
+};
+bool gnn_umma_map(GnnTmaMap *m, const __nv_bfloat16 *h, int n);
 // Launch attributes of the layer kernel (false: the kernel cannot run).
 bool gnn_umma_ready();
 // One offset-form layer on the tcgen05 tensor cores, `grid` persistent
-// blocks, planar activations hin -> hout.
-void gnn_layer_umma(cudaStream_t s, const GnnGraph &g, const float *pl, const __nv_bfloat16 *wf,
-                    const __nv_bfloat16 *pkl, const __nv_bfloat16 *hin, __nv_bfloat16 *hout, int *status, int grid);
+// blocks, hin (described by `map`) -> hout.
+void gnn_layer_umma(cudaStream_t s, const GnnGraph &g, const GnnTmaMap &map, const float *pl,
+                    const __nv_bfloat16 *wf, const __nv_bfloat16 *pkl, const __nv_bfloat16 *hin,
+                    __nv_bfloat16 *hout, int *status, int grid);
 
 // Training: forward, loss against `target` (units of the solution), backward;
 // adds this sample's gradient, scaled by `weight`, into grad[NPARAM] and

@@ -7,13 +7,12 @@
 //   a  = relu(D1 + c1)                                         (BF16)
 //   D2 = a . W2^T,      h'_i = h_i + (D2 + c2)                 (BF16)
 // where W1f holds the folded gates (see k_gnn_fold).  The seven 128-row
-// slices of U are contiguous row ranges of h (offset form); with h stored
-// channel-planar ([4][n][8] BF16) each slice is four contiguous runs of up to
-// 2 KB, copied by the bulk-copy engine, that land as [chunk][row][16 B] --
-// the K-major core-matrix layout without swizzle (8 rows x 16 B per core
-// matrix, 8-row groups 128 B apart, K chunks 2 KB apart).  Rows outside
-// [0, n) are not copied; they and the rows of directions a cell does not
-// have (mask bit clear) are zeroed in shared memory before the MMA.
+// slices of U are contiguous row ranges of h (offset form), so each is one
+// 2-D TMA tile load (8 KB, 128 rows x 64 B) with the 64-byte swizzle, which is
+// the K-major operand layout of the MMA for 64-byte rows (8-row groups 512 B
+// apart, a K = 16 step 32 bytes into the row); rows outside [0, n) read
+// zeros, and rows of directions a cell does not have (mask bit clear) are
+// zeroed in shared memory before the MMA is issued.
 //
 // Warp roles (one persistent block per SM):
 //   warps 0-11  three epilogue groups of four warps; group g owns the tiles
@@ -21,7 +20,7 @@
 //               each barrier's phases are consumed by one group, in order);
 //               thread r of a group is row r of the tile and TMEM lane r
 //               (warp w reads lanes 32 (w % 4) ..)
-//   warp 12     TMA producer
+//   warp 12     TMA producer (one thread)
 //   warp 13     TMEM allocation and the MMA issue (one elected thread)
 // The MMA thread issues whichever product is ready -- the first product of
 // a tile once its slices are masked, the second once its group has written
@@ -29,6 +28,9 @@
 // overlap.  Every wait is bounded: on
 // a time-out the block records a status, drains its copies and MMAs, frees
 // its TMEM and returns, and the decoder then writes a zero prediction.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -44,7 +46,7 @@ using bf16 = __nv_bfloat16;
 using namespace sm100;
 
 constexpr int UM_STAGES = 3;
-constexpr int UM_SLICE = GNN_TILE * GNN_H * 2;      // 8192 B: 4 chunks x 128 rows x 16 B
+constexpr int UM_SLICE = GNN_TILE * GNN_H * 2;      // 8192 B: 128 rows x 64 B
 constexpr int UM_STAGE = 7 * UM_SLICE;              // 57344 B
 constexpr int UM_B1 = 7 * GNN_H * GNN_H * 2;        // 14336 B: 28 K-groups of 32 rows x 16 B
 constexpr int UM_B2 = GNN_H * GNN_H * 2;            // 2048 B
@@ -105,7 +107,7 @@ struct UmmaBars {
 };
 
 __global__ void __launch_bounds__(UM_THREADS, 1)
-    k_gnn_layer_umma(GnnGraph g, const float *__restrict__ pl,
+    k_gnn_layer_umma(const __grid_constant__ CUtensorMap tmap, GnnGraph g, const float *__restrict__ pl,
                      const bf16 *__restrict__ wf, const bf16 *__restrict__ pkl, const bf16 *__restrict__ hin,
                      bf16 *__restrict__ hout, int ntiles, int *status)
 {
@@ -167,6 +169,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
     if (warp == WARP_TMA) {
         // ---------------------------------------------------------- producer
         if (lane == 0) {
+            tma_prefetch_desc(&tmap);
             int issued = 0;
             for (int j = 0;; j++) {
                 const int tile = blockIdx.x + j * gridDim.x;
@@ -176,28 +179,12 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
                     fail(1);
                     break;
                 }
+                mbar_arrive_expect_tx(bars.full(s), UM_STAGE);
                 const int y0 = tile * GNN_TILE;
                 const uint32_t dst = sbase + OFF_STAGE + s * UM_STAGE;
-                int lo[7], hi[7];
-                uint32_t bytes = 0;
+                tma_load_2d(dst, &tmap, bars.full(s), 0, y0);
 #pragma unroll
-                for (int t = 0; t < 7; t++) {  // the in-range rows of each slice
-                    const int y = y0 + (t ? g.doff[t - 1] : 0);
-                    lo[t] = max(y, 0);
-                    hi[t] = min(y + GNN_TILE, g.n);
-                    if (hi[t] > lo[t]) bytes += 4u * 16u * (uint32_t)(hi[t] - lo[t]);
-                }
-                mbar_arrive_expect_tx(bars.full(s), bytes);
-#pragma unroll
-                for (int t = 0; t < 7; t++) {
-                    if (hi[t] <= lo[t]) continue;
-                    const int y = y0 + (t ? g.doff[t - 1] : 0);
-                    const uint32_t run = 16u * (uint32_t)(hi[t] - lo[t]);
-#pragma unroll
-                    for (int c = 0; c < 4; c++)
-                        bulk_load(dst + t * UM_SLICE + c * 2048 + (lo[t] - y) * 16, hin + ((size_t)c * g.n + lo[t]) * 8,
-                                  run, bars.full(s));
-                }
+                for (int k = 0; k < 6; k++) tma_load_2d(dst + (1 + k) * UM_SLICE, &tmap, bars.full(s), 0, y0 + g.doff[k]);
                 issued = j + 1;
             }
             // every copy this block started lands before the block exits
@@ -222,8 +209,8 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
                     const uint32_t a0 = sbase + OFF_STAGE + s * UM_STAGE;
 #pragma unroll
                     for (int ks = 0; ks < 14; ks++) {
-                        const uint64_t ad = smem_desc(a0 + (ks >> 1) * UM_SLICE + (ks & 1) * 4096, 2048, 128,
-                                                      DESC_SWIZZLE_NONE);
+                        const uint64_t ad = smem_desc(a0 + (ks >> 1) * UM_SLICE + (ks & 1) * 32, 16, 512,
+                                                      DESC_SWIZZLE_64B);
                         const uint64_t bd = smem_desc(sbase + OFF_B1 + ks * 1024, 512, 128, DESC_SWIZZLE_NONE);
                         umma_f16(tmem + q * 64, ad, bd, idesc, ks > 0);
                     }
@@ -270,20 +257,20 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
             uint4 hv[4];
 #pragma unroll
             for (int c = 0; c < 4; c++)
-                hv[c] = in ? __ldg(reinterpret_cast<const uint4 *>(hin + ((size_t)c * g.n + i) * 8)) : make_uint4(0, 0, 0, 0);
+                hv[c] = in ? __ldg(reinterpret_cast<const uint4 *>(hin + (size_t)i * GNN_H) + c) : make_uint4(0, 0, 0, 0);
             bool ok = mbar_wait(bars.full(s), (j / UM_STAGES) & 1, abort_flag, WAIT_LIMIT);
             if (!__all_sync(FULL, ok)) {
                 fail(6);
                 break;
             }
             // rows of directions this cell does not have read zeros
-            const uint32_t row0 = sbase + OFF_STAGE + s * UM_STAGE + r * 16;
+            const uint32_t row0 = sbase + OFF_STAGE + s * UM_STAGE + r * 64;  // the swizzle stays inside a row
 #pragma unroll
             for (int k = 0; k < 6; k++)
                 if (!((mk >> k) & 1u)) {
                     const uint32_t a = row0 + (1 + k) * UM_SLICE;
 #pragma unroll
-                    for (int c = 0; c < 4; c++) st_shared_v4(a + 2048 * c, 0u, 0u, 0u, 0u);
+                    for (int c = 0; c < 4; c++) st_shared_v4(a + 16 * c, 0u, 0u, 0u, 0u);
                 }
             if (mk != 0x3fu) fence_proxy_async_smem();  // only a thread that wrote zeros has to order them
             mbar_arrive(bars.masked(s));
@@ -333,7 +320,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
                         o[e] = pack_bf16(h2.x + (__uint_as_float(v[col]) + sC2[col]),
                                          h2.y + (__uint_as_float(v[col + 1]) + sC2[col + 1]));
                     }
-                    *reinterpret_cast<uint4 *>(hout + ((size_t)c * g.n + i) * 8) = make_uint4(o[0], o[1], o[2], o[3]);
+                    *reinterpret_cast<uint4 *>(hout + (size_t)i * GNN_H + c * 8) = make_uint4(o[0], o[1], o[2], o[3]);
                 }
             }
         }
@@ -357,6 +344,43 @@ GnnLayerPath gnn_layer_path()
     return GnnLayerPath::Umma;
 }
 
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+} // namespace
+
+bool gnn_umma_map(GnnTmaMap *m, const bf16 *h, int n)
+{
+    static_assert(sizeof(GnnTmaMap) == sizeof(CUtensorMap), "tensor map size");
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn || n <= 0 || (reinterpret_cast<uintptr_t>(h) & 15u)) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)GNN_H, (cuuint64_t)n};
+    const cuuint64_t strides[1] = {(cuuint64_t)GNN_H * sizeof(bf16)};
+    const cuuint32_t box[2] = {(cuuint32_t)GNN_H, (cuuint32_t)GNN_TILE};
+    const cuuint32_t estr[2] = {1, 1};
+    CUtensorMap t;
+    if (fn(&t, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(h), dims, strides, box, estr,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    std::memcpy(m->raw, &t, sizeof(t));
+    return true;
+}
+
 bool gnn_umma_ready()
 {
     static int state = 0;  // 0 unknown, 1 ready, -1 failed
@@ -368,11 +392,13 @@ bool gnn_umma_ready()
     return state > 0;
 }
 
-void gnn_layer_umma(cudaStream_t s, const GnnGraph &g, const float *pl, const bf16 *wf, const bf16 *pkl,
-                    const bf16 *hin, bf16 *hout, int *status, int grid)
+void gnn_layer_umma(cudaStream_t s, const GnnGraph &g, const GnnTmaMap &map, const float *pl, const bf16 *wf,
+                    const bf16 *pkl, const bf16 *hin, bf16 *hout, int *status, int grid)
 {
+    CUtensorMap t;
+    std::memcpy(&t, map.raw, sizeof(t));
     const int ntiles = (g.n + GNN_TILE - 1) / GNN_TILE;
-    k_gnn_layer_umma<<<std::max(1, std::min(grid, ntiles)), UM_THREADS, UM_SMEM, s>>>(g, pl, wf, pkl, hin, hout,
+    k_gnn_layer_umma<<<std::max(1, std::min(grid, ntiles)), UM_THREADS, UM_SMEM, s>>>(t, g, pl, wf, pkl, hin, hout,
                                                                                        ntiles, status);
 }
 

@@ -102,24 +102,6 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const void *tmap, uint
                  : "memory");
 }
 
-// Contiguous bulk copy global -> shared (no multicast): both addresses
-// 16-byte aligned, `bytes` a multiple of 16; completion counted on `bar`.
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-
-// 3-D tile load (no multicast), same completion rule.
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const void *tmap, uint32_t bar, int x, int y, int z)
-{
-    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
-                 "%5}], [%2];" ::"r"(dst),
-                 "l"(reinterpret_cast<uint64_t>(tmap)), "r"(bar), "r"(x), "r"(y), "r"(z)
-                 : "memory");
-}
-
 // ------------------------------------------------------------------ tcgen05
 
 // Whole warp: allocate `ncols` TMEM columns (a power of two >= 32); the base
