@@ -280,34 +280,11 @@ __global__ void __launch_bounds__(DENSE_THREADS) k_amg_dense_factor(AmgLevelT<T>
     }
 }
 
-// e = (A + sigma 1 1^T)^{-1} r on the coarsest level: one dense product with
-// the symmetric inverse formed at setup; thread t computes row t (the reads
-// dense[j][t] are coalesced across threads).
-constexpr int DENSE_SOLVE_PARTS = 8;  // threads per row of the dense product
-
-template <typename T>
-__global__ void __launch_bounds__(AMG_COARSEST_MAX * DENSE_SOLVE_PARTS)
-    k_amg_dense_solve(AmgLevelT<T> L, const double *__restrict__ dense, const PcgState *st)
-{
-    if (st->done) return;
-    __shared__ double r[AMG_COARSEST_MAX];
-    __shared__ double part[DENSE_SOLVE_PARTS][AMG_COARSEST_MAX];
-    const int n = L.n, t = threadIdx.x, row = t % AMG_COARSEST_MAX, q = t / AMG_COARSEST_MAX;
-    if (t < n) r[t] = (double)L.r[t];
-    __syncthreads();
-    const int chunk = (n + DENSE_SOLVE_PARTS - 1) / DENSE_SOLVE_PARTS;
-    double y = 0.0;
-    if (row < n)
-        for (int j = q * chunk; j < min(n, (q + 1) * chunk); j++) y += dense[(size_t)j * n + row] * r[j];
-    part[q][row] = y;
-    __syncthreads();
-    if (t < n) {
-        double s = 0.0;
-#pragma unroll
-        for (int k = 0; k < DENSE_SOLVE_PARTS; k++) s += part[k][t];
-        L.e[0][t] = (T)s;
-    }
-}
+// e = (A + sigma 1 1^T)^{-1} r on the coarsest level is one dense product
+// with the symmetric inverse formed at setup (k_amg_coarse_cycle): each row
+// is split over DENSE_SOLVE_PARTS threads (the reads dense[j][row] are
+// coalesced across threads) and the parts are summed in a fixed order.
+constexpr int DENSE_SOLVE_PARTS = 8;
 
 template <typename T>
 __global__ void k_amg_smooth_first(AmgLevelT<T> L, T omega, T *__restrict__ e, const PcgState *st)
@@ -328,18 +305,31 @@ __global__ void k_amg_jacobi(AmgLevelT<T> L, T omega, const T *__restrict__ ein,
     eout[i] = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
 }
 
+// Residual of the fine rows of coarse row I, summed: 8 lanes per coarse
+// row (an aggregate has at most 8 rows; larger ones loop), each lane one
+// fine row, then a fixed-order shuffle sum.  Every lane of the warp must call.
+template <typename T>
+__device__ __forceinline__ void restrict_row8(const AmgLevelT<T> &fine, const AmgLevelT<T> &coarse,
+                                              const T *__restrict__ e, int I, int m)
+{
+    T s = (T)0;
+    if (I < coarse.n)
+        for (int t = fine.mptr[I] + m; t < fine.mptr[I + 1]; t += 8) {
+            const int i = fine.mlist[t];
+            s += fine.r[i] - row_apply(fine, i, e);
+        }
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 4);
+    if (I < coarse.n && m == 0) coarse.r[I] = s;
+}
+
 template <typename T>
 __global__ void k_amg_restrict(AmgLevelT<T> fine, AmgLevelT<T> coarse, const T *__restrict__ e, const PcgState *st)
 {
     if (st->done) return;
-    const int I = blockIdx.x * blockDim.x + threadIdx.x;
-    if (I >= coarse.n) return;
-    T s = (T)0;
-    for (int t = fine.mptr[I]; t < fine.mptr[I + 1]; t++) {
-        const int i = fine.mlist[t];
-        s += fine.r[i] - row_apply(fine, i, e);
-    }
-    coarse.r[I] = s;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    restrict_row8(fine, coarse, e, g >> 3, g & 7);
 }
 
 template <typename T>
@@ -380,10 +370,90 @@ __global__ void __launch_bounds__(MCB_THREADS) k_amg_final(AmgLevelT<T> L, T ome
     }
 }
 
+// The coarse end of the V-cycle in one block: levels fused_from .. L-1
+// (each at most AMG_FUSE_MAX_ROWS rows), with __syncthreads between the
+// steps instead of kernel boundaries.  Same steps, order and sweeps as the
+// per-level kernels: on every level but the last, nu damped-Jacobi sweeps
+// (the first from e = 0) and the restriction of the residual; the dense
+// solve; then, back up, prolongation (scaled by alpha) and nu sweeps.  The
+// result on the first fused level ends in e[(2 nu - 1) & 1] (or e[0] when
+// the coarsest level is the only one).
+template <typename T>
+struct AmgCoarse {
+    AmgLevelT<T> lv[AMG_FUSED_LEVELS];
+    int nl;
+};
+
+constexpr int AMG_FUSED_THREADS = AMG_COARSEST_MAX * DENSE_SOLVE_PARTS;  // 1024
+
+template <typename T>
+__global__ void __launch_bounds__(AMG_FUSED_THREADS)
+    k_amg_coarse_cycle(const __grid_constant__ AmgCoarse<T> C, const double *__restrict__ dense, T omega, T alpha,
+                       int sweeps, const PcgState *st)
+{
+    if (st->done) return;
+    __shared__ double rs[AMG_COARSEST_MAX];
+    __shared__ double part[DENSE_SOLVE_PARTS][AMG_COARSEST_MAX];
+    const int t = threadIdx.x, nt = blockDim.x;
+    const int c_pre = (sweeps - 1) & 1;
+    for (int l = 0; l + 1 < C.nl; l++) {
+        const AmgLevelT<T> &L = C.lv[l];
+        for (int i = t; i < L.n; i += nt) L.e[0][i] = omega * L.r[i] * inv_or_zero(L.diag[i]);
+        __syncthreads();
+        int c = 0;
+        for (int sw = 1; sw < sweeps; sw++) {
+            const T *ein = L.e[c];
+            T *eout = L.e[c ^ 1];
+            for (int i = t; i < L.n; i += nt) eout[i] = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
+            c ^= 1;
+            __syncthreads();
+        }
+        const AmgLevelT<T> &Cl = C.lv[l + 1];
+        for (int g = t; g < ((Cl.n + 3) & ~3) * 8; g += nt) restrict_row8(L, Cl, L.e[c], g >> 3, g & 7);
+        __syncthreads();
+    }
+    {  // dense solve on the coarsest level
+        const AmgLevelT<T> &L = C.lv[C.nl - 1];
+        const int n = L.n, row = t % AMG_COARSEST_MAX, q = t / AMG_COARSEST_MAX;
+        if (t < n) rs[t] = (double)L.r[t];
+        __syncthreads();
+        const int chunk = (n + DENSE_SOLVE_PARTS - 1) / DENSE_SOLVE_PARTS;
+        double y = 0.0;
+        if (row < n)
+            for (int j = q * chunk; j < min(n, (q + 1) * chunk); j++) y += dense[(size_t)j * n + row] * rs[j];
+        part[q][row] = y;
+        __syncthreads();
+        if (t < n) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k < DENSE_SOLVE_PARTS; k++) s += part[k][t];
+            L.e[0][t] = (T)s;
+        }
+        __syncthreads();
+    }
+    int c_up = 0;  // buffer of the coarser level's result
+    for (int l = C.nl - 2; l >= 0; l--) {
+        const AmgLevelT<T> &L = C.lv[l];
+        const T *ec = C.lv[l + 1].e[c_up];
+        int c = c_pre;
+        for (int i = t; i < L.n; i += nt) L.e[c][i] += alpha * ec[L.agg[i]];
+        __syncthreads();
+        for (int sw = 1; sw <= sweeps; sw++) {
+            const T *ein = L.e[c];
+            T *eout = L.e[c ^ 1];
+            for (int i = t; i < L.n; i += nt) eout[i] = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
+            c ^= 1;
+            __syncthreads();
+        }
+        c_up = c;
+    }
+}
+
 // ------------------------------------------------------------------ drivers
 
 namespace {
 inline int blocks(int n) { return std::max(1, (n + MCB_THREADS - 1) / MCB_THREADS); }
+inline int blocks8(int n) { return std::max(1, (8 * n + MCB_THREADS - 1) / MCB_THREADS); }  // 8 threads per row
 inline size_t dense_smem(int n) { return (size_t)n * (n + 1) * sizeof(double); }
 
 template <typename T>
@@ -399,8 +469,6 @@ void set_dense_attributes()
     static bool done = false;
     if (done) return;
     cudaFuncSetAttribute(k_amg_dense_factor<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)dense_smem(AMG_COARSEST_MAX));
-    cudaFuncSetAttribute(k_amg_dense_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)dense_smem(AMG_COARSEST_MAX));
     done = true;
 }
@@ -422,7 +490,14 @@ void amg_setup_values(cudaStream_t s, const AmgHierarchy &H)
     k_amg_dense_factor<T><<<1, DENSE_THREADS, dense_smem(C.n), s>>>(C, H.dense);
 }
 
-int amg_kernels_per_vcycle(const AmgHierarchy &H) { return (H.levels - 1) * (2 * H.sweeps + 2) + 1; }
+void amg_plan_fused(AmgHierarchy &H)
+{
+    int f = H.levels - 1;
+    while (f > 1 && H.lv[f - 1].n <= AMG_FUSE_MAX_ROWS && H.levels - (f - 1) <= AMG_FUSED_LEVELS) f--;
+    H.fused_from = f;
+}
+
+int amg_kernels_per_vcycle(const AmgHierarchy &H) { return H.fused_from * (2 * H.sweeps + 2) + 1; }
 
 template <typename T>
 void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out_v, PcgState *st, double *partials,
@@ -430,15 +505,14 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
 {
     using T2 = typename Pair<T>::type;
     T2 *zp_out = (T2 *)zp_out_v;
-    const int L = H.levels;
+    const int L = H.levels, F = H.fused_from;
     const T omega = (T)H.omega, alpha = (T)H.alpha;
     int cur[AMG_MAX_LEVELS] = {0};
     AmgLevelT<T> lv[AMG_MAX_LEVELS];
     const AmgLevelT<T> *src = levels_of<T>(H);
     for (int l = 0; l < L; l++) lv[l] = src[l];
     lv[0].r = const_cast<T *>(r0);
-    set_dense_attributes<T>();
-    for (int l = 0; l + 1 < L; l++) {
+    for (int l = 0; l < F; l++) {
         k_amg_smooth_first<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, lv[l].e[0], st);
         int c = 0;
         for (int sw = 1; sw < H.sweeps; sw++) {
@@ -446,11 +520,14 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
             c ^= 1;
         }
         cur[l] = c;
-        k_amg_restrict<T><<<blocks(lv[l + 1].n), MCB_THREADS, 0, s>>>(lv[l], lv[l + 1], lv[l].e[c], st);
+        k_amg_restrict<T><<<blocks8(lv[l + 1].n), MCB_THREADS, 0, s>>>(lv[l], lv[l + 1], lv[l].e[c], st);
     }
-    k_amg_dense_solve<T><<<1, AMG_COARSEST_MAX * DENSE_SOLVE_PARTS, 0, s>>>(lv[L - 1], H.dense, st);
-    cur[L - 1] = 0;
-    for (int l = L - 2; l >= 0; l--) {
+    AmgCoarse<T> C;
+    C.nl = L - F;
+    for (int q = 0; q < C.nl; q++) C.lv[q] = lv[F + q];
+    k_amg_coarse_cycle<T><<<1, AMG_FUSED_THREADS, 0, s>>>(C, H.dense, omega, alpha, H.sweeps, st);
+    cur[F] = (F < L - 1) ? (2 * H.sweeps - 1) & 1 : 0;
+    for (int l = F - 1; l >= 0; l--) {
         int c = cur[l];
         k_amg_prolong<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], alpha, lv[l + 1].e[cur[l + 1]], lv[l].e[c], st);
         for (int sw = 1; sw <= H.sweeps; sw++) {

@@ -31,6 +31,10 @@ namespace mcb {
 
 constexpr int AMG_MAX_LEVELS = 16;
 constexpr int AMG_COARSEST_MAX = 128;
+// Levels with at most this many rows (down to the coarsest) run as one
+// single-block kernel per V-cycle; at most AMG_FUSED_LEVELS of them.
+constexpr int AMG_FUSE_MAX_ROWS = 1024;
+constexpr int AMG_FUSED_LEVELS = 6;
 
 // Device view of one level; T is the storage type of values and vectors.
 template <typename T>
@@ -65,7 +69,11 @@ struct AmgHierarchy {
     int sweeps = 2;
     double omega = 0.6667;
     double alpha = 1.0;
+    int fused_from = 0;   // first level of the single-block coarse cycle (set by amg_plan_fused)
 };
+
+// Choose the levels that the single-block coarse cycle takes over.
+void amg_plan_fused(AmgHierarchy &H);
 
 // Host-side construction of the pattern data.  Inputs: level-0 ELL columns
 // (col0[6][N], boundary slots = own row) and directional neighbours dn0[6][N]

@@ -1243,6 +1243,8 @@ int build_amg(mc_flow *h, const HostMesh &hm)
     auto add = [&](void *pp, size_t bytes) { items.push_back({(void **)pp, std::max<size_t>(bytes, 8)}); };
     AmgHierarchy &H = h->amg;
     H.levels = L;
+    for (int l = 0; l < L; l++) H.lv[l].n = lv[l].n;
+    amg_plan_fused(H);
     H.sweeps = h->prm.amg_sweeps;
     H.omega = h->prm.amg_omega;
     H.alpha = h->prm.amg_alpha;
