@@ -136,21 +136,29 @@ int amg_build_host(int N, const std::vector<int> &col0, const std::vector<int> &
 
 namespace {
 
-template <typename T>
-__device__ __forceinline__ T row_apply(const AmgLevelT<T> &L, int i, const T *__restrict__ e)
+// (A v)_i where v(j) yields the vector's value at row j (a stored vector, or
+// one evaluated where it is needed).
+template <typename T, typename V>
+__device__ __forceinline__ T row_apply_v(const AmgLevelT<T> &L, int i, V &&v)
 {
-    const T s0 = L.diag[i] * e[i];
+    const T s0 = L.diag[i] * v(i);
     if (L.dc.code) {
         return with_row_cols(L.dc, L.col, L.n, i, [&](const int(&c)[6]) {
             T s = s0;
 #pragma unroll
-            for (int q = 0; q < 6; q++) s += L.off[(size_t)q * L.n + i] * e[c[q]];
+            for (int q = 0; q < 6; q++) s += L.off[(size_t)q * L.n + i] * v(c[q]);
             return s;
         });
     }
     T s = s0;
-    for (int q = 0; q < L.k; q++) s += L.off[(size_t)q * L.n + i] * e[L.col[(size_t)q * L.n + i]];
+    for (int q = 0; q < L.k; q++) s += L.off[(size_t)q * L.n + i] * v(L.col[(size_t)q * L.n + i]);
     return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T row_apply(const AmgLevelT<T> &L, int i, const T *__restrict__ e)
+{
+    return row_apply_v(L, i, [&](int j) { return e[j]; });
 }
 
 template <typename T>
@@ -293,6 +301,32 @@ __global__ void k_amg_smooth_first(AmgLevelT<T> L, T omega, T *__restrict__ e, c
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= L.n) return;
     e[i] = omega * L.r[i] * inv_or_zero(L.diag[i]);
+}
+
+// The first two sweeps from e = 0 in one pass: e1 = e0 + omega D^-1 (r - A e0)
+// with e0 = omega D^-1 r evaluated at each row where it is needed.
+template <typename T>
+__global__ void k_amg_smooth_first2(AmgLevelT<T> L, T omega, T *__restrict__ eout, const PcgState *st)
+{
+    if (st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.n) return;
+    auto e0 = [&](int j) { return omega * L.r[j] * inv_or_zero(L.diag[j]); };
+    eout[i] = e0(i) + omega * (L.r[i] - row_apply_v(L, i, e0)) * inv_or_zero(L.diag[i]);
+}
+
+// Prolongation and the first post-smoothing sweep in one pass: the
+// corrected iterate e + alpha ec[agg] is evaluated at each row where the
+// sweep needs it and not stored.
+template <typename T>
+__global__ void k_amg_prolong_jacobi(AmgLevelT<T> L, T omega, T alpha, const T *__restrict__ ec,
+                                     const T *__restrict__ e, T *__restrict__ eout, const PcgState *st)
+{
+    if (st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.n) return;
+    auto ein = [&](int j) { return e[j] + alpha * ec[L.agg[j]]; };
+    eout[i] = ein(i) + omega * (L.r[i] - row_apply_v(L, i, ein)) * inv_or_zero(L.diag[i]);
 }
 
 template <typename T>
@@ -497,7 +531,18 @@ void amg_plan_fused(AmgHierarchy &H)
     H.fused_from = f;
 }
 
-int amg_kernels_per_vcycle(const AmgHierarchy &H) { return H.fused_from * (2 * H.sweeps + 2) + 1; }
+// FP32 V-cycles with nu >= 2 run the first two sweeps before the coarse
+// correction, and the prolongation with the first sweep after it, as single
+// kernels (in FP64 the extra gathers of the evaluated iterate cost more than
+// the saved passes).
+bool amg_paired_sweeps(const AmgHierarchy &H, bool fp32) { return fp32 && H.sweeps >= 2; }
+
+// Per level above the fused ones: nu sweeps before and after the coarse
+// correction and the restriction.
+int amg_kernels_per_vcycle(const AmgHierarchy &H, bool fp32)
+{
+    return H.fused_from * (2 * H.sweeps + (amg_paired_sweeps(H, fp32) ? 0 : 2)) + 1;
+}
 
 template <typename T>
 void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out_v, PcgState *st, double *partials,
@@ -512,10 +557,17 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
     const AmgLevelT<T> *src = levels_of<T>(H);
     for (int l = 0; l < L; l++) lv[l] = src[l];
     lv[0].r = const_cast<T *>(r0);
+    const bool pair = amg_paired_sweeps(H, sizeof(T) == sizeof(float));
     for (int l = 0; l < F; l++) {
-        k_amg_smooth_first<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, lv[l].e[0], st);
-        int c = 0;
-        for (int sw = 1; sw < H.sweeps; sw++) {
+        int c = 0, sw = 1;
+        if (pair) {
+            k_amg_smooth_first2<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, lv[l].e[1], st);
+            c = 1;
+            sw = 2;
+        } else {
+            k_amg_smooth_first<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, lv[l].e[0], st);
+        }
+        for (; sw < H.sweeps; sw++) {
             k_amg_jacobi<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, lv[l].e[c], lv[l].e[c ^ 1], st);
             c ^= 1;
         }
@@ -528,9 +580,17 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
     k_amg_coarse_cycle<T><<<1, AMG_FUSED_THREADS, 0, s>>>(C, H.dense, omega, alpha, H.sweeps, st);
     cur[F] = (F < L - 1) ? (2 * H.sweeps - 1) & 1 : 0;
     for (int l = F - 1; l >= 0; l--) {
-        int c = cur[l];
-        k_amg_prolong<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], alpha, lv[l + 1].e[cur[l + 1]], lv[l].e[c], st);
-        for (int sw = 1; sw <= H.sweeps; sw++) {
+        int c = cur[l], sw = 1;
+        if (pair) {
+            k_amg_prolong_jacobi<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, alpha, lv[l + 1].e[cur[l + 1]],
+                                                                            lv[l].e[c], lv[l].e[c ^ 1], st);
+            c ^= 1;
+            sw = 2;
+        } else {
+            k_amg_prolong<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], alpha, lv[l + 1].e[cur[l + 1]], lv[l].e[c],
+                                                                    st);
+        }
+        for (; sw <= H.sweeps; sw++) {
             if (l == 0 && sw == H.sweeps) {
                 k_amg_final<T><<<krylov_grid(lv[0].n), MCB_THREADS, 0, s>>>(lv[0], omega, lv[0].e[c], zp_out, st,
                                                                            partials, counter, is_init);

@@ -102,6 +102,6 @@ struct PcgState;
 template <typename T>
 void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out, PcgState *st, double *partials,
                 unsigned int *counter, int is_init);
-int amg_kernels_per_vcycle(const AmgHierarchy &H);
+int amg_kernels_per_vcycle(const AmgHierarchy &H, bool fp32);
 
 } // namespace mcb

@@ -459,7 +459,7 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
                [&] { pcg_init_amg(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, 1, use_x0); });
         launch(h, K_AMG_VCYCLE,
                [&] { amg_vcycle<double>(h->stream, h->amg, v.r, v.zp[0], v.st, v.partials, v.counter, 1); });
-        h->launches += amg_kernels_per_vcycle(h->amg) - 1;
+        h->launches += amg_kernels_per_vcycle(h->amg, false) - 1;
     } else {
         launch(h, K_PCG_INIT,
                [&] { pcg_init(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, use_x0, 1); });
@@ -469,7 +469,7 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
     // The device marks the solve done at max_iters; the host bound is a second guard.
     const int batch_iters = amg ? PCG_AMG_BATCH : PCG_BATCH;
     const long max_batches = h->prm.max_iters / batch_iters + 2;
-    const int per_iter = amg ? 2 + amg_kernels_per_vcycle(h->amg) : PCG_KERNELS_PER_ITER;
+    const int per_iter = amg ? 2 + amg_kernels_per_vcycle(h->amg, false) : PCG_KERNELS_PER_ITER;
     auto iterations = [&](int count) {
         for (int it = 0; it < count; it++) {
             const int pin = it & 1;
@@ -479,7 +479,7 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
                 launch(h, K_AMG_VCYCLE, [&] {
                     amg_vcycle<double>(h->stream, h->amg, v.r, v.zp[pin ^ 1], v.st, v.partials, v.counter, 0);
                 });
-                h->launches += amg_kernels_per_vcycle(h->amg) - 1;
+                h->launches += amg_kernels_per_vcycle(h->amg, false) - 1;
             } else {
                 launch(h, K_PCG_ITER2, [&] { pcg_iter2(h->stream, A, v, pin ^ 1); });
             }
@@ -527,7 +527,7 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
     });
     int rc = check_launch(h);
     if (rc) return rc;
-    const int per_iter = 2 + amg_kernels_per_vcycle(h->amg);
+    const int per_iter = 2 + amg_kernels_per_vcycle(h->amg, true);
     const long max_batches = h->prm.max_iters / PCG_AMG_BATCH + 2;
     int inner_total = 0, worst = MC_OK;
     for (int outer = 0;; outer++) {
@@ -545,7 +545,7 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
                [&] { pcg_init_amg<float>(h->stream, A32, in, inner_rtol, 0.0, h->prm.max_iters, 0); });
         launch(h, K_AMG_VCYCLE32,
                [&] { amg_vcycle<float>(h->stream, h->amg, in.r, in.zp[0], in.st, in.partials, in.counter, 1); });
-        h->launches += amg_kernels_per_vcycle(h->amg) - 1;
+        h->launches += amg_kernels_per_vcycle(h->amg, true) - 1;
         rc = check_launch(h);
         if (rc) return rc;
         auto iterations = [&](int count) {
@@ -556,7 +556,7 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
                 launch(h, K_AMG_VCYCLE32, [&] {
                     amg_vcycle<float>(h->stream, h->amg, in.r, in.zp[pin ^ 1], in.st, in.partials, in.counter, 0);
                 });
-                h->launches += amg_kernels_per_vcycle(h->amg) - 1;
+                h->launches += amg_kernels_per_vcycle(h->amg, true) - 1;
             }
         };
         const bool looped =
