@@ -297,6 +297,7 @@ constexpr int DENSE_SOLVE_PARTS = 8;
 template <typename T>
 __global__ void k_amg_smooth_first(AmgLevelT<T> L, T omega, T *__restrict__ e, const PcgState *st)
 {
+    pdl_wait();
     if (st->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= L.n) return;
@@ -308,6 +309,7 @@ __global__ void k_amg_smooth_first(AmgLevelT<T> L, T omega, T *__restrict__ e, c
 template <typename T>
 __global__ void k_amg_smooth_first2(AmgLevelT<T> L, T omega, T *__restrict__ eout, const PcgState *st)
 {
+    pdl_wait();
     if (st->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= L.n) return;
@@ -322,6 +324,7 @@ template <typename T>
 __global__ void k_amg_prolong_jacobi(AmgLevelT<T> L, T omega, T alpha, const T *__restrict__ ec,
                                      const T *__restrict__ e, T *__restrict__ eout, const PcgState *st)
 {
+    pdl_wait();
     if (st->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= L.n) return;
@@ -333,6 +336,7 @@ template <typename T>
 __global__ void k_amg_jacobi(AmgLevelT<T> L, T omega, const T *__restrict__ ein, T *__restrict__ eout,
                              const PcgState *st)
 {
+    pdl_wait();
     if (st->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= L.n) return;
@@ -361,6 +365,7 @@ __device__ __forceinline__ void restrict_row8(const AmgLevelT<T> &fine, const Am
 template <typename T>
 __global__ void k_amg_restrict(AmgLevelT<T> fine, AmgLevelT<T> coarse, const T *__restrict__ e, const PcgState *st)
 {
+    pdl_wait();
     if (st->done) return;
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     restrict_row8(fine, coarse, e, g >> 3, g & 7);
@@ -370,6 +375,7 @@ template <typename T>
 __global__ void k_amg_prolong(AmgLevelT<T> fine, T alpha, const T *__restrict__ ec, T *__restrict__ e,
                               const PcgState *st)
 {
+    pdl_wait();
     if (st->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= fine.n) return;
@@ -382,6 +388,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_amg_final(AmgLevelT<T> L, T ome
                                                            typename Pair<T>::type *__restrict__ zp, PcgState *st,
                                                            double *partials, unsigned int *counter, int is_init)
 {
+    pdl_wait();
     __shared__ double sh[1][MCB_THREADS];
     if (st->done) return;
     double acc[1] = {0.0};
@@ -425,6 +432,7 @@ __global__ void __launch_bounds__(AMG_FUSED_THREADS)
     k_amg_coarse_cycle(const __grid_constant__ AmgCoarse<T> C, const double *__restrict__ dense, T omega, T alpha,
                        int sweeps, const PcgState *st)
 {
+    pdl_wait();
     if (st->done) return;
     __shared__ double rs[AMG_COARSEST_MAX];
     __shared__ double part[DENSE_SOLVE_PARTS][AMG_COARSEST_MAX];
@@ -438,7 +446,8 @@ __global__ void __launch_bounds__(AMG_FUSED_THREADS)
         for (int sw = 1; sw < sweeps; sw++) {
             const T *ein = L.e[c];
             T *eout = L.e[c ^ 1];
-            for (int i = t; i < L.n; i += nt) eout[i] = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
+            for (int i = t; i < L.n; i += nt)
+                eout[i] = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
             c ^= 1;
             __syncthreads();
         }
@@ -475,7 +484,8 @@ __global__ void __launch_bounds__(AMG_FUSED_THREADS)
         for (int sw = 1; sw <= sweeps; sw++) {
             const T *ein = L.e[c];
             T *eout = L.e[c ^ 1];
-            for (int i = t; i < L.n; i += nt) eout[i] = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
+            for (int i = t; i < L.n; i += nt)
+                eout[i] = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
             c ^= 1;
             __syncthreads();
         }
@@ -558,45 +568,48 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
     for (int l = 0; l < L; l++) lv[l] = src[l];
     lv[0].r = const_cast<T *>(r0);
     const bool pair = amg_paired_sweeps(H, sizeof(T) == sizeof(float));
+    const dim3 nt(MCB_THREADS);
     for (int l = 0; l < F; l++) {
+        const AmgLevelT<T> &V = lv[l];
+        const dim3 g(blocks(V.n));
         int c = 0, sw = 1;
         if (pair) {
-            k_amg_smooth_first2<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, lv[l].e[1], st);
+            pdl_launch(k_amg_smooth_first2<T>, g, nt, 0, s, V, omega, V.e[1], st);
             c = 1;
             sw = 2;
         } else {
-            k_amg_smooth_first<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, lv[l].e[0], st);
+            pdl_launch(k_amg_smooth_first<T>, g, nt, 0, s, V, omega, V.e[0], st);
         }
         for (; sw < H.sweeps; sw++) {
-            k_amg_jacobi<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, lv[l].e[c], lv[l].e[c ^ 1], st);
+            pdl_launch(k_amg_jacobi<T>, g, nt, 0, s, V, omega, V.e[c], V.e[c ^ 1], st);
             c ^= 1;
         }
         cur[l] = c;
-        k_amg_restrict<T><<<blocks8(lv[l + 1].n), MCB_THREADS, 0, s>>>(lv[l], lv[l + 1], lv[l].e[c], st);
+        pdl_launch(k_amg_restrict<T>, dim3(blocks8(lv[l + 1].n)), nt, 0, s, V, lv[l + 1], V.e[c], st);
     }
     AmgCoarse<T> C;
     C.nl = L - F;
     for (int q = 0; q < C.nl; q++) C.lv[q] = lv[F + q];
-    k_amg_coarse_cycle<T><<<1, AMG_FUSED_THREADS, 0, s>>>(C, H.dense, omega, alpha, H.sweeps, st);
+    pdl_launch(k_amg_coarse_cycle<T>, dim3(1), dim3(AMG_FUSED_THREADS), 0, s, C, H.dense, omega, alpha, H.sweeps, st);
     cur[F] = (F < L - 1) ? (2 * H.sweeps - 1) & 1 : 0;
     for (int l = F - 1; l >= 0; l--) {
+        const AmgLevelT<T> &V = lv[l];
+        const dim3 g(blocks(V.n));
+        const T *ec = lv[l + 1].e[cur[l + 1]];
         int c = cur[l], sw = 1;
         if (pair) {
-            k_amg_prolong_jacobi<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, alpha, lv[l + 1].e[cur[l + 1]],
-                                                                            lv[l].e[c], lv[l].e[c ^ 1], st);
+            pdl_launch(k_amg_prolong_jacobi<T>, g, nt, 0, s, V, omega, alpha, ec, V.e[c], V.e[c ^ 1], st);
             c ^= 1;
             sw = 2;
         } else {
-            k_amg_prolong<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], alpha, lv[l + 1].e[cur[l + 1]], lv[l].e[c],
-                                                                    st);
+            pdl_launch(k_amg_prolong<T>, g, nt, 0, s, V, alpha, ec, V.e[c], st);
         }
         for (; sw <= H.sweeps; sw++) {
             if (l == 0 && sw == H.sweeps) {
-                k_amg_final<T><<<krylov_grid(lv[0].n), MCB_THREADS, 0, s>>>(lv[0], omega, lv[0].e[c], zp_out, st,
-                                                                           partials, counter, is_init);
+                pdl_launch(k_amg_final<T>, dim3(krylov_grid(V.n)), nt, 0, s, V, omega, V.e[c], zp_out, st, partials,
+                           counter, is_init);
             } else {
-                k_amg_jacobi<T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l], omega, lv[l].e[c], lv[l].e[c ^ 1],
-                                                                       st);
+                pdl_launch(k_amg_jacobi<T>, g, nt, 0, s, V, omega, V.e[c], V.e[c ^ 1], st);
                 c ^= 1;
             }
         }

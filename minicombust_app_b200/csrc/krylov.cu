@@ -4,6 +4,7 @@
 #include "krylov.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "mc_reduce.cuh"
 
@@ -13,6 +14,17 @@
 #endif
 
 namespace mcb {
+
+bool pdl_enabled()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = std::getenv("MC_PDL");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
 
 namespace {
 
@@ -106,6 +118,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(EllT<T> A, PcgVectors
                                                            const typename Pair<T>::type *__restrict__ X,
                                                            typename Pair<T>::type *__restrict__ Y)
 {
+    pdl_wait();
     using T2 = typename Pair<T>::type;
     __shared__ double sh[1][MCB_THREADS];
     const PcgState *st = v.st;
@@ -160,6 +173,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(EllT<T> A, PcgVectors
 // x += alpha p; r -= alpha q; z = r / diag; convergence on ||r||.
 __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2(Ell A, PcgVectors v, double2 *__restrict__ Y)
 {
+    pdl_wait();
     __shared__ double sh[2][MCB_THREADS];
     const PcgState *st = v.st;
     if (st->done) return;
@@ -258,6 +272,7 @@ template <typename T>
 __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2_amg(EllT<T> A, PcgVectorsT<T> v,
                                                                const typename Pair<T>::type *__restrict__ Y)
 {
+    pdl_wait();
     __shared__ double sh[1][MCB_THREADS];
     const PcgState *st = v.st;
     if (st->done) return;
@@ -429,6 +444,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_guess_apply(int N, double *__re
 __global__ void __launch_bounds__(MCB_THREADS) k_ir_add(int N, double *__restrict__ x, const float *__restrict__ e,
                                                         const PcgState *st)
 {
+    pdl_wait();
     if (st->done) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) x[i] += (double)e[i];
 }
@@ -438,6 +454,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_ir_residual(Ell A, const double
                                                              float *__restrict__ r32, PcgState *st, double *partials,
                                                              unsigned int *counter)
 {
+    pdl_wait();
     __shared__ double sh[1][MCB_THREADS];
     if (st->done) return;
     const int N = A.N;
@@ -504,7 +521,7 @@ void pcg_init(cudaStream_t s, const Ell &A, const PcgVectors &v, double rtol, do
 template <typename T>
 void pcg_iter1(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, int pin)
 {
-    k_pcg_iter1<T><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.zp[pin], v.zp[pin ^ 1]);
+    pdl_launch(k_pcg_iter1<T>, krylov_grid(A.N), MCB_THREADS, 0, s, A, v, v.zp[pin], v.zp[pin ^ 1]);
 }
 void pcg_iter2(cudaStream_t s, const Ell &A, const PcgVectors &v, int pnew)
 {
@@ -519,7 +536,7 @@ void pcg_init_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, dou
 template <typename T>
 void pcg_iter2_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, int pnew)
 {
-    k_pcg_iter2_amg<T><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.zp[pnew]);
+    pdl_launch(k_pcg_iter2_amg<T>, krylov_grid(A.N), MCB_THREADS, 0, s, A, v, v.zp[pnew]);
 }
 #define MCB_INSTANTIATE_PCG(T)                                                                                  \
     template void pcg_iter1<T>(cudaStream_t, const EllT<T> &, const PcgVectorsT<T> &, int);                   \
@@ -652,6 +669,7 @@ __global__ void __launch_bounds__(MCB_THREADS, SPLIT ? 8 : 4) k_bicg_1(EllT<T> A
                                                         const T *__restrict__ vo, T *__restrict__ pn,
                                                         T *__restrict__ vn)
 {
+    pdl_wait();
     __shared__ double sh[R][MCB_THREADS];
     const BicgState<R> *st = v.st;
     if (st->all_done) return;
@@ -738,6 +756,7 @@ __global__ void __launch_bounds__(MCB_THREADS, SPLIT ? 8 : 4) k_bicg_1(EllT<T> A
 template <typename T, int R, bool SPLIT>
 __global__ void __launch_bounds__(MCB_THREADS, SPLIT ? 8 : 4) k_bicg_2(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ vv)
 {
+    pdl_wait();
     __shared__ double sh[2 * R][MCB_THREADS];
     const BicgState<R> *st = v.st;
     if (st->all_done) return;
@@ -824,6 +843,7 @@ __global__ void __launch_bounds__(MCB_THREADS, SPLIT ? 8 : 4) k_bicg_2(EllT<T> A
 template <typename T, int R, bool SPLIT>
 __global__ void __launch_bounds__(MCB_THREADS, SPLIT ? 8 : 1) k_bicg_3(EllT<T> A, BicgVectorsT<T, R> v, const T *__restrict__ p)
 {
+    pdl_wait();
     __shared__ double sh[2 * R][MCB_THREADS];
     const BicgState<R> *st = v.st;
     if (st->all_done) return;
@@ -1051,21 +1071,21 @@ template <typename T, int R>
 void bicg_1_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int pin)
 {
     constexpr bool S = bicg_split<T, R>();
-    k_bicg_1<T, R, S><<<krylov_grid(A.N) * (S ? R : 1), MCB_THREADS, 0, s>>>(A, v, v.p[pin], v.v[pin], v.p[pin ^ 1],
-                                                                            v.v[pin ^ 1]);
+    pdl_launch(k_bicg_1<T, R, S>, krylov_grid(A.N) * (S ? R : 1), MCB_THREADS, 0, s, A, v, v.p[pin], v.v[pin],
+               v.p[pin ^ 1], v.v[pin ^ 1]);
 }
 // The second product gathers two vectors per right-hand side: one pass over
 // the matrix for all of them is faster than the split form here.
 template <typename T, int R>
 void bicg_2_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int vnew)
 {
-    k_bicg_2<T, R, false><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, v.v[vnew]);
+    pdl_launch(k_bicg_2<T, R, false>, krylov_grid(A.N), MCB_THREADS, 0, s, A, v, v.v[vnew]);
 }
 template <typename T, int R>
 void bicg_3_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int pnew)
 {
     constexpr bool S = bicg_split<T, R>();
-    k_bicg_3<T, R, S><<<krylov_grid(A.N) * (S ? R : 1), MCB_THREADS, 0, s>>>(A, v, v.p[pnew]);
+    pdl_launch(k_bicg_3<T, R, S>, krylov_grid(A.N) * (S ? R : 1), MCB_THREADS, 0, s, A, v, v.p[pnew]);
 }
 template <int R>
 void bicg_init(cudaStream_t s, const Ell &A, const BicgVectors<R> &v, double rtol, int max_iters)

@@ -229,6 +229,30 @@ enum { KRYLOV_OK = 0, KRYLOV_NOT_CONVERGED = 1, KRYLOV_NONFINITE = 2 };
 // Grid size used by the Krylov kernels for N rows.
 int krylov_grid(int N);
 
+// Programmatic dependent launch: a kernel started with pdl_launch may be
+// scheduled while its stream predecessor drains; pdl_wait (its first
+// statement) blocks until the predecessor has completed and its memory is
+// visible.  In a kernel launched the ordinary way pdl_wait returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+bool pdl_enabled();  // MC_PDL=0 launches every kernel the ordinary way
+
+template <typename... KArgs, typename... Args>
+inline void pdl_launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args &&...args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, static_cast<Args &&>(args)...);
+}
+
 // Single-kernel launchers (asynchronous on stream).  PCG uses Jacobi
 // preconditioning; with project != 0 the right-hand side and the solution are
 // projected onto mean zero (the singular pure-Neumann pressure-correction
