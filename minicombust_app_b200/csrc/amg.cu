@@ -207,11 +207,10 @@ __global__ void k_amg_galerkin(AmgLevelT<TF> fine, AmgLevelT<T> coarse)
     }
 }
 
-// Dense Cholesky of A + sigma 1 1^T (sigma = mean diagonal / n) on the
-// coarsest level, one block of DENSE_THREADS, FP64 (factor in shared memory),
-// then its explicit symmetric inverse, row-major in `dense` for the V-cycle's
-// solve.  The trailing updates run one warp per row (lanes over columns);
-// the inverse one warp per column, with warp-reduced inner products.
+// Explicit inverse of A + sigma 1 1^T (sigma = mean diagonal / n) on the
+// coarsest level, one block of DENSE_THREADS, FP64 in shared memory, by
+// Gauss-Jordan elimination; symmetrised exactly and stored row-major in
+// `dense` for the V-cycle's solve.
 constexpr int DENSE_THREADS = 1024;
 
 __device__ __forceinline__ double warp_sum(double v)
@@ -249,42 +248,32 @@ __global__ void __launch_bounds__(DENSE_THREADS) k_amg_dense_factor(AmgLevelT<T>
         }
     }
     __syncthreads();
-    for (int j = 0; j < n; j++) {
-        // column j below the pivot divided by sqrt(pivot); the pivot itself is
-        // replaced only after the trailing update, which does not read it
-        const double d = A[j * ld + j], sq = d > 0.0 ? sqrt(d) : 1.0;
-        if (t > j && t < n) A[t * ld + j] /= sq;
-        __syncthreads();
-        for (int r = j + 1 + warp; r < n; r += nwarps) {
-            const double lrj = A[r * ld + j];
-            for (int c = j + 1 + lane; c <= r; c += 32) A[r * ld + c] -= lrj * A[c * ld + j];
-        }
-        if (t == j) A[j * ld + j] = sq;
-        __syncthreads();
-    }
-    // L^{-1} in place, columns from the last to the first: for i > j,
-    // Linv[i][j] = -(sum_{k=j+1..i} Linv[i][k] L[k][j]) / L[j][j] uses the
-    // finished columns k > j and the still original column j.
-    __shared__ double colj[AMG_COARSEST_MAX];
-    for (int j = n - 1; j >= 0; j--) {
-        for (int i = j + 1 + warp; i < n; i += nwarps) {
-            double p = 0.0;
-            for (int k = j + 1 + lane; k <= i; k += 32) p += A[i * ld + k] * A[k * ld + j];
-            p = warp_sum(p);
-            if (lane == 0) colj[i] = -p / A[j * ld + j];
+    // In-place Gauss-Jordan inversion (no pivoting: the matrix is symmetric
+    // positive definite).  Step k: the pivot row, with the identity's column k
+    // in place of column k, divided by the pivot; every other row minus its
+    // old column-k entry times that row.  Two barriers per step; thread t
+    // owns column t % n of rows t / n, t / n + rows_per_pass, ...
+    __shared__ double rk[AMG_COARSEST_MAX], ck[AMG_COARSEST_MAX];
+    const int rpp = blockDim.x / n, jc = t % n, i0 = t / n;
+    for (int k = 0; k < n; k++) {
+        const double p = A[k * ld + k];
+        const double pinv = p != 0.0 ? 1.0 / p : 0.0;
+        if (t < n) {
+            rk[t] = (t == k ? 1.0 : A[k * ld + t]) * pinv;
+            ck[t] = A[t * ld + k];
         }
         __syncthreads();
-        if (t > j && t < n) A[t * ld + j] = colj[t];
-        if (t == j) A[j * ld + j] = 1.0 / A[j * ld + j];
+        if (i0 < rpp) {
+            const double r = rk[jc];
+            for (int i = i0; i < n; i += rpp)
+                A[i * ld + jc] = i == k ? r : (jc == k ? 0.0 : A[i * ld + jc]) - ck[i] * r;
+        }
         __syncthreads();
     }
-    // (A + sigma 1 1^T)^{-1} = L^{-T} L^{-1}: entry (i, j) = sum_{k >= max(i, j)} Linv[k][i] Linv[k][j],
-    // the same sum in the same order for (j, i), so the result is exactly symmetric
+    // exactly symmetric result: both triangles take the same average
     for (int idx = t; idx < n * n; idx += blockDim.x) {
-        const int i = idx / n, j = idx % n;
-        double p = 0.0;
-        for (int k = max(i, j); k < n; k++) p += A[k * ld + i] * A[k * ld + j];
-        dense[idx] = p;
+        const int i = idx / n, j = idx - i * n;
+        dense[idx] = 0.5 * (A[i * ld + j] + A[j * ld + i]);
     }
 }
 

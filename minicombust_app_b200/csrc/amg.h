@@ -9,7 +9,7 @@
 // piecewise-constant prolongation P; their values are recomputed on the GPU
 // whenever the fine values change, by summing precomputed lists of fine
 // entries (a gather, deterministic).  The coarsest level (<= 128 rows) is
-// solved exactly with a dense Cholesky factor of A_c + sigma 1 1^T, which for
+// solved exactly with the explicit inverse of A_c + sigma 1 1^T, which for
 // the singular pure-Neumann system gives the minimum-norm solution of a
 // consistent right-hand side.
 //
@@ -65,7 +65,7 @@ struct AmgHierarchy {
     AmgLevelT<double> lv[AMG_MAX_LEVELS];    // FP64 values (level 0 = the pressure-correction matrix)
     AmgLevelT<float> lv32[AMG_MAX_LEVELS];   // FP32 values, when the refined FP32 path is enabled
     bool has32 = false;
-    double *dense = nullptr;    // coarsest Cholesky factor [n][n] (row-major, lower), FP64
+    double *dense = nullptr;    // coarsest inverse [n][n] (row-major, exactly symmetric), FP64
     int sweeps = 2;
     double omega = 0.6667;
     double alpha = 1.0;
