@@ -103,7 +103,7 @@ typedef struct mc_flow_params {
     int max_iters;            /* per Krylov solve */
     int pressure_solver;      /* MC_PSOLVER_* */
     int precision;            /* MC_PRECISION_* */
-    int initial_guess;        /* MC_GUESS_* for the pressure correction */
+    int initial_guess;        /* MC_GUESS_* for the first pressure correction of a pass (later ones start at 0) */
     int device;               /* CUDA device ordinal */
     int amg_sweeps;           /* MC_PSOLVER_PCG_AMG: damped-Jacobi sweeps before and after the coarse correction */
     double amg_omega;         /* Jacobi damping */

@@ -398,10 +398,12 @@ __global__ void k_snapshot_pack(int N, const double *__restrict__ b, const PcgSt
 // written into x.  Returns 1 when x holds the guess (0: start from zero).
 int select_guess(mc_flow *h, const Ell &A, const double *b, const PcgState *st, double *x)
 {
-    if (h->prm.initial_guess == MC_GUESS_ZERO) return 0;
-    // the network runs for the first corrector of a pass; the later ones, whose
-    // right-hand sides are already small, use the previous correction alone
-    const bool learned = h->prm.initial_guess == MC_GUESS_LEARNED && h->corrector == 1;
+    // Only the first corrector of a pass starts from a guess: the later ones
+    // solve for the small non-orthogonal remainder, which on the benchmark box
+    // converges at the initial residual check, so a guess there is pure cost
+    // (the reference starts every corrector from PP = 0).
+    if (h->prm.initial_guess == MC_GUESS_ZERO || h->corrector > 1) return 0;
+    const bool learned = h->prm.initial_guess == MC_GUESS_LEARNED;
     if (learned) {
         launch(h, K_GNN, [&] {
             GnnInput<double> in{b, &st->mean, A.diag, h->pp_prev};
@@ -424,9 +426,9 @@ int select_guess(mc_flow *h, const Ell &A, const double *b, const PcgState *st, 
 // next solve's previous correction.
 int after_pressure_solve(mc_flow *h)
 {
-    if (h->prm.initial_guess != MC_GUESS_ZERO) {
+    if (h->prm.initial_guess != MC_GUESS_ZERO && h->corrector == 1) {
         const GuessState &g = *h->h_gs;  // the copy was ordered before the solve's final synchronisation
-        if (h->corrector == 1 && h->prm.initial_guess == MC_GUESS_LEARNED && g.net_status)
+        if (h->prm.initial_guess == MC_GUESS_LEARNED && g.net_status)
             return fail(h, MC_ERR_TIMEOUT, "learned-guess layer kernel gave up waiting (prediction zeroed)");
         h->guess_choice = g.choice;
         h->guess_rel = g.bb > 0 ? std::sqrt((g.choice < 0 ? g.bb : g.rc) / g.bb) : 1.0;
