@@ -158,6 +158,7 @@ struct mc_flow {
     bool gnn_loaded = false;
     int guess_choice = -1;
     int corrector = 1;                // pressure-correction solve within the pass (1 = first)
+    bool guess_used = false;          // the last pressure solve started from a guess
     double guess_rel = 1.0;
     // snapshot dataset writer
     FILE *snap = nullptr;
@@ -456,6 +457,7 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
     const bool amg = h->use_amg;
     launch(h, K_PCG_MEAN, [&] { pcg_mean(h->stream, A, v); });
     const int use_x0 = select_guess(h, A, v.b, v.st, v.x);
+    h->guess_used = use_x0 != 0;
     if (amg) {
         launch(h, K_PCG_INIT_AMG,
                [&] { pcg_init_amg(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, 1, use_x0); });
@@ -523,6 +525,7 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
     constexpr int kMaxOuter = 50;
     launch(h, K_PCG_MEAN, [&] { pcg_mean(h->stream, A, o); });
     const int use_x0 = select_guess(h, A, o.b, o.st, o.x);
+    h->guess_used = use_x0 != 0;
     launch(h, K_IR, [&] {
         ir_init(h->stream, A, o.b, o.x, o.r, h->r32, o.st, o.partials, o.counter, h->prm.p_rtol, abs_floor, kMaxOuter,
                 use_x0);
@@ -862,6 +865,14 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
                 st->guess_rel_residual_first = h->guess_rel;
             }
             st->pressure_rel_residual = relres;
+        }
+        // A solve that met its tolerance at the initial check from the zero
+        // guess leaves PP = 0 exactly: the corrections below would add zeros
+        // (signed zeros aside) and max|PP| = 0 ends the loop, so skip them.
+        if (rc == MC_OK && its == 0 && !h->guess_used) {
+            if (!simple && h->first_pressure) h->first_pressure = 0;
+            if (loop == 1 && st) st->pressure_correction_max_first = 0.0;
+            break;
         }
         launch(h, K_PP_MAX, [&] {
             k_pp_max<<<krylov_grid(h->N), MCB_THREADS, 0, h->stream>>>(h->N, h->ph.cell0, h->phi[G_PP], h->partials,
