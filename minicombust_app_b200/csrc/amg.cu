@@ -508,7 +508,7 @@ void set_dense_attributes()
 } // namespace
 
 template <typename T>
-void amg_setup_values(cudaStream_t s, const AmgHierarchy &H)
+void amg_setup_levels(cudaStream_t s, const AmgHierarchy &H)
 {
     const AmgLevelT<T> *lv = levels_of<T>(H);
     if (sizeof(T) == sizeof(float))
@@ -518,9 +518,14 @@ void amg_setup_values(cudaStream_t s, const AmgHierarchy &H)
     if (H.levels > 1) k_amg_galerkin<double, T><<<blocks(lv[1].n), MCB_THREADS, 0, s>>>(H.lv[0], lv[1]);
     for (int l = 2; l < H.levels; l++)
         k_amg_galerkin<T, T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l - 1], lv[l]);
+}
+
+template <typename T>
+void amg_coarsest_inverse(cudaStream_t s, const AmgHierarchy &H, double *out)
+{
     set_dense_attributes<T>();
-    const AmgLevelT<T> &C = lv[H.levels - 1];
-    k_amg_dense_factor<T><<<1, DENSE_THREADS, dense_smem(C.n), s>>>(C, H.dense);
+    const AmgLevelT<T> &C = levels_of<T>(H)[H.levels - 1];
+    k_amg_dense_factor<T><<<1, DENSE_THREADS, dense_smem(C.n), s>>>(C, out);
 }
 
 void amg_plan_fused(AmgHierarchy &H)
@@ -606,8 +611,10 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
     }
 }
 
-template void amg_setup_values<double>(cudaStream_t, const AmgHierarchy &);
-template void amg_setup_values<float>(cudaStream_t, const AmgHierarchy &);
+template void amg_setup_levels<double>(cudaStream_t, const AmgHierarchy &);
+template void amg_setup_levels<float>(cudaStream_t, const AmgHierarchy &);
+template void amg_coarsest_inverse<double>(cudaStream_t, const AmgHierarchy &, double *);
+template void amg_coarsest_inverse<float>(cudaStream_t, const AmgHierarchy &, double *);
 template void amg_vcycle<double>(cudaStream_t, const AmgHierarchy &, const double *, void *, PcgState *, double *,
                                  unsigned int *, int);
 template void amg_vcycle<float>(cudaStream_t, const AmgHierarchy &, const float *, void *, PcgState *, double *,

@@ -65,7 +65,8 @@ struct AmgHierarchy {
     AmgLevelT<double> lv[AMG_MAX_LEVELS];    // FP64 values (level 0 = the pressure-correction matrix)
     AmgLevelT<float> lv32[AMG_MAX_LEVELS];   // FP32 values, when the refined FP32 path is enabled
     bool has32 = false;
-    double *dense = nullptr;    // coarsest inverse [n][n] (row-major, exactly symmetric), FP64
+    double *dense = nullptr;       // coarsest inverse [n][n] (row-major, exactly symmetric), FP64
+    double *dense_next = nullptr;  // the inverse being formed for the next pass (lagged setup)
     int sweeps = 2;
     double omega = 0.6667;
     double alpha = 1.0;
@@ -90,11 +91,14 @@ int amg_build_host(int N, const std::vector<int> &col0, const std::vector<int> &
                    std::string &err);
 
 // Device work, all asynchronous on stream s.
-// Galerkin values of levels 1..L-1 and the coarsest dense factor, for the
-// FP64 (T = double) or the FP32 (T = float; level 0 rounded from FP64 first)
-// hierarchy.
+// Galerkin values of levels 1..L-1 for the FP64 (T = double) or the FP32
+// (T = float; level 0 rounded from FP64 first) hierarchy.
 template <typename T>
-void amg_setup_values(cudaStream_t s, const AmgHierarchy &H);
+void amg_setup_levels(cudaStream_t s, const AmgHierarchy &H);
+// Explicit inverse of the coarsest level's current values into `out`
+// (n x n FP64); reads only the coarsest level.
+template <typename T>
+void amg_coarsest_inverse(cudaStream_t s, const AmgHierarchy &H, double *out);
 // z = V-cycle(r0) on level 0; z goes to zp[i].x (the PCG interleaved buffer)
 // and r0 . z (FP64 sum) into the PCG state.  Kernels are no-ops once
 // st->done is set.

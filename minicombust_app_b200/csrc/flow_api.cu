@@ -119,6 +119,11 @@ struct mc_flow {
     BicgState<1> *h_b1 = nullptr;      // pinned
     double *h_scalars = nullptr;       // pinned
     cudaGraphExec_t g_pcg = nullptr, g_b3 = nullptr, g_b1 = nullptr, g_pcg_amg = nullptr;
+    // lagged coarsest inverse: formed on a side stream while the pass runs,
+    // used from the next pass on
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_levels = nullptr, ev_inverse = nullptr;
+    bool inverse_ready = false, inverse_pending = false, inverse_deferred = false;
     // device-side loops (conditional WHILE graphs) of the same solves
     cudaGraphExec_t l_pcg = nullptr, l_b3 = nullptr, l_b1 = nullptr, l_pcg_amg = nullptr;
     cudaGraphExec_t l_pcg_amg32 = nullptr, l_b3_32 = nullptr, l_b1_32 = nullptr;
@@ -450,6 +455,8 @@ int after_pressure_solve(mc_flow *h)
     return MC_OK;
 }
 
+int launch_deferred_inverse(mc_flow *h);
+
 int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, double *bnorm)
 {
     const Ell A = pressure_matrix(h);
@@ -458,6 +465,7 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
     launch(h, K_PCG_MEAN, [&] { pcg_mean(h->stream, A, v); });
     const int use_x0 = select_guess(h, A, v.b, v.st, v.x);
     h->guess_used = use_x0 != 0;
+    if (const int rl = launch_deferred_inverse(h)) return rl;
     if (amg) {
         launch(h, K_PCG_INIT_AMG,
                [&] { pcg_init_amg(h->stream, A, v, h->prm.p_rtol, abs_floor, h->prm.max_iters, 1, use_x0); });
@@ -526,6 +534,7 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
     launch(h, K_PCG_MEAN, [&] { pcg_mean(h->stream, A, o); });
     const int use_x0 = select_guess(h, A, o.b, o.st, o.x);
     h->guess_used = use_x0 != 0;
+    if (const int rl = launch_deferred_inverse(h)) return rl;
     launch(h, K_IR, [&] {
         ir_init(h->stream, A, o.b, o.x, o.r, h->r32, o.st, o.partials, o.counter, h->prm.p_rtol, abs_floor, kMaxOuter,
                 use_x0);
@@ -773,6 +782,73 @@ int stage_set_up_field(mc_flow *h)
     return check_launch(h);
 }
 
+// MC_AMG_LAGGED_INVERSE=0 forms the coarsest inverse on the critical path
+// every pass.
+bool lagged_inverse_enabled()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = std::getenv("MC_AMG_LAGGED_INVERSE");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
+// AMG values for a new pressure matrix.  The coarse levels follow the matrix
+// at once; the explicit inverse on the coarsest level (one block, about a
+// quarter of a millisecond) is formed on a side stream from this pass's
+// coarsest values and used from the next pass on, so the V-cycles of a pass
+// use the inverse of the previous pass's coarsest matrix (the first pass
+// forms its own in line).  The V-cycle stays one fixed symmetric operator
+// within a solve.  The side launch is deferred until after the initial
+// guess (launch_deferred_inverse): its block must not hold an SM while the
+// network's persistent layer kernel wants every SM.
+int setup_amg_values(mc_flow *h)
+{
+    AmgHierarchy &H = h->amg;
+    const int nc = H.lv[H.levels - 1].n;
+    if (h->inverse_pending) {  // the next-pass inverse formed during the previous pass
+        CUDA_TRY(h, cudaStreamWaitEvent(h->stream, h->ev_inverse, 0));
+        CUDA_TRY(h, cudaMemcpyAsync(H.dense, H.dense_next, (size_t)nc * nc * sizeof(double), cudaMemcpyDeviceToDevice,
+                                    h->stream));
+        h->inverse_pending = false;
+    }
+    if (h->refined)
+        amg_setup_levels<float>(h->stream, H);
+    else
+        amg_setup_levels<double>(h->stream, H);
+    h->launches += h->refined ? H.levels - 1 : H.levels - 2;  // with the one the caller's launch() counts
+    if (h->inverse_ready && h->side && lagged_inverse_enabled()) {
+        h->inverse_deferred = true;
+        return MC_OK;
+    }
+    if (h->refined)
+        amg_coarsest_inverse<float>(h->stream, H, H.dense);
+    else
+        amg_coarsest_inverse<double>(h->stream, H, H.dense);
+    h->launches += 1;
+    h->inverse_ready = true;
+    return MC_OK;
+}
+
+// The deferred coarsest inverse of this pass, on the side stream.
+int launch_deferred_inverse(mc_flow *h)
+{
+    if (!h->inverse_deferred) return MC_OK;
+    h->inverse_deferred = false;
+    AmgHierarchy &H = h->amg;
+    CUDA_TRY(h, cudaEventRecord(h->ev_levels, h->stream));
+    CUDA_TRY(h, cudaStreamWaitEvent(h->side, h->ev_levels, 0));
+    if (h->refined)
+        amg_coarsest_inverse<float>(h->side, H, H.dense_next);
+    else
+        amg_coarsest_inverse<double>(h->side, H, H.dense_next);
+    CUDA_TRY(h, cudaEventRecord(h->ev_inverse, h->side));
+    h->launches += 1;
+    h->inverse_pending = true;
+    return MC_OK;
+}
+
 int stage_momentum(mc_flow *h, mc_iter_stats *st)
 {
     MomentumArgs a{};
@@ -828,13 +904,9 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
             k_pressure_rows<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a);
         });
         if (h->use_amg) {
-            launch(h, K_AMG_SETUP, [&] {
-                if (h->refined)
-                    amg_setup_values<float>(h->stream, h->amg);
-                else
-                    amg_setup_values<double>(h->stream, h->amg);
-            });
-            h->launches += h->amg.levels - 1;
+            int rs = MC_OK;
+            launch(h, K_AMG_SETUP, [&] { rs = setup_amg_values(h); });
+            if (rs) return rs;
         }
     }
     int rc = check_launch(h);
@@ -1285,6 +1357,7 @@ int build_amg(mc_flow *h, const HostMesh &hm)
     }
     const int nc = lv[L - 1].n;
     add(&H.dense, (size_t)nc * nc * 8);
+    add(&H.dense_next, (size_t)nc * nc * 8);
     const bool fp32 = h->prm.precision == MC_PRECISION_FP32_REFINED;
     PcgState *inner_state = nullptr;
     if (fp32) {
@@ -1459,6 +1532,9 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
         }
         cudaError_t e = cudaSetDevice(params->device);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_levels, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_inverse, cudaEventDisableTiming);
         if (e != cudaSuccess) {
             mc_flow_destroy(h);
             return MC_ERR_CUDA;
@@ -1586,7 +1662,11 @@ int mc_flow_destroy(mc_flow *h)
     if (h->bir_mem) cudaFree(h->bir_mem);
     for (void *p : {(void *)h->h_bi3, (void *)h->h_bi1, (void *)h->h_bo3, (void *)h->h_bo1})
         if (p) cudaFreeHost(p);
+    if (h->side) cudaStreamSynchronize(h->side);  // no inverse still being formed into freed memory
     if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->ev_levels) cudaEventDestroy(h->ev_levels);
+    if (h->ev_inverse) cudaEventDestroy(h->ev_inverse);
     delete h;
     return MC_OK;
 }
