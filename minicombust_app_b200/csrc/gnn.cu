@@ -666,40 +666,51 @@ __global__ void __launch_bounds__(GNN_TILE) k_gnn_decode(GnnGraph g, const float
 {
     __shared__ __align__(16) bf16 sH[GNN_TILE * LDH];
     __shared__ __align__(16) bf16 sW[GNN_H * LDH];
+    __shared__ float sCD[GNN_H], sWO[GNN_H];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int n = g.n, base = blockIdx.x * GNN_TILE;
+    const int n = g.n, ntiles = (n + GNN_TILE - 1) / GNN_TILE;
     for (int e = tid; e < GNN_H * GNN_H; e += GNN_TILE) sW[(e >> 5) * LDH + (e & 31)] = pkd[e];
-    load_tile(sH, hin, base, n);
-    __syncthreads();
-    const int gq = lane >> 2, tq = lane & 3;
-    float acc[2][4][4];
-    zero(acc);
-    warp_gemm<2, 4, 2>(acc, sH + warp * 32 * LDH, LDH, sW, LDH, lane);
+    if (tid < GNN_H) {
+        sCD[tid] = pd[GPD_CD + tid];
+        sWO[tid] = pd[GPD_WO + tid];
+    }
+    const float co = pd[GPD_CO];
     const double sx = scp->sx;
+    const bool zeroed = *status != 0;
+    const int gq = lane >> 2, tq = lane & 3;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {  // the block's tiles share its weights
+        const int base = tile * GNN_TILE;
+        __syncthreads();  // the previous tile's reads of sH are done
+        load_tile(sH, hin, base, n);
+        __syncthreads();
+        float acc[2][4][4];
+        zero(acc);
+        warp_gemm<2, 4, 2>(acc, sH + warp * 32 * LDH, LDH, sW, LDH, lane);
 #pragma unroll
-    for (int mt = 0; mt < 2; mt++)
+        for (int mt = 0; mt < 2; mt++)
 #pragma unroll
-        for (int hf = 0; hf < 2; hf++) {
-            const int row = warp * 32 + mt * 16 + gq + 8 * hf, i = base + row;
-            float s = 0.f;
+            for (int hf = 0; hf < 2; hf++) {
+                const int row = warp * 32 + mt * 16 + gq + 8 * hf, i = base + row;
+                float s = 0.f;
 #pragma unroll
-            for (int nt = 0; nt < 4; nt++) {
-                const int col = nt * 8 + 2 * tq;
-                const float q0 = fmaxf(acc[mt][nt][2 * hf] + pd[GPD_CD + col], 0.f);
-                const float q1 = fmaxf(acc[mt][nt][2 * hf + 1] + pd[GPD_CD + col + 1], 0.f);
-                const bf162 qv = __floats2bfloat162_rn(q0, q1);
-                const float2 qr = __bfloat1622float2(qv);
-                s += pd[GPD_WO + col] * qr.x + pd[GPD_WO + col + 1] * qr.y;
-                if (TRAIN && i < n) *reinterpret_cast<bf162 *>(qsave + (size_t)i * GNN_H + col) = qv;
+                for (int nt = 0; nt < 4; nt++) {
+                    const int col = nt * 8 + 2 * tq;
+                    const float q0 = fmaxf(acc[mt][nt][2 * hf] + sCD[col], 0.f);
+                    const float q1 = fmaxf(acc[mt][nt][2 * hf + 1] + sCD[col + 1], 0.f);
+                    const bf162 qv = __floats2bfloat162_rn(q0, q1);
+                    const float2 qr = __bfloat1622float2(qv);
+                    s += sWO[col] * qr.x + sWO[col + 1] * qr.y;
+                    if (TRAIN && i < n) *reinterpret_cast<bf162 *>(qsave + (size_t)i * GNN_H + col) = qv;
+                }
+                s += __shfl_xor_sync(FULL, s, 1);
+                s += __shfl_xor_sync(FULL, s, 2);
+                if (tq == 0 && i < n) {
+                    const float yi = zeroed ? 0.f : s + co;
+                    y[i] = yi;
+                    if (x0) x0[i] = sx * (double)yi;
+                }
             }
-            s += __shfl_xor_sync(FULL, s, 1);
-            s += __shfl_xor_sync(FULL, s, 2);
-            if (tq == 0 && i < n) {
-                const float yi = *status ? 0.f : s + pd[GPD_CO];
-                y[i] = yi;
-                if (x0) x0[i] = sx * (double)yi;
-            }
-        }
+    }
 }
 
 // ---------------------------------------------------------------- training
@@ -1208,10 +1219,11 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
             k_gnn_layer<false><<<nb, LAYER_THREADS, LAYER_SMEM, s>>>(g, pl, pkl, w.h[l & 1], w.h[(l + 1) & 1], nullptr);
     }
     const bf16 *hl = train ? w.h[GNN_L] : w.h[GNN_L & 1];
+    const int gd = std::min(nb, 16 * sm_count());  // the decoder loops over tiles
     if (train)
-        k_gnn_decode<true><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, w.q, w.status);
+        k_gnn_decode<true><<<gd, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, w.q, w.status);
     else
-        k_gnn_decode<false><<<nb, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, nullptr,
+        k_gnn_decode<false><<<gd, GNN_TILE, 0, s>>>(g, p + GP_DEC, pk + GK_WD, hl, w.scales, w.y, x0, nullptr,
                                                     w.status);
 }
 

@@ -310,6 +310,36 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter2_amg(EllT<T> A, PcgVec
 // residual r = b' - A x with b' = b - mean(b), FP64 norms; each inner FP32
 // solve gets r rounded to FP32 as its right-hand side.
 
+// (A x)_i of the FP64 system.
+__device__ __forceinline__ double ell_row(const Ell &A, const double *__restrict__ x, int i)
+{
+    return with_row_cols(A.dc, A.col, A.N, i, [&](const int(&c)[6]) {
+        double ax = A.diag[i] * x[i];
+#pragma unroll
+        for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * A.N + i] * x[c[k]];
+        return ax;
+    });
+}
+
+// (A xa)_i and (A xb)_i in one pass over the row (a null vector gives 0).
+struct RowPair {
+    double u, w;
+};
+__device__ __forceinline__ RowPair ell_row2(const Ell &A, const double *__restrict__ xa, const double *__restrict__ xb,
+                                            int i)
+{
+    return with_row_cols(A.dc, A.col, A.N, i, [&](const int(&c)[6]) {
+        RowPair o{xa ? A.diag[i] * xa[i] : 0.0, xb ? A.diag[i] * xb[i] : 0.0};
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const double a = A.off[(size_t)k * A.N + i];
+            if (xa) o.u += a * xa[c[k]];
+            if (xb) o.w += a * xb[c[k]];
+        }
+        return o;
+    });
+}
+
 __global__ void __launch_bounds__(MCB_THREADS) k_ir_init(Ell A, const double *__restrict__ b, double *__restrict__ x,
                                                          double *__restrict__ r, float *__restrict__ r32, PcgState *st,
                                                          double *partials, unsigned int *counter, double rtol,
@@ -323,12 +353,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_ir_init(Ell A, const double *__
         const double bi = b[i] - mean;
         double ri = bi;
         if (use_x0) {
-            double ax = A.diag[i] * x[i];
-            int c_[6];
-            row_cols(A, i, c_);
-#pragma unroll
-            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * x[c_[k]];
-            ri = bi - ax;
+            ri = bi - ell_row(A, x, i);
         } else {
             x[i] = 0.0;
         }
@@ -357,15 +382,6 @@ __global__ void __launch_bounds__(MCB_THREADS) k_ir_init(Ell A, const double *__
     }
 }
 
-__device__ __forceinline__ double ell_row(const Ell &A, const double *__restrict__ x, int i)
-{
-    double ax = A.diag[i] * x[i];
-    int c_[6];
-    row_cols(A, i, c_);
-#pragma unroll
-    for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * A.N + i] * x[c_[k]];
-    return ax;
-}
 
 // Dot products of b' = b - mean, u = A xa and w = A xb; the last block
 // solves the 2 x 2 least-squares problem min ||b' - alpha u - beta w||
@@ -383,8 +399,8 @@ __global__ void __launch_bounds__(MCB_THREADS) k_guess_residuals(Ell A, const do
     double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const double bi = b[i] - mean;
-        const double u = xa ? ell_row(A, xa, i) : 0.0;
-        const double w = xb ? ell_row(A, xb, i) : 0.0;
+        const RowPair uw = ell_row2(A, xa, xb, i);
+        const double u = uw.u, w = uw.w;
         acc[0] += bi * bi;
         acc[1] += bi * u;
         acc[2] += bi * w;
