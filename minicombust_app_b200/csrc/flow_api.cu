@@ -544,10 +544,29 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
     const int per_iter = 2 + amg_kernels_per_vcycle(h->amg, true);
     const long max_batches = h->prm.max_iters / PCG_AMG_BATCH + 2;
     int inner_total = 0, worst = MC_OK;
+    // A device-looped inner solve is followed at once by the outer update;
+    // its state is read together with the next outer check (one
+    // synchronisation per outer iteration).
+    bool inner_pending = false;
+    auto account_inner = [&](bool looped) -> int {
+        if (looped) {
+            if (!h->h_pcg_inner->done) return fail(h, MC_ERR_CUDA, "inner solve loop ended before convergence");
+            h->launches += loop_launches(h->h_pcg_inner->iter, per_iter);
+        }
+        inner_total += h->h_pcg_inner->iter;
+        if (h->h_pcg_inner->status == KRYLOV_NONFINITE) return fail(h, MC_ERR_NONFINITE, "inner FP32 solve");
+        return MC_OK;
+    };
     for (int outer = 0;; outer++) {
         CUDA_TRY(h, cudaMemcpyAsync(h->h_pcg, o.st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
+        if (inner_pending)
+            CUDA_TRY(h, cudaMemcpyAsync(h->h_pcg_inner, in.st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
         flush_timing(h);
+        if (inner_pending) {
+            inner_pending = false;
+            if ((rc = account_inner(true))) return rc;
+        }
         if (h->h_pcg->done) break;
         if (outer > kMaxOuter) return fail(h, MC_ERR_NOT_CONVERGED, "refinement state did not advance");
         // each inner solve asks for the reduction still missing (with a
@@ -573,21 +592,21 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
                 h->launches += amg_kernels_per_vcycle(h->amg, true) - 1;
             }
         };
-        const bool looped =
-            use_loops(h) && run_loop(h, &h->l_pcg_amg32, &in.st->done, [&] { iterations(LOOP_ITERS); });
-        for (long batch = 0;; batch++) {
-            CUDA_TRY(h, cudaMemcpyAsync(h->h_pcg_inner, in.st, sizeof(PcgState), cudaMemcpyDeviceToHost, h->stream));
-            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-            flush_timing(h);
-            if (h->h_pcg_inner->done) break;
-            if (looped) return fail(h, MC_ERR_CUDA, "inner solve loop ended before convergence");
-            if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "inner solve state did not advance");
-            rc = run_batch(h, &h->g_pcg_amg32, PCG_AMG_BATCH * per_iter, [&] { iterations(PCG_AMG_BATCH); });
-            if (rc) return rc;
+        if (use_loops(h) && run_loop(h, &h->l_pcg_amg32, &in.st->done, [&] { iterations(LOOP_ITERS); })) {
+            inner_pending = true;
+        } else {
+            for (long batch = 0;; batch++) {
+                CUDA_TRY(h, cudaMemcpyAsync(h->h_pcg_inner, in.st, sizeof(PcgState), cudaMemcpyDeviceToHost,
+                                            h->stream));
+                CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+                flush_timing(h);
+                if (h->h_pcg_inner->done) break;
+                if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "inner solve state did not advance");
+                rc = run_batch(h, &h->g_pcg_amg32, PCG_AMG_BATCH * per_iter, [&] { iterations(PCG_AMG_BATCH); });
+                if (rc) return rc;
+            }
+            if ((rc = account_inner(false))) return rc;
         }
-        if (looped) h->launches += loop_launches(h->h_pcg_inner->iter, per_iter);
-        inner_total += h->h_pcg_inner->iter;
-        if (h->h_pcg_inner->status == KRYLOV_NONFINITE) return fail(h, MC_ERR_NONFINITE, "inner FP32 solve");
         launch(h, K_IR, [&] { ir_add(h->stream, h->N, o.x, in.x, o.st); });
         launch(h, K_IR, [&] { ir_residual(h->stream, A, o.b, o.x, o.r, h->r32, o.st, o.partials, o.counter); });
         rc = check_launch(h);
@@ -657,10 +676,30 @@ int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const B
     if (rc) return rc;
     for (int j = 0; j < R; j++) iters_out[j] = 0;
     const long max_batches = h->prm.max_iters / BICG_BATCH + 2;
+    // as in the refined pressure solve: a device-looped inner solve's state
+    // is read together with the next outer check
+    bool inner_pending = false;
+    auto account_inner = [&](bool looped) -> int {
+        if (looped) {
+            if (!hin->all_done) return fail(h, MC_ERR_CUDA, "BiCGStab loop ended before convergence");
+            h->launches += loop_launches(*std::max_element(hin->iter, hin->iter + R), BICG_KERNELS_PER_ITER);
+        }
+        for (int j = 0; j < R; j++) {
+            iters_out[j] += hin->iter[j];
+            if (hin->status[j] == KRYLOV_NONFINITE) return fail(h, MC_ERR_NONFINITE, "inner FP32 BiCGStab");
+        }
+        return MC_OK;
+    };
     for (int outer = 0;; outer++) {
         CUDA_TRY(h, cudaMemcpyAsync(hout, out.st, sizeof(BirState<R>), cudaMemcpyDeviceToHost, h->stream));
+        if (inner_pending)
+            CUDA_TRY(h, cudaMemcpyAsync(hin, in.st, sizeof(BicgState<R>), cudaMemcpyDeviceToHost, h->stream));
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
         flush_timing(h);
+        if (inner_pending) {
+            inner_pending = false;
+            if ((rc = account_inner(true))) return rc;
+        }
         if (hout->all_done) break;
         if (outer > kMaxOuter) return fail(h, MC_ERR_NOT_CONVERGED, "refinement state did not advance");
         double inner_rtol = 0.5;
@@ -677,21 +716,19 @@ int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const B
                 launch(h, kid1_32 + 2, [&] { bicg_3_t<float, R>(h->stream, A32, in, pin ^ 1); });
             }
         };
-        const bool looped = use_loops(h) && run_loop(h, loop, &in.st->all_done, [&] { iterations(LOOP_ITERS); });
-        for (long batch = 0;; batch++) {
-            CUDA_TRY(h, cudaMemcpyAsync(hin, in.st, sizeof(BicgState<R>), cudaMemcpyDeviceToHost, h->stream));
-            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-            flush_timing(h);
-            if (hin->all_done) break;
-            if (looped) return fail(h, MC_ERR_CUDA, "BiCGStab loop ended before convergence");
-            if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "BiCGStab state did not advance");
-            rc = run_batch(h, exec, BICG_BATCH * BICG_KERNELS_PER_ITER, [&] { iterations(BICG_BATCH); });
-            if (rc) return rc;
-        }
-        if (looped) h->launches += loop_launches(*std::max_element(hin->iter, hin->iter + R), BICG_KERNELS_PER_ITER);
-        for (int j = 0; j < R; j++) {
-            iters_out[j] += hin->iter[j];
-            if (hin->status[j] == KRYLOV_NONFINITE) return fail(h, MC_ERR_NONFINITE, "inner FP32 BiCGStab");
+        if (use_loops(h) && run_loop(h, loop, &in.st->all_done, [&] { iterations(LOOP_ITERS); })) {
+            inner_pending = true;
+        } else {
+            for (long batch = 0;; batch++) {
+                CUDA_TRY(h, cudaMemcpyAsync(hin, in.st, sizeof(BicgState<R>), cudaMemcpyDeviceToHost, h->stream));
+                CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+                flush_timing(h);
+                if (hin->all_done) break;
+                if (batch > max_batches) return fail(h, MC_ERR_NOT_CONVERGED, "BiCGStab state did not advance");
+                rc = run_batch(h, exec, BICG_BATCH * BICG_KERNELS_PER_ITER, [&] { iterations(BICG_BATCH); });
+                if (rc) return rc;
+            }
+            if ((rc = account_inner(false))) return rc;
         }
         launch(h, K_BIR, [&] { bir_add<R>(h->stream, A.N, out); });
         launch(h, K_BIR, [&] { bir_residual<R>(h->stream, A, out); });
