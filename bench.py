@@ -151,6 +151,15 @@ def kernel_bytes(name, N, F, nnz_off):
         "bicg3_32_2_spmv": 76 * N,     # FP32: matrix 28 + 3 x 16
         "bicg3_32_3_update": 84 * N,
         "gnn_forward": 708 * N,        # inputs 24 + vhat 4, h0 out 64, 4 layers x (h in 64 + h out 64 + mask 1), decode 64 in + y, x0 out 12
+        # one V-cycle, per fine row.  FP32 (matrix by direction), level 0: first
+        # two sweeps 36, sweep 40, restriction 40, prolongation + sweep 44,
+        # sweep 40, last sweep with r.z 40 = 240; level 1 (1/8 of the rows,
+        # column lists, about 384 bytes per row) 48; level 2 and below 6
+        "amg32_vcycle": 294 * N,
+        # FP64 (direction codes), level 0: first sweep 24, sweeps 4 x 84,
+        # restriction 81, prolongation 21, last sweep 84 = 546; level 1 84;
+        # level 2 and below 11
+        "amg_vcycle": 641 * N,
         "lsq_gradients_uvwpt": 208 * N,
         "momentum_assemble": 56 * F + 296 * N,
         "mass_flux": 88 * F + 176 * N,
