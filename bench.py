@@ -172,7 +172,8 @@ def kernel_bytes(name, N, F, nnz_off):
 # 2 x 96^3 case (a full capture of the 2 x 128^3 case is too large); scaled by
 # rows to the bench size for the roofline's `traffic`.
 NCU_DRAM_BYTES_PER_ROW = {
-    "pcg_iter1_spmv": 101.7, "pcg32_iter1_spmv": 43.0, "bicg3_1_spmv": 211.9, "bicg3_32_1_spmv": 102.5,
+    "pcg_iter1_spmv": 101.7, "pcg32_iter1_spmv": 38.9, "bicg3_1_spmv": 211.9, "bicg3_32_1_spmv": 98.5,
+    "amg32_vcycle": 275.4,  # the 25 kernels of one V-cycle, summed
 }
 
 
