@@ -94,11 +94,60 @@ int amg_build_host(int N, const std::vector<int> &col0, const std::vector<int> &
             std::sort(cs.begin(), cs.end());
             kmax = std::max(kmax, (int)cs.size());
         }
-        nxt.k = std::max(kmax, 1);
+        // Direction order: when every coarse neighbour of every aggregate is
+        // its directional neighbour at a fixed offset per direction (six
+        // distinct offsets), slot s is the direction with the s-th smallest
+        // offset, so the kernels compute columns instead of reading them.
+        int dir_off[6];
+        bool dia = nagg > 1;
+        for (int d = 0; d < 6 && dia; d++) {
+            bool seen = false;
+            for (int A = 0; A < nagg && dia; A++) {
+                const int J = dnc[(size_t)d * nagg + A];
+                if (J < 0) continue;
+                if (!seen) dir_off[d] = J - A, seen = true;
+                else if (J - A != dir_off[d]) dia = false;
+            }
+            dia = dia && seen && dir_off[d] != 0;
+        }
+        int slot_dir[6] = {0, 1, 2, 3, 4, 5};
+        if (dia) {
+            std::sort(slot_dir, slot_dir + 6, [&](int a, int b) { return dir_off[a] < dir_off[b]; });
+            for (int s = 0; s + 1 < 6 && dia; s++) dia = dir_off[slot_dir[s]] != dir_off[slot_dir[s + 1]];
+        }
+        for (int A = 0; A < nagg && dia; A++) {
+            int present = 0;
+            for (int d = 0; d < 6; d++) present += dnc[(size_t)d * nagg + A] >= 0;
+            dia = present == (int)cols[A].size();
+            for (int J : cols[A]) {
+                bool found = false;
+                for (int d = 0; d < 6; d++) found = found || dnc[(size_t)d * nagg + A] == J;
+                dia = dia && found;
+            }
+        }
+        nxt.k = dia ? 6 : std::max(kmax, 1);
         const int kc = nxt.k;
         nxt.col.assign((size_t)kc * nagg, 0);
-        for (int A = 0; A < nagg; A++)
-            for (int s = 0; s < kc; s++) nxt.col[(size_t)s * nagg + A] = s < (int)cols[A].size() ? cols[A][s] : A;
+        if (dia) {
+            nxt.dia = 1;
+            for (int s = 0; s < 6; s++) nxt.doff[s] = dir_off[slot_dir[s]];
+            for (int A = 0; A < nagg; A++)
+                for (int s = 0; s < 6; s++) {
+                    const int J = dnc[(size_t)slot_dir[s] * nagg + A];
+                    nxt.col[(size_t)s * nagg + A] = J >= 0 ? J : A;
+                }
+        } else {
+            for (int A = 0; A < nagg; A++)
+                for (int s = 0; s < kc; s++) nxt.col[(size_t)s * nagg + A] = s < (int)cols[A].size() ? cols[A][s] : A;
+        }
+        auto slot_in = [&](int A, int J) {
+            if (dia) {
+                for (int s = 0; s < 6; s++)
+                    if (nxt.col[(size_t)s * nagg + A] == J) return 1 + s;
+                return 0;  // not reached: every coarse column is a directional neighbour
+            }
+            return 1 + (int)(std::lower_bound(cols[A].begin(), cols[A].end(), J) - cols[A].begin());
+        };
         std::vector<int> count((size_t)nagg * (kc + 1) + 1, 0);
         struct Contrib { int entry, id; };
         std::vector<Contrib> contrib;
@@ -112,7 +161,7 @@ int amg_build_host(int N, const std::vector<int> &col0, const std::vector<int> &
                     if (j == i) continue;
                     const int J = agg[j];
                     int slot = 0;
-                    if (J != A) slot = 1 + (int)(std::lower_bound(cols[A].begin(), cols[A].end(), J) - cols[A].begin());
+                    if (J != A) slot = slot_in(A, J);
                     contrib.push_back({A * (kc + 1) + slot, n + s * n + i});
                 }
             }
@@ -142,7 +191,7 @@ template <typename T, typename V>
 __device__ __forceinline__ T row_apply_v(const AmgLevelT<T> &L, int i, V &&v)
 {
     const T s0 = L.diag[i] * v(i);
-    if (L.dc.code) {
+    if (L.dc.code || L.dc.dia) {
         return with_row_cols(L.dc, L.col, L.n, i, [&](const int(&c)[6]) {
             T s = s0;
 #pragma unroll

@@ -85,6 +85,12 @@ struct AmgHostLevel {
     std::vector<int> col;               // [k][n]
     std::vector<int> agg, mptr, mlist;  // restriction to the next level
     std::vector<int> gptr, gidx;        // Galerkin lists for this level (levels >= 1)
+    // Levels >= 1 whose rows all reach their neighbours through six fixed
+    // offsets (the coarse levels of a structured box): slot s holds the
+    // neighbour at row + doff[s] (offsets ascending, the same order as sorted
+    // columns), with value 0 and column = row where the row has none.
+    int dia = 0;
+    int doff[6] = {0, 0, 0, 0, 0, 0};
 };
 
 int amg_build_host(int N, const std::vector<int> &col0, const std::vector<int> &dn0, std::vector<AmgHostLevel> &out,

@@ -1440,6 +1440,11 @@ int build_amg(mc_flow *h, const HostMesh &hm)
             d.col = d_col[l];
             d.gptr = d_gptr[l];
             d.gidx = d_gidx[l];
+            d.dc = DirCodes{};
+            if (lv[l].dia) {  // values in direction order: the kernels compute the columns
+                d.dc.dia = 1;
+                for (int q = 0; q < 6; q++) d.dc.doff[q] = lv[l].doff[q];
+            }
         }
         if (l + 1 < L) {
             int rc = put(d_agg[l], lv[l].agg);
