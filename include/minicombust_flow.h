@@ -108,10 +108,12 @@ typedef struct mc_flow_params {
     int amg_sweeps;           /* MC_PSOLVER_PCG_AMG: damped-Jacobi sweeps before and after the coarse correction */
     double amg_omega;         /* Jacobi damping */
     double amg_alpha;         /* coarse-correction scaling */
-    double ir_inner_rtol;     /* MC_PRECISION_FP32_REFINED: each inner FP32 solve reduces its residual by
-                                 the factor still missing to p_rtol (with a margin of 2), but by no less
-                                 than this: the smallest relative tolerance asked of an FP32 solve */
+    double ir_inner_rtol;     /* MC_PRECISION_FP32_REFINED: each inner FP32 pressure solve reduces its
+                                 residual by the factor still missing to p_rtol (with a margin of 2), but
+                                 by no less than this: the smallest relative tolerance asked of it */
     int reorder;              /* MC_REORDER_* */
+    double ir_inner_rtol_bicg; /* the same floor for the inner FP32 BiCGStab solves of momentum and
+                                  temperature (their target is u_rtol) */
 } mc_flow_params;
 
 /* Per-pass statistics. */

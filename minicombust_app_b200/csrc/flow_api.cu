@@ -663,7 +663,7 @@ int solve_bicg(mc_flow *h, const Ell &A, const BicgVectors<R> &v, BicgState<R> *
 
 // FP64 iterative refinement around FP32 BiCGStab solves (momentum, R = 3;
 // temperature, R = 1): each inner solve asks for the reduction still missing
-// (margin 2, floor ir_inner_rtol); the outer loop stops on the FP64 true
+// (margin 2, floor ir_inner_rtol_bicg); the outer loop stops on the FP64 true
 // residual, ||b - A x|| <= u_rtol ||b|| per system.
 template <int R>
 int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const BicgVectorsT<float, R> &in,
@@ -706,7 +706,7 @@ int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const B
         for (int j = 0; j < R; j++)
             if (!hout->done[j] && hout->rr[j] > 0)
                 inner_rtol = std::min(inner_rtol, 0.5 * std::sqrt(hout->tol2[j] / hout->rr[j]));
-        inner_rtol = std::max(inner_rtol, h->prm.ir_inner_rtol);
+        inner_rtol = std::max(inner_rtol, h->prm.ir_inner_rtol_bicg);
         launch(h, kid_init32, [&] { bicg_init_t<float, R>(h->stream, A32, in, inner_rtol, h->prm.max_iters); });
         auto iterations = [&](int count) {
             for (int it = 0; it < count; it++) {
@@ -1506,7 +1506,8 @@ void mc_flow_default_params(mc_flow_params *p, int mode)
     p->amg_sweeps = 3;
     p->amg_omega = 0.6667;
     p->amg_alpha = 2.0;
-    p->ir_inner_rtol = 1e-4;
+    p->ir_inner_rtol = 1e-5;
+    p->ir_inner_rtol_bicg = 1e-4;
     p->reorder = MC_REORDER_NONE;
     if (mode == MC_MODE_COMPAT) {
         p->viscosity = 0.000014;
@@ -1538,7 +1539,8 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
         return MC_ERR_ARG;
     if (params->reorder != MC_REORDER_NONE && params->reorder != MC_REORDER_RCM) return MC_ERR_ARG;
     if (params->precision == MC_PRECISION_FP32_REFINED &&
-        (params->pressure_solver != MC_PSOLVER_PCG_AMG || !(params->ir_inner_rtol > 0) || params->ir_inner_rtol >= 1))
+        (params->pressure_solver != MC_PSOLVER_PCG_AMG || !(params->ir_inner_rtol > 0) || params->ir_inner_rtol >= 1 ||
+         !(params->ir_inner_rtol_bicg > 0) || params->ir_inner_rtol_bicg >= 1))
         return MC_ERR_UNSUPPORTED;
     if (params->pressure_solver == MC_PSOLVER_PCG_AMG &&
         (params->amg_sweeps < 1 || !(params->amg_omega > 0) || !(params->amg_alpha > 0)))
