@@ -16,16 +16,21 @@
 //
 // Warp roles (one persistent block per SM):
 //   warps 0-11  three epilogue groups of four warps; group g owns the tiles
-//               j = g, g + 3, ... of the block and their copy stage g (so
-//               each barrier's phases are consumed by one group, in order);
-//               thread r of a group is row r of the tile and TMEM lane r
-//               (warp w reads lanes 32 (w % 4) ..)
+//               j = g, g + 3, ... of the block, their copy stage g and
+//               their TMEM columns (so each barrier's phases are consumed in
+//               order); thread r of a group is row r of the tile and TMEM
+//               lane r (warp w reads lanes 32 (w % 4) ..)
 //   warp 12     TMA producer (one thread)
 //   warp 13     TMEM allocation and the MMA issue (one elected thread)
+//   warps 14-17 masking: thread r zeroes the missing-direction rows of row r
+//               of each tile as soon as its copies land
 // The MMA thread issues whichever product is ready -- the first product of
-// a tile once its slices are masked, the second once its group has written
-// the a-tile -- so the copies, the tensor core and three tiles' epilogues
-// overlap.  Every wait is bounded: on
+// a tile once its slices are masked and its group has read the previous
+// first product out of TMEM, the second once the group has written the
+// a-tile.  A stage is refilled as soon as its first product completes, so
+// the copies run ahead of the epilogues instead of waiting for them, and
+// the copies, the tensor core and three tiles' epilogues overlap.  Every
+// wait is bounded: on
 // a time-out the block records a status, drains its copies and MMAs, frees
 // its TMEM and returns, and the decoder then writes a zero prediction.
 #include <cuda.h>
@@ -52,9 +57,9 @@ constexpr int UM_B1 = 7 * GNN_H * GNN_H * 2;        // 14336 B: 28 K-groups of 3
 constexpr int UM_B2 = GNN_H * GNN_H * 2;            // 2048 B
 constexpr int UM_A1 = GNN_TILE * GNN_H * 2;         // 8192 B per epilogue group
 constexpr int UM_GROUPS = 3;  // one copy stage per group
-constexpr int UM_THREADS = 128 * UM_GROUPS + 64;
+constexpr int UM_THREADS = 128 * UM_GROUPS + 64 + 128;
 constexpr uint32_t UM_TMEM_COLS = 256;  // >= 64 per group (D1 and D2, 32 columns each), a power of two
-constexpr int WARP_TMA = 4 * UM_GROUPS, WARP_MMA = 4 * UM_GROUPS + 1;
+constexpr int WARP_TMA = 4 * UM_GROUPS, WARP_MMA = 4 * UM_GROUPS + 1, WARP_MASK = 4 * UM_GROUPS + 2;
 
 constexpr int OFF_STAGE = 0;
 constexpr int OFF_B1 = OFF_STAGE + UM_STAGES * UM_STAGE;
@@ -62,8 +67,8 @@ constexpr int OFF_B2 = OFF_B1 + UM_B1;
 constexpr int OFF_A1 = OFF_B2 + UM_B2;
 constexpr int OFF_BIAS = OFF_A1 + UM_GROUPS * UM_A1;
 constexpr int OFF_BAR = OFF_BIAS + 2 * GNN_H * 4;
-// barriers: full[3], masked[3], empty[3], d1full[3], a1full[3], d2full[3], fin
-constexpr int NBAR = 3 * UM_STAGES + 3 * UM_GROUPS + 1;
+// barriers: full[3], masked[3], empty[3], d1full[3], a1full[3], d2full[3], d1free[3], fin
+constexpr int NBAR = 3 * UM_STAGES + 4 * UM_GROUPS + 1;
 constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
 constexpr int UM_SMEM_USED = OFF_MISC + 16;
 constexpr int UM_SMEM = UM_SMEM_USED + 1024;        // slack for the 1024-byte alignment of the base
@@ -103,7 +108,8 @@ struct UmmaBars {
     __device__ uint32_t d1full(int g) const { return base + 8 * (3 * UM_STAGES + g); }
     __device__ uint32_t a1full(int g) const { return base + 8 * (3 * UM_STAGES + UM_GROUPS + g); }
     __device__ uint32_t d2full(int g) const { return base + 8 * (3 * UM_STAGES + 2 * UM_GROUPS + g); }
-    __device__ uint32_t fin() const { return base + 8 * (3 * UM_STAGES + 3 * UM_GROUPS); }
+    __device__ uint32_t d1free(int g) const { return base + 8 * (3 * UM_STAGES + 3 * UM_GROUPS + g); }
+    __device__ uint32_t fin() const { return base + 8 * (3 * UM_STAGES + 4 * UM_GROUPS); }
 };
 
 __global__ void __launch_bounds__(UM_THREADS, 1)
@@ -132,6 +138,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
             mbar_init(bars.d1full(q), 1);
             mbar_init(bars.a1full(q), 128);
             mbar_init(bars.d2full(q), 1);
+            mbar_init(bars.d1free(q), 128);
         }
         mbar_init(bars.fin(), 1);
         *abort_flag = 0;
@@ -203,7 +210,8 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
             uint32_t idle = 0;
             while (j2 < nj) {
                 bool progressed = false;
-                if (j1 < nj && mbar_test_wait(bars.masked(j1 % UM_STAGES), (j1 / UM_STAGES) & 1)) {
+                if (j1 < nj && mbar_test_wait(bars.masked(j1 % UM_STAGES), (j1 / UM_STAGES) & 1) &&
+                    (j1 < UM_GROUPS || mbar_test_wait(bars.d1free(j1 % UM_GROUPS), ((j1 / UM_GROUPS) - 1) & 1))) {
                     tc_fence_after();
                     const int s = j1 % UM_STAGES, q = j1 % UM_GROUPS;
                     const uint32_t a0 = sbase + OFF_STAGE + s * UM_STAGE;
@@ -243,22 +251,15 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
             umma_commit(bars.fin());
             if (!mbar_wait(bars.fin(), 0, nullptr, WAIT_LIMIT)) fail(5);
         }
-    } else {
-        // ---------------------------------------------------------- epilogue
-        const int q = warp >> 2, r = tid & 127;  // group, row
-        const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
-        const uint32_t a1 = sbase + OFF_A1 + q * UM_A1 + r * 16;
-        for (int j = q;; j += UM_GROUPS) {
+    } else if (warp >= WARP_MASK) {
+        // ---------------------------------------------------------- masking
+        const int r = tid - 32 * WARP_MASK;  // row of the tile
+        for (int j = 0;; j++) {
             const int tile = blockIdx.x + j * gridDim.x;
             if (tile >= ntiles) break;
             const int s = j % UM_STAGES, i = tile * GNN_TILE + r;
-            const bool in = i < g.n;
-            const unsigned mk = in ? g.mask[i] : 0u;
-            uint4 hv[4];
-#pragma unroll
-            for (int c = 0; c < 4; c++)
-                hv[c] = in ? __ldg(reinterpret_cast<const uint4 *>(hin + (size_t)i * GNN_H) + c) : make_uint4(0, 0, 0, 0);
-            bool ok = mbar_wait(bars.full(s), (j / UM_STAGES) & 1, abort_flag, WAIT_LIMIT);
+            const unsigned mk = i < g.n ? g.mask[i] : 0u;
+            const bool ok = mbar_wait(bars.full(s), (j / UM_STAGES) & 1, abort_flag, WAIT_LIMIT);
             if (!__all_sync(FULL, ok)) {
                 fail(6);
                 break;
@@ -274,9 +275,25 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
                 }
             if (mk != 0x3fu) fence_proxy_async_smem();  // only a thread that wrote zeros has to order them
             mbar_arrive(bars.masked(s));
+        }
+    } else {
+        // ---------------------------------------------------------- epilogue
+        const int q = warp >> 2, r = tid & 127;  // group, row
+        const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+        const uint32_t a1 = sbase + OFF_A1 + q * UM_A1 + r * 16;
+        for (int j = q;; j += UM_GROUPS) {
+            const int tile = blockIdx.x + j * gridDim.x;
+            if (tile >= ntiles) break;
+            const int i = tile * GNN_TILE + r;
+            const bool in = i < g.n;
+            uint4 hv[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                hv[c] = in ? __ldg(reinterpret_cast<const uint4 *>(hin + (size_t)i * GNN_H) + c) : make_uint4(0, 0, 0, 0);
 
-            // a = relu(D1 + c1) into the group's K-major a-tile
-            ok = mbar_wait(bars.d1full(q), (j / UM_GROUPS) & 1, abort_flag, WAIT_LIMIT);
+            // a = relu(D1 + c1) into the group's K-major a-tile; D1 is
+            // released for the group's next tile as soon as it is read
+            bool ok = mbar_wait(bars.d1full(q), (j / UM_GROUPS) & 1, abort_flag, WAIT_LIMIT);
             if (!__all_sync(FULL, ok)) {
                 fail(7);
                 break;
@@ -284,6 +301,8 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
             tc_fence_after();
             uint32_t v[32];
             tmem_ld32(tmem + q * 64 + lane_base, v);
+            tc_fence_before();
+            mbar_arrive(bars.d1free(q));
 #pragma unroll
             for (int c = 0; c < 4; c++) {
                 uint32_t pk[4];
