@@ -1078,10 +1078,11 @@ void bicg_init_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, 
 {
     k_bicg_init<T, R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, max_iters);
 }
-// FP32 systems with several right-hand sides run the first product and the
-// update in the split form (one block range per right-hand side).
+// FP32 systems run the first product and the update in the split form (one
+// block range per right-hand side; with one right-hand side the split form
+// is the fused one with the register cap of full occupancy).
 template <typename T, int R>
-constexpr bool bicg_split() { return sizeof(T) == 4 && R > 1; }
+constexpr bool bicg_split() { return sizeof(T) == 4; }
 
 template <typename T, int R>
 void bicg_1_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int pin)
@@ -1091,11 +1092,13 @@ void bicg_1_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int
                v.p[pin ^ 1], v.v[pin ^ 1]);
 }
 // The second product gathers two vectors per right-hand side: one pass over
-// the matrix for all of them is faster than the split form here.
+// the matrix for all of them is faster than the split form here (which FP32
+// uses with one right-hand side, for its occupancy).
 template <typename T, int R>
 void bicg_2_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int vnew)
 {
-    pdl_launch(k_bicg_2<T, R, false>, krylov_grid(A.N), MCB_THREADS, 0, s, A, v, v.v[vnew]);
+    constexpr bool S = sizeof(T) == 4 && R == 1;
+    pdl_launch(k_bicg_2<T, R, S>, krylov_grid(A.N), MCB_THREADS, 0, s, A, v, v.v[vnew]);
 }
 template <typename T, int R>
 void bicg_3_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int pnew)
