@@ -358,8 +358,12 @@ __global__ void k_amg_smooth_first2(AmgLevelT<T> L, T omega, T *__restrict__ eou
 // Prolongation and the first post-smoothing sweep in one pass: the
 // corrected iterate e + alpha ec[agg] is evaluated at each row where the
 // sweep needs it and not stored.
+// The FP32 forms of this kernel, the restriction and the last sweep are held
+// to 32 registers (8 blocks of 256 per SM: full occupancy); 0 leaves the FP64
+// forms to the compiler.
 template <typename T>
-__global__ void k_amg_prolong_jacobi(AmgLevelT<T> L, T omega, T alpha, const T *__restrict__ ec,
+__global__ void __launch_bounds__(MCB_THREADS, sizeof(T) == 4 ? 8 : 0)
+    k_amg_prolong_jacobi(AmgLevelT<T> L, T omega, T alpha, const T *__restrict__ ec,
                                      const T *__restrict__ e, T *__restrict__ eout, const PcgState *st)
 {
     pdl_wait();
@@ -401,7 +405,8 @@ __device__ __forceinline__ void restrict_row8(const AmgLevelT<T> &fine, const Am
 }
 
 template <typename T>
-__global__ void k_amg_restrict(AmgLevelT<T> fine, AmgLevelT<T> coarse, const T *__restrict__ e, const PcgState *st)
+__global__ void __launch_bounds__(MCB_THREADS, sizeof(T) == 4 ? 8 : 0)
+    k_amg_restrict(AmgLevelT<T> fine, AmgLevelT<T> coarse, const T *__restrict__ e, const PcgState *st)
 {
     pdl_wait();
     if (st->done) return;
@@ -422,7 +427,7 @@ __global__ void k_amg_prolong(AmgLevelT<T> fine, T alpha, const T *__restrict__ 
 
 // Last post-smoothing sweep on level 0: z into zp[i].x and the PCG's r . z (FP64 sum).
 template <typename T>
-__global__ void __launch_bounds__(MCB_THREADS) k_amg_final(AmgLevelT<T> L, T omega, const T *__restrict__ ein,
+__global__ void __launch_bounds__(MCB_THREADS, sizeof(T) == 4 ? 8 : 0) k_amg_final(AmgLevelT<T> L, T omega, const T *__restrict__ ein,
                                                            typename Pair<T>::type *__restrict__ zp, PcgState *st,
                                                            double *partials, unsigned int *counter, int is_init)
 {
