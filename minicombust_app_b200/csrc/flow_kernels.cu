@@ -47,8 +47,10 @@ __device__ __forceinline__ int grid_stride_start() { return blockIdx.x * blockDi
 // Over slot f in cell_faces order: dX = x_nbr - x_c (equal to the reference's
 // mask * (x1 - x0)), boundary dX = x_face - x_c; dphi likewise, or 0 on
 // boundary faces for pressure-like fields.
+// The five-field form is held to 3 blocks of 256 per SM (80 registers, a few
+// spilled) instead of the 106 registers and 2 blocks it takes unbounded.
 template <int NF>
-__global__ void __launch_bounds__(MCB_THREADS) k_lsq_gradients(int N, const int *__restrict__ nbr,
+__global__ void __launch_bounds__(MCB_THREADS, NF > 1 ? 3 : 0) k_lsq_gradients(int N, const int *__restrict__ nbr,
                                                               const int *__restrict__ fc1, const double *__restrict__ xc,
                                                               const double *__restrict__ yc,
                                                               const double *__restrict__ zc,
