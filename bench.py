@@ -151,15 +151,15 @@ def kernel_bytes(name, N, F, nnz_off):
         "bicg3_32_2_spmv": 76 * N,     # FP32: matrix 28 + 3 x 16
         "bicg3_32_3_update": 84 * N,
         "gnn_forward": 708 * N,        # inputs 24 + vhat 4, h0 out 64, 4 layers x (h in 64 + h out 64 + mask 1), decode 64 in + y, x0 out 12
-        # one V-cycle, per fine row.  FP32 (matrix by direction), level 0: first
-        # two sweeps 36, sweep 40, restriction 40, prolongation + sweep 44,
-        # sweep 40, last sweep with r.z 40 = 240; level 1 (1/8 of the rows,
-        # column lists, about 384 bytes per row) 48; level 2 and below 6
-        "amg32_vcycle": 294 * N,
-        # FP64 (direction codes), level 0: first sweep 24, sweeps 4 x 84,
-        # restriction 81, prolongation 21, last sweep 84 = 546; level 1 84;
-        # level 2 and below 11
-        "amg_vcycle": 641 * N,
+        # one V-cycle, per fine row.  FP32 (every level's matrix by direction),
+        # level 0: first two sweeps 36, sweep 40, restriction 40, prolongation
+        # + sweep 44, sweep 40, last sweep with r.z 40 = 240; level 1 (1/8 of
+        # the rows, about 241 bytes per row) 30; level 2 and below 4
+        "amg32_vcycle": 274 * N,
+        # FP64 (level 0 direction codes, coarse levels by direction), level 0:
+        # first sweep 24, sweeps 4 x 84, restriction 81, prolongation 21, last
+        # sweep 84 = 546; level 1 66; level 2 and below 9
+        "amg_vcycle": 621 * N,
         "lsq_gradients_uvwpt": 208 * N,
         "momentum_assemble": 56 * F + 296 * N,
         "mass_flux": 88 * F + 176 * N,
@@ -173,7 +173,7 @@ def kernel_bytes(name, N, F, nnz_off):
 # rows to the bench size for the roofline's `traffic`.
 NCU_DRAM_BYTES_PER_ROW = {
     "pcg_iter1_spmv": 101.7, "pcg32_iter1_spmv": 38.9, "bicg3_1_spmv": 211.9, "bicg3_32_1_spmv": 98.5,
-    "amg32_vcycle": 275.4,  # the 25 kernels of one V-cycle, summed
+    "amg32_vcycle": 255.2,  # the 25 kernels of one V-cycle, summed
 }
 
 
@@ -301,6 +301,12 @@ def roofline_of(solver, mesh, N):
     solver.simple_iteration()
     solver.set_timing(False)
     kt = solver.kernel_times()
+    # An inner PCG solve of k iterations applies k V-cycles (the one of the
+    # initial residual and those of iterations 1 .. k-1); the host-polled
+    # batches of the timing pass also launch V-cycles that find the solve
+    # converged and return at once.  Their time stays in the total (so the
+    # average is an upper bound), the count is the V-cycles that did work.
+    working_vcycles = int(solver.last_stats.as_dict()["pressure_iters_total"])
     nnz_off = int(np.sum(mesh.face_cells[:, 1] < N)) * 2
     total = sum(v[0] for v in kt.values())
     ranked = sorted(((ms, name, cnt) for name, (ms, cnt) in kt.items() if cnt > 0), reverse=True)
@@ -310,6 +316,9 @@ def roofline_of(solver, mesh, N):
         b = kernel_bytes(name, N, mesh.n_faces, nnz_off)
         if b is None:
             continue
+        early = 0
+        if name in ("amg32_vcycle", "amg_vcycle") and 0 < working_vcycles <= cnt:
+            early, cnt = cnt - working_vcycles, working_vcycles
         avg_s = ms / cnt / 1e3
         achieved = b / avg_s / 1e9
         per_row = NCU_DRAM_BYTES_PER_ROW.get(name)
@@ -318,7 +327,8 @@ def roofline_of(solver, mesh, N):
                 "traffic": per_row * N if per_row else None,
                 "traffic_source": "ncu dram__bytes_read+write on 2x96^3, scaled by rows" if per_row else None,
                 "bytes_per_launch": b,
-                "avg_launch_us": avg_s * 1e6, "launches_per_step": cnt, "share_of_step": ms / total}
+                "avg_launch_us": avg_s * 1e6, "launches_per_step": cnt, "early_exit_launches": early,
+                "share_of_step": ms / total}
         break
     return roof, {k: round(v[0], 4) for k, v in kt.items() if v[1] > 0}
 
