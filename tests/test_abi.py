@@ -95,6 +95,21 @@ def test_bad_arguments_are_rejected_without_gpu():
     assert L.mc_flow_simple_iteration(None, None) == flow.MC_ERR_ARG
 
 
+def test_refinement_floors():
+    p = flow.default_params(flow.MODE_SIMPLE)
+    assert (p.ir_inner_rtol, p.ir_inner_rtol_bicg) == (1e-5, 1e-4)
+    L = flow.library()
+    h = ctypes.c_void_p()
+    mesh = flow.Mesh.box(2, 1, 1, 0.2, 0.1, 0.1)
+    mv = mesh.view()
+    for field, bad in (("ir_inner_rtol", 0.0), ("ir_inner_rtol", 1.0), ("ir_inner_rtol_bicg", 0.0),
+                       ("ir_inner_rtol_bicg", 2.0)):
+        q = flow.default_params(flow.MODE_SIMPLE, pressure_solver=flow.PSOLVER_PCG_AMG,
+                                precision=flow.PRECISION_FP32_REFINED)
+        setattr(q, field, bad)
+        assert L.mc_flow_create(ctypes.byref(mv), ctypes.byref(q), ctypes.byref(h)) == flow.MC_ERR_UNSUPPORTED, field
+
+
 def test_inconsistent_mesh_is_rejected():
     L = flow.library()
     mesh = flow.Mesh.box(3, 2, 2, 0.3, 0.2, 0.2)
