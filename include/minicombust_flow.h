@@ -106,7 +106,7 @@ typedef struct mc_flow_params {
     int initial_guess;        /* MC_GUESS_* for the first pressure correction of a pass (later ones start at 0) */
     int device;               /* CUDA device ordinal */
     int amg_sweeps;           /* MC_PSOLVER_PCG_AMG: damped-Jacobi sweeps before and after the coarse correction */
-    double amg_omega;         /* Jacobi damping */
+    double amg_omega;         /* Jacobi damping (every sweep, when amg_cheb_ratio is 0) */
     double amg_alpha;         /* coarse-correction scaling */
     double ir_inner_rtol;     /* MC_PRECISION_FP32_REFINED: each inner FP32 pressure solve reduces its
                                  residual by the factor still missing to p_rtol (with a margin of 2), but
@@ -114,6 +114,10 @@ typedef struct mc_flow_params {
     int reorder;              /* MC_REORDER_* */
     double ir_inner_rtol_bicg; /* the same floor for the inner FP32 BiCGStab solves of momentum and
                                   temperature (their target is u_rtol) */
+    double amg_cheb_ratio;    /* MC_PSOLVER_PCG_AMG: > 1 gives the amg_sweeps sweeps the damping of a
+                                 Chebyshev smoother on [2 / ratio, 2] (a different damping per sweep,
+                                 the reciprocal roots of the polynomial); 0: every sweep damps by
+                                 amg_omega */
 } mc_flow_params;
 
 /* Per-pass statistics. */

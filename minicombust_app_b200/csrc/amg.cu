@@ -2,6 +2,7 @@
 #include "amg.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "krylov.cuh"
@@ -345,14 +346,14 @@ __global__ void k_amg_smooth_first(AmgLevelT<T> L, T omega, T *__restrict__ e, c
 // The first two sweeps from e = 0 in one pass: e1 = e0 + omega D^-1 (r - A e0)
 // with e0 = omega D^-1 r evaluated at each row where it is needed.
 template <typename T>
-__global__ void k_amg_smooth_first2(AmgLevelT<T> L, T omega, T *__restrict__ eout, const PcgState *st)
+__global__ void k_amg_smooth_first2(AmgLevelT<T> L, T omega, T omega2, T *__restrict__ eout, const PcgState *st)
 {
     pdl_wait();
     if (st->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= L.n) return;
     auto e0 = [&](int j) { return omega * L.r[j] * inv_or_zero(L.diag[j]); };
-    eout[i] = e0(i) + omega * (L.r[i] - row_apply_v(L, i, e0)) * inv_or_zero(L.diag[i]);
+    eout[i] = e0(i) + omega2 * (L.r[i] - row_apply_v(L, i, e0)) * inv_or_zero(L.diag[i]);
 }
 
 // Prolongation and the first post-smoothing sweep in one pass: the
@@ -466,13 +467,14 @@ template <typename T>
 struct AmgCoarse {
     AmgLevelT<T> lv[AMG_FUSED_LEVELS];
     int nl;
+    T w[AMG_MAX_SWEEPS];  // damping of sweep k before the coarse correction (reversed after)
 };
 
 constexpr int AMG_FUSED_THREADS = AMG_COARSEST_MAX * DENSE_SOLVE_PARTS;  // 1024
 
 template <typename T>
 __global__ void __launch_bounds__(AMG_FUSED_THREADS)
-    k_amg_coarse_cycle(const __grid_constant__ AmgCoarse<T> C, const double *__restrict__ dense, T omega, T alpha,
+    k_amg_coarse_cycle(const __grid_constant__ AmgCoarse<T> C, const double *__restrict__ dense, T alpha,
                        int sweeps, const PcgState *st)
 {
     pdl_wait();
@@ -483,12 +485,13 @@ __global__ void __launch_bounds__(AMG_FUSED_THREADS)
     const int c_pre = (sweeps - 1) & 1;
     for (int l = 0; l + 1 < C.nl; l++) {
         const AmgLevelT<T> &L = C.lv[l];
-        for (int i = t; i < L.n; i += nt) L.e[0][i] = omega * L.r[i] * inv_or_zero(L.diag[i]);
+        for (int i = t; i < L.n; i += nt) L.e[0][i] = C.w[0] * L.r[i] * inv_or_zero(L.diag[i]);
         __syncthreads();
         int c = 0;
         for (int sw = 1; sw < sweeps; sw++) {
             const T *ein = L.e[c];
             T *eout = L.e[c ^ 1];
+            const T omega = C.w[sw];
             for (int i = t; i < L.n; i += nt)
                 eout[i] = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
             c ^= 1;
@@ -527,6 +530,7 @@ __global__ void __launch_bounds__(AMG_FUSED_THREADS)
         for (int sw = 1; sw <= sweeps; sw++) {
             const T *ein = L.e[c];
             T *eout = L.e[c ^ 1];
+            const T omega = C.w[sweeps - sw];
             for (int i = t; i < L.n; i += nt)
                 eout[i] = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
             c ^= 1;
@@ -582,6 +586,21 @@ void amg_coarsest_inverse(cudaStream_t s, const AmgHierarchy &H, double *out)
     k_amg_dense_factor<T><<<1, DENSE_THREADS, dense_smem(C.n), s>>>(C, out);
 }
 
+void amg_set_damping(AmgHierarchy &H, double ratio)
+{
+    for (int k = 0; k < AMG_MAX_SWEEPS; k++) H.omega_sweep[k] = H.omega;
+    if (!(ratio > 1.0)) return;
+    // Chebyshev smoothing as damped-Jacobi sweeps: with sweep k damping by
+    // 1 / lambda_k, lambda_k the roots of the degree-nu Chebyshev polynomial
+    // on [b / ratio, b], nu sweeps apply that polynomial of D^-1 A, the one of
+    // least maximum on the interval.  b = 2 bounds the spectrum of D^-1 A for
+    // every level (Gershgorin: the rows are weakly diagonally dominant, and
+    // the Galerkin products of piecewise-constant aggregation keep them so).
+    const double b = 2.0, a = b / ratio, pi = 3.14159265358979323846;
+    for (int k = 0; k < H.sweeps; k++)
+        H.omega_sweep[k] = 1.0 / (0.5 * (b + a) + 0.5 * (b - a) * std::cos((2 * k + 1) * pi / (2 * H.sweeps)));
+}
+
 void amg_plan_fused(AmgHierarchy &H)
 {
     int f = H.levels - 1;
@@ -609,7 +628,8 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
     using T2 = typename Pair<T>::type;
     T2 *zp_out = (T2 *)zp_out_v;
     const int L = H.levels, F = H.fused_from;
-    const T omega = (T)H.omega, alpha = (T)H.alpha;
+    const T alpha = (T)H.alpha;
+    auto w = [&](int k) { return (T)H.omega_sweep[k]; };  // sweep k before the coarse correction
     int cur[AMG_MAX_LEVELS] = {0};
     AmgLevelT<T> lv[AMG_MAX_LEVELS];
     const AmgLevelT<T> *src = levels_of<T>(H);
@@ -622,14 +642,14 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
         const dim3 g(blocks(V.n));
         int c = 0, sw = 1;
         if (pair) {
-            pdl_launch(k_amg_smooth_first2<T>, g, nt, 0, s, V, omega, V.e[1], st);
+            pdl_launch(k_amg_smooth_first2<T>, g, nt, 0, s, V, w(0), w(1), V.e[1], st);
             c = 1;
             sw = 2;
         } else {
-            pdl_launch(k_amg_smooth_first<T>, g, nt, 0, s, V, omega, V.e[0], st);
+            pdl_launch(k_amg_smooth_first<T>, g, nt, 0, s, V, w(0), V.e[0], st);
         }
         for (; sw < H.sweeps; sw++) {
-            pdl_launch(k_amg_jacobi<T>, g, nt, 0, s, V, omega, V.e[c], V.e[c ^ 1], st);
+            pdl_launch(k_amg_jacobi<T>, g, nt, 0, s, V, w(sw), V.e[c], V.e[c ^ 1], st);
             c ^= 1;
         }
         cur[l] = c;
@@ -638,7 +658,8 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
     AmgCoarse<T> C;
     C.nl = L - F;
     for (int q = 0; q < C.nl; q++) C.lv[q] = lv[F + q];
-    pdl_launch(k_amg_coarse_cycle<T>, dim3(1), dim3(AMG_FUSED_THREADS), 0, s, C, H.dense, omega, alpha, H.sweeps, st);
+    for (int k = 0; k < AMG_MAX_SWEEPS; k++) C.w[k] = w(k);
+    pdl_launch(k_amg_coarse_cycle<T>, dim3(1), dim3(AMG_FUSED_THREADS), 0, s, C, H.dense, alpha, H.sweeps, st);
     cur[F] = (F < L - 1) ? (2 * H.sweeps - 1) & 1 : 0;
     for (int l = F - 1; l >= 0; l--) {
         const AmgLevelT<T> &V = lv[l];
@@ -646,7 +667,7 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
         const T *ec = lv[l + 1].e[cur[l + 1]];
         int c = cur[l], sw = 1;
         if (pair) {
-            pdl_launch(k_amg_prolong_jacobi<T>, g, nt, 0, s, V, omega, alpha, ec, V.e[c], V.e[c ^ 1], st);
+            pdl_launch(k_amg_prolong_jacobi<T>, g, nt, 0, s, V, w(H.sweeps - 1), alpha, ec, V.e[c], V.e[c ^ 1], st);
             c ^= 1;
             sw = 2;
         } else {
@@ -654,10 +675,10 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
         }
         for (; sw <= H.sweeps; sw++) {
             if (l == 0 && sw == H.sweeps) {
-                pdl_launch(k_amg_final<T>, dim3(krylov_grid(V.n)), nt, 0, s, V, omega, V.e[c], zp_out, st, partials,
-                           counter, is_init);
+                pdl_launch(k_amg_final<T>, dim3(krylov_grid(V.n)), nt, 0, s, V, w(H.sweeps - sw), V.e[c], zp_out, st,
+                           partials, counter, is_init);
             } else {
-                pdl_launch(k_amg_jacobi<T>, g, nt, 0, s, V, omega, V.e[c], V.e[c ^ 1], st);
+                pdl_launch(k_amg_jacobi<T>, g, nt, 0, s, V, w(H.sweeps - sw), V.e[c], V.e[c ^ 1], st);
                 c ^= 1;
             }
         }

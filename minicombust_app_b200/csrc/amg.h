@@ -35,6 +35,7 @@ constexpr int AMG_COARSEST_MAX = 128;
 // single-block kernel per V-cycle; at most AMG_FUSED_LEVELS of them.
 constexpr int AMG_FUSE_MAX_ROWS = 1024;
 constexpr int AMG_FUSED_LEVELS = 6;
+constexpr int AMG_MAX_SWEEPS = 8;
 
 // Device view of one level; T is the storage type of values and vectors.
 template <typename T>
@@ -69,9 +70,14 @@ struct AmgHierarchy {
     double *dense_next = nullptr;  // the inverse being formed for the next pass (lagged setup)
     int sweeps = 2;
     double omega = 0.6667;
+    double omega_sweep[AMG_MAX_SWEEPS] = {};  // damping of sweep k before the coarse correction (reversed after)
     double alpha = 1.0;
     int fused_from = 0;   // first level of the single-block coarse cycle (set by amg_plan_fused)
 };
+
+// Damping of each sweep: amg_omega for every sweep (ratio 0), or the
+// reciprocal Chebyshev roots on [2 / ratio, 2] (ratio > 1).
+void amg_set_damping(AmgHierarchy &H, double ratio);
 
 // Choose the levels that the single-block coarse cycle takes over.
 void amg_plan_fused(AmgHierarchy &H);

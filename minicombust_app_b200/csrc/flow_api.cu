@@ -1369,6 +1369,7 @@ int build_amg(mc_flow *h, const HostMesh &hm)
     amg_plan_fused(H);
     H.sweeps = h->prm.amg_sweeps;
     H.omega = h->prm.amg_omega;
+    amg_set_damping(H, h->prm.amg_cheb_ratio);
     H.alpha = h->prm.amg_alpha;
     std::vector<int *> d_col(L), d_agg(L), d_mptr(L), d_mlist(L), d_gptr(L), d_gidx(L);
     for (int l = 0; l < L; l++) {
@@ -1508,6 +1509,7 @@ void mc_flow_default_params(mc_flow_params *p, int mode)
     p->amg_alpha = 2.0;
     p->ir_inner_rtol = 1e-5;
     p->ir_inner_rtol_bicg = 1e-4;
+    p->amg_cheb_ratio = 4.0;
     p->reorder = MC_REORDER_NONE;
     if (mode == MC_MODE_COMPAT) {
         p->viscosity = 0.000014;
@@ -1543,7 +1545,8 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
          !(params->ir_inner_rtol_bicg > 0) || params->ir_inner_rtol_bicg >= 1))
         return MC_ERR_UNSUPPORTED;
     if (params->pressure_solver == MC_PSOLVER_PCG_AMG &&
-        (params->amg_sweeps < 1 || !(params->amg_omega > 0) || !(params->amg_alpha > 0)))
+        (params->amg_sweeps < 1 || params->amg_sweeps > AMG_MAX_SWEEPS || !(params->amg_omega > 0) ||
+         !(params->amg_alpha > 0) || !(params->amg_cheb_ratio == 0 || params->amg_cheb_ratio > 1)))
         return MC_ERR_ARG;
     if (!(params->delta > 0) || !(params->urf_momentum > 0) || !(params->urf_temperature > 0) ||
         !(params->u_rtol > 0) || !(params->p_rtol > 0) || params->max_iters <= 0)

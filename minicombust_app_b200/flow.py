@@ -75,7 +75,8 @@ class FlowParams(ctypes.Structure):
                 ("flux_corr", c_dbl), ("u_rtol", c_dbl), ("p_rtol", c_dbl), ("max_iters", c_int),
                 ("pressure_solver", c_int), ("precision", c_int), ("initial_guess", c_int), ("device", c_int),
                 ("amg_sweeps", c_int), ("amg_omega", c_dbl), ("amg_alpha", c_dbl), ("ir_inner_rtol", c_dbl),
-                ("reorder", c_int), ("ir_inner_rtol_bicg", c_dbl)]
+                ("reorder", c_int), ("ir_inner_rtol_bicg", c_dbl),
+                ("amg_cheb_ratio", c_dbl)]
 
 
 class IterStats(ctypes.Structure):

@@ -110,6 +110,19 @@ def test_refinement_floors():
         assert L.mc_flow_create(ctypes.byref(mv), ctypes.byref(q), ctypes.byref(h)) == flow.MC_ERR_UNSUPPORTED, field
 
 
+def test_chebyshev_damping_parameter():
+    p = flow.default_params(flow.MODE_SIMPLE)
+    assert p.amg_cheb_ratio == 4.0
+    L = flow.library()
+    h = ctypes.c_void_p()
+    mv = flow.Mesh.box(2, 1, 1, 0.2, 0.1, 0.1).view()
+    for bad in (0.5, 1.0, -3.0):
+        q = flow.default_params(flow.MODE_SIMPLE, pressure_solver=flow.PSOLVER_PCG_AMG, amg_cheb_ratio=bad)
+        assert L.mc_flow_create(ctypes.byref(mv), ctypes.byref(q), ctypes.byref(h)) == flow.MC_ERR_ARG, bad
+    q = flow.default_params(flow.MODE_SIMPLE, pressure_solver=flow.PSOLVER_PCG_AMG, amg_sweeps=9)
+    assert L.mc_flow_create(ctypes.byref(mv), ctypes.byref(q), ctypes.byref(h)) == flow.MC_ERR_ARG
+
+
 def test_inconsistent_mesh_is_rejected():
     L = flow.library()
     mesh = flow.Mesh.box(3, 2, 2, 0.3, 0.2, 0.2)
