@@ -662,9 +662,11 @@ int solve_bicg(mc_flow *h, const Ell &A, const BicgVectors<R> &v, BicgState<R> *
 }
 
 // FP64 iterative refinement around FP32 BiCGStab solves (momentum, R = 3;
-// temperature, R = 1): each inner solve asks for the reduction still missing
-// (margin 2, floor ir_inner_rtol_bicg); the outer loop stops on the FP64 true
-// residual, ||b - A x|| <= u_rtol ||b|| per system.
+// temperature, R = 1): each inner solve works on the row-scaled system
+// D^-1 A e = D^-1 r (FP32 copies from round_ell, D = diag A) and asks for
+// the reduction still missing (margin 2, floor ir_inner_rtol_bicg); the
+// outer loop stops on the FP64 true residual, ||b - A x|| <= u_rtol ||b||
+// per system.
 template <int R>
 int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const BicgVectorsT<float, R> &in,
                        const BirVectors<R> &out, BicgState<R> *hin, BirState<R> *hout, cudaGraphExec_t *exec,

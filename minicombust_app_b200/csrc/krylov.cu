@@ -942,7 +942,8 @@ __global__ void __launch_bounds__(MCB_THREADS, SPLIT ? 8 : 1) k_bicg_3(EllT<T> A
     }
 }
 
-// Refinement: x = 0, r32 = (float) b, norms and tolerances.
+// Refinement: x = 0, r32 = (float) D^-1 b (the inner FP32 systems are the
+// rows of A scaled by 1 / diag, see k_round_ell), norms and tolerances.
 template <int R>
 __global__ void __launch_bounds__(MCB_THREADS) k_bir_init(Ell A, BirVectors<R> v, double rtol, int max_outer)
 {
@@ -956,7 +957,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bir_init(Ell A, BirVectors<R> v
         for (int j = 0; j < R; j++) {
             const double bi = v.b[(size_t)j * N + i];
             v.x[j][i] = 0.0;
-            v.r32[(size_t)j * N + i] = (float)bi;
+            v.r32[(size_t)j * N + i] = (float)(bi * row_scale(A.diag, i));
             acc[j] += bi * bi;
         }
     }
@@ -1030,7 +1031,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_bir_residual(Ell A, BirVectors<
 #pragma unroll
             for (int k = 0; k < 6; k++) ax += offk[k] * x[colk[k]];
             const double ri = v.b[o] - ax;
-            v.r32[o] = (float)ri;
+            v.r32[o] = (float)(ri * (d != 0.0 ? 1.0 / d : 1.0));  // the row-scaled inner system
             acc[j] += ri * ri;
         }
     }
@@ -1065,9 +1066,10 @@ __global__ void __launch_bounds__(MCB_THREADS) k_round_ell(int N, const double *
                                                            float *__restrict__ d32, float *__restrict__ o32)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        d32[i] = (float)diag[i];
+        const double sc = row_scale(diag, i);
+        d32[i] = (float)(diag[i] * sc);
         float o[6];
-        round_row_by_direction(off, code, N, i, o);
+        round_row_by_direction(off, code, N, i, o, sc);
 #pragma unroll
         for (int k = 0; k < 6; k++) o32[(size_t)k * N + i] = o[k];
     }

@@ -124,7 +124,7 @@ __device__ __forceinline__ auto with_row_cols(const DirCodes &dc, const int *__r
 // FP32 values of row i; with codes in direction order (slot d = direction d,
 // zero for a direction the row lacks), else in the original slot order.
 __device__ __forceinline__ void round_row_by_direction(const double *__restrict__ off, const uint32_t *__restrict__ code,
-                                                       int N, int i, float (&o)[6])
+                                                       int N, int i, float (&o)[6], double scale = 1.0)
 {
     if (code) {
         const uint32_t cw = code[i];
@@ -133,14 +133,22 @@ __device__ __forceinline__ void round_row_by_direction(const double *__restrict_
 #pragma unroll
         for (int k = 0; k < 6; k++) {
             const unsigned d = (cw >> (3 * k)) & 7u;
-            const float v = (float)off[(size_t)k * N + i];
+            const float v = (float)(off[(size_t)k * N + i] * scale);
 #pragma unroll
             for (int q = 0; q < 6; q++) o[q] = (d == (unsigned)q) ? v : o[q];
         }
     } else {
 #pragma unroll
-        for (int k = 0; k < 6; k++) o[k] = (float)off[(size_t)k * N + i];
+        for (int k = 0; k < 6; k++) o[k] = (float)(off[(size_t)k * N + i] * scale);
     }
+}
+
+// Row scaling of the FP32 inner BiCGStab systems (Jacobi preconditioning
+// from the left): 1 / diag, or 1 for a row without a diagonal.
+__device__ __forceinline__ double row_scale(const double *__restrict__ diag, int i)
+{
+    const double d = diag[i];
+    return d != 0.0 ? 1.0 / d : 1.0;
 }
 
 // 7-point system in ELL form; T is the storage type of the values.
@@ -311,8 +319,9 @@ template <int R>
 void bir_add(cudaStream_t s, int N, const BirVectors<R> &v);
 template <int R>
 void bir_residual(cudaStream_t s, const Ell &A, const BirVectors<R> &v);
-// FP32 copy of a 7-point matrix's values, by direction when `code` is given
-// (see DirCodes::dia), else in slot order.
+// FP32 copy of a 7-point matrix's rows scaled by 1 / diag (the inner systems
+// of the refined BiCGStab solves), by direction when `code` is given (see
+// DirCodes::dia), else in slot order.
 void round_ell(cudaStream_t s, int N, const double *diag, const double *off, const uint32_t *code, float *diag32,
                float *off32);
 
