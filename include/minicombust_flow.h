@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define MC_FLOW_ABI_VERSION 1
+#define MC_FLOW_ABI_VERSION 2
 
 typedef enum mc_status {
     MC_OK = 0,
@@ -64,7 +64,10 @@ enum {
     MC_FIELD_FUL = 9, MC_FIELD_PRO = 10, MC_FIELD_VARF = 11, MC_FIELD_VARP = 12
 };
 
-/* Linear systems readable with mc_flow_get_csr. */
+/* Linear systems readable with mc_flow_get_csr.  MC_SYSTEM_TEMPERATURE is the
+ * scalar-transport system assembled last: T, or with transport_scalars the
+ * last of TE, ED, TEM, FUL, PRO, VARF, VARP that ran (they share storage, as
+ * they share the reference's A/b, FlowSolver.inl:2885-2960). */
 enum { MC_SYSTEM_MOMENTUM = 0, MC_SYSTEM_PRESSURE = 1, MC_SYSTEM_TEMPERATURE = 2 };
 
 /* Mesh in the reference layout (Mesh<T> public arrays, Mesh.hpp:86-106). */
@@ -118,6 +121,13 @@ typedef struct mc_flow_params {
                                  Chebyshev smoother on [2 / ratio, 2] (a different damping per sweep,
                                  the reciprocal roots of the polynomial); 0: every sweep damps by
                                  amg_omega */
+    int transport_scalars;    /* 0: a pass transports u, v, w, p and T only (none of them depends on
+                                 the other scalars); 1: it also solves the reference's other scalar
+                                 transports -- turbulent kinetic energy and dissipation (k-epsilon
+                                 with wall functions), mixture fraction, progress variable and their
+                                 two variances -- in the reference's order TE, ED, TEM, FUL, PRO,
+                                 VARF, VARP (FlowSolver.inl:3229-3261).  Default: 1 in
+                                 MC_MODE_COMPAT, 0 in MC_MODE_SIMPLE. */
 } mc_flow_params;
 
 /* Per-pass statistics. */
@@ -128,12 +138,17 @@ typedef struct mc_iter_stats {
     int pressure_iters_total;
     int pressure_iters_first;
     double pressure_correction_max_first;
-    double pressure_rel_residual;    /* last pressure solve, ||r|| / ||b|| */
+    double pressure_rel_residual;    /* max over the pass's pressure solves of ||r|| / ||b_1||, b_1 the
+                                        first solve's right-hand side (later correctors stop on
+                                        p_rtol ||b_1||) */
     double mass_imbalance;           /* max over cells |div(mdot) - mass source| after the pass */
     int guess_choice_first;          /* initial guess of the first pressure solve: -1 zero, 2 the
                                         residual-minimising combination of the previous correction and
                                         (MC_GUESS_LEARNED) the network's prediction */
     double guess_rel_residual_first; /* ||b - A x0|| / ||b|| of that guess (1 for zero) */
+    double pressure_rel_residual_first; /* ||r|| / ||b|| at the end of the first pressure solve */
+    int scalar_iters[6];             /* transport_scalars: BiCGStab iterations of TE, ED, FUL, PRO,
+                                        VARF, VARP (0 when not run) */
 } mc_iter_stats;
 
 typedef struct mc_flow mc_flow;
@@ -147,11 +162,13 @@ void mc_flow_default_params(mc_flow_params *params, int mode);
 int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_flow **out);
 int mc_flow_destroy(mc_flow *flow);
 
-/* Field access, cells + 6 doubles (FlowSolver::phi).  Fields outside the
- * coupled set U, V, W, P, PP, TEM return MC_ERR_UNSUPPORTED. */
+/* Field access, cells + 6 doubles (FlowSolver::phi).  Without
+ * transport_scalars, fields outside the coupled set U, V, W, P, PP, TEM
+ * return MC_ERR_UNSUPPORTED; with it all 13 fields are held. */
 int mc_flow_set_field(mc_flow *flow, int field, const double *host_values);
 int mc_flow_get_field(mc_flow *flow, int field, double *host_values);
-/* Least-squares gradient of U, V, W, P, PP or TEM, [cells][3]. */
+/* Least-squares gradient of U, V, W, P, PP or TEM (and, with
+ * transport_scalars, TE, ED, FUL, PRO, VARF, VARP), [cells][3]. */
 int mc_flow_get_gradient(mc_flow *flow, int field, double *host_values);
 /* Particle source terms, [cells][5] particle_aos<double> (Mesh::particle_terms). */
 int mc_flow_set_sources(mc_flow *flow, const double *host_particle_terms);
@@ -197,6 +214,11 @@ int mc_flow_stage_set_up_field(mc_flow *flow);/* set_up_field, FlowSolver.inl:11
 int mc_flow_stage_momentum(mc_flow *flow, mc_iter_stats *stats);    /* calculate_UVW, :1655-1810 */
 int mc_flow_stage_pressure(mc_flow *flow, mc_iter_stats *stats);    /* calculate_pressure, :2317-2514 */
 int mc_flow_stage_temperature(mc_flow *flow, mc_iter_stats *stats); /* Scalar_solve(TEMP), :2885-3076 */
+/* Scalar_solve for one transported scalar (FlowSolver.inl:2885-3076, with
+ * FluxScalar :2516-2744 and solveTurbulenceModels :2746-2883): field is
+ * MC_FIELD_TE, _ED, _TEM, _FUL, _PRO, _VARF or _VARP.  The fields other than
+ * TEM need transport_scalars (MC_ERR_UNSUPPORTED otherwise). */
+int mc_flow_stage_scalar(mc_flow *flow, int field, mc_iter_stats *stats);
 
 /* Kernel timing on the handle's stream (CUDA events around each launch).
  * While enabled, passes run without graph replay.  Times accumulate until
@@ -215,9 +237,11 @@ const char *mc_flow_last_error(mc_flow *flow);
 const char *mc_status_string(int status);
 
 /* Allocation-free solve.  No counterpart in the reference: it is offered to
- * callers that must not allocate device memory -- code that issues work while
- * a CUDA stream capture is in progress (cudaMalloc is not permitted then) and
- * hosts whose device memory is owned by their own pool or budget.
+ * callers that must not allocate device memory -- hosts that hand all device
+ * memory to their own pool or fixed budget at start-up (a cudaMalloc from a
+ * library would fail there, or take memory the host has promised elsewhere),
+ * and callers inside a time-critical loop, where cudaMalloc and cudaFree can
+ * synchronise the device and stall the host's other streams.
  *
  * Solves A x = b with the BiCGStab kernels the temperature stage uses (zero
  * initial guess, ||b - A x|| <= rtol ||b||), on a 7-point system the caller
@@ -229,9 +253,10 @@ const char *mc_status_string(int status);
  * one file-scope device array sized for MC_SOLVE_NOALLOC_MAX_ROWS rows (about
  * 16 MB, held by every device that loads the library until the process
  * exits).  n above that limit returns MC_ERR_ARG.  All calls share the array,
- * so calls that overlap on the GPU race.  The first call on a device looks up
- * the array's address (cudaGetSymbolAddress, once per device); make that call
- * before any stream capture.  iterations (may be NULL) receives the count. */
+ * which keeps the last call's contents (each call clears what must start at
+ * zero), so calls that overlap on the GPU race.  The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress, once per device, with
+ * that device current).  iterations (may be NULL) receives the count. */
 #define MC_SOLVE_NOALLOC_MAX_ROWS 262144
 int mc_solve_bicgstab_noalloc(int n, const double *diag, const double *off, const int *col, const double *b,
                               double *x, double rtol, int max_iters, void *stream, int *iterations);

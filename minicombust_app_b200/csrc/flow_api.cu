@@ -34,7 +34,7 @@ enum KernelId {
     K_BICG1_1, K_BICG1_2, K_BICG1_3, K_AMG_SETUP, K_PCG_INIT_AMG, K_PCG_ITER2_AMG, K_AMG_VCYCLE,
     K_IR, K_PCG_INIT_AMG32, K_PCG_ITER1_32, K_PCG_ITER2_AMG32, K_AMG_VCYCLE32, K_PERMUTE, K_GUESS, K_GNN,
     K_SNAPSHOT, K_BIR, K_ROUND_ELL, K_BICG3_INIT32, K_BICG3_1_32, K_BICG3_2_32, K_BICG3_3_32, K_BICG1_INIT32,
-    K_BICG1_1_32, K_BICG1_2_32, K_BICG1_3_32, K_COUNT
+    K_BICG1_1_32, K_BICG1_2_32, K_BICG1_3_32, K_GRAD6, K_SCALAR, K_SCALAR_CLIP, K_COUNT
 };
 
 const char *kKernelNames[K_COUNT] = {
@@ -47,7 +47,7 @@ const char *kKernelNames[K_COUNT] = {
     "pcg32_iter1_spmv", "pcg32_iter2_amg_update", "amg32_vcycle", "permute", "guess_select", "gnn_forward",
     "snapshot_pack", "bicg_refine_fp64_residual", "round_fp32", "bicg3_32_init", "bicg3_32_1_spmv",
     "bicg3_32_2_spmv", "bicg3_32_3_update", "bicg1_32_init", "bicg1_32_1_spmv", "bicg1_32_2_spmv",
-    "bicg1_32_3_update"};
+    "bicg1_32_3_update", "lsq_gradients_scalars", "scalar_assemble", "scalar_clip_negative"};
 
 constexpr int PCG_BATCH = 16;   // iterations per status read (even: ping-pong buffers)
 constexpr int PCG_AMG_BATCH = 4;
@@ -172,6 +172,18 @@ struct mc_flow {
     float *snap_host = nullptr;       // pinned [4][N]
     char *snap_mem = nullptr;
 
+    // the other scalar transports (transport_scalars): TE, ED, TP, FUL, PRO,
+    // VARF, VARP fields and the gradients of all but TP, by MC_FIELD id
+    bool has_scalars = false;
+    char *scal_mem = nullptr;
+    double *sfield[MC_FIELD_VARP + 1] = {};
+    double *sgrad[MC_FIELD_VARP + 1][3] = {};
+    double *xs = nullptr;             // a scalar solve's solution, copied into its field
+    BicgVectors<1> bs{};              // the single-system BiCGStab buffers with x = xs
+    cudaGraphExec_t g_bs = nullptr, l_bs = nullptr;
+    int *neg_list = nullptr;          // negative k / epsilon cells after a solve
+    unsigned int *neg_count = nullptr;
+
     // state of the reference's control flow
     int first_pressure = 1;
     uint64_t timestep_count = 0;
@@ -257,6 +269,34 @@ int grad_index(int field)
     case MC_FIELD_TEM: return G_T;
     default: return -1;
     }
+}
+
+// The six scalar fields with a gradient, and TP, held only with transport_scalars.
+constexpr int kScalarFields[7] = {MC_FIELD_TE, MC_FIELD_ED, MC_FIELD_TP, MC_FIELD_FUL, MC_FIELD_PRO, MC_FIELD_VARF,
+                                  MC_FIELD_VARP};
+constexpr int kClipCap = 4096;
+
+bool is_scalar_field(int field)
+{
+    for (int f : kScalarFields)
+        if (f == field) return true;
+    return false;
+}
+
+// Device array of a field (cells + 6), or null when the handle does not hold it.
+double *field_ptr(mc_flow *h, int field)
+{
+    const int g = grad_index(field);
+    if (g >= 0) return h->phi[g];
+    return (h->has_scalars && is_scalar_field(field)) ? h->sfield[field] : nullptr;
+}
+
+// Device gradient component d of a field, or null.
+double *grad_ptr(mc_flow *h, int field, int d)
+{
+    const int g = grad_index(field);
+    if (g >= 0) return h->grad[g][d];
+    return (h->has_scalars && is_scalar_field(field) && field != MC_FIELD_TP) ? h->sgrad[field][d] : nullptr;
 }
 
 Ell momentum_matrix(mc_flow *h) { return Ell{h->N, h->AU, h->off_m, h->col, h->dc}; }
@@ -806,9 +846,28 @@ void launch_mass_flux(mc_flow *h)
         });
 }
 
+// Gradients of the six other scalars, with those of u, v, w, p, T at the
+// start of a pass (get_phi_gradients computes all eleven, FlowSolver.inl:917-1063).
+void launch_gradients_scalars(mc_flow *h)
+{
+    GradArgs<6> a{};
+    const int fields[6] = {MC_FIELD_TE, MC_FIELD_ED, MC_FIELD_FUL, MC_FIELD_PRO, MC_FIELD_VARF, MC_FIELD_VARP};
+    for (int k = 0; k < 6; k++) {
+        a.phi[k] = h->sfield[fields[k]];
+        a.gx[k] = h->sgrad[fields[k]][0];
+        a.gy[k] = h->sgrad[fields[k]][1];
+        a.gz[k] = h->sgrad[fields[k]][2];
+    }
+    a.zero_boundary = 0u;
+    launch(h, K_GRAD6, [&] {
+        launch_lsq_gradients6(h->stream, h->N, h->nbr, h->fc1, h->xc, h->yc, h->zc, h->xf, h->yf, h->zf, a);
+    });
+}
+
 int stage_gradients(mc_flow *h)
 {
     launch_gradients5(h);
+    if (h->has_scalars) launch_gradients_scalars(h);
     return check_launch(h);
 }
 
@@ -974,8 +1033,12 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
                 st->pressure_iters_first = its;
                 st->guess_choice_first = h->guess_choice;
                 st->guess_rel_residual_first = h->guess_rel;
+                st->pressure_rel_residual_first = relres;
             }
-            st->pressure_rel_residual = relres;
+            // every corrector's final residual against the first corrector's
+            // right-hand side (the norm the later correctors' floor uses)
+            const double rel_ref = h->p_bnorm_ref > 0 ? relres * bnorm / h->p_bnorm_ref : relres;
+            st->pressure_rel_residual = std::max(st->pressure_rel_residual, rel_ref);
         }
         // A solve that met its tolerance at the initial check from the zero
         // guess leaves PP = 0 exactly: the corrections below would add zeros
@@ -1059,6 +1122,73 @@ int stage_temperature(mc_flow *h, mc_iter_stats *st)
     }
     if (st) st->temperature_iters = its[0];
     return rc;
+}
+
+// Scalar_solve for TE, ED, FUL, PRO, VARF or VARP (FlowSolver.inl:2885-3076):
+// assembly (with the k-epsilon sources), FP64 BiCGStab from zero into xs,
+// the solution copied into the field, and for k and epsilon the
+// replacement of negative values (:2956-2985).  TEM goes to the temperature
+// stage.
+int stage_scalar(mc_flow *h, int field, mc_iter_stats *st)
+{
+    if (field == MC_FIELD_TEM) return stage_temperature(h, st);
+    int type = -1, slot = -1;
+    switch (field) {
+    case MC_FIELD_TE: type = SC_TERBTE; slot = 0; break;
+    case MC_FIELD_ED: type = SC_TERBED; slot = 1; break;
+    case MC_FIELD_FUL: type = SC_FUEL; slot = 2; break;
+    case MC_FIELD_PRO: type = SC_PROG; slot = 3; break;
+    case MC_FIELD_VARF: type = SC_VARFU; slot = 4; break;
+    case MC_FIELD_VARP: type = SC_VARPR; slot = 5; break;
+    default: return fail(h, MC_ERR_ARG, "not a transported scalar");
+    }
+    if (!h->has_scalars) return fail(h, MC_ERR_UNSUPPORTED, "transport_scalars is off");
+    double *phi = h->sfield[field];
+    ScalarArgs a{};
+    a.phi = phi;
+    for (int d = 0; d < 3; d++) a.g[d] = h->sgrad[field][d];
+    a.mdot = h->mdot;
+    a.src = nullptr;
+    a.off = h->off_t;
+    a.diag = h->diag_t;
+    a.b = h->b_t;
+    TurbArgs t{};
+    t.U = h->phi[G_U];
+    t.V = h->phi[G_V];
+    t.W = h->phi[G_W];
+    for (int d = 0; d < 3; d++) {
+        t.gU[d] = h->grad[G_U][d];
+        t.gV[d] = h->grad[G_V][d];
+        t.gW[d] = h->grad[G_W][d];
+    }
+    t.TE = h->sfield[MC_FIELD_TE];
+    t.ED = h->sfield[MC_FIELD_ED];
+    t.TP = h->sfield[MC_FIELD_TP];
+    launch(h, K_SCALAR, [&] { launch_scalar_assemble(h->stream, type, h->ph, h->margs, a, t); });
+    int rc = check_launch(h);
+    if (rc) return rc;
+    int its[1] = {0};
+    const int solve_rc =
+        solve_bicg<1>(h, temperature_matrix(h), h->bs, h->h_b1, &h->g_bs, &h->l_bs, K_BICG1_INIT, K_BICG1_1, its);
+    if (solve_rc == MC_ERR_CUDA) return solve_rc;
+    CUDA_TRY(h, cudaMemcpyAsync(phi, h->xs, (size_t)h->N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    if (type == SC_TERBTE || type == SC_TERBED) {
+        ClipArgs c{};
+        c.phi = phi;
+        c.nbr = h->nbr;
+        c.key = h->reordered ? h->d_cell_n2o : nullptr;
+        c.o2n = h->reordered ? h->d_cell_o2n : nullptr;
+        c.list = h->neg_list;
+        c.count = h->neg_count;
+        c.cap = kClipCap;
+        launch(h, K_SCALAR_CLIP,
+               [&] { k_scalar_negatives<<<krylov_grid(h->N), MCB_THREADS, 0, h->stream>>>(h->N, c); });
+        launch(h, K_SCALAR_CLIP, [&] { k_scalar_clip<<<1, 1024, 0, h->stream>>>(h->N, c); });
+    }
+    rc = check_launch(h);
+    if (rc) return rc;
+    if (st) st->scalar_iters[slot] = its[0];
+    return solve_rc;
 }
 
 // ------------------------------------------------------------------ create
@@ -1190,7 +1320,53 @@ int initial_fields(mc_flow *h, const int btype[6])
     rc = rc ? rc : put(G_P, p.pressure0, p.pressure0, p.pressure0, p.pressure0);
     rc = rc ? rc : put(G_PP, 0.0, 0.0, 0.0, 0.0);
     rc = rc ? rc : put(G_T, p.temperature0, p.temperature0, p.temperature0, p.temperature0);
+    if (rc || !h->has_scalars) return rc;
+    // the other scalars (FlowSolver.hpp:320-327 interior; :411-469 boundary
+    // slots by type: inlet k and epsilon from the inlet speed)
+    auto put_field = [&](int field, double interior, double inlet, double outlet, double wall) -> int {
+        std::fill(v.begin(), v.begin() + h->N, interior);
+        for (int s = 0; s < 6; s++) v[h->N + s] = btype[s] == INLET ? inlet : (btype[s] == OUTLET ? outlet : wall);
+        CUDA_TRY(h, cudaMemcpy(h->sfield[field], v.data(), NB * sizeof(double), cudaMemcpyHostToDevice));
+        return MC_OK;
+    };
+    const double te_in = h->ph.sc_inlet[SC_TERBTE], ed_in = h->ph.sc_inlet[SC_TERBED];
+    rc = put_field(MC_FIELD_TE, 0.0001, te_in, 0.0001, 0.0001);
+    rc = rc ? rc : put_field(MC_FIELD_ED, 0.0, ed_in, 0.0, 0.0);
+    rc = rc ? rc : put_field(MC_FIELD_TP, 0.0, 0.0, 0.0, 0.0);
+    rc = rc ? rc : put_field(MC_FIELD_FUL, 0.1, 0.1, 0.1, 0.0);
+    rc = rc ? rc : put_field(MC_FIELD_PRO, 0.001, 0.0, 0.001, 0.0);
+    rc = rc ? rc : put_field(MC_FIELD_VARF, 0.1, 0.1, 0.1, 0.0);
+    rc = rc ? rc : put_field(MC_FIELD_VARP, 0.001, 0.0, 0.001, 0.0);
     return rc;
+}
+
+// Device storage of the other scalar transports: seven fields, eighteen
+// gradient components, the solve's solution vector and the negative-cell list.
+int setup_scalars(mc_flow *h)
+{
+    const size_t N = (size_t)h->N, NB = N + 6;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t bytes = 7 * al(NB * 8) + 18 * al(N * 8) + al(N * 8) + al(kClipCap * 4) + 256;
+    CUDA_TRY(h, cudaMalloc((void **)&h->scal_mem, bytes));
+    CUDA_TRY(h, cudaMemsetAsync(h->scal_mem, 0, bytes, h->stream));
+    char *p = h->scal_mem;
+    for (int f : kScalarFields) {
+        h->sfield[f] = (double *)p;
+        p += al(NB * 8);
+        if (f == MC_FIELD_TP) continue;
+        for (int d = 0; d < 3; d++) {
+            h->sgrad[f][d] = (double *)p;
+            p += al(N * 8);
+        }
+    }
+    h->xs = (double *)p;
+    p += al(N * 8);
+    h->neg_list = (int *)p;
+    p += al(kClipCap * 4);
+    h->neg_count = (unsigned int *)p;
+    h->bs = h->b1;
+    h->bs.x[0] = h->xs;
+    return MC_OK;
 }
 
 // FP32-refined momentum and temperature solves: FP32 matrix copies, the
@@ -1513,6 +1689,7 @@ void mc_flow_default_params(mc_flow_params *p, int mode)
     p->ir_inner_rtol_bicg = 1e-4;
     p->amg_cheb_ratio = 4.0;
     p->reorder = MC_REORDER_NONE;
+    p->transport_scalars = mode == MC_MODE_COMPAT ? 1 : 0;
     if (mode == MC_MODE_COMPAT) {
         p->viscosity = 0.000014;
         p->temperature0 = 2000.0;
@@ -1616,6 +1793,23 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
                 rc = rc ? rc : upload(h, h->d_face_o2n, h->face_o2n.data(), F);
                 if (!rc) cudaStreamSynchronize(h->stream);
             }
+            if (!rc) {
+                // inlet values of the scalars, as the reference computes them
+                // (FlowSolver.inl:2625-2659; FlowSolver.hpp:421, 431-432)
+                const double u = params->inlet_u;
+                const double velmag2 = std::pow(u, 2) + std::pow(0.0, 2) + std::pow(0.0, 2);
+                Physics &ph0 = h->ph;
+                ph0.sc_inlet[SC_TERBTE] = 3.0 / 2.0 * ((0.1 * 0.1) * velmag2);
+                ph0.sc_inlet[SC_TERBED] = std::pow(0.09, 0.75) * std::pow((3.0 / 2.0 * ((0.1 * 0.1) * velmag2)), 1.5);
+                ph0.sc_inlet[SC_TEMP] = params->temperature0;
+                ph0.sc_inlet[SC_FUEL] = 0.1;
+                ph0.sc_inlet[SC_PROG] = 0.0;
+                ph0.sc_inlet[SC_VARFU] = 0.1;
+                ph0.sc_inlet[SC_VARPR] = 0.0;
+                ph0.cmu75 = std::pow(0.09, 0.75);
+                h->has_scalars = params->transport_scalars != 0;
+                if (h->has_scalars) rc = setup_scalars(h);
+            }
             rc = rc ? rc : initial_fields(h, hm.btype);
             if (!rc) {
                 std::vector<uint32_t> code;
@@ -1709,6 +1903,9 @@ int mc_flow_destroy(mc_flow *h)
     if (h->h_gs) cudaFreeHost(h->h_gs);
     if (h->gnn_mem) cudaFree(h->gnn_mem);
     if (h->bir_mem) cudaFree(h->bir_mem);
+    if (h->scal_mem) cudaFree(h->scal_mem);
+    for (cudaGraphExec_t g : {h->g_bs, h->l_bs})
+        if (g) cudaGraphExecDestroy(g);
     for (void *p : {(void *)h->h_bi3, (void *)h->h_bi1, (void *)h->h_bo3, (void *)h->h_bo1})
         if (p) cudaFreeHost(p);
     if (h->side) cudaStreamSynchronize(h->side);  // no inverse still being formed into freed memory
@@ -1723,14 +1920,14 @@ int mc_flow_destroy(mc_flow *h)
 int mc_flow_set_field(mc_flow *h, int field, const double *vals)
 {
     if (!h || !vals) return MC_ERR_ARG;
-    const int g = grad_index(field);
-    if (g < 0) return MC_ERR_UNSUPPORTED;
+    double *dst = field_ptr(h, field);
+    if (!dst) return MC_ERR_UNSUPPORTED;
     const size_t NB = (size_t)h->N + 6;
     if (h->reordered) {
         CUDA_TRY(h, cudaMemcpyAsync(h->stage, vals, NB * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        permute(h, h->phi[g], h->stage, h->d_cell_n2o, h->N, 6);
+        permute(h, dst, h->stage, h->d_cell_n2o, h->N, 6);
     } else {
-        CUDA_TRY(h, cudaMemcpyAsync(h->phi[g], vals, NB * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(dst, vals, NB * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     }
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return MC_OK;
@@ -1739,10 +1936,9 @@ int mc_flow_set_field(mc_flow *h, int field, const double *vals)
 int mc_flow_get_field(mc_flow *h, int field, double *vals)
 {
     if (!h || !vals) return MC_ERR_ARG;
-    const int g = grad_index(field);
-    if (g < 0) return MC_ERR_UNSUPPORTED;
+    const double *src = field_ptr(h, field);
+    if (!src) return MC_ERR_UNSUPPORTED;
     const size_t NB = (size_t)h->N + 6;
-    const double *src = h->phi[g];
     if (h->reordered) {
         permute(h, h->stage, src, h->d_cell_o2n, h->N, 6);
         src = h->stage;
@@ -1820,11 +2016,10 @@ int mc_flow_get_cell_order(mc_flow *h, int *cell_new_to_old)
 int mc_flow_get_gradient(mc_flow *h, int field, double *vals)
 {
     if (!h || !vals) return MC_ERR_ARG;
-    const int g = grad_index(field);
-    if (g < 0) return MC_ERR_UNSUPPORTED;
+    if (!grad_ptr(h, field, 0)) return MC_ERR_UNSUPPORTED;
     std::vector<double> tmp((size_t)h->N);
     for (int d = 0; d < 3; d++) {
-        const double *src = h->grad[g][d];
+        const double *src = grad_ptr(h, field, d);
         if (h->reordered) {
             permute(h, h->stage, src, h->d_cell_o2n, h->N, 0);
             src = h->stage;
@@ -1987,6 +2182,17 @@ int mc_flow_stage_temperature(mc_flow *h, mc_iter_stats *st)
     return rc;
 }
 
+int mc_flow_stage_scalar(mc_flow *h, int field, mc_iter_stats *st)
+{
+    if (!h) return MC_ERR_ARG;
+    const int rc = stage_scalar(h, field, st);
+    const int rs = check_launch(h);
+    if (rs) return rs;
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    flush_timing(h);
+    return rc;
+}
+
 // One pass of FlowSolver::timestep's loop (FlowSolver.inl:3188-3268).
 int mc_flow_simple_iteration(mc_flow *h, mc_iter_stats *st)
 {
@@ -2008,7 +2214,15 @@ int mc_flow_simple_iteration(mc_flow *h, mc_iter_stats *st)
     }
     if ((rc = track(stage_momentum(h, s)))) return rc;
     if ((rc = track(stage_pressure(h, s)))) return rc;
-    if ((rc = track(stage_temperature(h, s)))) return rc;
+    if (h->has_scalars) {
+        // the reference's order, FlowSolver.inl:3229-3261
+        const int order[7] = {MC_FIELD_TE, MC_FIELD_ED, MC_FIELD_TEM, MC_FIELD_FUL, MC_FIELD_PRO, MC_FIELD_VARF,
+                              MC_FIELD_VARP};
+        for (int f : order)
+            if ((rc = track(stage_scalar(h, f, s)))) return rc;
+    } else {
+        if ((rc = track(stage_temperature(h, s)))) return rc;
+    }
     launch(h, K_IMBALANCE, [&] {
         k_mass_imbalance<<<krylov_grid(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, h->mdot,
                                                                            h->sources_set ? h->src : nullptr,

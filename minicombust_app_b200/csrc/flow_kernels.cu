@@ -126,6 +126,14 @@ void launch_lsq_gradients1(cudaStream_t s, int N, const int *nbr, const int *fc1
                                                                                   zf, a);
 }
 
+void launch_lsq_gradients6(cudaStream_t s, int N, const int *nbr, const int *fc1, const double *xc,
+                           const double *yc, const double *zc, const double *xf, const double *yf, const double *zf,
+                           const GradArgs<6> &a)
+{
+    k_lsq_gradients<6><<<(N + MCB_THREADS - 1) / MCB_THREADS, MCB_THREADS, 0, s>>>(N, nbr, fc1, xc, yc, zc, xf, yf,
+                                                                                  zf, a);
+}
+
 // -------------------------------------------------------------- precomp_AU
 // precomp_AU (FlowSolver.inl:1065-1104): inlet/outlet viscous part plus rho V / dt.
 __global__ void __launch_bounds__(MCB_THREADS) k_precomp_au(Physics ph, MeshArgs m, const double *__restrict__ mdot,
@@ -395,6 +403,292 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_temperature_assemble(Physics
     a.diag[c] = at;
 #pragma unroll
     for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
+}
+
+// ------------------------------------------------------ other scalar transports
+// Scalar_solve (FlowSolver.inl:2885-2955) for TE, ED, FUL, PRO, VARF, VARP:
+// FluxScalar (:2516-2744) with the scalar's diffusivity and inlet value, the
+// unsteady term, for TE and ED the k-epsilon sources and wall functions of
+// solveTurbulenceModels (:2746-2883), then setup_sparse_matrix (:1186-1297)
+// with under-relaxation 0.5 (TE, ED) or 0.95.  One thread per cell as in the
+// temperature kernel: the cell's faces in reference face order, then its
+// wall faces again in that order for the wall functions.
+
+namespace {
+
+// Effective diffusivity from Visac = face viscosity - mu (FluxScalar,
+// FlowSolver.inl:2543-2561).
+template <int TYPE>
+__device__ __forceinline__ double scalar_visac(double mu, double v)
+{
+    if (TYPE == SC_TERBTE) return mu + v;
+    if (TYPE == SC_TERBED) return mu + v / 1.219;
+    return (mu + v / 0.9) / 0.9;
+}
+
+// x^1.5 rounded once: s = sqrt(x) is corrected by the exact residual
+// x - s^2 (one Newton step on the square root), and x * s is formed exactly
+// as a sum of two doubles (the FMA product split of Ogita, Rump and Oishi,
+// "Accurate sum and dot product", SIAM J. Sci. Comput. 2005), so the result
+// carries about 100 bits before its single rounding.
+__device__ __forceinline__ double pow_three_halves(double x)
+{
+    const double s = sqrt(x);
+    const double e = fma(-s, s, x);
+    const double c = e / (2.0 * s);
+    const double p = x * s;
+    const double pl = fma(x, s, -p);
+    return p + (pl + x * c);
+}
+
+} // namespace
+
+template <int TYPE>
+__global__ void __launch_bounds__(MCB_THREADS, 4) k_scalar_assemble(Physics ph, MeshArgs m, ScalarArgs a, TurbArgs t)
+{
+    const int N = ph.N;
+    const int c = grid_stride_start();
+    if (c >= N) return;
+    const double xcc = m.xc[c], ycc = m.yc[c], zcc = m.zc[c];
+    double phic = a.phi[c];
+    const double mu = ph.mu;
+    double st = 0.0, at = 0.0, offv[6];
+    unsigned internal = 0u, wall = 0u;
+    for (int k = 0; k < 6; k++) {
+        const int face = m.sface[(size_t)k * N + c];
+        const int c0 = m.fc0[face], c1 = m.fc1[face];
+        const double Sx = m.Sx[face], Sy = m.Sy[face], Sz = m.Sz[face];
+        const double md = a.mdot[face];
+        if (c1 < N) {
+            internal |= 1u << k;
+            const double l0 = m.lam[face];
+            const double l1 = 1.0 - l0;
+            double Visac = mu * l0 + mu * l1;
+            Visac -= mu;
+            Visac = scalar_visac<TYPE>(mu, Visac);
+            const double dx = a.g[0][c0] * l0 + a.g[0][c1] * l1;
+            const double dy = a.g[1][c0] * l0 + a.g[1][c1] * l1;
+            const double dz = a.g[2][c0] * l0 + a.g[2][c1] * l1;
+            const double Xx = m.xc[c1] - m.xc[c0], Xy = m.yc[c1] - m.yc[c0], Xz = m.zc[c1] - m.zc[c0];
+            const double VisFace = Visac * m.rl[face];
+            const double fde1 = Visac * (dx * Sx + dy * Sy + dz * Sz);
+            const double fdi = VisFace * (dx * Xx + dy * Xy + dz * Xz);
+            if (c == c0) {
+                st = st + fde1 - fdi;
+                offv[k] = -VisFace + smin(md, 0.0);
+            } else {
+                st = st - fde1 + fdi;
+                offv[k] = -VisFace - smax(md, 0.0);
+            }
+        } else {
+            offv[k] = 0.0;
+            const int side = c1 - N;
+            const int bt = ph.btype[side];
+            const double dx = a.g[0][c], dy = a.g[1][c], dz = a.g[2][c];
+            const double Xx = m.xf[face] - xcc, Xy = m.yf[face] - ycc, Xz = m.zf[face] - zcc;
+            if (bt == INLET) {
+                const double PhiFace = ph.sc_inlet[TYPE];
+                double Visac = ph.inlet_mu;
+                Visac -= mu;
+                Visac = scalar_visac<TYPE>(mu, Visac);
+                const double VisFace = Visac * m.rl[face];
+                const double fde = Visac * (dx * Sx + dy * Sy + dz * Sz);
+                const double fdi = VisFace * (dx * Xx + dy * Xy + dz * Xz);
+                const double f = -VisFace + smin(md, 0.0);
+                at = at - f;
+                st = st - f * PhiFace + fde - fdi;
+                if (face == ph.last_bface[side]) a.phi[c1] = PhiFace;
+            } else if (bt == OUTLET) {
+                double Visac = mu;
+                Visac -= mu;
+                Visac = scalar_visac<TYPE>(mu, Visac);
+                const double PhiFace = phic + (dx * Xx + dy * Xy + dz * Xz);
+                const double VisFace = Visac * m.rl[face];
+                const double fde = Visac * (dx * Sx + dy * Sy + dz * Sz);
+                const double fdi = VisFace * (dx * Xx + dy * Xy + dz * Xz);
+                st = st + fde - fdi;
+                if (face == ph.last_bface[side]) a.phi[c1] = PhiFace;
+            } else if (bt == WALL) {
+                wall |= 1u << k;
+                if (face == ph.last_bface[side]) a.phi[c1] = phic;
+            }
+        }
+    }
+    const double rho = m.rho[c], vol = m.vol[c];
+    const double f = rho * vol * ph.rdelta;
+    st += f * phic;
+    at += f;
+    if (TYPE == SC_TERBTE) {
+        // production (zero: the turbulent viscosity is mu - mu) and
+        // dissipation, :2754-2775
+        const double uxx = t.gU[0][c], uxy = t.gU[1][c], uxz = t.gU[2][c];
+        const double vxx = t.gV[0][c], vxy = t.gV[1][c], vxz = t.gV[2][c];
+        const double wxx = t.gW[0][c], wxy = t.gW[1][c], wxz = t.gW[2][c];
+        const double s1 = (uxx + uxx) * uxx + (uxy + vxx) * uxy + (uxz + wxx) * uxz;
+        const double s2 = (vxx + uxy) * vxx + (vxy + vxy) * vxy + (vxz + wxy) * vxz;
+        const double s3 = (wxx + uxz) * wxx + (wxy + vxz) * wxy + (wxz + wxz) * wxz;
+        const double VisT = mu - mu;
+        double TP = VisT * (s1 + s2 + s3);
+        const double Dis = rho * t.ED[c];
+        st = st + TP * vol;
+        at = at + Dis / (phic + 0.000000000000000001) * vol;
+        // wall functions, :2778-2822
+        for (int k = 0; k < 6; k++) {
+            if (!((wall >> k) & 1u)) continue;
+            const int face = m.sface[(size_t)k * N + c];
+            st = st - TP * vol;
+            const double Xx = m.xf[face] - xcc, Xy = m.yf[face] - ycc, Xz = m.zf[face] - zcc;
+            const double Upx = t.U[c] - 0., Upy = t.V[c] - 0., Upz = t.W[c] - 0.;
+            const double Sx = m.Sx[face], Sy = m.Sy[face], Sz = m.Sz[face];
+            const double mag = sqrt(Sx * Sx + Sy * Sy + Sz * Sz);
+            const double nx = Sx / mag, ny = Sy / mag, nz = Sz / mag;
+            const double dp = Upx * nx + Upy * ny + Upz * nz;
+            const double Utx = Upx - nx * dp, Uty = Upy - ny * dp, Utz = Upz - nz * dp;
+            const double Uvel = sqrt(Utx * Utx + Uty * Uty + Utz * Utz);
+            const double distance_to_face = sqrt(Xx * Xx + Xy * Xy + Xz * Xz);
+            const double rkapdn = 1.0 / (0.419 * distance_to_face);
+            const double Tau_w = mu * Uvel / distance_to_face;
+            const double Utau = sqrt(Tau_w / rho);
+            TP = Tau_w * Utau * rkapdn;
+            st = st + TP * vol;
+            const double DisP = ph.cmu75 * sqrt(phic) * rkapdn;
+            at = at + rho * DisP * vol;
+        }
+        t.TP[c] = TP;
+    } else if (TYPE == SC_TERBED) {
+        // epsilon sources, :2826-2831
+        const double fact = phic / (t.TE[c] + 0.000000000000000001) * vol;
+        st = st + 1.44 * fact * t.TP[c];
+        at = at + 1.92 * fact * rho;
+        if (wall) {
+            // fixed dissipation at wall cells, their own side of face_fields
+            // zeroed (:2835-2878): the row keeps only its diagonal
+            const double turb = t.TE[c];
+            double Dis = 0.0;
+            for (int k = 0; k < 6; k++) {
+                if (!((wall >> k) & 1u)) continue;
+                const int face = m.sface[(size_t)k * N + c];
+                const double Xx = m.xf[face] - xcc, Xy = m.yf[face] - ycc, Xz = m.zf[face] - zcc;
+                const double distance = sqrt(Xx * Xx + Xy * Xy + Xz * Xz);
+                Dis = ph.cmu75 * pow_three_halves(turb) / (distance * 0.419);
+                const int side = m.fc1[face] - N;
+                if (face == ph.last_bface[side]) a.phi[N + side] = Dis;
+            }
+            phic = Dis;
+            st = Dis;
+            at = 1;
+            for (int k = 0; k < 6; k++) offv[k] = 0.0;
+        }
+    }
+    for (int k = 0; k < 6; k++)
+        if ((internal >> k) & 1u) at -= offv[k];
+    const double URF = (TYPE == SC_TERBTE || TYPE == SC_TERBED) ? 0.5 : 0.95;
+    const double RURF = 1. / URF;
+    at *= RURF;
+    a.b[c] = st + (1.0 - URF) * at * phic;
+    a.diag[c] = at;
+#pragma unroll
+    for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
+}
+
+void launch_scalar_assemble(cudaStream_t s, int type, const Physics &ph, const MeshArgs &m, const ScalarArgs &a,
+                            const TurbArgs &t)
+{
+    const int grid = (ph.N + MCB_THREADS - 1) / MCB_THREADS;
+    switch (type) {
+    case SC_TERBTE: k_scalar_assemble<SC_TERBTE><<<grid, MCB_THREADS, 0, s>>>(ph, m, a, t); break;
+    case SC_TERBED: k_scalar_assemble<SC_TERBED><<<grid, MCB_THREADS, 0, s>>>(ph, m, a, t); break;
+    default: k_scalar_assemble<SC_FUEL><<<grid, MCB_THREADS, 0, s>>>(ph, m, a, t); break;
+    }
+}
+
+// Negative k or epsilon after the solve: list them (unordered, up to cap).
+__global__ void __launch_bounds__(MCB_THREADS) k_scalar_negatives(int N, ClipArgs a)
+{
+    for (int c = grid_stride_start(); c < N; c += gridDim.x * blockDim.x) {
+        if (a.phi[c] < 0.0) {
+            const unsigned int i = atomicAdd(a.count, 1u);
+            if (i < (unsigned int)a.cap) a.list[i] = c;
+        }
+    }
+}
+
+namespace {
+
+// One cell of the reference's loop (FlowSolver.inl:2961-2983): the mean of
+// its internal neighbours' current values, at least 1e-12.
+__device__ void clip_cell(int N, const ClipArgs &a, int c)
+{
+    if (!(a.phi[c] < 0.0)) return;
+    int count = 0;
+    double phisum = 0.0;
+    for (int j = 0; j < 6; j++) {
+        const int nb = a.nbr[(size_t)j * N + c];
+        if (nb >= 0) {
+            count++;
+            phisum += a.phi[nb];
+        }
+    }
+    phisum = (phisum / count);
+    a.phi[c] = smax(phisum, 0.000000000001);
+}
+
+} // namespace
+
+// The listed cells, replaced one at a time in ascending caller order, so a
+// cell sees the replaced values of the earlier cells and the old values of
+// the later ones, as in the reference's sequential loop.  One block: the
+// list (at most 4096 cells) is sorted in shared memory; a longer list falls
+// back to one thread walking every cell in caller order.  Resets the count.
+__global__ void __launch_bounds__(1024) k_scalar_clip(int N, ClipArgs a)
+{
+    constexpr int kCap = 4096;
+    __shared__ int skey[kCap];
+    __shared__ int sval[kCap];
+    const unsigned int cnt = *a.count;
+    if (cnt == 0) return;
+    if (cnt > (unsigned int)a.cap || cnt > (unsigned int)kCap) {
+        if (threadIdx.x == 0) {
+            for (int o = 0; o < N; o++) clip_cell(N, a, a.o2n ? a.o2n[o] : o);
+            *a.count = 0u;
+        }
+        return;
+    }
+    int n2 = 1;
+    while (n2 < (int)cnt) n2 <<= 1;
+    for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+        if (i < (int)cnt) {
+            const int c = a.list[i];
+            skey[i] = a.key ? a.key[c] : c;
+            sval[i] = c;
+        } else {
+            skey[i] = 0x7fffffff;
+            sval[i] = -1;
+        }
+    }
+    __syncthreads();
+    for (int k = 2; k <= n2; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const bool up = (i & k) == 0;
+                    if ((skey[i] > skey[ixj]) == up) {
+                        const int tk = skey[i], tv = sval[i];
+                        skey[i] = skey[ixj];
+                        sval[i] = sval[ixj];
+                        skey[ixj] = tk;
+                        sval[ixj] = tv;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < (int)cnt; i++) clip_cell(N, a, sval[i]);
+        *a.count = 0u;
+    }
 }
 
 // --------------------------------------------------------------- mass flux

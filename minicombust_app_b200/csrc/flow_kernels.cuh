@@ -43,6 +43,25 @@ struct ScalarArgs {
     double *off, *diag, *b;
 };
 
+// Extra inputs of the k and epsilon transports (solveTurbulenceModels).
+struct TurbArgs {
+    const double *U, *V, *W;
+    const double *gU[3], *gV[3], *gW[3];
+    const double *TE, *ED;      // k and epsilon (the one being assembled is also ScalarArgs::phi)
+    double *TP;                 // turbulent production: written by k, read by epsilon
+};
+
+// Replacement of negative k / epsilon values after their solve.
+struct ClipArgs {
+    double *phi;
+    const int *nbr;             // [6][N]
+    const int *key;             // caller's id of each cell (null: identity)
+    const int *o2n;             // caller's id -> cell (null: identity)
+    int *list;                  // [cap] negative cells
+    unsigned int *count;        // zero before the first launch; reset by k_scalar_clip
+    int cap;
+};
+
 struct MassFluxArgs {
     const double *U, *V, *W, *P, *AU;
     const double *gU[3], *gV[3], *gW[3], *gP[3];
@@ -79,6 +98,17 @@ void launch_lsq_gradients1(cudaStream_t s, int N, const int *nbr, const int *fc1
 __global__ void k_precomp_au(Physics ph, MeshArgs m, const double *mdot, double *AU);
 __global__ void k_momentum_assemble(Physics ph, MeshArgs m, MomentumArgs a);
 __global__ void k_temperature_assemble(Physics ph, MeshArgs m, ScalarArgs a);
+// FluxScalar + Scalar_solve assembly of one of TE, ED, FUL, PRO, VARF, VARP
+// (type = SC_*), with the k-epsilon sources for TE and ED.
+void launch_scalar_assemble(cudaStream_t s, int type, const Physics &ph, const MeshArgs &m, const ScalarArgs &a,
+                            const TurbArgs &t);
+void launch_lsq_gradients6(cudaStream_t s, int N, const int *nbr, const int *fc1, const double *xc,
+                           const double *yc, const double *zc, const double *xf, const double *yf, const double *zf,
+                           const GradArgs<6> &a);
+// Negative k / epsilon values after the solve (FlowSolver.inl:2956-2985):
+// list them, then replace them one at a time in the caller's cell order.
+__global__ void k_scalar_negatives(int N, ClipArgs a);
+__global__ void k_scalar_clip(int N, ClipArgs a);
 __global__ void k_mass_flux(Physics ph, MeshArgs m, MassFluxArgs a);
 __global__ void k_outlet_fix(Physics ph, MeshArgs m, double *mdot, double *U, double *V, double *W,
                              const FluxBalance *bal);

@@ -48,7 +48,15 @@ struct Physics {
     int cell0;            // the handle's id of the reference's cell 0
     double mu, inlet_mu, u_in, rho_in, T_ref, rdelta;
     double urf_u, urf_T, urf_p, flux_corr;
+    // scalar transports: inlet value per scalar type (SC_*), computed on the
+    // host as the reference computes it (FlowSolver.inl:2625-2659), and
+    // Cmu^0.75 of the k-epsilon wall functions (:2786, :2834)
+    double sc_inlet[7];
+    double cmu75;
 };
+
+// Scalar types of Scalar_solve (the reference's utils.hpp:31-37).
+enum ScalarType { SC_TERBTE = 0, SC_TERBED = 1, SC_TEMP = 2, SC_FUEL = 3, SC_PROG = 4, SC_VARFU = 5, SC_VARPR = 6 };
 
 // Balance of boundary fluxes (calculate_mass_flux, FlowSolver.inl:2010-2079).
 struct FluxBalance {

@@ -5,9 +5,11 @@
 // kernels (k_bicg_init/1/2/3 with one right-hand side, as in the temperature
 // stage) on a system the caller owns, with every scratch byte taken from the
 // file-scope array below instead.  It exists for callers that must not
-// allocate device memory: code that issues work while a stream capture is in
-// progress (cudaMalloc is not permitted there), and hosts whose device memory
-// is owned by a pool or a fixed budget they manage themselves.
+// allocate device memory: hosts that reserve all device memory for their own
+// pool or fixed budget at start-up (a library cudaMalloc would then fail, or
+// take memory the host has promised elsewhere), and callers inside a
+// time-critical loop, where cudaMalloc/cudaFree can synchronise the device and
+// stall their other streams.
 //
 // Limits and sharing:
 //   - at most MC_SOLVE_NOALLOC_MAX_ROWS rows; the array holds 8 vectors of that
@@ -17,21 +19,28 @@
 //     different streams or host threads) race; the status counter is cleared
 //     at the start of each call, and every vector is initialised by the solve;
 //   - the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (once per device, with that device current); make
-//     that first call before any stream capture.
+//     cudaGetSymbolAddress (once per device, with that device current).
 #include <cuda_runtime.h>
 
 #include <mutex>
 
 #include "krylov.cuh"
+#include "mc_reduce.cuh"
 #include "minicombust_flow.h"
 
 namespace {
 
 constexpr int kMaxRows = MC_SOLVE_NOALLOC_MAX_ROWS;
 constexpr int kVectors = 8;                       // r, r0, p[2], v[2], s, t
-constexpr int kMaxBlocks = (kMaxRows + 255) / 256;  // grid of the Krylov kernels for kMaxRows rows
+// The Krylov kernels run MCB_THREADS threads per block and at most one block
+// per MCB_THREADS rows (krylov_grid), so kMaxRows rows need at most kMaxBlocks
+// blocks; the single-system BiCGStab kernels publish at most 2 partials per
+// block (publish_partials<2 * R>, R = 1).  The call also checks krylov_grid(n)
+// against kMaxBlocks at run time.
+constexpr int kMaxBlocks = (kMaxRows + MCB_THREADS - 1) / MCB_THREADS;
 constexpr int kPartialsPerBlock = 8;
+static_assert(MCB_THREADS == 256, "scratch partitioning assumes 256-thread Krylov blocks");
+static_assert(kPartialsPerBlock >= 2, "BiCGStab with one right-hand side publishes 2 partials per block");
 constexpr size_t kStatusDoubles = 64;             // counter (first 8 bytes) + BicgState<1>
 constexpr size_t kScratchDoubles =
     (size_t)kVectors * kMaxRows + (size_t)kMaxBlocks * kPartialsPerBlock + kStatusDoubles;
@@ -68,6 +77,7 @@ extern "C" int mc_solve_bicgstab_noalloc(int n, const double *diag, const double
 {
     if (n <= 0 || n > kMaxRows) return MC_ERR_ARG;  // larger systems need the handle-based solver
     if (!diag || !off || !col || !b || !x || !(rtol > 0.0) || max_iters <= 0) return MC_ERR_ARG;
+    if (mcb::krylov_grid(n) > kMaxBlocks) return MC_ERR_UNSUPPORTED;  // partials would not fit
     double *base = nullptr;
     int rc = scratch_for_current_device(&base);
     if (rc != MC_OK) return rc;

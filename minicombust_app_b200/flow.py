@@ -39,6 +39,17 @@ PRECISION_FP64, PRECISION_FP32_REFINED = 0, 1
 REORDER_NONE, REORDER_RCM = 0, 1
 GUESS_ZERO, GUESS_PREVIOUS, GUESS_LEARNED = 0, 1, 2
 SNAPSHOT_MAGIC = b"MCSNAP01"
+HEADER_PATH = os.path.join(os.path.dirname(_PKG), "include", "minicombust_flow.h")
+
+
+def header_define(name, path=HEADER_PATH):
+    """Integer value of a ``#define`` in the C header (ctypes cannot see macros)."""
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 3 and parts[0] == "#define" and parts[1] == name:
+                return int(parts[2])
+    raise KeyError(f"{name} is not defined in {path}")
 
 
 def read_snapshots(path):
@@ -76,14 +87,15 @@ class FlowParams(ctypes.Structure):
                 ("pressure_solver", c_int), ("precision", c_int), ("initial_guess", c_int), ("device", c_int),
                 ("amg_sweeps", c_int), ("amg_omega", c_dbl), ("amg_alpha", c_dbl), ("ir_inner_rtol", c_dbl),
                 ("reorder", c_int), ("ir_inner_rtol_bicg", c_dbl),
-                ("amg_cheb_ratio", c_dbl)]
+                ("amg_cheb_ratio", c_dbl), ("transport_scalars", c_int)]
 
 
 class IterStats(ctypes.Structure):
     _fields_ = [("momentum_iters", c_int * 3), ("temperature_iters", c_int), ("pressure_solves", c_int),
                 ("pressure_iters_total", c_int), ("pressure_iters_first", c_int),
                 ("pressure_correction_max_first", c_dbl), ("pressure_rel_residual", c_dbl),
-                ("mass_imbalance", c_dbl), ("guess_choice_first", c_int), ("guess_rel_residual_first", c_dbl)]
+                ("mass_imbalance", c_dbl), ("guess_choice_first", c_int), ("guess_rel_residual_first", c_dbl),
+                ("pressure_rel_residual_first", c_dbl), ("scalar_iters", c_int * 6)]
 
     def as_dict(self):
         return {"momentum_iters": list(self.momentum_iters), "temperature_iters": self.temperature_iters,
@@ -92,7 +104,9 @@ class IterStats(ctypes.Structure):
                 "pressure_correction_max_first": self.pressure_correction_max_first,
                 "pressure_rel_residual": self.pressure_rel_residual, "mass_imbalance": self.mass_imbalance,
                 "guess_choice_first": self.guess_choice_first,
-                "guess_rel_residual_first": self.guess_rel_residual_first}
+                "guess_rel_residual_first": self.guess_rel_residual_first,
+                "pressure_rel_residual_first": self.pressure_rel_residual_first,
+                "scalar_iters": list(self.scalar_iters)}
 
 
 class FlowError(RuntimeError):
@@ -124,6 +138,7 @@ _SIGNATURES = {
     "mc_flow_stage_momentum": (c_int, [c_vp, ctypes.POINTER(IterStats)]),
     "mc_flow_stage_pressure": (c_int, [c_vp, ctypes.POINTER(IterStats)]),
     "mc_flow_stage_temperature": (c_int, [c_vp, ctypes.POINTER(IterStats)]),
+    "mc_flow_stage_scalar": (c_int, [c_vp, c_int, ctypes.POINTER(IterStats)]),
     "mc_flow_set_timing": (c_int, [c_vp, c_int]),
     "mc_flow_kernel_count": (c_int, []),
     "mc_flow_kernel_name": (ctypes.c_char_p, [c_int]),
@@ -390,6 +405,11 @@ class FlowSolver:
               "pressure": lambda: self.L.mc_flow_stage_pressure(self.h, ctypes.byref(s)),
               "temperature": lambda: self.L.mc_flow_stage_temperature(self.h, ctypes.byref(s))}[name]
         _check(fn(), self.h, name)
+
+    def stage_scalar(self, name):
+        """Scalar_solve for one transported field: TE, ED, TEM, FUL, PRO, VARF or VARP."""
+        _check(self.L.mc_flow_stage_scalar(self.h, FIELDS[name], ctypes.byref(self.last_stats)), self.h,
+               f"stage_scalar({name})")
 
     # --- instrumentation --------------------------------------------------
     def set_timing(self, on):

@@ -49,6 +49,7 @@ struct mco_solver {
     const uint64_t *faces;      /* borrowed from the mesh: [F][2] */
     const uint64_t *cell_faces; /* [N][6] */
     const double *cc;           /* [N][3] */
+    const uint64_t *cell_nbrs;  /* [N][6], MESH_BOUNDARY on the domain boundary */
     uint64_t btype[6];
     double *farea, *flam, *frl, *fnorm, *fcen; /* face geometry */
     double *vol, *rho;
@@ -371,6 +372,7 @@ mco_solver *mco_create(const mco_mesh *m, const mco_params *prm)
     s->faces = m->face_cells;
     s->cell_faces = m->cell_faces;
     s->cc = m->cell_centers;
+    s->cell_nbrs = m->cell_neighbours;
     memcpy(s->btype, m->boundary_types, sizeof(s->btype));
     s->farea = (double *)calloc(F, sizeof(double));
     s->flam = (double *)calloc(F, sizeof(double));
@@ -380,8 +382,9 @@ mco_solver *mco_create(const mco_mesh *m, const mco_params *prm)
     s->vol = (double *)calloc(N, sizeof(double));
     s->rho = (double *)calloc(N, sizeof(double));
     for (int k = 0; k < MCO_NFIELDS; k++) s->phi[k] = (double *)calloc(N + 6, sizeof(double));
-    const int gfields[6] = {MCO_U, MCO_V, MCO_W, MCO_P, MCO_PP, MCO_TEM};
-    for (int k = 0; k < 6; k++) s->grad[gfields[k]] = (double *)calloc(3 * N, sizeof(double));
+    const int gfields[12] = {MCO_U, MCO_V, MCO_W, MCO_P, MCO_PP, MCO_TEM,
+                             MCO_TE, MCO_ED, MCO_FUL, MCO_PRO, MCO_VARF, MCO_VARP};
+    for (int k = 0; k < (prm->scalars ? 12 : 6); k++) s->grad[gfields[k]] = (double *)calloc(3 * N, sizeof(double));
     s->AU = (double *)calloc(N + 6, sizeof(double));
     s->AV = (double *)calloc(N + 6, sizeof(double));
     s->AW = (double *)calloc(N + 6, sizeof(double));
@@ -468,6 +471,22 @@ mco_solver *mco_create(const mco_mesh *m, const mco_params *prm)
         s->phi[MCO_P][i] = prm->pressure0;
         s->phi[MCO_PP][i] = 0.0;
         s->phi[MCO_TEM][i] = prm->temperature0;
+        /* the other scalars: defaults, then per boundary type */
+        double te = 0.0001, ed = 0.0, ful = 0.1, pro = 0.001, varf = 0.1, varp = 0.001;
+        if (t == INLET) {
+            te = 3.0 / 2.0 * ((0.1 * 0.1) * velmag2);
+            ed = pow(0.09, 0.75) * pow(te, 1.5);
+            ful = 0.1; pro = 0.0; varf = 0.1; varp = 0.0;
+        } else if (t == WALL) {
+            ful = 0.0; pro = 0.0; varf = 0.0; varp = 0.0;
+        }
+        s->phi[MCO_TE][i] = te;
+        s->phi[MCO_ED][i] = ed;
+        s->phi[MCO_TP][i] = 0.0;
+        s->phi[MCO_FUL][i] = ful;
+        s->phi[MCO_PRO][i] = pro;
+        s->phi[MCO_VARF][i] = varf;
+        s->phi[MCO_VARP][i] = varp;
     }
     s->first_pressure = 1;
     return s;
@@ -628,6 +647,11 @@ void mco_stage_gradients(mco_solver *s)
     static const int fields[5] = {MCO_U, MCO_V, MCO_W, MCO_P, MCO_TEM};
     static const int zb[5] = {0, 0, 0, 1, 0};
     lsq_gradients(s, fields, zb, 5);
+    if (s->prm.scalars) {
+        static const int more[6] = {MCO_TE, MCO_ED, MCO_FUL, MCO_PRO, MCO_VARF, MCO_VARP};
+        static const int zb6[6] = {0, 0, 0, 0, 0, 0};
+        lsq_gradients(s, more, zb6, 6);
+    }
 }
 
 static void single_gradient_pressure(mco_solver *s, int field)
@@ -1135,16 +1159,57 @@ int mco_stage_calculate_pressure(mco_solver *s)
     return bad ? -1 : 0;
 }
 
-/* ------------------------------------------------------------- temperature */
+/* --------------------------------------------------------- scalar transports */
 
-/* FluxScalar for TEMP (FlowSolver.inl:2516-2744) */
-static void flux_scalar_temperature(mco_solver *s)
+/* Scalar types of Scalar_solve (utils.hpp:31-37). */
+enum { SC_TERBTE = 0, SC_TERBED = 1, SC_TEMP = 2, SC_FUEL = 3, SC_PROG = 4, SC_VARFU = 5, SC_VARPR = 6 };
+
+static int scalar_type_of_field(int field)
+{
+    switch (field) {
+    case MCO_TE: return SC_TERBTE;
+    case MCO_ED: return SC_TERBED;
+    case MCO_TEM: return SC_TEMP;
+    case MCO_FUL: return SC_FUEL;
+    case MCO_PRO: return SC_PROG;
+    case MCO_VARF: return SC_VARFU;
+    case MCO_VARP: return SC_VARPR;
+    default: return -1;
+    }
+}
+
+/* Effective diffusivity of a scalar from Visac = (face viscosity - mu)
+ * (FluxScalar, FlowSolver.inl:2543-2561, repeated at :2663-2681 and :2703-2721). */
+static double scalar_visac(int type, double mu, double Visac)
+{
+    if (type == SC_TEMP) return (mu + Visac / 0.9) / 0.6905;
+    if (type == SC_TERBTE) return mu + Visac;
+    if (type == SC_TERBED) return mu + Visac / 1.219;
+    return (mu + Visac / 0.9) / 0.9;
+}
+
+/* Inlet value of a scalar (FluxScalar, FlowSolver.inl:2625-2659). */
+static double scalar_inlet(const mco_solver *s, int type)
+{
+    const double velmag2 = pow(s->prm.inlet_u, 2) + pow(0.0, 2) + pow(0.0, 2);
+    switch (type) {
+    case SC_TEMP: return s->prm.temperature0;
+    case SC_TERBTE: return 3.0 / 2.0 * ((0.1 * 0.1) * velmag2);
+    case SC_TERBED: return pow(0.09, 0.75) * pow((3.0 / 2.0 * ((0.1 * 0.1) * velmag2)), 1.5);
+    case SC_FUEL: return 0.1;
+    case SC_VARFU: return 0.1;
+    default: return 0.0; /* PROG, VARPR */
+    }
+}
+
+/* FluxScalar (FlowSolver.inl:2516-2744): implicit upwind convection and
+ * diffusion into face_fields, explicit diffusion into S_phi.U, boundary
+ * values and inlet coefficients into A_phi.V. */
+static void flux_scalar(mco_solver *s, int type, double *phi, const double *g)
 {
     const uint64_t N = s->N;
     const double mu = s->eff_visc;
     const double GammaBlend = 0.0;
-    double *T = s->phi[MCO_TEM];
-    const double *gT = s->grad[MCO_TEM];
     for (uint64_t face = 0; face < s->F; face++) {
         const uint64_t c0 = s->faces[2 * face], c1 = s->faces[2 * face + 1];
         const v3 S = ld3(s->fnorm, face);
@@ -1154,14 +1219,14 @@ static void flux_scalar_temperature(mco_solver *s)
             const double lambda1 = 1.0 - lambda0;
             double Visac = mu * lambda0 + mu * lambda1;
             Visac -= mu;
-            Visac = (mu + Visac / 0.9) / 0.6905;
-            const v3 dPhi = vadd(vscale(ld3(gT, c0), lambda0), vscale(ld3(gT, c1), lambda1));
+            Visac = scalar_visac(type, mu, Visac);
+            const v3 dPhi = vadd(vscale(ld3(g, c0), lambda0), vscale(ld3(g, c1), lambda1));
             const v3 Xpn = vsub(ld3(s->cc, c1), ld3(s->cc, c0));
             const double VisFace = Visac * s->frl[face];
-            const double PhiFace = (md >= 0.0) ? T[c0] : T[c1];
+            const double PhiFace = (md >= 0.0) ? phi[c0] : phi[c1];
             const double fce = md * PhiFace;
             const double fde1 = Visac * vdot(dPhi, S);
-            const double fci = smin(md, 0.0) * T[c0] + smax(md, 0.0) * T[c1];
+            const double fci = smin(md, 0.0) * phi[c0] + smax(md, 0.0) * phi[c1];
             const double fdi = VisFace * vdot(dPhi, Xpn);
             s->ff[2 * face] = -VisFace - smax(md, 0.0);
             s->ff[2 * face + 1] = -VisFace + smin(md, 0.0);
@@ -1171,57 +1236,167 @@ static void flux_scalar_temperature(mco_solver *s)
         } else {
             const uint64_t bc = c1 - N;
             const int t = (int)s->btype[bc];
-            const v3 dPhi = ld3(gT, c0);
+            const v3 dPhi = ld3(g, c0);
             const v3 Xpn = vsub(ld3(s->fcen, face), ld3(s->cc, c0));
             if (t == INLET) {
-                const double PhiFace = s->prm.temperature0;
+                const double PhiFace = scalar_inlet(s, type);
                 double Visac = s->inlet_eff_visc;
                 Visac -= mu;
-                Visac = (mu + Visac / 0.9) / 0.6905;
+                Visac = scalar_visac(type, mu, Visac);
                 const double VisFace = Visac * s->frl[face];
                 const double fde = Visac * vdot(dPhi, S);
                 const double fdi = VisFace * vdot(dPhi, Xpn);
                 const double f = -VisFace + smin(md, 0.0);
                 s->AV[c0] = s->AV[c0] - f;
                 s->SU[c0] = s->SU[c0] - f * PhiFace + fde - fdi;
-                T[N + bc] = PhiFace;
+                phi[N + bc] = PhiFace;
             } else if (t == OUTLET) {
                 double Visac = mu;
                 Visac -= mu;
-                Visac = (mu + Visac / 0.9) / 0.6905;
-                const double PhiFace = T[c0] + vdot(dPhi, Xpn);
+                Visac = scalar_visac(type, mu, Visac);
+                const double PhiFace = phi[c0] + vdot(dPhi, Xpn);
                 const double VisFace = Visac * s->frl[face];
                 const double fde = Visac * vdot(dPhi, S);
                 const double fdi = VisFace * vdot(dPhi, Xpn);
                 s->SU[c0] = s->SU[c0] + fde - fdi;
-                T[N + bc] = PhiFace;
+                phi[N + bc] = PhiFace;
             } else if (t == WALL) {
-                T[N + bc] = T[c0];
+                /* the reference's condition (type != TERBTE or type != TERBED) always holds */
+                phi[N + bc] = phi[c0];
             }
         }
     }
 }
 
-/* Scalar_solve(TEMP, ...) (FlowSolver.inl:2885-3076); simple mode adds the
- * particle energy the reference leaves commented out (:2919-2925). */
-int mco_stage_scalar_temperature(mco_solver *s)
+/* solveTurbulenceModels (FlowSolver.inl:2746-2883): k production and
+ * dissipation with the wall-function production at wall cells (TERBTE);
+ * epsilon sources and the fixed wall-cell dissipation, whose rows are
+ * decoupled by zeroing their side of face_fields (TERBED). */
+static void solve_turbulence(mco_solver *s, int type)
 {
     const uint64_t N = s->N;
+    const double mu = s->eff_visc;
+    double *TE = s->phi[MCO_TE], *ED = s->phi[MCO_ED], *TP = s->phi[MCO_TP];
+    const double Cmu = 0.09;
+    const double Cmu75 = pow(Cmu, 0.75);
+    if (type == SC_TERBTE) {
+        const double *gU = s->grad[MCO_U], *gV = s->grad[MCO_V], *gW = s->grad[MCO_W];
+        for (uint64_t i = 0; i < N; i++) {
+            const v3 dU = ld3(gU, i), dV = ld3(gV, i), dW = ld3(gW, i);
+            const double s1 = (dU.x + dU.x) * dU.x + (dU.y + dV.x) * dU.y + (dU.z + dW.x) * dU.z;
+            const double s2 = (dV.x + dU.y) * dV.x + (dV.y + dV.y) * dV.y + (dV.z + dW.y) * dV.z;
+            const double s3 = (dW.x + dU.z) * dW.x + (dW.y + dV.z) * dW.y + (dW.z + dW.z) * dW.z;
+            const double VisT = mu - mu;
+            const double Pk = VisT * (s1 + s2 + s3);
+            TP[i] = Pk;
+            const double Dis = s->rho[i] * ED[i];
+            s->SU[i] = s->SU[i] + TP[i] * s->vol[i];
+            s->AV[i] = s->AV[i] + Dis / (TE[i] + 0.000000000000000001) * s->vol[i];
+        }
+        for (uint64_t face = 0; face < s->F; face++) {
+            const uint64_t c0 = s->faces[2 * face], c1 = s->faces[2 * face + 1];
+            if (c1 < N) continue;
+            const uint64_t bc = c1 - N;
+            if ((int)s->btype[bc] != WALL) continue;
+            s->SU[c0] = s->SU[c0] - TP[c0] * s->vol[c0];
+            const double Visc = mu;
+            const v3 Xpn = vsub(ld3(s->fcen, face), ld3(s->cc, c0));
+            const v3 Up = mk(s->phi[MCO_U][c0] - 0., s->phi[MCO_V][c0] - 0., s->phi[MCO_W][c0] - 0.);
+            const v3 nrm = vnorm(ld3(s->fnorm, face));
+            const double dp = vdot(Up, nrm);
+            const v3 Ut = vsub(Up, vscale(nrm, dp));
+            const double Uvel = sqrt(vdot(Ut, Ut));
+            const double distance_to_face = vmag(Xpn);
+            const double rkapdn = 1.0 / (0.419 * distance_to_face);
+            const double Tau_w = Visc * Uvel / distance_to_face;
+            const double Utau = sqrt(Tau_w / s->rho[c0]);
+            TP[c0] = Tau_w * Utau * rkapdn;
+            TE[N + bc] = TE[c0];
+            s->SU[c0] = s->SU[c0] + TP[c0] * s->vol[c0];
+            const double DisP = Cmu75 * sqrt(TE[c0]) * rkapdn;
+            s->AV[c0] = s->AV[c0] + s->rho[c0] * DisP * s->vol[c0];
+        }
+    } else if (type == SC_TERBED) {
+        for (uint64_t i = 0; i < N; i++) {
+            const double fact = ED[i] / (TE[i] + 0.000000000000000001) * s->vol[i];
+            s->SU[i] = s->SU[i] + 1.44 * fact * TP[i];
+            s->AV[i] = s->AV[i] + 1.92 * fact * s->rho[i];
+        }
+        for (uint64_t face = 0; face < s->F; face++) {
+            const uint64_t c0 = s->faces[2 * face], c1 = s->faces[2 * face + 1];
+            if (c1 < N) continue;
+            const uint64_t bc = c1 - N;
+            if ((int)s->btype[bc] != WALL) continue;
+            const double turb = TE[c0];
+            const double distance = vmag(vsub(ld3(s->fcen, face), ld3(s->cc, c0)));
+            const double Dis = Cmu75 * pow(turb, 1.5) / (distance * 0.419);
+            for (int j = 0; j < 6; j++) {
+                const uint64_t nf = s->cell_faces[6 * c0 + j];
+                const uint64_t a = s->faces[2 * nf], b = s->faces[2 * nf + 1];
+                if (a < N && b < N) {
+                    if (a == c0) s->ff[2 * nf + 1] = 0.0;
+                    else if (b == c0) s->ff[2 * nf] = 0.0;
+                }
+            }
+            ED[c0] = Dis;
+            s->SU[c0] = Dis;
+            s->AV[c0] = 1;
+            ED[N + bc] = ED[c0];
+        }
+    }
+}
+
+/* Scalar_solve (FlowSolver.inl:2885-3076) for one scalar: fluxes, the
+ * unsteady term, turbulence sources, the system with its under-relaxation,
+ * BiCGStab, and for k and epsilon the replacement of negative values by the
+ * mean of the internal neighbours (:2956-2985).  Simple mode adds the
+ * particle energy to T (left commented out in the reference, :2919-2925). */
+int mco_stage_scalar(mco_solver *s, int field)
+{
+    const int type = scalar_type_of_field(field);
+    if (type < 0 || !s->grad[field]) return -1;
+    const uint64_t N = s->N;
+    double *phi = s->phi[field];
     for (uint64_t i = 0; i < N; i++) { s->AV[i] = 0.0; s->SU[i] = 0.0; }
-    flux_scalar_temperature(s);
+    flux_scalar(s, type, phi, s->grad[field]);
     const double rdelta = 1.0 / s->prm.delta;
-    double *T = s->phi[MCO_TEM];
     for (uint64_t i = 0; i < N; i++) {
         const double f = s->rho[i] * s->vol[i] * rdelta;
-        s->SU[i] += f * T[i];
+        s->SU[i] += f * phi[i];
         s->AV[i] += f;
     }
-    if (s->prm.mode == MCO_MODE_SIMPLE)
+    if (type == SC_TEMP && s->prm.mode == MCO_MODE_SIMPLE)
         for (uint64_t i = 0; i < N; i++) s->SU[i] += s->src[5 * i + 3];
-    setup_sparse_matrix(s, s->prm.urf_temperature, s->AV, T, s->SU);
-    s->stats.temperature_iters = solve_sparse_matrix(s, T);
-    return s->stats.temperature_iters < 0 ? -1 : 0;
+    if (type == SC_TERBTE || type == SC_TERBED) solve_turbulence(s, type);
+    double underrelax;
+    if (type == SC_TERBTE || type == SC_TERBED) underrelax = 0.5;
+    else if (type == SC_TEMP) underrelax = s->prm.urf_temperature;
+    else underrelax = 0.95;
+    setup_sparse_matrix(s, underrelax, s->AV, phi, s->SU);
+    const int its = solve_sparse_matrix(s, phi);
+    if (type == SC_TERBTE || type == SC_TERBED) {
+        for (uint64_t i = 0; i < N; i++) {
+            int count = 0;
+            double phisum = 0.0;
+            if (phi[i] < 0.0) {
+                for (int j = 0; j < 6; j++) {
+                    const uint64_t nb = s->cell_nbrs[6 * i + j];
+                    if (nb < N) {
+                        count++;
+                        phisum += phi[nb];
+                    }
+                }
+                phisum = (phisum / count);
+                phi[i] = smax(phisum, 0.000000000001);
+            }
+        }
+    }
+    if (type == SC_TEMP) s->stats.temperature_iters = its;
+    else s->stats.scalar_iters[type < SC_TEMP ? type : type - 1] = its;
+    return its < 0 ? -1 : 0;
 }
+
+int mco_stage_scalar_temperature(mco_solver *s) { return mco_stage_scalar(s, MCO_TEM); }
 
 /* ---------------------------------------------------------------- the pass */
 
@@ -1243,10 +1418,10 @@ static double mass_imbalance(const mco_solver *s)
     return m;
 }
 
-/* One iteration of the loop in FlowSolver::timestep (FlowSolver.inl:3188-3268)
- * for the coupled fields.  The six other scalar transports and the FGM lookup
- * are not restated: they read u, v, w, p, T but write nothing that the
- * coupled fields read before it is recomputed. */
+/* One iteration of the loop in FlowSolver::timestep (FlowSolver.inl:3188-3268):
+ * the coupled fields, and with params.scalars the other six scalar transports
+ * in the reference's order.  The FGM lookup (:1138-1184) is not restated: it
+ * only writes S_phi.U, which every later stage zeroes before use. */
 int mco_pass(mco_solver *s)
 {
     const int i = s->pass_in_step;
@@ -1256,7 +1431,12 @@ int mco_pass(mco_solver *s)
     int rc = 0;
     rc |= mco_stage_calculate_uvw(s);
     rc |= mco_stage_calculate_pressure(s);
-    rc |= mco_stage_scalar_temperature(s);
+    if (s->prm.scalars) {
+        static const int order[7] = {MCO_TE, MCO_ED, MCO_TEM, MCO_FUL, MCO_PRO, MCO_VARF, MCO_VARP};
+        for (int k = 0; k < 7; k++) rc |= mco_stage_scalar(s, order[k]);
+    } else {
+        rc |= mco_stage_scalar_temperature(s);
+    }
     s->stats.mass_imbalance = mass_imbalance(s);
     s->pass_in_step++;
     if (s->pass_in_step == 3) {

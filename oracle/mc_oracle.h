@@ -7,8 +7,10 @@
  *
  * It restates, function by function, the reference CPU FlowSolver
  * (include/flow/FlowSolver.{hpp,inl}) and mesh builder
- * (src/examples/mesh_examples.cpp), for the fields the SIMPLE pass couples:
- * u, v, w, p, the pressure correction and T.  Each function in mc_oracle.c
+ * (src/examples/mesh_examples.cpp): the fields the SIMPLE pass couples (u, v,
+ * w, p, the pressure correction and T) and, with params.scalars, the other
+ * scalar transports (k, epsilon, mixture fraction, progress variable and the
+ * two variances).  Each function in mc_oracle.c
  * cites the reference lines it follows.  Two modes:
  *
  *   MCO_MODE_COMPAT  the reference's control flow, constants and quirks
@@ -58,6 +60,7 @@ typedef struct mco_params {
     double u_rtol;         /* momentum and temperature BiCGStab tolerance */
     double p_rtol;         /* pressure-correction CG tolerance */
     int max_iters;
+    int scalars;           /* 1: also the six other scalar transports (TE, ED, FUL, PRO, VARF, VARP) */
 } mco_params;
 
 typedef struct mco_mesh {
@@ -106,6 +109,9 @@ void mco_stage_set_up_field(mco_solver *s);
 int mco_stage_calculate_uvw(mco_solver *s);
 int mco_stage_calculate_pressure(mco_solver *s);
 int mco_stage_scalar_temperature(mco_solver *s);
+/* Scalar_solve for one scalar field: MCO_TE, MCO_ED, MCO_TEM, MCO_FUL, MCO_PRO,
+ * MCO_VARF or MCO_VARP (the six other than MCO_TEM need params.scalars). */
+int mco_stage_scalar(mco_solver *s, int field);
 
 typedef struct mco_stats {
     int momentum_iters[3];
@@ -115,6 +121,7 @@ typedef struct mco_stats {
     int pressure_iters_first;
     double pressure_correction_max_first;
     double mass_imbalance;        /* ||div(mdot) - sources||_inf after the pass */
+    int scalar_iters[6];          /* TE, ED, FUL, PRO, VARF, VARP */
 } mco_stats;
 void mco_get_stats(const mco_solver *s, mco_stats *out);
 double mco_inlet_effective_viscosity(const mco_solver *s);

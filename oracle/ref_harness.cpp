@@ -296,6 +296,22 @@ void mcref_stage_scalar_temperature(void *vh)
     FlowSolver<double> *s = ((RefHandle *)vh)->solver;
     s->Scalar_solve(TEMP, s->phi.TEM, s->phi_grad.TEM);
 }
+// Scalar_solve for one transported field (phi_vector member index:
+// 5 TE, 6 ED, 8 TEM, 9 FUL, 10 PRO, 11 VARF, 12 VARP).
+int mcref_stage_scalar(void *vh, int field)
+{
+    FlowSolver<double> *s = ((RefHandle *)vh)->solver;
+    switch (field) {
+    case 5: s->Scalar_solve(TERBTE, s->phi.TE, s->phi_grad.TE); return 0;
+    case 6: s->Scalar_solve(TERBED, s->phi.ED, s->phi_grad.ED); return 0;
+    case 8: s->Scalar_solve(TEMP, s->phi.TEM, s->phi_grad.TEM); return 0;
+    case 9: s->Scalar_solve(FUEL, s->phi.FUL, s->phi_grad.FUL); return 0;
+    case 10: s->Scalar_solve(PROG, s->phi.PRO, s->phi_grad.PRO); return 0;
+    case 11: s->Scalar_solve(VARFU, s->phi.VARF, s->phi_grad.VARF); return 0;
+    case 12: s->Scalar_solve(VARPR, s->phi.VARP, s->phi_grad.VARP); return 0;
+    default: return -1;
+    }
+}
 int mcref_first_pressure(void *vh) { return ((RefHandle *)vh)->solver->first_pressure ? 1 : 0; }
 uint64_t mcref_timestep_count(void *vh) { return ((RefHandle *)vh)->solver->timestep_count; }
 double mcref_inlet_effective_viscosity(void *vh) { return ((RefHandle *)vh)->solver->inlet_effective_viscosity; }

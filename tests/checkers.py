@@ -56,7 +56,8 @@ class _McoParams(ctypes.Structure):
     _fields_ = [("mode", c_int), ("delta", c_dbl), ("density", c_dbl), ("viscosity", c_dbl),
                 ("inlet_u", c_dbl), ("pressure0", c_dbl), ("temperature0", c_dbl),
                 ("urf_momentum", c_dbl), ("urf_pressure", c_dbl), ("urf_temperature", c_dbl),
-                ("flux_corr", c_dbl), ("u_rtol", c_dbl), ("p_rtol", c_dbl), ("max_iters", c_int)]
+                ("flux_corr", c_dbl), ("u_rtol", c_dbl), ("p_rtol", c_dbl), ("max_iters", c_int),
+                ("scalars", c_int)]
 
 
 class _McoMesh(ctypes.Structure):
@@ -70,7 +71,7 @@ class _McoMesh(ctypes.Structure):
 class _McoStats(ctypes.Structure):
     _fields_ = [("momentum_iters", c_int * 3), ("temperature_iters", c_int), ("pressure_solves", c_int),
                 ("pressure_iters_total", c_int), ("pressure_iters_first", c_int),
-                ("pressure_correction_max_first", c_dbl), ("mass_imbalance", c_dbl)]
+                ("pressure_correction_max_first", c_dbl), ("mass_imbalance", c_dbl), ("scalar_iters", c_int * 6)]
 
 
 _oracle_lib = None
@@ -97,6 +98,8 @@ def oracle_lib():
             getattr(L, fn).restype = c_int
         for fn in ("mco_stage_gradients", "mco_stage_set_up_field"):
             getattr(L, fn).argtypes = [c_vp]
+        L.mco_stage_scalar.argtypes = [c_vp, c_int]
+        L.mco_stage_scalar.restype = c_int
         L.mco_get_stats.argtypes = [c_vp, ctypes.POINTER(_McoStats)]
         L.mco_inlet_effective_viscosity.argtypes = [c_vp]
         L.mco_inlet_effective_viscosity.restype = c_dbl
@@ -217,6 +220,9 @@ class Oracle:
     def step(self):
         return self.L.mco_pass(self.h)
 
+    def stage_scalar(self, name):
+        return self.L.mco_stage_scalar(self.h, FIELDS[name])
+
     def stats(self):
         s = _McoStats()
         self.L.mco_get_stats(self.h, ctypes.byref(s))
@@ -249,6 +255,8 @@ def ref_lib():
             getattr(L, fn).restype = c_int
         L.mcref_get_csr.argtypes = [c_vp, c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int), c_vp, c_vp, c_vp]
         L.mcref_first_pressure.argtypes = [c_vp]
+        L.mcref_stage_scalar.argtypes = [c_vp, c_int]
+        L.mcref_stage_scalar.restype = c_int
         L.mcref_timestep_count.argtypes = [c_vp]
         L.mcref_timestep_count.restype = c_u64
         L.mcref_inlet_effective_viscosity.argtypes = [c_vp]
@@ -336,6 +344,9 @@ class Reference:
 
     def timestep(self):
         self.L.mcref_timestep(self.h)
+
+    def stage_scalar(self, name):
+        assert self.L.mcref_stage_scalar(self.h, FIELDS[name]) == 0
 
     def inlet_effective_viscosity(self):
         return self.L.mcref_inlet_effective_viscosity(self.h)

@@ -5,11 +5,14 @@ oracle/Makefile into oracle/_ref/libmcref.so, against single-rank MPI/PETSc
 shims) on seeded inputs and stores its outputs:
 
   ref_box6x3x3.npz      6x3x3 cells on a 0.06 x 0.03 x 0.03 m box: mesh arrays,
-                        face geometry, and u, v, w, p, T plus face mass fluxes
-                        after each of 4 SIMPLE passes; CSR pattern of the
-                        momentum and pressure-correction matrices.
+                        face geometry, and all 13 fields (u, v, w, p, the
+                        pressure correction, k, epsilon, turbulent production,
+                        T, mixture fraction, progress variable and the two
+                        variances) plus face mass fluxes after each of 4 SIMPLE
+                        passes; CSR pattern of the momentum and
+                        pressure-correction matrices.
   ref_cfg1_10passes.npz 40x20x20 = 16,000 cells on the 0.2 x 0.1 x 0.1 m box:
-                        u, v, w, p, T after 10 SIMPLE passes (the parity gate).
+                        all 13 fields after 10 SIMPLE passes (the parity gate).
 
 Both start from the reference's initial state with u, v, w, p, T replaced by
 the inlet state plus seeded uniform noise (+-1%, numpy PCG64, seed 0), and use
@@ -28,6 +31,7 @@ from checkers import Reference, noisy_initial_fields, ref_available  # noqa: E40
 
 BASE = {"U": 50.0, "V": 0.0, "W": 0.0, "P": 4000.0, "TEM": 2000.0}
 FIELDS = ("U", "V", "W", "P", "TEM")
+ALL_FIELDS = ("U", "V", "W", "P", "PP", "TE", "ED", "TP", "TEM", "FUL", "PRO", "VARF", "VARP")
 
 
 def seeded_reference(ex, ey, ez, lx, ly, lz, seed=0):
@@ -55,7 +59,7 @@ def make_small():
         out[f"init_{name}"] = init[name]
     for p in range(4):
         ref.step()
-        for name in FIELDS:
+        for name in ALL_FIELDS:
             out[f"pass{p + 1}_{name}"] = ref.field(name)
         out[f"pass{p + 1}_mdot"] = ref.face_array(0)
         if p == 0:
@@ -72,7 +76,7 @@ def make_cfg1():
     for _ in range(10):
         ref.step()
     out = {"dims": np.array([ex, ey, ez]), "lengths": np.array(L), "passes": np.array(10)}
-    for name in FIELDS:
+    for name in ALL_FIELDS:
         out[name] = ref.field(name)
     rp, col, _ = ref.csr(1)
     out["pressure_rowptr"], out["pressure_col"] = rp, col

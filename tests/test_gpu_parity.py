@@ -46,8 +46,8 @@ def make_pair(dims, lengths, mode=COMPAT, **kw):
     mesh = flow.Mesh.box(*dims, *lengths)
     om = oracle_mesh(*dims, *lengths)
     okw = {k: v for k, v in kw.items() if k in ("u_rtol", "p_rtol", "max_iters")}
-    orc = Oracle(om, oracle_params(mode, **okw))
     p = flow.default_params(mode, **kw)
+    orc = Oracle(om, oracle_params(mode, scalars=p.transport_scalars, **okw))
     solver = flow.FlowSolver(mesh, params=p)
     return solver, orc
 
