@@ -175,6 +175,27 @@ int mc_flow_set_sources(mc_flow *flow, const double *host_particle_terms);
 /* Face arrays in reference face order.  which: 0 mass flux [faces], 1 area,
  * 2 lambda, 3 rlencos, 4 face_fields [faces][2], 5 normals [faces][3], 6 centres [faces][3]. */
 int mc_flow_get_face_array(mc_flow *flow, int which, double *host_values);
+/* Flow-field output for visualisation, the file the reference's
+ * VisitWriter<T>::write_flow writes (include/visit/VisitWriter.hpp:127-234,
+ * called by FlowSolver::output_data, FlowSolver.inl:18-23): legacy-VTK
+ * POLYDATA at the cell centres, file "<prefix>_flow0_timestep<id>.vtk", with
+ * the velocity vector and the scalar blocks in the reference's order, labels
+ * and number formatting (the blocks labelled flow_ful and flow_pro carry the
+ * progress variable and the mixture fraction, as the reference writes them).
+ * Scalars the handle does not transport are written as zeros. */
+int mc_flow_write_vtk(mc_flow *flow, const char *prefix, int id);
+/* Checkpoint and resume.  No reference counterpart (the reference restarts
+ * from its initial state).  The file holds the state a pass carries to the
+ * next -- every field with its boundary slots, face mass fluxes, the
+ * pressure-correction system (reused across passes in compat mode), sources,
+ * the previous correction, the timestep counters -- in the handle's own cell
+ * order, behind a 128-byte header ("MCCKPT01").  It can be read into a handle
+ * created with the same mesh and the same mode, reorder, precision, pressure
+ * solver and transport_scalars (MC_ERR_ARG otherwise); continuing from it
+ * gives the passes the uninterrupted run would have given. */
+int mc_flow_checkpoint_write(mc_flow *flow, const char *path);
+int mc_flow_checkpoint_read(mc_flow *flow, const char *path);
+
 /* The handle's cell order: cell_new_to_old[i] = caller's id of the handle's
  * i-th cell (the identity without reordering).  No reference counterpart. */
 int mc_flow_get_cell_order(mc_flow *flow, int *cell_new_to_old);

@@ -9,7 +9,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <iomanip>
 #include <new>
+#include <sstream>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -2004,6 +2007,215 @@ int mc_flow_snapshot_close(mc_flow *h)
         h->snap_dev = nullptr;
     }
     return rc;
+}
+
+// ------------------------------------------------------------- VTK output
+
+namespace {
+
+// A field in the caller's numbering (cells + 6 values).
+int fetch_field(mc_flow *h, int field, std::vector<double> &out)
+{
+    out.resize((size_t)h->N + 6);
+    return mc_flow_get_field(h, field, out.data());
+}
+
+// "x y z" as the reference's print_vec writes it (a fresh stream: default
+// precision), utils.hpp:357-362.
+std::string vec_text(double x, double y, double z)
+{
+    std::stringstream b;
+    b << x << " " << y << " " << z;
+    return b.str();
+}
+
+} // namespace
+
+int mc_flow_write_vtk(mc_flow *h, const char *prefix, int id)
+{
+    if (!h || !prefix) return MC_ERR_ARG;
+    const int N = h->N;
+    static const int needed[] = {MC_FIELD_U, MC_FIELD_V, MC_FIELD_W, MC_FIELD_P, MC_FIELD_TE, MC_FIELD_ED,
+                                 MC_FIELD_TEM, MC_FIELD_FUL, MC_FIELD_PRO, MC_FIELD_VARF, MC_FIELD_VARP};
+    std::vector<double> f[MC_FIELD_VARP + 1];
+    for (int k : needed) {
+        if (!field_ptr(h, k)) {
+            f[k].assign((size_t)N + 6, 0.0);  // not transported by this handle: written as zeros
+            continue;
+        }
+        const int rc = fetch_field(h, k, f[k]);
+        if (rc) return rc;
+    }
+    // cell centres in the caller's numbering
+    std::vector<double> c[3];
+    const double *dc[3] = {h->xc, h->yc, h->zc};
+    std::vector<double> tmp((size_t)N);
+    for (int d = 0; d < 3; d++) {
+        CUDA_TRY(h, cudaMemcpy(tmp.data(), dc[d], (size_t)N * 8, cudaMemcpyDeviceToHost));
+        c[d].resize((size_t)N);
+        for (int i = 0; i < N; i++) c[d][i] = tmp[h->reordered ? h->cell_o2n[i] : i];
+    }
+    const std::string name = std::string(prefix) + "_flow0_timestep" + std::to_string(id) + ".vtk";
+    std::ofstream v(name);
+    if (!v) return fail(h, MC_ERR_ARG, "cannot open " + name);
+    v << "# vtk DataFile Version 3.0 " << std::endl;
+    v << "MiniCOMBUST " << std::endl;
+    v << "ASCII " << std::endl;
+    v << "DATASET POLYDATA " << std::endl;
+    v << std::endl << "POINTS " << (uint64_t)N << " float" << std::endl;
+    for (int i = 0; i < N; i++) {
+        if (i % 10 == 0)
+            v << std::endl;
+        else
+            v << "  ";
+        v << vec_text(c[0][i], c[1][i], c[2][i]) << "\t";
+    }
+    v << std::endl << std::endl;
+    v << std::endl << "VERTICES " << (uint64_t)N << " " << (uint64_t)N * 2 << std::endl;
+    for (uint64_t i = 0; i < (uint64_t)N; i++) v << "1 " << i << "\t";
+    v << std::endl;
+    v << std::endl << "POINT_DATA " << (uint64_t)N << std::endl;
+    v << "VECTORS flow_velocity float" << std::endl;
+    for (int i = 0; i < N; i++) v << f[MC_FIELD_U][i] << " " << f[MC_FIELD_V][i] << " " << f[MC_FIELD_W][i] << " " << "\t";
+    v << std::endl;
+    // the scalar blocks in the reference's order and labels (the ones labelled
+    // flow_ful and flow_pro carry PRO and FUL respectively, as there); from
+    // flow_tem on, values are written with 11 significant digits
+    struct Block { const char *label; int field; bool p11; };
+    static const Block blocks[] = {{"flow_pressure", MC_FIELD_P, false}, {"flow_te", MC_FIELD_TE, false},
+                                   {"flow_ed", MC_FIELD_ED, false},      {"flow_tem", MC_FIELD_TEM, true},
+                                   {"flow_ful", MC_FIELD_PRO, true},     {"flow_pro", MC_FIELD_FUL, true},
+                                   {"flow_varf", MC_FIELD_VARF, true},   {"flow_varp", MC_FIELD_VARP, true}};
+    for (const Block &b : blocks) {
+        v << "SCALARS " << b.label << " float" << std::endl;
+        v << "LOOKUP_TABLE default" << std::endl;
+        for (int i = 0; i < N; i++) {
+            if (b.p11) v << std::setprecision(11);
+            v << f[b.field][i] << "\t";
+        }
+        v << std::endl;
+    }
+    v.close();
+    if (!v) return fail(h, MC_ERR_ARG, "write failed: " + name);
+    return MC_OK;
+}
+
+// ------------------------------------------------------- checkpoint / resume
+
+namespace {
+
+constexpr char kCkptMagic[8] = {'M', 'C', 'C', 'K', 'P', 'T', '0', '1'};
+
+struct CkptHeader {
+    char magic[8];
+    uint32_t version, cells, faces, mode, reorder, scalars, precision, pressure_solver;
+    uint64_t timestep_count;
+    int32_t pass_in_step, first_pressure, sources_set, pad;
+    double mass_source_total;
+    char reserved[128 - 8 - 8 * 4 - 8 - 4 * 4 - 8];
+};
+static_assert(sizeof(CkptHeader) == 128, "checkpoint header is 128 bytes");
+
+// The device arrays that carry state from one pass to the next, in the
+// handle's own cell and face order: the fields, the face mass fluxes, the
+// pressure-correction system (stale across passes in compat mode), the
+// particle sources, the previous correction and the momentum diagonal.
+std::vector<std::pair<double *, size_t>> checkpoint_arrays(mc_flow *h)
+{
+    const size_t N = (size_t)h->N, NB = N + 6, F = (size_t)h->F;
+    std::vector<std::pair<double *, size_t>> a;
+    for (int g = 0; g < G_NFIELDS; g++) a.push_back({h->phi[g], NB});
+    if (h->has_scalars)
+        for (int f : kScalarFields) a.push_back({h->sfield[f], NB});
+    a.push_back({h->mdot, F});
+    a.push_back({h->off_p, 6 * N});
+    a.push_back({h->diag_p, N});
+    a.push_back({h->b_p, N});
+    a.push_back({h->src, 5 * N});
+    a.push_back({h->pp_prev, N});
+    a.push_back({h->AU, N});
+    return a;
+}
+
+} // namespace
+
+int mc_flow_checkpoint_write(mc_flow *h, const char *path)
+{
+    if (!h || !path) return MC_ERR_ARG;
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    FILE *fp = std::fopen(path, "wb");
+    if (!fp) return fail(h, MC_ERR_ARG, std::string("cannot open ") + path);
+    CkptHeader hd{};
+    std::memcpy(hd.magic, kCkptMagic, 8);
+    hd.version = 1;
+    hd.cells = (uint32_t)h->N;
+    hd.faces = (uint32_t)h->F;
+    hd.mode = (uint32_t)h->prm.mode;
+    hd.reorder = (uint32_t)h->prm.reorder;
+    hd.scalars = h->has_scalars ? 1u : 0u;
+    hd.precision = (uint32_t)h->prm.precision;
+    hd.pressure_solver = (uint32_t)h->prm.pressure_solver;
+    hd.timestep_count = h->timestep_count;
+    hd.pass_in_step = h->pass_in_step;
+    hd.first_pressure = h->first_pressure;
+    hd.sources_set = h->sources_set;
+    hd.mass_source_total = h->mass_source_total;
+    bool ok = std::fwrite(&hd, sizeof(hd), 1, fp) == 1;
+    std::vector<double> buf;
+    for (const auto &arr : checkpoint_arrays(h)) {
+        if (!ok) break;
+        buf.resize(arr.second);
+        if (cudaMemcpy(buf.data(), arr.first, arr.second * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            std::fclose(fp);
+            return fail(h, MC_ERR_CUDA, "checkpoint copy");
+        }
+        ok = std::fwrite(buf.data(), 8, arr.second, fp) == arr.second;
+    }
+    if (std::fclose(fp) != 0) ok = false;
+    return ok ? MC_OK : fail(h, MC_ERR_ARG, std::string("checkpoint write failed: ") + path);
+}
+
+int mc_flow_checkpoint_read(mc_flow *h, const char *path)
+{
+    if (!h || !path) return MC_ERR_ARG;
+    FILE *fp = std::fopen(path, "rb");
+    if (!fp) return fail(h, MC_ERR_ARG, std::string("cannot open ") + path);
+    CkptHeader hd{};
+    if (std::fread(&hd, sizeof(hd), 1, fp) != 1 || std::memcmp(hd.magic, kCkptMagic, 8) != 0 || hd.version != 1) {
+        std::fclose(fp);
+        return fail(h, MC_ERR_ARG, std::string("not a checkpoint: ") + path);
+    }
+    if (hd.cells != (uint32_t)h->N || hd.faces != (uint32_t)h->F || hd.mode != (uint32_t)h->prm.mode ||
+        hd.reorder != (uint32_t)h->prm.reorder || hd.scalars != (h->has_scalars ? 1u : 0u) ||
+        hd.precision != (uint32_t)h->prm.precision || hd.pressure_solver != (uint32_t)h->prm.pressure_solver) {
+        std::fclose(fp);
+        return fail(h, MC_ERR_ARG, "checkpoint was written by a handle with another mesh size or options");
+    }
+    std::vector<double> buf;
+    for (const auto &arr : checkpoint_arrays(h)) {
+        buf.resize(arr.second);
+        if (std::fread(buf.data(), 8, arr.second, fp) != arr.second) {
+            std::fclose(fp);
+            return fail(h, MC_ERR_ARG, "checkpoint is truncated");
+        }
+        CUDA_TRY(h, cudaMemcpy(arr.first, buf.data(), arr.second * 8, cudaMemcpyHostToDevice));
+    }
+    std::fclose(fp);
+    h->timestep_count = hd.timestep_count;
+    h->pass_in_step = hd.pass_in_step;
+    h->first_pressure = hd.first_pressure;
+    h->sources_set = hd.sources_set;
+    h->mass_source_total = hd.mass_source_total;
+    // a pressure system carried over from before (compat mode) needs its AMG
+    // values; the coarsest inverse is formed in line
+    if (h->use_amg && !h->first_pressure) {
+        h->inverse_ready = false;
+        h->inverse_pending = false;
+        const int rs = setup_amg_values(h);
+        if (rs) return rs;
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return check_launch(h);
 }
 
 int mc_flow_get_cell_order(mc_flow *h, int *cell_new_to_old)

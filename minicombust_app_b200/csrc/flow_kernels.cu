@@ -598,7 +598,11 @@ void launch_scalar_assemble(cudaStream_t s, int type, const Physics &ph, const M
     switch (type) {
     case SC_TERBTE: k_scalar_assemble<SC_TERBTE><<<grid, MCB_THREADS, 0, s>>>(ph, m, a, t); break;
     case SC_TERBED: k_scalar_assemble<SC_TERBED><<<grid, MCB_THREADS, 0, s>>>(ph, m, a, t); break;
-    default: k_scalar_assemble<SC_FUEL><<<grid, MCB_THREADS, 0, s>>>(ph, m, a, t); break;
+    case SC_FUEL: k_scalar_assemble<SC_FUEL><<<grid, MCB_THREADS, 0, s>>>(ph, m, a, t); break;
+    case SC_PROG: k_scalar_assemble<SC_PROG><<<grid, MCB_THREADS, 0, s>>>(ph, m, a, t); break;
+    case SC_VARFU: k_scalar_assemble<SC_VARFU><<<grid, MCB_THREADS, 0, s>>>(ph, m, a, t); break;
+    case SC_VARPR: k_scalar_assemble<SC_VARPR><<<grid, MCB_THREADS, 0, s>>>(ph, m, a, t); break;
+    default: break;
     }
 }
 

@@ -126,6 +126,9 @@ _SIGNATURES = {
     "mc_flow_set_sources": (c_int, [c_vp, c_vp]),
     "mc_flow_get_face_array": (c_int, [c_vp, c_int, c_vp]),
     "mc_flow_get_cell_order": (c_int, [c_vp, c_vp]),
+    "mc_flow_write_vtk": (c_int, [c_vp, ctypes.c_char_p, c_int]),
+    "mc_flow_checkpoint_write": (c_int, [c_vp, ctypes.c_char_p]),
+    "mc_flow_checkpoint_read": (c_int, [c_vp, ctypes.c_char_p]),
     "mc_flow_set_guess_params": (c_int, [c_vp, c_vp, c_int]),
     "mc_flow_snapshot_open": (c_int, [c_vp, ctypes.c_char_p, c_int]),
     "mc_flow_snapshot_close": (c_int, [c_vp]),
@@ -360,6 +363,18 @@ class FlowSolver:
 
     def snapshot_close(self):
         _check(self.L.mc_flow_snapshot_close(self.h), self.h, "snapshot_close")
+
+    def output_data(self, timestep, prefix="out/flow/minicombust"):
+        """FlowSolver::output_data (FlowSolver.inl:18-23): the VTK flow file of
+        this timestep, as the reference's VisitWriter writes it."""
+        _check(self.L.mc_flow_write_vtk(self.h, os.fsencode(prefix), int(timestep)), self.h, "write_vtk")
+        return f"{prefix}_flow0_timestep{int(timestep)}.vtk"
+
+    def checkpoint(self, path):
+        _check(self.L.mc_flow_checkpoint_write(self.h, os.fsencode(path)), self.h, "checkpoint_write")
+
+    def resume(self, path):
+        _check(self.L.mc_flow_checkpoint_read(self.h, os.fsencode(path)), self.h, "checkpoint_read")
 
     def cell_order(self):
         """The handle's internal cell order: new-to-old ids (identity unless reordered)."""

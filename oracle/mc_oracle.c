@@ -11,6 +11,7 @@
 #include "mc_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -252,29 +253,141 @@ static void mat_set(const mco_solver *s, double *val, uint64_t r, uint64_t c, do
     abort();
 }
 
-static void spmv(const mco_solver *s, const double *val, const double *x, double *y)
+/* Threads of the linear solves (mco_set_threads).  With one thread every
+ * sum runs in index order, as in the reference's shim solvers; with more, the
+ * loops are split across POSIX threads and dot products are summed in a
+ * fixed number of chunks (a result that does not depend on the thread count,
+ * but is not the serial rounding). */
+static int g_threads = 1;
+#define MCO_CHUNKS 512
+
+void mco_set_threads(int n) { g_threads = n > 1 ? (n < 256 ? n : 256) : 1; }
+
+typedef void (*range_fn)(void *ctx, uint64_t lo, uint64_t hi, int chunk);
+typedef struct { range_fn fn; void *ctx; uint64_t n; int chunks, first, step; } par_job;
+
+static void *par_worker(void *arg)
 {
-    for (uint64_t i = 0; i < s->N; i++) {
+    const par_job *j = (const par_job *)arg;
+    for (int c = j->first; c < j->chunks; c += j->step)
+        j->fn(j->ctx, j->n * (uint64_t)c / (uint64_t)j->chunks, j->n * (uint64_t)(c + 1) / (uint64_t)j->chunks, c);
+    return NULL;
+}
+
+/* fn over `chunks` equal ranges of [0, n): serially in order with one thread,
+ * else chunk c on thread c mod g_threads. */
+static void par_for(uint64_t n, int chunks, range_fn fn, void *ctx)
+{
+    if (g_threads <= 1) {
+        for (int c = 0; c < chunks; c++) fn(ctx, n * (uint64_t)c / (uint64_t)chunks, n * (uint64_t)(c + 1) / (uint64_t)chunks, c);
+        return;
+    }
+    const int T = g_threads;
+    pthread_t th[256];
+    par_job jobs[256];
+    int joined[256] = {0};
+    for (int t = 0; t < T; t++) jobs[t] = (par_job){fn, ctx, n, chunks, t, T};
+    for (int t = 1; t < T; t++) {
+        if (pthread_create(&th[t], NULL, par_worker, &jobs[t]) == 0)
+            joined[t] = 1;
+        else
+            par_worker(&jobs[t]); /* could not start a thread: run its share here */
+    }
+    par_worker(&jobs[0]);
+    for (int t = 1; t < T; t++)
+        if (joined[t]) pthread_join(th[t], NULL);
+}
+
+typedef struct { const mco_solver *s; const double *val, *x; double *y; } spmv_ctx;
+static void spmv_range(void *vc, uint64_t lo, uint64_t hi, int chunk)
+{
+    const spmv_ctx *c = (const spmv_ctx *)vc;
+    (void)chunk;
+    for (uint64_t i = lo; i < hi; i++) {
         double acc = 0.0;
-        for (int k = s->rp[i]; k < s->rp[i + 1]; k++) acc += val[k] * x[s->col[k]];
-        y[i] = acc;
+        for (int k = c->s->rp[i]; k < c->s->rp[i + 1]; k++) acc += c->val[k] * c->x[c->s->col[k]];
+        c->y[i] = acc;
     }
 }
 
-static double dotn(const double *a, const double *b, uint64_t n)
+static void spmv(const mco_solver *s, const double *val, const double *x, double *y)
 {
+    spmv_ctx c = {s, val, x, y};
+    par_for(s->N, g_threads <= 1 ? 1 : 4 * g_threads, spmv_range, &c);
+}
+
+typedef struct { const double *a, *b; double *part; } dot_ctx;
+static void dot_range(void *vc, uint64_t lo, uint64_t hi, int chunk)
+{
+    const dot_ctx *c = (const dot_ctx *)vc;
     double acc = 0.0;
-    for (uint64_t i = 0; i < n; i++) acc += a[i] * b[i];
+    if (c->b)
+        for (uint64_t i = lo; i < hi; i++) acc += c->a[i] * c->b[i];
+    else
+        for (uint64_t i = lo; i < hi; i++) acc += c->a[i];
+    c->part[chunk] = acc;
+}
+
+/* sum of a[i] * b[i] (b null: sum of a[i]) */
+static double sumn(const double *a, const double *b, uint64_t n)
+{
+    if (g_threads <= 1) {
+        double acc = 0.0;
+        if (b)
+            for (uint64_t i = 0; i < n; i++) acc += a[i] * b[i];
+        else
+            for (uint64_t i = 0; i < n; i++) acc += a[i];
+        return acc;
+    }
+    double part[MCO_CHUNKS];
+    dot_ctx c = {a, b, part};
+    par_for(n, MCO_CHUNKS, dot_range, &c);
+    double acc = 0.0;
+    for (int k = 0; k < MCO_CHUNKS; k++) acc += part[k];
     return acc;
 }
 
+static double dotn(const double *a, const double *b, uint64_t n) { return sumn(a, b, n); }
+
 static void project_mean_zero(double *v, uint64_t n)
 {
-    double acc = 0.0;
-    for (uint64_t i = 0; i < n; i++) acc += v[i];
+    const double acc = sumn(v, NULL, n);
     const double m = acc / (double)n;
     for (uint64_t i = 0; i < n; i++) v[i] -= m;
 }
+
+/* Vector updates of the Krylov loops, split like spmv. */
+typedef struct { int op; double a, b; double *x, *y, *z; const double *u, *v, *w; } axpy_ctx;
+static void axpy_range(void *vc, uint64_t lo, uint64_t hi, int chunk)
+{
+    const axpy_ctx *c = (const axpy_ctx *)vc;
+    (void)chunk;
+    switch (c->op) {
+    case 0: /* p = r + beta (p - omega v) */
+        for (uint64_t i = lo; i < hi; i++) c->x[i] = c->u[i] + c->a * (c->x[i] - c->b * c->v[i]);
+        break;
+    case 1: /* s = r - alpha v */
+        for (uint64_t i = lo; i < hi; i++) c->x[i] = c->u[i] - c->a * c->v[i];
+        break;
+    case 2: /* x += alpha p + omega s; r = s - omega t */
+        for (uint64_t i = lo; i < hi; i++) {
+            c->x[i] += c->a * c->u[i] + c->b * c->v[i];
+            c->y[i] = c->v[i] - c->b * c->w[i];
+        }
+        break;
+    case 3: /* x += alpha p; r -= alpha q */
+        for (uint64_t i = lo; i < hi; i++) {
+            c->x[i] += c->a * c->u[i];
+            c->y[i] -= c->a * c->v[i];
+        }
+        break;
+    case 4: /* p = r + beta p */
+        for (uint64_t i = lo; i < hi; i++) c->x[i] = c->u[i] + c->a * c->x[i];
+        break;
+    }
+}
+
+static void vec_op(uint64_t n, axpy_ctx c) { par_for(n, g_threads <= 1 ? 1 : 4 * g_threads, axpy_range, &c); }
 
 /* KSPBCGS with PCNONE from a zero guess (the reference's KSP for momentum and
  * scalars, FlowSolver.hpp:513-519; solve at FlowSolver.inl:1341-1375). */
@@ -296,17 +409,14 @@ static int solve_bicgstab(const mco_solver *s, const double *val, const double *
             const double rho_new = dotn(r0, r, n);
             if (rho_new == 0.0) { its = -k; break; }
             const double beta = (rho_new / rho) * (alpha / omega);
-            for (uint64_t i = 0; i < n; i++) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+            vec_op(n, (axpy_ctx){0, beta, omega, p, NULL, NULL, r, v, NULL});
             spmv(s, val, p, v);
             alpha = rho_new / dotn(r0, v, n);
-            for (uint64_t i = 0; i < n; i++) sv[i] = r[i] - alpha * v[i];
+            vec_op(n, (axpy_ctx){1, alpha, 0.0, sv, NULL, NULL, r, v, NULL});
             spmv(s, val, sv, t);
             const double tt = dotn(t, t, n);
             omega = (tt != 0.0) ? dotn(t, sv, n) / tt : 0.0;
-            for (uint64_t i = 0; i < n; i++) {
-                x[i] += alpha * p[i] + omega * sv[i];
-                r[i] = sv[i] - omega * t[i];
-            }
+            vec_op(n, (axpy_ctx){2, alpha, omega, x, r, NULL, p, sv, t});
             rho = rho_new;
             const double rn = sqrt(dotn(r, r, n));
             if (rn <= rtol * bnorm) { its = k; break; }
@@ -341,15 +451,12 @@ static int solve_cg_projected(const mco_solver *s, const double *val, const doub
         for (k = 1; k <= s->prm.max_iters; k++) {
             spmv(s, val, p, q);
             const double alpha = rr / dotn(p, q, n);
-            for (uint64_t i = 0; i < n; i++) {
-                x[i] += alpha * p[i];
-                r[i] -= alpha * q[i];
-            }
+            vec_op(n, (axpy_ctx){3, alpha, 0.0, x, r, NULL, p, q, NULL});
             const double rr_new = dotn(r, r, n);
             if (sqrt(rr_new) <= tol) break;
             const double beta = rr_new / rr;
             rr = rr_new;
-            for (uint64_t i = 0; i < n; i++) p[i] = r[i] + beta * p[i];
+            vec_op(n, (axpy_ctx){4, beta, 0.0, p, NULL, NULL, r, NULL, NULL});
         }
         project_mean_zero(x, n);
         if (k > s->prm.max_iters) k = -s->prm.max_iters;

@@ -79,6 +79,12 @@ typedef struct mco_solver mco_solver;
 
 void mco_default_params(mco_params *p, int mode);
 
+/* Host threads of the linear solves (default 1).  With 1 every sum runs in
+ * index order, which is what the pinning against the reference needs; more
+ * threads split the vector loops and sum dot products in fixed chunks (for
+ * large checks, where the result only has to meet a tolerance). */
+void mco_set_threads(int n);
+
 /* load_mesh for one flow rank (mesh_examples.cpp:120-571). */
 int mco_mesh_box(uint64_t ex, uint64_t ey, uint64_t ez, double lx, double ly, double lz, mco_mesh *m);
 void mco_mesh_free(mco_mesh *m);

@@ -312,6 +312,14 @@ int mcref_stage_scalar(void *vh, int field)
     default: return -1;
     }
 }
+// FlowSolver::output_data's writer (VisitWriter<T>::write_flow,
+// VisitWriter.hpp:127-234) on the current fields.
+void mcref_write_flow(void *vh, const char *prefix, int id)
+{
+    RefHandle *h = (RefHandle *)vh;
+    VisitWriter<double> w(h->mesh, &h->mpi);
+    w.write_flow(prefix, id, &h->solver->phi);
+}
 int mcref_first_pressure(void *vh) { return ((RefHandle *)vh)->solver->first_pressure ? 1 : 0; }
 uint64_t mcref_timestep_count(void *vh) { return ((RefHandle *)vh)->solver->timestep_count; }
 double mcref_inlet_effective_viscosity(void *vh) { return ((RefHandle *)vh)->solver->inlet_effective_viscosity; }

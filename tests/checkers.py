@@ -98,6 +98,7 @@ def oracle_lib():
             getattr(L, fn).restype = c_int
         for fn in ("mco_stage_gradients", "mco_stage_set_up_field"):
             getattr(L, fn).argtypes = [c_vp]
+        L.mco_set_threads.argtypes = [c_int]
         L.mco_stage_scalar.argtypes = [c_vp, c_int]
         L.mco_stage_scalar.restype = c_int
         L.mco_get_stats.argtypes = [c_vp, ctypes.POINTER(_McoStats)]
@@ -256,6 +257,7 @@ def ref_lib():
         L.mcref_get_csr.argtypes = [c_vp, c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int), c_vp, c_vp, c_vp]
         L.mcref_first_pressure.argtypes = [c_vp]
         L.mcref_stage_scalar.argtypes = [c_vp, c_int]
+        L.mcref_write_flow.argtypes = [c_vp, ctypes.c_char_p, c_int]
         L.mcref_stage_scalar.restype = c_int
         L.mcref_timestep_count.argtypes = [c_vp]
         L.mcref_timestep_count.restype = c_u64
@@ -347,6 +349,11 @@ class Reference:
 
     def stage_scalar(self, name):
         assert self.L.mcref_stage_scalar(self.h, FIELDS[name]) == 0
+
+    def write_flow(self, prefix, id):
+        """The reference's VisitWriter output of the current fields; returns the file name."""
+        self.L.mcref_write_flow(self.h, os.fsencode(prefix), int(id))
+        return f"{prefix}_flow0_timestep{int(id)}.vtk"
 
     def inlet_effective_viscosity(self):
         return self.L.mcref_inlet_effective_viscosity(self.h)

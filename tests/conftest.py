@@ -1,5 +1,4 @@
 import os
-import subprocess
 import sys
 
 import pytest
@@ -14,10 +13,11 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "slow: larger CPU cases")
 
 
-def _build_checkers():
-    # liboracle.so always; oracle/_ref/libmcref.so only where the reference tree exists.
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True,
-                   stdout=subprocess.DEVNULL)
+def _build_checkers(front):
+    # liboracle.so always; oracle/_ref/* only where the reference tree exists.
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import build_checkers
+    build_checkers.build(front=front)
 
 
 def _build_library():
@@ -27,8 +27,9 @@ def _build_library():
 
 @pytest.fixture(scope="session", autouse=True)
 def built():
-    _build_checkers()
+    _build_checkers(front=False)
     _build_library()
+    _build_checkers(front=True)  # the front's driver links the library
     yield
 
 
