@@ -175,6 +175,34 @@ int mc_flow_set_sources(mc_flow *flow, const double *host_particle_terms);
 /* Face arrays in reference face order.  which: 0 mass flux [faces], 1 area,
  * 2 lambda, 3 rlencos, 4 face_fields [faces][2], 5 normals [faces][3], 6 centres [faces][3]. */
 int mc_flow_get_face_array(mc_flow *flow, int which, double *host_values);
+/* Particle-to-cell source terms, the flow side of the flow/particle
+ * exchange (FlowSolver::update_flow_field, FlowSolver.inl:496-736; GPU
+ * back-end gpu_kernels.cu:131-149): `rows` rows from the particle ranks in
+ * arrival order, each a cell id (caller's numbering) and a particle_aos<double>
+ * {momentum.x, momentum.y, momentum.z, energy, fuel}.  They replace the
+ * handle's sources as mc_flow_set_sources does: every cell is zeroed and each
+ * row added to its cell, a cell's rows in arrival order, so the sums equal
+ * the reference's sequential loop bit for bit.  A cell id >= cells returns
+ * MC_ERR_ARG; more than 2^29 rows in one call, MC_ERR_UNSUPPORTED. */
+int mc_flow_ingest_particles(mc_flow *flow, int64_t rows, const uint64_t *cells, const double *terms);
+/* The handle's particle source terms, [cells][5] particle_aos<double>. */
+int mc_flow_get_sources(mc_flow *flow, double *terms);
+/* Flow state at mesh nodes for the particle side (get_neighbour_cells and
+ * interpolate_to_nodes, FlowSolver.inl:293-494; gpu_kernels.cu:2132-2198):
+ * for every distinct node of the n_cells given cells (caller ids), in
+ * ascending node id, the velocity, pressure and temperature interpolated
+ * from the cells around the node -- (8 - n_c)/8 of the reference gas state
+ * (inlet_u, 0, 0; pressure0; temperature0) for the n_c < 8 cells a boundary
+ * node lacks, plus, for each cell c sharing the node in ascending cell id,
+ * (phi_c + grad phi_c . (x_node - x_c)) / 8, with the current fields and the
+ * gradients of the last gradient stage.  node_ids[n] and node_fields[n][5] =
+ * flow_aos<double> {vel.x, vel.y, vel.z, pressure, temp}; *n_nodes receives n.
+ * With node_ids and node_fields NULL only n is computed; otherwise n above
+ * max_nodes returns MC_ERR_ARG.  The reference sums each node's cells in
+ * hash-set order, so its values differ from these in the last bits only. */
+int mc_flow_interpolate_nodes(mc_flow *flow, int64_t n_cells, const uint64_t *cells, int64_t max_nodes,
+                              int64_t *n_nodes, uint64_t *node_ids, double *node_fields);
+
 /* Flow-field output for visualisation, the file the reference's
  * VisitWriter<T>::write_flow writes (include/visit/VisitWriter.hpp:127-234,
  * called by FlowSolver::output_data, FlowSolver.inl:18-23): legacy-VTK

@@ -29,6 +29,7 @@ CUDA_SOURCES = [
     ("amg.cu", []),
     ("flow_api.cu", []),
     ("solve_noalloc.cu", []),
+    ("exchange.cu", ["-fmad=false"]),
     ("gnn.cu", []),
     ("gnn_umma.cu", []),
     ("gnn_api.cu", []),

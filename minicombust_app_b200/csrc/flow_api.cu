@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "amg.h"
+#include "exchange.cuh"
 #include "flow_kernels.cuh"
 #include "gnn.cuh"
 #include "krylov.cuh"
@@ -37,7 +38,7 @@ enum KernelId {
     K_BICG1_1, K_BICG1_2, K_BICG1_3, K_AMG_SETUP, K_PCG_INIT_AMG, K_PCG_ITER2_AMG, K_AMG_VCYCLE,
     K_IR, K_PCG_INIT_AMG32, K_PCG_ITER1_32, K_PCG_ITER2_AMG32, K_AMG_VCYCLE32, K_PERMUTE, K_GUESS, K_GNN,
     K_SNAPSHOT, K_BIR, K_ROUND_ELL, K_BICG3_INIT32, K_BICG3_1_32, K_BICG3_2_32, K_BICG3_3_32, K_BICG1_INIT32,
-    K_BICG1_1_32, K_BICG1_2_32, K_BICG1_3_32, K_GRAD6, K_SCALAR, K_SCALAR_CLIP, K_COUNT
+    K_BICG1_1_32, K_BICG1_2_32, K_BICG1_3_32, K_GRAD6, K_SCALAR, K_SCALAR_CLIP, K_EXCHANGE, K_COUNT
 };
 
 const char *kKernelNames[K_COUNT] = {
@@ -50,7 +51,7 @@ const char *kKernelNames[K_COUNT] = {
     "pcg32_iter1_spmv", "pcg32_iter2_amg_update", "amg32_vcycle", "permute", "guess_select", "gnn_forward",
     "snapshot_pack", "bicg_refine_fp64_residual", "round_fp32", "bicg3_32_init", "bicg3_32_1_spmv",
     "bicg3_32_2_spmv", "bicg3_32_3_update", "bicg1_32_init", "bicg1_32_1_spmv", "bicg1_32_2_spmv",
-    "bicg1_32_3_update", "lsq_gradients_scalars", "scalar_assemble", "scalar_clip_negative"};
+    "bicg1_32_3_update", "lsq_gradients_scalars", "scalar_assemble", "scalar_clip_negative", "particle_exchange"};
 
 constexpr int PCG_BATCH = 16;   // iterations per status read (even: ping-pong buffers)
 constexpr int PCG_AMG_BATCH = 4;
@@ -186,6 +187,20 @@ struct mc_flow {
     cudaGraphExec_t g_bs = nullptr, l_bs = nullptr;
     int *neg_list = nullptr;          // negative k / epsilon cells after a solve
     unsigned int *neg_count = nullptr;
+
+    // flow/particle exchange: the mesh's nodes (host copies taken at create;
+    // device tables built on the first node interpolation) and grow-on-demand
+    // buffers for the rows and requests of a call
+    int P = 0;
+    std::vector<int> h_cell_nodes;    // [N][8], caller order
+    std::vector<double> h_points;     // [P][3]
+    char *node_mem = nullptr;
+    int *d_cell_nodes = nullptr, *pc_off = nullptr, *pc_cells = nullptr, *node_list = nullptr;
+    int *node_counts = nullptr, *node_count = nullptr;
+    double *px = nullptr, *py = nullptr, *pz = nullptr, *node_out = nullptr;
+    unsigned char *node_flag = nullptr;
+    char *xin_mem = nullptr;
+    size_t xin_bytes = 0;
 
     // state of the reference's control flow
     int first_pressure = 1;
@@ -1742,6 +1757,25 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
         std::string err;
         HostPhysics hp{params->density};
         rc = build_host_mesh(mesh, hp, hm, err);
+        if (!rc) {
+            // the nodes, kept for the flow/particle exchange
+            const uint64_t P64 = mesh->points;
+            if (P64 == 0 || P64 >= (uint64_t)INT32_MAX) {
+                err = "points out of range";
+                rc = MC_ERR_MESH;
+            } else {
+                h->P = (int)P64;
+                h->h_points.assign(mesh->points_xyz, mesh->points_xyz + 3 * P64);
+                h->h_cell_nodes.resize((size_t)8 * mesh->cells);
+                for (size_t i = 0; i < (size_t)8 * mesh->cells && !rc; i++) {
+                    if (mesh->cell_nodes[i] >= P64) {
+                        err = "cell_nodes refers to a point that does not exist";
+                        rc = MC_ERR_MESH;
+                    }
+                    h->h_cell_nodes[i] = (int)mesh->cell_nodes[i];
+                }
+            }
+        }
         if (!rc && params->reorder == MC_REORDER_RCM) {
             std::vector<int> face_n2o;
             rcm_cell_order(hm, h->cell_n2o);
@@ -1907,6 +1941,8 @@ int mc_flow_destroy(mc_flow *h)
     if (h->gnn_mem) cudaFree(h->gnn_mem);
     if (h->bir_mem) cudaFree(h->bir_mem);
     if (h->scal_mem) cudaFree(h->scal_mem);
+    if (h->node_mem) cudaFree(h->node_mem);
+    if (h->xin_mem) cudaFree(h->xin_mem);
     for (cudaGraphExec_t g : {h->g_bs, h->l_bs})
         if (g) cudaGraphExecDestroy(g);
     for (void *p : {(void *)h->h_bi3, (void *)h->h_bi1, (void *)h->h_bo3, (void *)h->h_bo1})
@@ -2216,6 +2252,200 @@ int mc_flow_checkpoint_read(mc_flow *h, const char *path)
     }
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return check_launch(h);
+}
+
+// ------------------------------------------------------ flow/particle exchange
+
+namespace {
+
+// Device memory of at least `bytes` for the rows or requests of one call.
+int input_buffer(mc_flow *h, size_t bytes, char **out)
+{
+    if (bytes > h->xin_bytes) {
+        if (h->xin_mem) cudaFree(h->xin_mem);
+        h->xin_mem = nullptr;
+        h->xin_bytes = 0;
+        CUDA_TRY(h, cudaMalloc((void **)&h->xin_mem, bytes));
+        h->xin_bytes = bytes;
+    }
+    *out = h->xin_mem;
+    return MC_OK;
+}
+
+// The node tables of the interpolation: cell -> nodes (caller order), node
+// coordinates, node -> its cells (handle ids, ascending caller id).
+int setup_nodes(mc_flow *h)
+{
+    if (h->node_mem) return MC_OK;
+    const size_t N = (size_t)h->N, P = (size_t)h->P;
+    std::vector<int> off(P + 1, 0), cells(8 * N);
+    for (size_t i = 0; i < 8 * N; i++) off[(size_t)h->h_cell_nodes[i] + 1]++;
+    for (size_t p = 0; p < P; p++) off[p + 1] += off[p];
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (size_t c = 0; c < N; c++)  // caller ids ascending: each node's list is sorted by caller id
+        for (int v = 0; v < 8; v++) {
+            const int node = h->h_cell_nodes[8 * c + v];
+            cells[fill[node]++] = h->reordered ? h->cell_o2n[c] : (int)c;
+        }
+    std::vector<double> xyz[3];
+    for (int d = 0; d < 3; d++) {
+        xyz[d].resize(P);
+        for (size_t p = 0; p < P; p++) xyz[d][p] = h->h_points[3 * p + d];
+    }
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t nb = (P + 1023) / 1024 + 1;
+    const size_t bytes = al(8 * N * 4) + 3 * al(P * 8) + al((P + 1) * 4) + al(8 * N * 4) + al(P) + al(nb * 4) + 256 +
+                         al(P * 4) + al(5 * P * 8);
+    CUDA_TRY(h, cudaMalloc((void **)&h->node_mem, bytes));
+    char *q = h->node_mem;
+    auto take = [&](size_t b) { char *r = q; q += al(b); return r; };
+    h->d_cell_nodes = (int *)take(8 * N * 4);
+    h->px = (double *)take(P * 8);
+    h->py = (double *)take(P * 8);
+    h->pz = (double *)take(P * 8);
+    h->pc_off = (int *)take((P + 1) * 4);
+    h->pc_cells = (int *)take(8 * N * 4);
+    h->node_flag = (unsigned char *)take(P);
+    h->node_counts = (int *)take(nb * 4);
+    h->node_count = (int *)take(256);
+    h->node_list = (int *)take(P * 4);
+    h->node_out = (double *)take(5 * P * 8);
+    CUDA_TRY(h, cudaMemcpy(h->d_cell_nodes, h->h_cell_nodes.data(), 8 * N * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->px, xyz[0].data(), P * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->py, xyz[1].data(), P * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->pz, xyz[2].data(), P * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->pc_off, off.data(), (P + 1) * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->pc_cells, cells.data(), 8 * N * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemset(h->node_flag, 0, P));
+    return MC_OK;
+}
+
+} // namespace
+
+int mc_flow_ingest_particles(mc_flow *h, int64_t rows, const uint64_t *cells, const double *terms)
+{
+    if (!h || rows < 0 || (rows > 0 && (!cells || !terms))) return MC_ERR_ARG;
+    if (rows > (int64_t)1 << 29) return fail(h, MC_ERR_UNSUPPORTED, "more than 2^29 particle rows in one call");
+    const int n = (int)rows;
+    std::vector<int> cell32((size_t)n);
+    for (int i = 0; i < n; i++) {
+        if (cells[i] >= (uint64_t)h->N) return fail(h, MC_ERR_ARG, "particle row " + std::to_string(i) + ": no such cell");
+        cell32[i] = (int)cells[i];
+    }
+    const size_t N = (size_t)h->N;
+    CUDA_TRY(h, cudaMemsetAsync(h->src, 0, 5 * N * 8, h->stream));
+    if (n > 0) {
+        int n2 = 2048;
+        while (n2 < n) n2 <<= 1;
+        char *buf = nullptr;
+        const size_t keys_b = (size_t)n2 * 8, rows_b = ((size_t)5 * n * 8 + 255) & ~(size_t)255;
+        int rc = input_buffer(h, keys_b + rows_b + (size_t)n * 4, &buf);
+        if (rc) return rc;
+        uint64_t *keys = (uint64_t *)buf;
+        double *d_rows = (double *)(buf + keys_b);
+        int *d_cells = (int *)(buf + keys_b + rows_b);
+        CUDA_TRY(h, cudaMemcpyAsync(d_cells, cell32.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(d_rows, terms, (size_t)5 * n * 8, cudaMemcpyHostToDevice, h->stream));
+        launch(h, K_EXCHANGE, [&] { particle_keys(h->stream, n, n2, d_cells, keys); });
+        launch(h, K_EXCHANGE, [&] { sort_keys(h->stream, keys, n2); });
+        launch(h, K_EXCHANGE, [&] {
+            particle_sums(h->stream, n, keys, d_rows, h->reordered ? h->d_cell_o2n : nullptr, h->N, h->src);
+        });
+        rc = check_launch(h);
+        if (rc) return rc;
+    }
+    // the total mass source, summed in the caller's cell order as mc_flow_set_sources does
+    std::vector<double> fuel(N);
+    CUDA_TRY(h, cudaMemcpyAsync(fuel.data(), h->src + 4 * N, N * 8, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    double total = 0.0;
+    for (size_t i = 0; i < N; i++) total += fuel[h->reordered ? (size_t)h->cell_o2n[i] : i];
+    h->mass_source_total = total;
+    h->sources_set = 1;
+    return MC_OK;
+}
+
+int mc_flow_get_sources(mc_flow *h, double *terms)
+{
+    if (!h || !terms) return MC_ERR_ARG;
+    const size_t N = (size_t)h->N;
+    std::vector<double> soa(5 * N);
+    CUDA_TRY(h, cudaMemcpyAsync(soa.data(), h->src, 5 * N * 8, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    for (size_t i = 0; i < N; i++) {
+        const size_t j = h->reordered ? (size_t)h->cell_o2n[i] : i;
+        for (int k = 0; k < 5; k++) terms[5 * i + k] = soa[k * N + j];
+    }
+    return MC_OK;
+}
+
+int mc_flow_interpolate_nodes(mc_flow *h, int64_t n_cells, const uint64_t *cells, int64_t max_nodes,
+                              int64_t *n_nodes, uint64_t *node_ids, double *node_fields)
+{
+    if (!h || n_cells < 0 || (n_cells > 0 && !cells) || !n_nodes) return MC_ERR_ARG;
+    if (n_cells > INT32_MAX) return fail(h, MC_ERR_UNSUPPORTED, "too many requested cells");
+    const int n = (int)n_cells;
+    std::vector<int> req((size_t)n);
+    for (int i = 0; i < n; i++) {
+        if (cells[i] >= (uint64_t)h->N) return fail(h, MC_ERR_ARG, "requested cell " + std::to_string(i) + ": no such cell");
+        req[i] = (int)cells[i];
+    }
+    int rc = setup_nodes(h);
+    if (rc) return rc;
+    int count = 0;
+    if (n > 0) {
+        char *buf = nullptr;
+        rc = input_buffer(h, (size_t)n * 4, &buf);
+        if (rc) return rc;
+        int *d_req = (int *)buf;
+        CUDA_TRY(h, cudaMemcpyAsync(d_req, req.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h->stream));
+        launch(h, K_EXCHANGE, [&] { mark_nodes(h->stream, n, d_req, h->d_cell_nodes, h->node_flag); });
+        launch(h, K_EXCHANGE,
+               [&] { compact_nodes(h->stream, h->P, h->node_flag, h->node_counts, h->node_list, h->node_count); });
+        CUDA_TRY(h, cudaMemcpyAsync(&count, h->node_count, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        rc = check_launch(h);
+        if (rc) return rc;
+    }
+    *n_nodes = count;
+    if (!node_ids && !node_fields) return MC_OK;  // size query
+    if (count > max_nodes) return fail(h, MC_ERR_ARG, "max_nodes is smaller than the number of nodes");
+    if (count == 0) return MC_OK;
+    NodeArgs a{};
+    a.U = h->phi[G_U];
+    a.V = h->phi[G_V];
+    a.W = h->phi[G_W];
+    a.P = h->phi[G_P];
+    a.T = h->phi[G_T];
+    for (int d = 0; d < 3; d++) {
+        a.gU[d] = h->grad[G_U][d];
+        a.gV[d] = h->grad[G_V][d];
+        a.gW[d] = h->grad[G_W][d];
+        a.gP[d] = h->grad[G_P][d];
+        a.gT[d] = h->grad[G_T][d];
+    }
+    a.xc = h->xc;
+    a.yc = h->yc;
+    a.zc = h->zc;
+    a.px = h->px;
+    a.py = h->py;
+    a.pz = h->pz;
+    a.pc_off = h->pc_off;
+    a.pc_cells = h->pc_cells;
+    a.u_ref = h->prm.inlet_u;
+    a.p_ref = h->prm.pressure0;
+    a.t_ref = h->prm.temperature0;
+    launch(h, K_EXCHANGE, [&] { node_values(h->stream, count, h->node_list, a, h->node_out); });
+    rc = check_launch(h);
+    if (rc) return rc;
+    std::vector<int> ids((size_t)count);
+    CUDA_TRY(h, cudaMemcpyAsync(ids.data(), h->node_list, (size_t)count * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (node_fields)
+        CUDA_TRY(h, cudaMemcpyAsync(node_fields, h->node_out, (size_t)count * 5 * 8, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (node_ids)
+        for (int i = 0; i < count; i++) node_ids[i] = (uint64_t)ids[i];
+    return MC_OK;
 }
 
 int mc_flow_get_cell_order(mc_flow *h, int *cell_new_to_old)

@@ -127,6 +127,10 @@ _SIGNATURES = {
     "mc_flow_get_face_array": (c_int, [c_vp, c_int, c_vp]),
     "mc_flow_get_cell_order": (c_int, [c_vp, c_vp]),
     "mc_flow_write_vtk": (c_int, [c_vp, ctypes.c_char_p, c_int]),
+    "mc_flow_ingest_particles": (c_int, [c_vp, ctypes.c_int64, c_vp, c_vp]),
+    "mc_flow_get_sources": (c_int, [c_vp, c_vp]),
+    "mc_flow_interpolate_nodes": (c_int, [c_vp, ctypes.c_int64, c_vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
+                                          c_vp, c_vp]),
     "mc_flow_checkpoint_write": (c_int, [c_vp, ctypes.c_char_p]),
     "mc_flow_checkpoint_read": (c_int, [c_vp, ctypes.c_char_p]),
     "mc_flow_set_guess_params": (c_int, [c_vp, c_vp, c_int]),
@@ -346,6 +350,33 @@ class FlowSolver:
         if a.shape != (self.N, 5):
             raise ValueError("particle terms must be [cells][5]")
         _check(self.L.mc_flow_set_sources(self.h, _ptr(a)), self.h, "set_sources")
+
+    def ingest_particles(self, cells, terms):
+        """Particle rows (cell id, particle_aos) in arrival order become the
+        source terms (the flow side of update_flow_field)."""
+        c = np.ascontiguousarray(cells, dtype=np.uint64)
+        t = np.ascontiguousarray(terms, dtype=np.float64)
+        if t.shape != (c.shape[0], 5):
+            raise ValueError("terms must be [rows][5]")
+        _check(self.L.mc_flow_ingest_particles(self.h, c.shape[0], _ptr(c), _ptr(t)), self.h, "ingest_particles")
+
+    def sources(self):
+        a = np.empty((self.N, 5))
+        _check(self.L.mc_flow_get_sources(self.h, _ptr(a)), self.h, "get_sources")
+        return a
+
+    def interpolate_nodes(self, cells):
+        """(node ids ascending, [nodes][5] = vel.x, vel.y, vel.z, pressure, temp)
+        for the nodes of the given cells."""
+        c = np.ascontiguousarray(cells, dtype=np.uint64)
+        n = ctypes.c_int64()
+        _check(self.L.mc_flow_interpolate_nodes(self.h, c.shape[0], _ptr(c), 0, ctypes.byref(n), None, None),
+               self.h, "interpolate_nodes")
+        ids = np.empty(n.value, dtype=np.uint64)
+        vals = np.empty((n.value, 5))
+        _check(self.L.mc_flow_interpolate_nodes(self.h, c.shape[0], _ptr(c), n.value, ctypes.byref(n), _ptr(ids),
+                                                _ptr(vals)), self.h, "interpolate_nodes")
+        return ids, vals
 
     def face_array(self, which):
         width = {4: 2, 5: 3, 6: 3}.get(which, 1)

@@ -312,6 +312,17 @@ int mcref_stage_scalar(void *vh, int field)
     default: return -1;
     }
 }
+// The flow side of the flow/particle exchange (FlowSolver::update_flow_field,
+// FlowSolver.inl:496-736) with the messages staged in the MPI shim
+// (mcshim_inject_rank): particle terms summed into mesh->particle_terms and
+// node values sent back to each rank (mcshim_outbox_*).
+void mcref_update_flow_field(void *vh) { ((RefHandle *)vh)->solver->update_flow_field(); }
+void mcref_get_particle_terms(void *vh, double *out)
+{
+    RefHandle *h = (RefHandle *)vh;
+    std::memcpy(out, h->mesh->particle_terms, h->mesh->local_mesh_size * sizeof(particle_aos<double>));
+}
+
 // FlowSolver::output_data's writer (VisitWriter<T>::write_flow,
 // VisitWriter.hpp:127-234) on the current fields.
 void mcref_write_flow(void *vh, const char *prefix, int id)

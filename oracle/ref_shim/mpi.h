@@ -7,10 +7,13 @@
  *
  * Semantics with one rank:
  *  - reductions, gathers and broadcasts copy (or leave in place) the local value;
- *  - point-to-point traffic never happens (the solver has no halos on one rank);
- *  - MPI_Iprobe never finds a message, MPI_Test/Ibcast complete at once, which
- *    makes FlowSolver::update_flow_field (FlowSolver.inl:496-736) return after
- *    zeroing the particle terms;
+ *  - point-to-point traffic only exists as staged by the harness: messages
+ *    "from particle ranks" (cell indexes with tag 0, particle_aos rows with
+ *    tag 2) queued with mcshim_inject_rank are found by MPI_Iprobe and
+ *    delivered by MPI_Irecv, and every MPI_Isend is recorded in an outbox
+ *    (mcshim_outbox_*), so FlowSolver::update_flow_field
+ *    (FlowSolver.inl:496-736) runs its whole exchange; with nothing queued it
+ *    returns after zeroing the particle terms; MPI_Test/Ibcast complete at once;
  *  - MPI_Win_allocate_shared is a zeroed allocation.
  */
 #pragma once
@@ -70,6 +73,9 @@ extern "C" {
 #endif
 int mcshim_type_size(MPI_Datatype t);
 MPI_Datatype mcshim_type_register(int bytes);
+int mcshim_iprobe(int *flag, struct MPI_Status *st);
+int mcshim_irecv(void *buf, size_t bytes, int src, int tag);
+int mcshim_isend(const void *buf, size_t bytes, int dst, int tag);
 #ifdef __cplusplus
 }
 #endif
@@ -118,11 +124,11 @@ static inline int MPI_Ibcast(void *b, int n, MPI_Datatype t, int root, MPI_Comm 
 static inline int MPI_Bcast(void *b, int n, MPI_Datatype t, int root, MPI_Comm c)
 { (void)b; (void)n; (void)t; (void)root; (void)c; return 0; }
 static inline int MPI_Iprobe(int src, int tag, MPI_Comm c, int *flag, MPI_Status *st)
-{ (void)src; (void)tag; (void)c; (void)st; *flag = 0; return 0; }
+{ (void)src; (void)c; if (tag != 0) { *flag = 0; return 0; } return mcshim_iprobe(flag, st); }
 static inline int MPI_Probe(int src, int tag, MPI_Comm c, MPI_Status *st)
 { (void)src; (void)tag; (void)c; (void)st; abort(); return 0; }
 static inline int MPI_Get_count(const MPI_Status *st, MPI_Datatype t, int *count)
-{ (void)st; (void)t; *count = 0; return 0; }
+{ *count = st ? (int)(st->_ucount / (size_t)mcshim_type_size(t)) : 0; return 0; }
 static inline int MPI_Test(MPI_Request *req, int *flag, MPI_Status *st)
 { (void)st; *req = MPI_REQUEST_NULL; *flag = 1; return 0; }
 static inline int MPI_Testall(int n, MPI_Request *reqs, int *flag, MPI_Status *st)
@@ -130,12 +136,12 @@ static inline int MPI_Testall(int n, MPI_Request *reqs, int *flag, MPI_Status *s
 static inline int MPI_Wait(MPI_Request *req, MPI_Status *st) { (void)st; *req = MPI_REQUEST_NULL; return 0; }
 static inline int MPI_Waitall(int n, MPI_Request *reqs, MPI_Status *st)
 { (void)st; for (int i = 0; i < n; i++) reqs[i] = MPI_REQUEST_NULL; return 0; }
-/* Point-to-point never runs with one rank; reaching it means the harness set
- * up more than one flow block, which is a harness bug. */
+/* Staged point-to-point: receives come from the injected messages, sends go
+ * to the outbox; both complete at once.  Anything else aborts (a harness bug). */
 static inline int MPI_Isend(const void *b, int n, MPI_Datatype t, int dst, int tag, MPI_Comm c, MPI_Request *req)
-{ (void)b; (void)n; (void)t; (void)dst; (void)tag; (void)c; (void)req; abort(); return 0; }
+{ (void)c; *req = MPI_REQUEST_NULL; return mcshim_isend(b, (size_t)n * (size_t)mcshim_type_size(t), dst, tag); }
 static inline int MPI_Irecv(void *b, int n, MPI_Datatype t, int src, int tag, MPI_Comm c, MPI_Request *req)
-{ (void)b; (void)n; (void)t; (void)src; (void)tag; (void)c; (void)req; abort(); return 0; }
+{ (void)c; *req = MPI_REQUEST_NULL; return mcshim_irecv(b, (size_t)n * (size_t)mcshim_type_size(t), src, tag); }
 static inline int MPI_Recv(void *b, int n, MPI_Datatype t, int src, int tag, MPI_Comm c, MPI_Status *st)
 { (void)b; (void)n; (void)t; (void)src; (void)tag; (void)c; (void)st; abort(); return 0; }
 static inline int MPI_Send(const void *b, int n, MPI_Datatype t, int dst, int tag, MPI_Comm c)

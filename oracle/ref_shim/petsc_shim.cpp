@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <map>
 #include <string>
@@ -35,6 +36,85 @@ extern "C" MPI_Datatype mcshim_type_register(int bytes)
 {
     g_type_sizes.push_back(bytes);
     return (MPI_Datatype)(100 + (int)g_type_sizes.size() - 1);
+}
+
+// ------------------------------------------------- staged point-to-point
+// Messages from fake particle ranks for update_flow_field: per rank, tag 0
+// carries uint64 cell indexes and tag 2 the particle_aos rows.  Sends are
+// recorded as (destination, tag, bytes).
+struct StagedRank {
+    int rank;
+    std::vector<char> part[3];
+    bool probed = false;
+};
+static std::vector<StagedRank> g_staged;
+struct SentMessage {
+    int dst, tag;
+    std::vector<char> data;
+};
+static std::vector<SentMessage> g_outbox;
+
+extern "C" void mcshim_inject_reset()
+{
+    g_staged.clear();
+    g_outbox.clear();
+}
+
+extern "C" void mcshim_inject_rank(int rank, long n, const uint64_t *cells, const double *aos, int aos_doubles)
+{
+    StagedRank r;
+    r.rank = rank;
+    r.part[0].assign((const char *)cells, (const char *)cells + n * sizeof(uint64_t));
+    r.part[2].assign((const char *)aos, (const char *)aos + n * aos_doubles * sizeof(double));
+    g_staged.push_back(r);
+}
+
+extern "C" int mcshim_iprobe(int *flag, MPI_Status *st)
+{
+    *flag = 0;
+    for (StagedRank &r : g_staged) {
+        if (r.probed) continue;
+        r.probed = true;
+        *flag = 1;
+        if (st) {
+            st->MPI_SOURCE = r.rank;
+            st->MPI_TAG = 0;
+            st->_ucount = r.part[0].size();
+        }
+        return 0;
+    }
+    return 0;
+}
+
+extern "C" int mcshim_irecv(void *buf, size_t bytes, int src, int tag)
+{
+    for (StagedRank &r : g_staged) {
+        if (r.rank != src || (tag != 0 && tag != 2) || r.part[tag].size() < bytes) continue;
+        std::memcpy(buf, r.part[tag].data(), bytes);
+        return 0;
+    }
+    std::fprintf(stderr, "mpi shim: no staged message from %d with tag %d\n", src, tag);
+    std::abort();
+}
+
+extern "C" int mcshim_isend(const void *buf, size_t bytes, int dst, int tag)
+{
+    SentMessage m{dst, tag, std::vector<char>((const char *)buf, (const char *)buf + bytes)};
+    g_outbox.push_back(std::move(m));
+    return 0;
+}
+
+extern "C" long mcshim_outbox_count() { return (long)g_outbox.size(); }
+
+// Message i of the outbox: destination, tag and size; copies the bytes when out is given.
+extern "C" long mcshim_outbox_get(long i, int *dst, int *tag, void *out)
+{
+    if (i < 0 || (size_t)i >= g_outbox.size()) return -1;
+    const SentMessage &m = g_outbox[i];
+    *dst = m.dst;
+    *tag = m.tag;
+    if (out) std::memcpy(out, m.data.data(), m.data.size());
+    return (long)m.data.size();
 }
 
 // ---------------------------------------------------------------- PETSc

@@ -258,6 +258,13 @@ def ref_lib():
         L.mcref_first_pressure.argtypes = [c_vp]
         L.mcref_stage_scalar.argtypes = [c_vp, c_int]
         L.mcref_write_flow.argtypes = [c_vp, ctypes.c_char_p, c_int]
+        L.mcshim_inject_reset.argtypes = []
+        L.mcshim_inject_rank.argtypes = [c_int, ctypes.c_long, c_vp, c_vp, c_int]
+        L.mcshim_outbox_count.restype = ctypes.c_long
+        L.mcshim_outbox_get.argtypes = [ctypes.c_long, ctypes.POINTER(c_int), ctypes.POINTER(c_int), c_vp]
+        L.mcshim_outbox_get.restype = ctypes.c_long
+        L.mcref_update_flow_field.argtypes = [c_vp]
+        L.mcref_get_particle_terms.argtypes = [c_vp, c_vp]
         L.mcref_stage_scalar.restype = c_int
         L.mcref_timestep_count.argtypes = [c_vp]
         L.mcref_timestep_count.restype = c_u64
@@ -349,6 +356,33 @@ class Reference:
 
     def stage_scalar(self, name):
         assert self.L.mcref_stage_scalar(self.h, FIELDS[name]) == 0
+
+    def exchange(self, messages):
+        """FlowSolver::update_flow_field with the given messages from particle
+        ranks ({rank: (cells, rows[n][5])}, processed in that order).  Returns
+        the particle terms [cells][5] and, per rank, the node ids and the
+        flow_aos values [n][5] the reference sent back."""
+        L = self.L
+        L.mcshim_inject_reset()
+        keep = []
+        for rank, (cells, rows) in messages.items():
+            c = np.ascontiguousarray(cells, dtype=np.uint64)
+            r = np.ascontiguousarray(rows, dtype=np.float64)
+            keep += [c, r]
+            L.mcshim_inject_rank(rank, c.shape[0], _ptr(c), _ptr(r), 5)
+        L.mcref_update_flow_field(self.h)
+        terms = np.zeros((self.N, 5))
+        L.mcref_get_particle_terms(self.h, _ptr(terms))
+        sent = {}
+        for i in range(L.mcshim_outbox_count()):
+            d, t = c_int(), c_int()
+            nb = L.mcshim_outbox_get(i, ctypes.byref(d), ctypes.byref(t), None)
+            buf = np.zeros(nb // 8)
+            L.mcshim_outbox_get(i, ctypes.byref(d), ctypes.byref(t), _ptr(buf))
+            entry = sent.setdefault(d.value, {})
+            entry[t.value] = buf.view(np.uint64) if t.value == 0 else buf.reshape(-1, 5)
+        L.mcshim_inject_reset()
+        return terms, {r: (e[0], e[1]) for r, e in sent.items()}
 
     def write_flow(self, prefix, id):
         """The reference's VisitWriter output of the current fields; returns the file name."""

@@ -72,20 +72,29 @@ def test_all_fields_ten_passes_match_reference_golden(gpu, reorder):
 
 @pytest.mark.parametrize("reorder", [flow.REORDER_NONE, flow.REORDER_RCM], ids=["natural", "rcm"])
 def test_scalar_assembly_bitwise(gpu, reorder):
-    """Each Scalar_solve from the same developed state: gradients, matrix and
-    right-hand side bit for bit (epsilon's wall-cell right-hand sides within
-    one unit in the last place), fields after the solve within 1e-12."""
+    """Each Scalar_solve from the same state (seeded velocities, pressure, T and
+    random positive scalars; mass fluxes from set_up_field): gradients, matrix
+    and right-hand side bit for bit (epsilon's wall-cell right-hand sides
+    within one unit in the last place), fields after the solve within 1e-12."""
     dims, lengths = (9, 5, 4), (0.18, 0.1, 0.08)
     solver, orc = pair(dims, lengths, reorder=reorder)
     seed(solver, solver.N, BASE_COMPAT, 3)
     seed(orc, orc.N, BASE_COMPAT, 3)
-    for _ in range(2):
-        solver.simple_iteration()
-        orc.step()
-    for name in ALL_FIELDS:  # continue both from the oracle's state
-        solver.set_field(name, orc.field(name))
+    # developed-looking scalars (positive k and epsilon of varied size), the
+    # same on both sides; then the mass fluxes of set_up_field, which both
+    # sides compute bit for bit from the same fields
+    rng = np.random.default_rng(5)
+    for name, lo, hi in (("TE", 1e-3, 40.0), ("ED", 1e-2, 5e3), ("FUL", 0.0, 0.1), ("PRO", 0.0, 1e-3),
+                         ("VARF", 0.0, 0.1), ("VARP", 0.0, 1e-3)):
+        a = orc.field(name)
+        a[:orc.N] = rng.uniform(lo, hi, orc.N)
+        orc.set_field(name, a)
+        solver.set_field(name, a)
     solver.stage("gradients")
     orc.L.mco_stage_gradients(orc.h)
+    solver.stage("set_up_field")
+    orc.L.mco_stage_set_up_field(orc.h)
+    assert np.array_equal(solver.face_array(0), orc.face_array(0))
     for name in GRAD_FIELDS:
         assert np.array_equal(solver.gradient(name), orc.grad(name)), name
     for name in SCALARS:
