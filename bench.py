@@ -48,7 +48,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from minicombust_app_b200 import replicas  # noqa: E402
-from minicombust_app_b200.workload import gaussian_blobs, noisy_fields  # noqa: E402
+from minicombust_app_b200.workload import (blob_phases, blob_stencils, gaussian_blobs, noisy_fields,  # noqa: E402
+                                           varying_sources)
 
 METRIC = "SIMPLE iters/s at 4.2M cells: learned+FP32-refined vs plain FP64, same 1e-8 residual"
 UNIT = "iters/s"
@@ -68,6 +69,10 @@ def parse():
                     help="pressure-correction preconditioner of the plain path (aggregation AMG or Jacobi)")
     ap.add_argument("--no-field-check", action="store_true", help="skip the comparison with the CPU oracle")
     ap.add_argument("--oracle-passes", type=int, default=3, help="passes compared with the CPU oracle")
+    ap.add_argument("--source-period", type=int, default=0,
+                    help="> 0: blob amplitudes vary as sin(2 pi pass / period + random phase), sources updated "
+                         "on the device every pass (the largest benchmark configuration)")
+    ap.add_argument("--reorder", default="none", choices=["none", "rcm"], help="cell order inside the solver")
     ap.add_argument("--ref-sample-m", type=int, default=48,
                     help="--impl reference: each step is one reference pass on the 2m x m x m box")
     ap.add_argument("--config", default="both", choices=["both", "headline", "plain"],
@@ -267,10 +272,11 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
-def oracle_run(m, blobs, passes, rtol, threads, warm=0):
+def oracle_run(m, blobs, passes, rtol, threads, warm=0, period=0):
     """The CPU oracle (the C restatement, simple mode) on the benchmark box
     from the benchmark's initial state: fields after warm + passes passes,
-    and the seconds per pass of the last `passes`."""
+    and the seconds per pass of the last `passes` (with period > 0 the
+    time-varying sources of each pass are set before it)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from checkers import SIMPLE, Oracle, oracle_lib, oracle_mesh, oracle_params
     dims, lengths = (2 * m, m, m), (0.2, 0.1, 0.1)
@@ -280,14 +286,24 @@ def oracle_run(m, blobs, passes, rtol, threads, warm=0):
         a = orc.field(name)
         a[:orc.N] = vals
         orc.set_field(name, a)
-    orc.set_sources(gaussian_blobs(dims, lengths, blobs, seed=0))
+    if period > 0:
+        stencils, phases = blob_stencils(dims, lengths, blobs, seed=0), blob_phases(blobs, seed=0)
+    else:
+        orc.set_sources(gaussian_blobs(dims, lengths, blobs, seed=0))
+    it = 0
     for _ in range(warm):
+        if period > 0:
+            orc.set_sources(varying_sources(orc.N, stencils, phases, it, period))
         if orc.step() != 0:
             raise RuntimeError("oracle solve did not converge")
+        it += 1
     t0 = time.perf_counter()
     for _ in range(passes):
+        if period > 0:
+            orc.set_sources(varying_sources(orc.N, stencils, phases, it, period))
         if orc.step() != 0:
             raise RuntimeError("oracle solve did not converge")
+        it += 1
     dt = (time.perf_counter() - t0) / passes
     fields = {n: orc.field(n)[:orc.N].copy() for n in FIELD_NAMES}
     orc.close()
@@ -301,15 +317,16 @@ FIELD_NAMES = ("U", "V", "W", "P", "TEM")
 
 def make_solver(flow, mesh, dims, lengths, args, rank, local, headline):
     """The benchmark solver of one configuration, seeded identically."""
+    reorder = flow.REORDER_RCM if args.reorder == "rcm" else flow.REORDER_NONE
     if headline:
         from minicombust_app_b200 import train_guess
         params = flow.default_params(flow.MODE_SIMPLE, device=local, p_rtol=1e-8, u_rtol=1e-8,
                                      pressure_solver=flow.PSOLVER_PCG_AMG, precision=flow.PRECISION_FP32_REFINED,
-                                     initial_guess=flow.GUESS_LEARNED)
+                                     initial_guess=flow.GUESS_LEARNED, reorder=reorder)
     else:
         psolver = flow.PSOLVER_PCG_AMG if args.psolver == "amg" else flow.PSOLVER_PCG_JACOBI
         params = flow.default_params(flow.MODE_SIMPLE, device=local, p_rtol=1e-8, u_rtol=1e-8,
-                                     pressure_solver=psolver)
+                                     pressure_solver=psolver, reorder=reorder)
     solver = flow.FlowSolver(mesh, params=params)
     if headline:
         solver.set_guess_params(train_guess.load_params())
@@ -318,13 +335,41 @@ def make_solver(flow, mesh, dims, lengths, args, rank, local, headline):
         a = solver.field(name)
         a[:N] = vals
         solver.set_field(name, a)
-    solver.set_sources(gaussian_blobs(dims, lengths, args.blobs, seed=rank))
+    if args.source_period <= 0:
+        solver.set_sources(gaussian_blobs(dims, lengths, args.blobs, seed=rank))
     return solver
 
 
-def timed_steps(torch, solver, stream, steps, barrier, max_over_ranks, local):
+class VaryingSources:
+    """The time-varying blob sources on the device: g = G w(pass), G the
+    [cells x blobs] stencil matrix (CSR), w_b = sin(2 pi pass / period +
+    phase_b); sources [5][cells] = (g, 0, 0, 1e3 g, 1e-2 g), handed to the
+    solver with mc_flow_set_sources_device on its stream every pass."""
+
+    def __init__(self, torch, dims, lengths, blobs, period, seed, device):
+        cells, values, blob = blob_stencils(dims, lengths, blobs, seed)
+        n = dims[0] * dims[1] * dims[2]
+        G = torch.sparse_coo_tensor(np.stack([cells, blob]), values, (n, blobs), dtype=torch.float64)
+        self.G = G.coalesce().to_sparse_csr().to(device)
+        self.phases = torch.tensor(blob_phases(blobs, seed), dtype=torch.float64, device=device)
+        self.coef = torch.tensor([1.0, 0.0, 0.0, 1.0e3, 1.0e-2], dtype=torch.float64, device=device)
+        self.src = torch.zeros((5, n), dtype=torch.float64, device=device)
+        self.period = period
+        self.torch = torch
+
+    def apply(self, solver, stream, it):
+        torch = self.torch
+        with torch.cuda.stream(stream):
+            w = torch.sin(2.0 * np.pi * it / self.period + self.phases)
+            g = (self.G @ w.unsqueeze(1)).squeeze(1)
+            torch.outer(self.coef, g, out=self.src)
+        solver.set_sources_device(self.src.data_ptr())
+
+
+def timed_steps(torch, solver, stream, steps, barrier, max_over_ranks, local, sources=None, it0=0):
     """Device-timed SIMPLE passes (CUDA events on the solver's stream,
-    barrier + synchronize on both sides, max over ranks), clocks sampled."""
+    barrier + synchronize on both sides, max over ranks), clocks sampled;
+    with time-varying sources each pass first updates them on the device."""
     stats = []
     launches0 = solver.launch_count()
     sampler = ClockSampler(local)
@@ -333,7 +378,9 @@ def timed_steps(torch, solver, stream, steps, barrier, max_over_ranks, local):
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    for _ in range(steps):
+    for k in range(steps):
+        if sources is not None:
+            sources.apply(solver, stream, it0 + k)
         solver.simple_iteration()
         stats.append(solver.last_stats.as_dict())
     ev1.record(stream)
@@ -437,14 +484,21 @@ def main():
     dims, lengths = (2 * m, m, m), (0.2, 0.1, 0.1)
     mesh = flow.Mesh.box(*dims, *lengths)
     N = mesh.n_cells
+    sources = None
+    if args.source_period > 0:
+        sources = VaryingSources(torch, dims, lengths, args.blobs, args.source_period, rank,
+                                 torch.device("cuda", local))
     runs = {}
     order = {"both": ("plain", "headline"), "headline": ("headline",), "plain": ("plain",)}[args.config]
     for cfg in order:
         solver = make_solver(flow, mesh, dims, lengths, args, rank, local, cfg == "headline")
         stream = torch.cuda.ExternalStream(solver.stream(), device=torch.device("cuda", local))
-        for _ in range(args.warmup):
+        for k in range(args.warmup):
+            if sources is not None:
+                sources.apply(solver, stream, k)
             solver.simple_iteration()
-        t, stats, clocks, launches = timed_steps(torch, solver, stream, args.steps, barrier, max_over_ranks, local)
+        t, stats, clocks, launches = timed_steps(torch, solver, stream, args.steps, barrier, max_over_ranks, local,
+                                                 sources, args.warmup)
         fields = {n: solver.field(n)[:N].copy() for n in FIELD_NAMES} if rank == 0 else None
         r = {"t": t, "stats": stats, "clocks": clocks, "launches": launches, "fields": fields}
         if cfg == order[-1]:
@@ -457,9 +511,11 @@ def main():
             barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            for _ in range(args.steps):
+            for k in range(args.steps):
                 for n in FIELD_NAMES:
                     flow._check(L.mc_flow_set_field(h, flow.FIELDS[n], pinned[n].data_ptr()), h, "set_field")
+                if sources is not None:
+                    sources.apply(solver, stream, args.warmup + args.steps + k)
                 solver.simple_iteration()
                 for n in FIELD_NAMES:
                     flow._check(L.mc_flow_get_field(h, flow.FIELDS[n], pinned[n].data_ptr()), h, "get_field")
@@ -480,12 +536,15 @@ def main():
         gpu_fields = {}
         for cfg in order:
             sv = make_solver(flow, mesh, dims, lengths, args, rank, local, cfg == "headline")
-            for _ in range(P):
+            sv_stream = torch.cuda.ExternalStream(sv.stream(), device=torch.device("cuda", local))
+            for k in range(P):
+                if sources is not None:
+                    sources.apply(sv, sv_stream, k)
                 sv.simple_iteration()
             gpu_fields[cfg] = {n: sv.field(n)[:N].copy() for n in FIELD_NAMES}
             sv.close()
         threads = host_threads()
-        ofields, _ = oracle_run(m, args.blobs, P, 1e-12, threads)
+        ofields, _ = oracle_run(m, args.blobs, P, 1e-12, threads, period=args.source_period)
         oracle_cmp = {"passes": P, "oracle": "CPU oracle (C restatement), simple mode, solves to 1e-12",
                       "oracle_threads": threads}
         for cfg in order:
@@ -501,7 +560,7 @@ def main():
             # a real pass of the CPU oracle (the port) on the benchmark box at
             # the benchmark's tolerances, on the host's cores
             threads = host_threads()
-            _, per_pass = oracle_run(m, args.blobs, 1, 1e-8, threads, warm=1)
+            _, per_pass = oracle_run(m, args.blobs, 1, 1e-8, threads, warm=1, period=args.source_period)
             cpu = {"value": 1.0 / per_pass, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"1 real SIMPLE pass of the CPU oracle (C restatement, simple mode, solves to 1e-8, "
                              f"unpreconditioned CG for the pressure correction) on the full 2*{m}^3 box after its "
@@ -528,7 +587,11 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if main_cfg == "headline" else "f64",
                 "data": "synthetic",
                 "config": {"workload": f"simple-mode SIMPLE pass, box 2*{m}x{m}x{m} = {N} cells, {args.blobs} "
-                                       f"source blobs, {desc}, BiCGStab momentum/T, rtol 1e-8",
+                                       + ("source blobs, " if args.source_period <= 0 else
+                                          f"source blobs with amplitudes sin(2 pi pass / {args.source_period} + "
+                                          "random phase) updated on the device every pass, ")
+                                       + f"{desc}, BiCGStab momentum/T, rtol 1e-8"
+                                       + (", RCM cell order" if args.reorder == "rcm" else ""),
                            "cells": N, "faces": mesh.n_faces, "l2": "inputs larger than L2 (~4.5 GB working set)",
                            "parallelism": "replicas" if world > 1 else "single GPU"},
                 "e2e": {"value": R["e2e"], "unit": UNIT, "h2d_bytes_per_step": R["e2e_bytes"],

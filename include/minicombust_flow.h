@@ -128,6 +128,10 @@ typedef struct mc_flow_params {
                                  two variances -- in the reference's order TE, ED, TEM, FUL, PRO,
                                  VARF, VARP (FlowSolver.inl:3229-3261).  Default: 1 in
                                  MC_MODE_COMPAT, 0 in MC_MODE_SIMPLE. */
+    int ir_line_steps;        /* MC_PRECISION_FP32_REFINED, momentum and temperature: k > 0 makes each inner
+                                 FP32 solve k steps of x-line block Jacobi (each x-line's tridiagonal block
+                                 solved exactly) on meshes whose cells run x-fastest along whole lines; 0,
+                                 or another mesh: inner BiCGStab.  Default 2. */
 } mc_flow_params;
 
 /* Per-pass statistics. */
@@ -172,6 +176,12 @@ int mc_flow_get_field(mc_flow *flow, int field, double *host_values);
 int mc_flow_get_gradient(mc_flow *flow, int field, double *host_values);
 /* Particle source terms, [cells][5] particle_aos<double> (Mesh::particle_terms). */
 int mc_flow_set_sources(mc_flow *flow, const double *host_particle_terms);
+/* The same from device memory the caller owns: terms_soa[5][cells] (component
+ * k of cell i at k * cells + i, caller's numbering) on the handle's device.
+ * The copy and the total mass source are formed on the handle's stream (the
+ * data must be ready on it); nothing crosses to the host, so time-varying
+ * sources can be updated every pass.  No reference counterpart. */
+int mc_flow_set_sources_device(mc_flow *flow, const double *terms_soa);
 /* Face arrays in reference face order.  which: 0 mass flux [faces], 1 area,
  * 2 lambda, 3 rlencos, 4 face_fields [faces][2], 5 normals [faces][3], 6 centres [faces][3]. */
 int mc_flow_get_face_array(mc_flow *flow, int which, double *host_values);

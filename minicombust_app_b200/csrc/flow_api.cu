@@ -38,7 +38,8 @@ enum KernelId {
     K_BICG1_1, K_BICG1_2, K_BICG1_3, K_AMG_SETUP, K_PCG_INIT_AMG, K_PCG_ITER2_AMG, K_AMG_VCYCLE,
     K_IR, K_PCG_INIT_AMG32, K_PCG_ITER1_32, K_PCG_ITER2_AMG32, K_AMG_VCYCLE32, K_PERMUTE, K_GUESS, K_GNN,
     K_SNAPSHOT, K_BIR, K_ROUND_ELL, K_BICG3_INIT32, K_BICG3_1_32, K_BICG3_2_32, K_BICG3_3_32, K_BICG1_INIT32,
-    K_BICG1_1_32, K_BICG1_2_32, K_BICG1_3_32, K_GRAD6, K_SCALAR, K_SCALAR_CLIP, K_EXCHANGE, K_COUNT
+    K_BICG1_1_32, K_BICG1_2_32, K_BICG1_3_32, K_GRAD6, K_SCALAR, K_SCALAR_CLIP, K_EXCHANGE, K_LINE3, K_LINE1,
+    K_COUNT
 };
 
 const char *kKernelNames[K_COUNT] = {
@@ -51,7 +52,8 @@ const char *kKernelNames[K_COUNT] = {
     "pcg32_iter1_spmv", "pcg32_iter2_amg_update", "amg32_vcycle", "permute", "guess_select", "gnn_forward",
     "snapshot_pack", "bicg_refine_fp64_residual", "round_fp32", "bicg3_32_init", "bicg3_32_1_spmv",
     "bicg3_32_2_spmv", "bicg3_32_3_update", "bicg1_32_init", "bicg1_32_1_spmv", "bicg1_32_2_spmv",
-    "bicg1_32_3_update", "lsq_gradients_scalars", "scalar_assemble", "scalar_clip_negative", "particle_exchange"};
+    "bicg1_32_3_update", "lsq_gradients_scalars", "scalar_assemble", "scalar_clip_negative", "particle_exchange",
+    "line_jacobi3_32", "line_jacobi1_32"};
 
 constexpr int PCG_BATCH = 16;   // iterations per status read (even: ping-pong buffers)
 constexpr int PCG_AMG_BATCH = 4;
@@ -154,6 +156,11 @@ struct mc_flow {
     BirState<1> *h_bo1 = nullptr;
     cudaGraphExec_t g_b3_32 = nullptr, g_b1_32 = nullptr;
     char *bir_mem = nullptr;
+    // x-line block-Jacobi inner solves (ir_line_steps > 0 on a box whose
+    // cells run x-fastest): line length, the two systems and a scratch iterate
+    int line_ex = 0;
+    LineSystem line3{}, line1{};
+    float *line_scratch = nullptr;
     // initial guess of the pressure correction
     double *pp_prev = nullptr;        // previous converged correction [N]
     GuessState *gs = nullptr;
@@ -208,6 +215,7 @@ struct mc_flow {
     int pass_in_step = 0;
     int sources_set = 0;
     double mass_source_total = 0.0;
+    bool mass_source_on_device = false;  // sources set from device memory: total in scalars[2]
     double p_bnorm_ref = 0.0;
     long launches = 0;
     Timing timing;
@@ -731,6 +739,8 @@ int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const B
                        cudaGraphExec_t *loop, int kid_init32, int kid1_32, int iters_out[R])
 {
     constexpr int kMaxOuter = 30;
+    const LineSystem *line = nullptr;
+    if (h->prm.ir_line_steps > 0 && h->line_ex > 0) line = (R == 3) ? &h->line3 : &h->line1;
     launch(h, K_BIR, [&] { bir_init<R>(h->stream, A, out, h->prm.u_rtol, kMaxOuter); });
     int rc = check_launch(h);
     if (rc) return rc;
@@ -762,6 +772,25 @@ int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const B
         }
         if (hout->all_done) break;
         if (outer > kMaxOuter) return fail(h, MC_ERR_NOT_CONVERGED, "refinement state did not advance");
+        if (line) {
+            // a fixed number of x-line block-Jacobi steps on the row-scaled
+            // FP32 system; the last step writes the inner solution out.e
+            const int K = h->prm.ir_line_steps;
+            float *E[2] = {const_cast<float *>(out.e), h->line_scratch};
+            for (int k = 1; k <= K; k++) {
+                float *dst = E[(K - k) % 2];
+                const float *prev = E[(K - k + 1) % 2];
+                launch(h, R == 3 ? K_LINE3 : K_LINE1,
+                       [&] { line_step<R>(h->stream, *line, out.r32, prev, dst, k == 1 ? 1 : 0); });
+            }
+            for (int j = 0; j < R; j++)
+                if (!hout->done[j]) iters_out[j] += K;
+            launch(h, K_BIR, [&] { bir_add<R>(h->stream, A.N, out); });
+            launch(h, K_BIR, [&] { bir_residual<R>(h->stream, A, out); });
+            rc = check_launch(h);
+            if (rc) return rc;
+            continue;
+        }
         double inner_rtol = 0.5;
         for (int j = 0; j < R; j++)
             if (!hout->done[j] && hout->rr[j] > 0)
@@ -855,6 +884,8 @@ void launch_mass_flux(mc_flow *h)
     a.counter = h->counter;
     a.balance = h->balance;
     a.mass_source_total = (h->prm.mode == MC_MODE_SIMPLE && h->sources_set) ? h->mass_source_total : 0.0;
+    a.mass_source_dev = (h->prm.mode == MC_MODE_SIMPLE && h->sources_set && h->mass_source_on_device)
+                            ? h->scalars + 2 : nullptr;
     const int grid = std::min(blocks_for(h->F), krylov_grid(h->F));
     launch(h, K_MASS_FLUX, [&] { k_mass_flux<<<grid, MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a); });
     if (h->margs.n_outlet > 0)
@@ -1441,6 +1472,33 @@ int setup_bicg_refined(mc_flow *h)
     h->bo3 = BirVectors<3>{{h->phi[G_U], h->phi[G_V], h->phi[G_W]}, h->b_m, vec[1], vec[0], h->partials, h->counter,
                            bo3};
     h->bo1 = BirVectors<1>{{h->phi[G_T]}, h->b_t, vec[1], vec[0], h->partials, h->counter, bo1};
+    if (h->line_ex > 0) {
+        // the FP32 copies are stored by direction: slot d holds direction d
+        LineSystem L;
+        L.N = h->N;
+        L.ex = h->line_ex;
+        L.P = 1;
+        while (L.P < L.ex) L.P <<= 1;
+        int q = 0;
+        for (int d = 0; d < 6; d++) {
+            if (h->dc.doff[d] == -1)
+                L.dxm = d;
+            else if (h->dc.doff[d] == 1)
+                L.dxp = d;
+            else {
+                L.yz[q] = d;
+                L.yzoff[q] = h->dc.doff[d];
+                q++;
+            }
+        }
+        h->line3 = L;
+        h->line3.d = h->m32_diag;
+        h->line3.off = h->m32_off;
+        h->line1 = L;
+        h->line1.d = h->t32_diag;
+        h->line1.off = h->t32_off;
+        h->line_scratch = vec[2];  // the inner BiCGStab's r, unused by the line solver
+    }
     CUDA_TRY(h, cudaMallocHost((void **)&h->h_bi3, sizeof(BicgState<3>)));
     CUDA_TRY(h, cudaMallocHost((void **)&h->h_bi1, sizeof(BicgState<1>)));
     CUDA_TRY(h, cudaMallocHost((void **)&h->h_bo3, sizeof(BirState<3>)));
@@ -1498,6 +1556,32 @@ int setup_guess(mc_flow *h, const HostMesh &hm)
 
 // MC_DIR_CODES=0 keeps the column lists even where direction codes apply
 // (the tests use it to check both forms).
+// Length of the x-lines when the rows form them: the -x and +x neighbours
+// are row -/+ 1 (direction codes), every row at a multiple of ex lacks a -x
+// neighbour and every other row has one, and likewise for +x at the line
+// ends; 0 otherwise (or when a line would not fit one thread block).
+int x_line_length(const std::vector<uint32_t> &code, const int doff[6], int N)
+{
+    int dxm = -1, dxp = -1, ex = 0;
+    for (int d = 0; d < 6; d++) {
+        if (doff[d] == -1) dxm = d;
+        if (doff[d] == 1) dxp = d;
+    }
+    for (int d = 0; d < 6; d++)
+        if (doff[d] > 1 && (ex == 0 || doff[d] < ex)) ex = doff[d];
+    if (dxm < 0 || dxp < 0 || ex < 2 || ex > 1024 || N % ex != 0) return 0;
+    for (int i = 0; i < N; i++) {
+        bool m = false, p = false;
+        for (int k = 0; k < 6; k++) {
+            const unsigned d = (code[i] >> (3 * k)) & 7u;
+            m = m || d == (unsigned)dxm;
+            p = p || d == (unsigned)dxp;
+        }
+        if (m != (i % ex != 0) || p != (i % ex != ex - 1)) return 0;
+    }
+    return ex;
+}
+
 bool dir_codes_disabled()
 {
     const char *v = std::getenv("MC_DIR_CODES");
@@ -1708,6 +1792,7 @@ void mc_flow_default_params(mc_flow_params *p, int mode)
     p->amg_cheb_ratio = 4.0;
     p->reorder = MC_REORDER_NONE;
     p->transport_scalars = mode == MC_MODE_COMPAT ? 1 : 0;
+    p->ir_line_steps = 2;
     if (mode == MC_MODE_COMPAT) {
         p->viscosity = 0.000014;
         p->temperature0 = 2000.0;
@@ -1745,6 +1830,7 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
         (params->amg_sweeps < 1 || params->amg_sweeps > AMG_MAX_SWEEPS || !(params->amg_omega > 0) ||
          !(params->amg_alpha > 0) || !(params->amg_cheb_ratio == 0 || params->amg_cheb_ratio > 1)))
         return MC_ERR_ARG;
+    if (params->ir_line_steps < 0 || params->ir_line_steps > 8) return MC_ERR_ARG;
     if (!(params->delta > 0) || !(params->urf_momentum > 0) || !(params->urf_temperature > 0) ||
         !(params->u_rtol > 0) || !(params->p_rtol > 0) || params->max_iters <= 0)
         return MC_ERR_ARG;
@@ -1867,6 +1953,7 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
                         const unsigned d = (canon >> (3 * k)) & 7u;
                         h->dc.coff[k] = d < 6 ? doff[d] : 0;
                     }
+                    h->line_ex = x_line_length(code, doff, (int)N);
                 }
             }
             if (!rc && params->pressure_solver == MC_PSOLVER_PCG_AMG) rc = build_amg(h, hm);
@@ -2196,6 +2283,8 @@ int mc_flow_checkpoint_write(mc_flow *h, const char *path)
     hd.first_pressure = h->first_pressure;
     hd.sources_set = h->sources_set;
     hd.mass_source_total = h->mass_source_total;
+    if (h->mass_source_on_device)  // sources set from device memory: their total lives on the device
+        CUDA_TRY(h, cudaMemcpy(&hd.mass_source_total, h->scalars + 2, sizeof(double), cudaMemcpyDeviceToHost));
     bool ok = std::fwrite(&hd, sizeof(hd), 1, fp) == 1;
     std::vector<double> buf;
     for (const auto &arr : checkpoint_arrays(h)) {
@@ -2242,6 +2331,7 @@ int mc_flow_checkpoint_read(mc_flow *h, const char *path)
     h->first_pressure = hd.first_pressure;
     h->sources_set = hd.sources_set;
     h->mass_source_total = hd.mass_source_total;
+    h->mass_source_on_device = false;
     // a pressure system carried over from before (compat mode) needs its AMG
     // values; the coarsest inverse is formed in line
     if (h->use_amg && !h->first_pressure) {
@@ -2361,6 +2451,7 @@ int mc_flow_ingest_particles(mc_flow *h, int64_t rows, const uint64_t *cells, co
     double total = 0.0;
     for (size_t i = 0; i < N; i++) total += fuel[h->reordered ? (size_t)h->cell_o2n[i] : i];
     h->mass_source_total = total;
+    h->mass_source_on_device = false;
     h->sources_set = 1;
     return MC_OK;
 }
@@ -2487,6 +2578,29 @@ int mc_flow_set_sources(mc_flow *h, const double *terms)
     CUDA_TRY(h, cudaMemcpyAsync(h->src, soa.data(), 5 * N * 8, cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     h->mass_source_total = total;
+    h->mass_source_on_device = false;
+    h->sources_set = 1;
+    return MC_OK;
+}
+
+int mc_flow_set_sources_device(mc_flow *h, const double *terms_soa)
+{
+    if (!h || !terms_soa) return MC_ERR_ARG;
+    const size_t N = (size_t)h->N;
+    for (int k = 0; k < 5; k++) {
+        if (h->reordered)
+            permute(h, h->src + k * N, terms_soa + k * N, h->d_cell_n2o, h->N, 0);
+        else
+            CUDA_TRY(h, cudaMemcpyAsync(h->src + k * N, terms_soa + k * N, N * 8, cudaMemcpyDeviceToDevice,
+                                        h->stream));
+    }
+    launch(h, K_PERMUTE, [&] {
+        k_sum<<<krylov_grid(h->N), MCB_THREADS, 0, h->stream>>>(h->N, h->src + 4 * N, h->partials, h->counter,
+                                                                h->scalars + 2);
+    });
+    const int rc = check_launch(h);
+    if (rc) return rc;
+    h->mass_source_on_device = true;
     h->sources_set = 1;
     return MC_OK;
 }

@@ -784,7 +784,8 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_mass_flux(Physics ph, MeshAr
             bal->area_out = tot[2];
             bal->fallback = tot[1] < 0.0000000001;
             bal->rate_area = -tot[0] / tot[2];
-            bal->outlet_scale = (ph.mode == 1 && !bal->fallback) ? (a.mass_source_total - tot[0]) / tot[1] : 1.0;
+            const double msrc = a.mass_source_dev ? *a.mass_source_dev : a.mass_source_total;
+            bal->outlet_scale = (ph.mode == 1 && !bal->fallback) ? (msrc - tot[0]) / tot[1] : 1.0;
         }
     }
 }
@@ -987,6 +988,19 @@ __global__ void __launch_bounds__(MCB_THREADS) k_mass_imbalance(Physics ph, Mesh
     if (publish_partials<1, true>(v, partials, counter, sh)) {
         double tot[1];
         reduce_partials<1, true>(tot, partials, counter, sh);
+        if (threadIdx.x == 0) *out = tot[0];
+    }
+}
+
+__global__ void __launch_bounds__(MCB_THREADS) k_sum(int n, const double *__restrict__ x, double *partials,
+                                                     unsigned int *counter, double *out)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    double acc[1] = {0.0};
+    for (int i = grid_stride_start(); i < n; i += gridDim.x * blockDim.x) acc[0] += x[i];
+    if (publish_partials<1>(acc, partials, counter, sh)) {
+        double tot[1];
+        reduce_partials<1>(tot, partials, counter, sh);
         if (threadIdx.x == 0) *out = tot[0];
     }
 }

@@ -70,6 +70,7 @@ struct MassFluxArgs {
     unsigned int *counter;
     FluxBalance *balance;
     double mass_source_total;
+    const double *mass_source_dev;  // non-null: the total is read here instead (device-resident sources)
 };
 
 struct PressureRowArgs {
@@ -118,6 +119,8 @@ __global__ void k_pp_correct_cells(Physics ph, MeshArgs m, CorrectArgs a, int co
 __global__ void k_update_p_boundary(Physics ph, MeshArgs m, double *P, const double *gPx, const double *gPy,
                                     const double *gPz);
 __global__ void k_pp_max(int N, int cell0, const double *PP, double *partials, unsigned int *counter, double *out);
+// Sum of x[0..n) into *out, deterministic (per-block partials, last block reduces in order).
+__global__ void k_sum(int n, const double *x, double *partials, unsigned int *counter, double *out);
 __global__ void k_mass_imbalance(Physics ph, MeshArgs m, const double *mdot, const double *src, double *partials,
                                  unsigned int *counter, double *out);
 

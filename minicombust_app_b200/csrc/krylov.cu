@@ -1143,6 +1143,90 @@ void bir_residual(cudaStream_t s, const Ell &A, const BirVectors<R> &v)
 {
     k_bir_residual<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v);
 }
+// ------------------------------------------------------- x-line block Jacobi
+//
+// One thread block per x-line, one thread per cell (P >= ex threads, the
+// rows past the line's end are identity rows).  The right-hand side takes
+// the y and z couplings of the previous iterate (gathers of e_prev, read
+// from L2 mostly); the line's tridiagonal system is then reduced by
+// parallel cyclic reduction: at stride s every equation eliminates its
+// neighbours at distance s, log2(P) steps in shared memory, after which each
+// equation stands alone.
+template <int R>
+__global__ void __launch_bounds__(1024) k_line_step(LineSystem L, const float *__restrict__ r,
+                                                    const float *__restrict__ ep, float *__restrict__ en, int first)
+{
+    extern __shared__ float sm[];
+    const int P = L.P, t = threadIdx.x;
+    float *sa = sm, *sb = sm + P, *sc = sm + 2 * P, *sd = sm + 3 * P;
+    const int N = L.N;
+    const size_t i = (size_t)blockIdx.x * L.ex + t;
+    const bool in = t < L.ex;
+    float a = 0.f, b = 1.f, c = 0.f, d[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) d[j] = 0.f;
+    if (in) {
+        a = L.off[(size_t)L.dxm * N + i];
+        b = L.d[i];
+        c = L.off[(size_t)L.dxp * N + i];
+#pragma unroll
+        for (int j = 0; j < R; j++) d[j] = r[(size_t)j * N + i];
+        if (!first) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const float o = L.off[(size_t)L.yz[q] * N + i];
+                const long nb = min(max((long)i + L.yzoff[q], 0L), (long)N - 1);
+#pragma unroll
+                for (int j = 0; j < R; j++) d[j] -= o * ep[(size_t)j * N + nb];
+            }
+        }
+    }
+    for (int s = 1; s < P; s <<= 1) {
+        sa[t] = a;
+        sb[t] = b;
+        sc[t] = c;
+#pragma unroll
+        for (int j = 0; j < R; j++) sd[j * P + t] = d[j];
+        __syncthreads();
+        float na = 0.f, nc = 0.f, nb = b, nd[R];
+#pragma unroll
+        for (int j = 0; j < R; j++) nd[j] = d[j];
+        if (t >= s) {
+            const float k1 = a / sb[t - s];
+            na = -sa[t - s] * k1;
+            nb -= sc[t - s] * k1;
+#pragma unroll
+            for (int j = 0; j < R; j++) nd[j] -= sd[j * P + t - s] * k1;
+        }
+        if (t + s < P) {
+            const float k2 = c / sb[t + s];
+            nc = -sc[t + s] * k2;
+            nb -= sa[t + s] * k2;
+#pragma unroll
+            for (int j = 0; j < R; j++) nd[j] -= sd[j * P + t + s] * k2;
+        }
+        __syncthreads();
+        a = na;
+        b = nb;
+        c = nc;
+#pragma unroll
+        for (int j = 0; j < R; j++) d[j] = nd[j];
+    }
+    if (in) {
+#pragma unroll
+        for (int j = 0; j < R; j++) en[(size_t)j * N + i] = d[j] / b;
+    }
+}
+
+template <int R>
+void line_step(cudaStream_t s, const LineSystem &L, const float *r, const float *e_prev, float *e_new, int first)
+{
+    const size_t smem = (size_t)(3 + R) * L.P * sizeof(float);
+    k_line_step<R><<<L.N / L.ex, L.P, smem, s>>>(L, r, e_prev, e_new, first);
+}
+template void line_step<1>(cudaStream_t, const LineSystem &, const float *, const float *, float *, int);
+template void line_step<3>(cudaStream_t, const LineSystem &, const float *, const float *, float *, int);
+
 void round_ell(cudaStream_t s, int N, const double *diag, const double *off, const uint32_t *code, float *diag32,
                float *off32)
 {

@@ -87,7 +87,7 @@ class FlowParams(ctypes.Structure):
                 ("pressure_solver", c_int), ("precision", c_int), ("initial_guess", c_int), ("device", c_int),
                 ("amg_sweeps", c_int), ("amg_omega", c_dbl), ("amg_alpha", c_dbl), ("ir_inner_rtol", c_dbl),
                 ("reorder", c_int), ("ir_inner_rtol_bicg", c_dbl),
-                ("amg_cheb_ratio", c_dbl), ("transport_scalars", c_int)]
+                ("amg_cheb_ratio", c_dbl), ("transport_scalars", c_int), ("ir_line_steps", c_int)]
 
 
 class IterStats(ctypes.Structure):
@@ -129,6 +129,7 @@ _SIGNATURES = {
     "mc_flow_write_vtk": (c_int, [c_vp, ctypes.c_char_p, c_int]),
     "mc_flow_ingest_particles": (c_int, [c_vp, ctypes.c_int64, c_vp, c_vp]),
     "mc_flow_get_sources": (c_int, [c_vp, c_vp]),
+    "mc_flow_set_sources_device": (c_int, [c_vp, c_vp]),
     "mc_flow_interpolate_nodes": (c_int, [c_vp, ctypes.c_int64, c_vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
                                           c_vp, c_vp]),
     "mc_flow_checkpoint_write": (c_int, [c_vp, ctypes.c_char_p]),
@@ -359,6 +360,11 @@ class FlowSolver:
         if t.shape != (c.shape[0], 5):
             raise ValueError("terms must be [rows][5]")
         _check(self.L.mc_flow_ingest_particles(self.h, c.shape[0], _ptr(c), _ptr(t)), self.h, "ingest_particles")
+
+    def set_sources_device(self, ptr):
+        """Sources from device memory [5][cells] (a device pointer, e.g.
+        tensor.data_ptr()), ordered on the handle's stream."""
+        _check(self.L.mc_flow_set_sources_device(self.h, ptr), self.h, "set_sources_device")
 
     def sources(self):
         a = np.empty((self.N, 5))

@@ -224,14 +224,17 @@ def test_amg_pressure_solver_matches_oracle(gpu, dims, reorder):
 
 
 @pytest.mark.parametrize("dims", [(40, 20, 20), (7, 3, 5)])
-def test_fp32_refined_pressure_solver_matches_oracle(gpu, dims):
-    """FP64 iterative refinement around FP32 AMG-PCG inner solves reaches the
-    FP64 answer: the outer residual is the true FP64 residual, so with the
-    pressure tolerance at 1e-12 the fields meet the same 1e-9 gate as the
-    all-FP64 solvers."""
+@pytest.mark.parametrize("line_steps", [2, 0], ids=["xline", "bicgstab"])
+def test_fp32_refined_pressure_solver_matches_oracle(gpu, dims, line_steps):
+    """FP64 iterative refinement around FP32 inner solves (AMG-PCG for the
+    pressure correction; x-line block Jacobi or BiCGStab for momentum and
+    temperature) reaches the FP64 answer: the outer residual is the true FP64
+    residual, so with the tolerances at 1e-12/1e-13 the fields meet the same
+    1e-9 gate as the all-FP64 solvers."""
     lengths = (0.2, 0.1, 0.1)
     solver, orc = make_pair(dims, lengths, SIMPLE, u_rtol=1e-13, p_rtol=1e-12,
-                            pressure_solver=flow.PSOLVER_PCG_AMG, precision=flow.PRECISION_FP32_REFINED)
+                            pressure_solver=flow.PSOLVER_PCG_AMG, precision=flow.PRECISION_FP32_REFINED,
+                            ir_line_steps=line_steps)
     seed_both(solver, orc, BASE_SIMPLE, seed=3)
     for p in range(5):
         solver.simple_iteration()
@@ -242,16 +245,16 @@ def test_fp32_refined_pressure_solver_matches_oracle(gpu, dims):
         assert err <= PARITY, (name, err)
 
 
-def test_fp32_refined_reaches_rtol_at_default_tolerance(gpu):
-    """At the default 1e-8 pressure tolerance the refined solve stops on the
-    FP64 true residual and lands within the solver tolerance of the FP64 AMG
-    solve."""
+@pytest.mark.parametrize("line_steps", [2, 0], ids=["xline", "bicgstab"])
+def test_fp32_refined_reaches_rtol_at_default_tolerance(gpu, line_steps):
+    """At the default 1e-8 tolerances the refined solves stop on the FP64 true
+    residual and land within the solver tolerance of the FP64 solves."""
     dims, lengths = (48, 24, 24), (0.2, 0.1, 0.1)
     out = {}
     for prec in (flow.PRECISION_FP64, flow.PRECISION_FP32_REFINED):
         s = flow.FlowSolver(flow.Mesh.box(*dims, *lengths),
                             params=flow.default_params(flow.MODE_SIMPLE, pressure_solver=flow.PSOLVER_PCG_AMG,
-                                                       precision=prec))
+                                                       precision=prec, ir_line_steps=line_steps))
         init = noisy_initial_fields(s.N, BASE_SIMPLE, 5)
         for name, vals in init.items():
             a = s.field(name)
