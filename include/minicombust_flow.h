@@ -129,9 +129,10 @@ typedef struct mc_flow_params {
                                  VARF, VARP (FlowSolver.inl:3229-3261).  Default: 1 in
                                  MC_MODE_COMPAT, 0 in MC_MODE_SIMPLE. */
     int ir_line_steps;        /* MC_PRECISION_FP32_REFINED, momentum and temperature: k > 0 makes each inner
-                                 FP32 solve k steps of x-line block Jacobi (each x-line's tridiagonal block
-                                 solved exactly) on meshes whose cells run x-fastest along whole lines; 0,
-                                 or another mesh: inner BiCGStab.  Default 2. */
+                                 FP32 solve k steps of an x-line sweep (the splitting that keeps the
+                                 diagonal and the upwind -x couplings, solved along each line) on meshes
+                                 whose cells run x-fastest along whole lines; 0, or another mesh: inner
+                                 BiCGStab.  Default 2. */
 } mc_flow_params;
 
 /* Per-pass statistics. */

@@ -53,7 +53,7 @@ const char *kKernelNames[K_COUNT] = {
     "snapshot_pack", "bicg_refine_fp64_residual", "round_fp32", "bicg3_32_init", "bicg3_32_1_spmv",
     "bicg3_32_2_spmv", "bicg3_32_3_update", "bicg1_32_init", "bicg1_32_1_spmv", "bicg1_32_2_spmv",
     "bicg1_32_3_update", "lsq_gradients_scalars", "scalar_assemble", "scalar_clip_negative", "particle_exchange",
-    "line_jacobi3_32", "line_jacobi1_32"};
+    "line_sweep3_32", "line_sweep1_32"};
 
 constexpr int PCG_BATCH = 16;   // iterations per status read (even: ping-pong buffers)
 constexpr int PCG_AMG_BATCH = 4;
@@ -156,8 +156,8 @@ struct mc_flow {
     BirState<1> *h_bo1 = nullptr;
     cudaGraphExec_t g_b3_32 = nullptr, g_b1_32 = nullptr;
     char *bir_mem = nullptr;
-    // x-line block-Jacobi inner solves (ir_line_steps > 0 on a box whose
-    // cells run x-fastest): line length, the two systems and a scratch iterate
+    // x-line sweep inner solves (ir_line_steps > 0 on a box whose cells run
+    // x-fastest): line length, the two systems and a scratch iterate
     int line_ex = 0;
     LineSystem line3{}, line1{};
     float *line_scratch = nullptr;
@@ -773,8 +773,8 @@ int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const B
         if (hout->all_done) break;
         if (outer > kMaxOuter) return fail(h, MC_ERR_NOT_CONVERGED, "refinement state did not advance");
         if (line) {
-            // a fixed number of x-line block-Jacobi steps on the row-scaled
-            // FP32 system; the last step writes the inner solution out.e
+            // a fixed number of x-line sweep steps on the row-scaled FP32
+            // system; the last step writes the inner solution out.e
             const int K = h->prm.ir_line_steps;
             float *E[2] = {const_cast<float *>(out.e), h->line_scratch};
             for (int k = 1; k <= K; k++) {
@@ -1477,8 +1477,6 @@ int setup_bicg_refined(mc_flow *h)
         LineSystem L;
         L.N = h->N;
         L.ex = h->line_ex;
-        L.P = 1;
-        while (L.P < L.ex) L.P <<= 1;
         int q = 0;
         for (int d = 0; d < 6; d++) {
             if (h->dc.doff[d] == -1)

@@ -1143,86 +1143,120 @@ void bir_residual(cudaStream_t s, const Ell &A, const BirVectors<R> &v)
 {
     k_bir_residual<R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v);
 }
-// ------------------------------------------------------- x-line block Jacobi
+// ------------------------------------------------------- x-line sweeps
 //
-// One thread block per x-line, one thread per cell (P >= ex threads, the
-// rows past the line's end are identity rows).  The right-hand side takes
-// the y and z couplings of the previous iterate (gathers of e_prev, read
-// from L2 mostly); the line's tridiagonal system is then reduced by
-// parallel cyclic reduction: at stride s every equation eliminates its
-// neighbours at distance s, log2(P) steps in shared memory, after which each
-// equation stands alone.
-template <int R>
-__global__ void __launch_bounds__(1024) k_line_step(LineSystem L, const float *__restrict__ r,
+// Splitting A = M - (M - A) with M the diagonal and the -x couplings of each
+// x-line (a lower bidiagonal block per line: the upwind direction of the
+// x-directed flow): one step solves M e_new = r - (M - A) e_prev, i.e. the
+// +x, y and z couplings of the previous iterate go to the right-hand side
+// and each line is a first-order recurrence e_k = (rhs_k - a_k e_{k-1}) / b_k.
+// A is an M-matrix (positive diagonal, non-positive couplings, diagonally
+// dominant through the transient term), so this is a regular splitting and
+// the iteration converges; with convection along +x the neglected couplings
+// are small and each step reduces the residual by orders of magnitude.
+//
+// One warp per line, S consecutive cells per lane: each lane composes its
+// cells' affine maps e -> p + q e, a warp scan (shuffles) composes the
+// lanes' maps along the line, and each lane then evaluates its cells from the
+// value entering its segment.
+template <int R, int S>
+__global__ void __launch_bounds__(256) k_line_sweep(LineSystem L, const float *__restrict__ r,
                                                     const float *__restrict__ ep, float *__restrict__ en, int first)
 {
-    extern __shared__ float sm[];
-    const int P = L.P, t = threadIdx.x;
-    float *sa = sm, *sb = sm + P, *sc = sm + 2 * P, *sd = sm + 3 * P;
-    const int N = L.N;
-    const size_t i = (size_t)blockIdx.x * L.ex + t;
-    const bool in = t < L.ex;
-    float a = 0.f, b = 1.f, c = 0.f, d[R];
+    const int lane = threadIdx.x & 31;
+    const int line = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int N = L.N, ex = L.ex;
+    if (line >= N / ex) return;
+    const size_t base = (size_t)line * ex;
+    float p[S][R], q[S];
+    float P[R], Q = 1.f;
 #pragma unroll
-    for (int j = 0; j < R; j++) d[j] = 0.f;
-    if (in) {
-        a = L.off[(size_t)L.dxm * N + i];
-        b = L.d[i];
-        c = L.off[(size_t)L.dxp * N + i];
+    for (int j = 0; j < R; j++) P[j] = 0.f;
 #pragma unroll
-        for (int j = 0; j < R; j++) d[j] = r[(size_t)j * N + i];
-        if (!first) {
+    for (int k = 0; k < S; k++) {
+        const int c = lane * S + k;
+        q[k] = 1.f;
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const float o = L.off[(size_t)L.yz[q] * N + i];
-                const long nb = min(max((long)i + L.yzoff[q], 0L), (long)N - 1);
+        for (int j = 0; j < R; j++) p[k][j] = 0.f;
+        if (c < ex) {
+            const size_t i = base + c;
+            const float a = L.off[(size_t)L.dxm * N + i];
+            const float b = L.d[i];
+            float rhs[R];
 #pragma unroll
-                for (int j = 0; j < R; j++) d[j] -= o * ep[(size_t)j * N + nb];
+            for (int j = 0; j < R; j++) rhs[j] = r[(size_t)j * N + i];
+            if (!first) {
+                if (c + 1 < ex) {
+                    const float o = L.off[(size_t)L.dxp * N + i];
+#pragma unroll
+                    for (int j = 0; j < R; j++) rhs[j] -= o * ep[(size_t)j * N + i + 1];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const float o = L.off[(size_t)L.yz[u] * N + i];
+                    const long nb = min(max((long)i + L.yzoff[u], 0L), (long)N - 1);
+#pragma unroll
+                    for (int j = 0; j < R; j++) rhs[j] -= o * ep[(size_t)j * N + nb];
+                }
+            }
+            const float rb = 1.f / b;
+            q[k] = -a * rb;
+#pragma unroll
+            for (int j = 0; j < R; j++) p[k][j] = rhs[j] * rb;
+        }
+        // compose: the segment so far, then cell k
+#pragma unroll
+        for (int j = 0; j < R; j++) P[j] = p[k][j] + q[k] * P[j];
+        Q = q[k] * Q;
+    }
+    // inclusive scan of the lanes' maps along the line
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        float Pu[R];
+#pragma unroll
+        for (int j = 0; j < R; j++) Pu[j] = __shfl_up_sync(0xffffffffu, P[j], off);
+        const float Qu = __shfl_up_sync(0xffffffffu, Q, off);
+        if (lane >= off) {
+#pragma unroll
+            for (int j = 0; j < R; j++) P[j] = P[j] + Q * Pu[j];
+            Q = Q * Qu;
+        }
+    }
+    // the value entering this lane's segment: the end of the previous lane's
+    // (zero before the line's first cell)
+    float x[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        const float v = __shfl_up_sync(0xffffffffu, P[j], 1);
+        x[j] = lane > 0 ? v : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < S; k++) {
+        const int c = lane * S + k;
+        if (c < ex) {
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                x[j] = p[k][j] + q[k] * x[j];
+                en[(size_t)j * N + base + c] = x[j];
             }
         }
-    }
-    for (int s = 1; s < P; s <<= 1) {
-        sa[t] = a;
-        sb[t] = b;
-        sc[t] = c;
-#pragma unroll
-        for (int j = 0; j < R; j++) sd[j * P + t] = d[j];
-        __syncthreads();
-        float na = 0.f, nc = 0.f, nb = b, nd[R];
-#pragma unroll
-        for (int j = 0; j < R; j++) nd[j] = d[j];
-        if (t >= s) {
-            const float k1 = a / sb[t - s];
-            na = -sa[t - s] * k1;
-            nb -= sc[t - s] * k1;
-#pragma unroll
-            for (int j = 0; j < R; j++) nd[j] -= sd[j * P + t - s] * k1;
-        }
-        if (t + s < P) {
-            const float k2 = c / sb[t + s];
-            nc = -sc[t + s] * k2;
-            nb -= sa[t + s] * k2;
-#pragma unroll
-            for (int j = 0; j < R; j++) nd[j] -= sd[j * P + t + s] * k2;
-        }
-        __syncthreads();
-        a = na;
-        b = nb;
-        c = nc;
-#pragma unroll
-        for (int j = 0; j < R; j++) d[j] = nd[j];
-    }
-    if (in) {
-#pragma unroll
-        for (int j = 0; j < R; j++) en[(size_t)j * N + i] = d[j] / b;
     }
 }
 
 template <int R>
 void line_step(cudaStream_t s, const LineSystem &L, const float *r, const float *e_prev, float *e_new, int first)
 {
-    const size_t smem = (size_t)(3 + R) * L.P * sizeof(float);
-    k_line_step<R><<<L.N / L.ex, L.P, smem, s>>>(L, r, e_prev, e_new, first);
+    const int lines = L.N / L.ex;
+    const int grid = (lines * 32 + 255) / 256;
+    const int S = (L.ex + 31) / 32;
+    if (S <= 4)
+        k_line_sweep<R, 4><<<grid, 256, 0, s>>>(L, r, e_prev, e_new, first);
+    else if (S <= 8)
+        k_line_sweep<R, 8><<<grid, 256, 0, s>>>(L, r, e_prev, e_new, first);
+    else if (S <= 16)
+        k_line_sweep<R, 16><<<grid, 256, 0, s>>>(L, r, e_prev, e_new, first);
+    else
+        k_line_sweep<R, 32><<<grid, 256, 0, s>>>(L, r, e_prev, e_new, first);
 }
 template void line_step<1>(cudaStream_t, const LineSystem &, const float *, const float *, float *, int);
 template void line_step<3>(cudaStream_t, const LineSystem &, const float *, const float *, float *, int);

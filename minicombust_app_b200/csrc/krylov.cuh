@@ -232,24 +232,23 @@ struct BirVectors {
     BirState<R> *st;
 };
 
-// x-line block-Jacobi inner solver of the refined momentum and temperature
+// x-line sweeps: the inner solver of the refined momentum and temperature
 // systems (FP32, row-scaled, values by direction) on a structured box whose
-// cells run x-fastest: the rows of one x-line form a tridiagonal block (the
-// -x and +x couplings), solved exactly by parallel cyclic reduction in
-// shared memory, one line per thread block.
+// cells run x-fastest along whole lines.  The splitting keeps, per x-line,
+// the diagonal and the -x couplings (a first-order recurrence along the
+// line); the other couplings act through the previous iterate.
 struct LineSystem {
     int N = 0;
     int ex = 0;        // cells per x-line (the line length, <= 1024)
-    int P = 0;         // threads per block: the power of two >= ex
+    int P = 0;         // unused (kept 0)
     int dxm = 0, dxp = 0;      // by-direction slots of the -x and +x couplings
     int yz[4] = {0, 0, 0, 0};  // the other four slots
     int yzoff[4] = {0, 0, 0, 0};
     const float *d = nullptr;   // diagonal [N]
     const float *off = nullptr; // [6][N] by direction
 };
-// One line-Jacobi step for R right-hand sides [R][N]: with first set,
-// T e_new = r; otherwise T e_new = r - (A - T) e_prev (the y and z couplings
-// of the previous iterate).
+// One sweep step for R right-hand sides [R][N]: with first set, M e_new = r;
+// otherwise M e_new = r - (M - A) e_prev.
 template <int R>
 void line_step(cudaStream_t s, const LineSystem &L, const float *r, const float *e_prev, float *e_new, int first);
 
