@@ -1155,11 +1155,12 @@ void bir_residual(cudaStream_t s, const Ell &A, const BirVectors<R> &v)
 // the iteration converges; with convection along +x the neglected couplings
 // are small and each step reduces the residual by orders of magnitude.
 //
-// One warp per line, S consecutive cells per lane: each lane composes its
-// cells' affine maps e -> p + q e, a warp scan (shuffles) composes the
-// lanes' maps along the line, and each lane then evaluates its cells from the
-// value entering its segment.
-template <int R, int S>
+// One warp per line, walking it in chunks of 32 consecutive cells (one per
+// lane, so every load is coalesced): within a chunk a warp scan (shuffles)
+// composes the cells' affine maps e_k = p_k + q_k e_{k-1}, the value
+// entering the chunk is applied, and the chunk's last value is carried into
+// the next chunk.
+template <int R>
 __global__ void __launch_bounds__(256) k_line_sweep(LineSystem L, const float *__restrict__ r,
                                                     const float *__restrict__ ep, float *__restrict__ en, int first)
 {
@@ -1168,16 +1169,14 @@ __global__ void __launch_bounds__(256) k_line_sweep(LineSystem L, const float *_
     const int N = L.N, ex = L.ex;
     if (line >= N / ex) return;
     const size_t base = (size_t)line * ex;
-    float p[S][R], q[S];
-    float P[R], Q = 1.f;
+    float carry[R];
 #pragma unroll
-    for (int j = 0; j < R; j++) P[j] = 0.f;
+    for (int j = 0; j < R; j++) carry[j] = 0.f;
+    for (int c0 = 0; c0 < ex; c0 += 32) {
+        const int c = c0 + lane;
+        float p[R], q = 1.f;
 #pragma unroll
-    for (int k = 0; k < S; k++) {
-        const int c = lane * S + k;
-        q[k] = 1.f;
-#pragma unroll
-        for (int j = 0; j < R; j++) p[k][j] = 0.f;
+        for (int j = 0; j < R; j++) p[j] = 0.f;
         if (c < ex) {
             const size_t i = base + c;
             const float a = L.off[(size_t)L.dxm * N + i];
@@ -1200,45 +1199,28 @@ __global__ void __launch_bounds__(256) k_line_sweep(LineSystem L, const float *_
                 }
             }
             const float rb = 1.f / b;
-            q[k] = -a * rb;
+            q = -a * rb;
 #pragma unroll
-            for (int j = 0; j < R; j++) p[k][j] = rhs[j] * rb;
+            for (int j = 0; j < R; j++) p[j] = rhs[j] * rb;
         }
-        // compose: the segment so far, then cell k
+        // inclusive scan of the maps of the chunk's lanes
 #pragma unroll
-        for (int j = 0; j < R; j++) P[j] = p[k][j] + q[k] * P[j];
-        Q = q[k] * Q;
-    }
-    // inclusive scan of the lanes' maps along the line
+        for (int off = 1; off < 32; off <<= 1) {
+            float pu[R];
 #pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        float Pu[R];
+            for (int j = 0; j < R; j++) pu[j] = __shfl_up_sync(0xffffffffu, p[j], off);
+            const float qu = __shfl_up_sync(0xffffffffu, q, off);
+            if (lane >= off) {
 #pragma unroll
-        for (int j = 0; j < R; j++) Pu[j] = __shfl_up_sync(0xffffffffu, P[j], off);
-        const float Qu = __shfl_up_sync(0xffffffffu, Q, off);
-        if (lane >= off) {
-#pragma unroll
-            for (int j = 0; j < R; j++) P[j] = P[j] + Q * Pu[j];
-            Q = Q * Qu;
-        }
-    }
-    // the value entering this lane's segment: the end of the previous lane's
-    // (zero before the line's first cell)
-    float x[R];
-#pragma unroll
-    for (int j = 0; j < R; j++) {
-        const float v = __shfl_up_sync(0xffffffffu, P[j], 1);
-        x[j] = lane > 0 ? v : 0.f;
-    }
-#pragma unroll
-    for (int k = 0; k < S; k++) {
-        const int c = lane * S + k;
-        if (c < ex) {
-#pragma unroll
-            for (int j = 0; j < R; j++) {
-                x[j] = p[k][j] + q[k] * x[j];
-                en[(size_t)j * N + base + c] = x[j];
+                for (int j = 0; j < R; j++) p[j] = p[j] + q * pu[j];
+                q = q * qu;
             }
+        }
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const float x = p[j] + q * carry[j];
+            if (c < ex) en[(size_t)j * N + base + c] = x;
+            carry[j] = __shfl_sync(0xffffffffu, x, 31);
         }
     }
 }
@@ -1248,15 +1230,7 @@ void line_step(cudaStream_t s, const LineSystem &L, const float *r, const float 
 {
     const int lines = L.N / L.ex;
     const int grid = (lines * 32 + 255) / 256;
-    const int S = (L.ex + 31) / 32;
-    if (S <= 4)
-        k_line_sweep<R, 4><<<grid, 256, 0, s>>>(L, r, e_prev, e_new, first);
-    else if (S <= 8)
-        k_line_sweep<R, 8><<<grid, 256, 0, s>>>(L, r, e_prev, e_new, first);
-    else if (S <= 16)
-        k_line_sweep<R, 16><<<grid, 256, 0, s>>>(L, r, e_prev, e_new, first);
-    else
-        k_line_sweep<R, 32><<<grid, 256, 0, s>>>(L, r, e_prev, e_new, first);
+    k_line_sweep<R><<<grid, 256, 0, s>>>(L, r, e_prev, e_new, first);
 }
 template void line_step<1>(cudaStream_t, const LineSystem &, const float *, const float *, float *, int);
 template void line_step<3>(cudaStream_t, const LineSystem &, const float *, const float *, float *, int);
