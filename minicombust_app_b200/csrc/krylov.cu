@@ -1155,20 +1155,52 @@ void bir_residual(cudaStream_t s, const Ell &A, const BirVectors<R> &v)
 // the iteration converges; with convection along +x the neglected couplings
 // are small and each step reduces the residual by orders of magnitude.
 //
-// One warp per line, walking it in chunks of 32 consecutive cells (one per
-// lane, so every load is coalesced): within a chunk a warp scan (shuffles)
-// composes the cells' affine maps e_k = p_k + q_k e_{k-1}, the value
-// entering the chunk is applied, and the chunk's last value is carried into
-// the next chunk.
+// One warp per line.  First every cell's affine map e_k = p_k + q_k e_{k-1}
+// is formed from coalesced loads (32 consecutive cells per step, all of the
+// line's loads independent, so they overlap) and kept in shared memory; then
+// the warp walks the line in chunks of 32: a warp scan (shuffles) composes
+// the chunk's maps, the value entering the chunk is applied, and the chunk's
+// last value is carried into the next chunk.
 template <int R>
 __global__ void __launch_bounds__(256) k_line_sweep(LineSystem L, const float *__restrict__ r,
                                                     const float *__restrict__ ep, float *__restrict__ en, int first)
 {
-    const int lane = threadIdx.x & 31;
+    extern __shared__ float sline[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int line = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int N = L.N, ex = L.ex;
     if (line >= N / ex) return;
+    float *sq = sline + (size_t)warp * ex * (R + 1);  // q[ex], then p[R][ex]
+    float *sp = sq + ex;
     const size_t base = (size_t)line * ex;
+#pragma unroll 4
+    for (int c = lane; c < ex; c += 32) {
+        const size_t i = base + c;
+        const float a = L.off[(size_t)L.dxm * N + i];
+        const float b = L.d[i];
+        float rhs[R];
+#pragma unroll
+        for (int j = 0; j < R; j++) rhs[j] = r[(size_t)j * N + i];
+        if (!first) {
+            if (c + 1 < ex) {
+                const float o = L.off[(size_t)L.dxp * N + i];
+#pragma unroll
+                for (int j = 0; j < R; j++) rhs[j] -= o * ep[(size_t)j * N + i + 1];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const float o = L.off[(size_t)L.yz[u] * N + i];
+                const long nb = min(max((long)i + L.yzoff[u], 0L), (long)N - 1);
+#pragma unroll
+                for (int j = 0; j < R; j++) rhs[j] -= o * ep[(size_t)j * N + nb];
+            }
+        }
+        const float rb = 1.f / b;
+        sq[c] = -a * rb;
+#pragma unroll
+        for (int j = 0; j < R; j++) sp[j * ex + c] = rhs[j] * rb;
+    }
+    __syncwarp();
     float carry[R];
 #pragma unroll
     for (int j = 0; j < R; j++) carry[j] = 0.f;
@@ -1178,32 +1210,10 @@ __global__ void __launch_bounds__(256) k_line_sweep(LineSystem L, const float *_
 #pragma unroll
         for (int j = 0; j < R; j++) p[j] = 0.f;
         if (c < ex) {
-            const size_t i = base + c;
-            const float a = L.off[(size_t)L.dxm * N + i];
-            const float b = L.d[i];
-            float rhs[R];
+            q = sq[c];
 #pragma unroll
-            for (int j = 0; j < R; j++) rhs[j] = r[(size_t)j * N + i];
-            if (!first) {
-                if (c + 1 < ex) {
-                    const float o = L.off[(size_t)L.dxp * N + i];
-#pragma unroll
-                    for (int j = 0; j < R; j++) rhs[j] -= o * ep[(size_t)j * N + i + 1];
-                }
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const float o = L.off[(size_t)L.yz[u] * N + i];
-                    const long nb = min(max((long)i + L.yzoff[u], 0L), (long)N - 1);
-#pragma unroll
-                    for (int j = 0; j < R; j++) rhs[j] -= o * ep[(size_t)j * N + nb];
-                }
-            }
-            const float rb = 1.f / b;
-            q = -a * rb;
-#pragma unroll
-            for (int j = 0; j < R; j++) p[j] = rhs[j] * rb;
+            for (int j = 0; j < R; j++) p[j] = sp[j * ex + c];
         }
-        // inclusive scan of the maps of the chunk's lanes
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
             float pu[R];
@@ -1229,8 +1239,12 @@ template <int R>
 void line_step(cudaStream_t s, const LineSystem &L, const float *r, const float *e_prev, float *e_new, int first)
 {
     const int lines = L.N / L.ex;
-    const int grid = (lines * 32 + 255) / 256;
-    k_line_sweep<R><<<grid, 256, 0, s>>>(L, r, e_prev, e_new, first);
+    const size_t per_warp = (size_t)L.ex * (R + 1) * sizeof(float);
+    int warps = 8;
+    while (warps > 1 && warps * per_warp > 48 * 1024) warps >>= 1;
+    const int threads = 32 * warps;
+    const int grid = (lines + warps - 1) / warps;
+    k_line_sweep<R><<<grid, threads, warps * per_warp, s>>>(L, r, e_prev, e_new, first);
 }
 template void line_step<1>(cudaStream_t, const LineSystem &, const float *, const float *, float *, int);
 template void line_step<3>(cudaStream_t, const LineSystem &, const float *, const float *, float *, int);
