@@ -1020,13 +1020,16 @@ int stage_momentum(mc_flow *h, mc_iter_stats *st)
     a.off = h->off_m;
     a.AU = h->AU;
     a.b = h->b_m;
+    const bool fused32 = h->bir_mem && h->dc.code;  // the FP32 copy written by the assembly itself
+    if (fused32) a.f32 = Fp32Rows{h->m32_diag, h->m32_off, h->dc.code};
     launch(h, K_MOMENTUM, [&] { k_momentum_assemble<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a); });
     int rc = check_launch(h);
     if (rc) return rc;
     int its[3] = {0, 0, 0};
     if (h->bir_mem) {
-        launch(h, K_ROUND_ELL,
-               [&] { round_ell(h->stream, h->N, h->AU, h->off_m, h->dc.code, h->m32_diag, h->m32_off); });
+        if (!fused32)
+            launch(h, K_ROUND_ELL,
+                   [&] { round_ell(h->stream, h->N, h->AU, h->off_m, h->dc.code, h->m32_diag, h->m32_off); });
         const EllT<float> A32{h->N, h->m32_diag, h->m32_off, h->col, by_direction(h->dc)};
         rc = solve_bicg_refined<3>(h, momentum_matrix(h), A32, h->bi3, h->bo3, h->h_bi3, h->h_bo3, &h->g_b3_32,
                                    &h->l_b3_32, K_BICG3_INIT32, K_BICG3_1_32, its);
@@ -1160,6 +1163,11 @@ int stage_temperature(mc_flow *h, mc_iter_stats *st)
     a.off = h->off_t;
     a.diag = h->diag_t;
     a.b = h->b_t;
+    a.imbalance = h->scalars + 1;
+    a.partials = h->partials;
+    a.counter = h->counter;
+    const bool fused32 = h->bir_mem && h->dc.code;
+    if (fused32) a.f32 = Fp32Rows{h->t32_diag, h->t32_off, h->dc.code};
     launch(h, K_TEMPERATURE, [&] {
         k_temperature_assemble<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a);
     });
@@ -1167,8 +1175,9 @@ int stage_temperature(mc_flow *h, mc_iter_stats *st)
     if (rc) return rc;
     int its[1] = {0};
     if (h->bir_mem) {
-        launch(h, K_ROUND_ELL,
-               [&] { round_ell(h->stream, h->N, h->diag_t, h->off_t, h->dc.code, h->t32_diag, h->t32_off); });
+        if (!fused32)
+            launch(h, K_ROUND_ELL,
+                   [&] { round_ell(h->stream, h->N, h->diag_t, h->off_t, h->dc.code, h->t32_diag, h->t32_off); });
         const EllT<float> A32{h->N, h->t32_diag, h->t32_off, h->col, by_direction(h->dc)};
         rc = solve_bicg_refined<1>(h, temperature_matrix(h), A32, h->bi1, h->bo1, h->h_bi1, h->h_bo1, &h->g_b1_32,
                                    &h->l_b1_32, K_BICG1_INIT32, K_BICG1_1_32, its);
@@ -2783,11 +2792,7 @@ int mc_flow_simple_iteration(mc_flow *h, mc_iter_stats *st)
     } else {
         if ((rc = track(stage_temperature(h, s)))) return rc;
     }
-    launch(h, K_IMBALANCE, [&] {
-        k_mass_imbalance<<<krylov_grid(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, h->mdot,
-                                                                           h->sources_set ? h->src : nullptr,
-                                                                           h->partials, h->counter, h->scalars + 1);
-    });
+    // the mass imbalance was formed by the temperature stage's kernel
     CUDA_TRY(h, cudaMemcpyAsync(h->h_scalars + 1, h->scalars + 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     flush_timing(h);

@@ -40,6 +40,28 @@ __device__ __forceinline__ void cramer(double A00, double A10, double A20, doubl
 
 __device__ __forceinline__ int grid_stride_start() { return blockIdx.x * blockDim.x + threadIdx.x; }
 
+// The FP32 copy of an assembled row for the refined solves, written by the
+// assembly kernel itself: the row scaled by 1 / diag (1 when diag is 0) and
+// its six values stored by direction (slot k of code word cw holds
+// direction (cw >> 3k) & 7, or 7 for an unused slot) -- the same values the
+// separate rounding pass (k_round_ell) writes.
+__device__ __forceinline__ void store_fp32_row(const Fp32Rows &f, int N, int c, double diag, const double (&offv)[6])
+{
+    const double sc = diag != 0.0 ? 1.0 / diag : 1.0;
+    f.d32[c] = (float)(diag * sc);
+    const uint32_t cw = f.code[c];
+    float o[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        const unsigned d = (cw >> (3 * k)) & 7u;
+        const float v = (float)(offv[k] * sc);
+#pragma unroll
+        for (int q = 0; q < 6; q++) o[q] = (d == (unsigned)q) ? v : o[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) f.o32[(size_t)q * N + c] = o[q];
+}
+
 } // namespace
 
 // ------------------------------------------------------------- gradients
@@ -316,16 +338,19 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_momentum_assemble(Physics ph
     a.AU[c] = ac;
 #pragma unroll
     for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
+    if (a.f32.d32) store_fp32_row(a.f32, N, c, ac, offv);
 }
 
 // ------------------------------------------------------------- temperature
 // FluxScalar(TEMP) (FlowSolver.inl:2516-2744), unsteady term and
 // setup_sparse_matrix of Scalar_solve (:2885-2953).
-__global__ void __launch_bounds__(MCB_THREADS, 4) k_temperature_assemble(Physics ph, MeshArgs m, ScalarArgs a)
+// One cell's row; returns |div(mdot) - mass source| of the cell (the mass
+// imbalance after the pass: the temperature stage reads the pass's final
+// face fluxes anyway).
+__device__ __forceinline__ double temperature_row(const Physics &ph, const MeshArgs &m, const ScalarArgs &a, int c)
 {
     const int N = ph.N;
-    const int c = grid_stride_start();
-    if (c >= N) return;
+    double div = 0.0;
     const double xcc = m.xc[c], ycc = m.yc[c], zcc = m.zc[c];
     const double Tc = a.phi[c];
     const double mu = ph.mu;
@@ -336,6 +361,7 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_temperature_assemble(Physics
         const int c0 = m.fc0[face], c1 = m.fc1[face];
         const double Sx = m.Sx[face], Sy = m.Sy[face], Sz = m.Sz[face];
         const double md = a.mdot[face];
+        div += (c0 == c) ? md : -md;
         if (c1 < N) {
             internal |= 1u << k;
             const double l0 = m.lam[face];
@@ -403,6 +429,22 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_temperature_assemble(Physics
     a.diag[c] = at;
 #pragma unroll
     for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
+    if (a.f32.d32) store_fp32_row(a.f32, N, c, at, offv);
+    if (ph.mode == 1 && a.src) div -= a.src[4 * (size_t)N + c];
+    return fabs(div);
+}
+
+__global__ void __launch_bounds__(MCB_THREADS, 4) k_temperature_assemble(Physics ph, MeshArgs m, ScalarArgs a)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    const int c = grid_stride_start();
+    double v[1] = {0.0};
+    if (c < ph.N) v[0] = temperature_row(ph, m, a, c);
+    if (a.imbalance && publish_partials<1, true>(v, a.partials, a.counter, sh)) {
+        double tot[1];
+        reduce_partials<1, true>(tot, a.partials, a.counter, sh);
+        if (threadIdx.x == 0) *a.imbalance = tot[0];
+    }
 }
 
 // ------------------------------------------------------ other scalar transports
@@ -969,29 +1011,6 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pp_max(int N, int cell0, const 
 }
 
 // max over cells of |net outflow - mass source| (a diagnostic of the pass).
-__global__ void __launch_bounds__(MCB_THREADS) k_mass_imbalance(Physics ph, MeshArgs m, const double *__restrict__ mdot,
-                                                                const double *__restrict__ src, double *partials,
-                                                                unsigned int *counter, double *out)
-{
-    __shared__ double sh[1][MCB_THREADS];
-    const int N = ph.N;
-    double v[1] = {0.0};
-    for (int c = grid_stride_start(); c < N; c += gridDim.x * blockDim.x) {
-        double div = 0.0;
-        for (int k = 0; k < 6; k++) {
-            const int face = m.sface[(size_t)k * N + c];
-            div += (m.fc0[face] == c) ? mdot[face] : -mdot[face];
-        }
-        if (ph.mode == 1 && src) div -= src[4 * (size_t)N + c];
-        v[0] = fmax(v[0], fabs(div));
-    }
-    if (publish_partials<1, true>(v, partials, counter, sh)) {
-        double tot[1];
-        reduce_partials<1, true>(tot, partials, counter, sh);
-        if (threadIdx.x == 0) *out = tot[0];
-    }
-}
-
 __global__ void __launch_bounds__(MCB_THREADS) k_sum(int n, const double *__restrict__ x, double *partials,
                                                      unsigned int *counter, double *out)
 {

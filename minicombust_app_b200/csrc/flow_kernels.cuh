@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include "mc_internal.h"
 
@@ -15,6 +16,13 @@ struct MeshArgs {
     const double *xc, *yc, *zc, *vol, *rho;
     const int *outlet_faces;
     int n_outlet;
+};
+
+// FP32 copy of assembled rows (refined path): scaled by 1 / diag, by direction.
+struct Fp32Rows {
+    float *d32 = nullptr;        // null: no copy
+    float *o32 = nullptr;        // [6][N]
+    const uint32_t *code = nullptr;
 };
 
 template <int NF>
@@ -33,6 +41,7 @@ struct MomentumArgs {
     double *off;                // [6][N]
     double *AU;                 // diagonal after under-relaxation (A_phi.U)
     double *b;                  // [3][N]
+    Fp32Rows f32;
 };
 
 struct ScalarArgs {
@@ -41,6 +50,12 @@ struct ScalarArgs {
     const double *mdot;
     const double *src;
     double *off, *diag, *b;
+    // temperature kernel: the pass's mass imbalance max |div(mdot) - mass source|
+    // into *imbalance (null: not computed)
+    double *imbalance;
+    double *partials;
+    unsigned int *counter;
+    Fp32Rows f32;               // temperature kernel only
 };
 
 // Extra inputs of the k and epsilon transports (solveTurbulenceModels).
@@ -121,7 +136,6 @@ __global__ void k_update_p_boundary(Physics ph, MeshArgs m, double *P, const dou
 __global__ void k_pp_max(int N, int cell0, const double *PP, double *partials, unsigned int *counter, double *out);
 // Sum of x[0..n) into *out, deterministic (per-block partials, last block reduces in order).
 __global__ void k_sum(int n, const double *x, double *partials, unsigned int *counter, double *out);
-__global__ void k_mass_imbalance(Physics ph, MeshArgs m, const double *mdot, const double *src, double *partials,
-                                 unsigned int *counter, double *out);
+
 
 } // namespace mcb

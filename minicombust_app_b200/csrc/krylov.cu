@@ -1162,7 +1162,7 @@ void bir_residual(cudaStream_t s, const Ell &A, const BirVectors<R> &v)
 // the chunk's maps, the value entering the chunk is applied, and the chunk's
 // last value is carried into the next chunk.
 template <int R>
-__global__ void __launch_bounds__(256) k_line_sweep(LineSystem L, const float *__restrict__ r,
+__global__ void __launch_bounds__(256, R == 1 ? 8 : 6) k_line_sweep(LineSystem L, const float *__restrict__ r,
                                                     const float *__restrict__ ep, float *__restrict__ en, int first)
 {
     extern __shared__ float sline[];
@@ -1173,7 +1173,7 @@ __global__ void __launch_bounds__(256) k_line_sweep(LineSystem L, const float *_
     float *sq = sline + (size_t)warp * ex * (R + 1);  // q[ex], then p[R][ex]
     float *sp = sq + ex;
     const size_t base = (size_t)line * ex;
-#pragma unroll 4
+#pragma unroll 1
     for (int c = lane; c < ex; c += 32) {
         const size_t i = base + c;
         const float a = L.off[(size_t)L.dxm * N + i];
