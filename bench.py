@@ -73,6 +73,8 @@ def parse():
                     help="> 0: blob amplitudes vary as sin(2 pi pass / period + random phase), sources updated "
                          "on the device every pass (the largest benchmark configuration)")
     ap.add_argument("--reorder", default="none", choices=["none", "rcm"], help="cell order inside the solver")
+    ap.add_argument("--amg-sweeps", type=int, default=None, help="override the V-cycle sweeps (both configurations)")
+    ap.add_argument("--amg-cheb-ratio", type=float, default=None, help="override the Chebyshev ratio (both)")
     ap.add_argument("--ref-sample-m", type=int, default=48,
                     help="--impl reference: each step is one reference pass on the 2m x m x m box")
     ap.add_argument("--config", default="both", choices=["both", "headline", "plain"],
@@ -327,6 +329,10 @@ def make_solver(flow, mesh, dims, lengths, args, rank, local, headline):
         psolver = flow.PSOLVER_PCG_AMG if args.psolver == "amg" else flow.PSOLVER_PCG_JACOBI
         params = flow.default_params(flow.MODE_SIMPLE, device=local, p_rtol=1e-8, u_rtol=1e-8,
                                      pressure_solver=psolver, reorder=reorder)
+    if args.amg_sweeps is not None:
+        params.amg_sweeps = args.amg_sweeps
+    if args.amg_cheb_ratio is not None:
+        params.amg_cheb_ratio = args.amg_cheb_ratio
     solver = flow.FlowSolver(mesh, params=params)
     if headline:
         solver.set_guess_params(train_guess.load_params())

@@ -1164,8 +1164,7 @@ int stage_temperature(mc_flow *h, mc_iter_stats *st)
     a.diag = h->diag_t;
     a.b = h->b_t;
     a.imbalance = h->scalars + 1;
-    a.partials = h->partials;
-    a.counter = h->counter;
+    CUDA_TRY(h, cudaMemsetAsync(a.imbalance, 0, sizeof(double), h->stream));
     const bool fused32 = h->bir_mem && h->dc.code;
     if (fused32) a.f32 = Fp32Rows{h->t32_diag, h->t32_off, h->dc.code};
     launch(h, K_TEMPERATURE, [&] {

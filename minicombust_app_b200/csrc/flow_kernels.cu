@@ -434,16 +434,20 @@ __device__ __forceinline__ double temperature_row(const Physics &ph, const MeshA
     return fabs(div);
 }
 
+// The imbalance maximum: a warp maximum, then one atomicMax per warp on the
+// bits of the (non-negative) value -- for non-negative doubles the order of
+// the bit patterns is the order of the values, and a maximum does not depend
+// on the order of the updates.  *imbalance must be zero before the launch.
 __global__ void __launch_bounds__(MCB_THREADS, 4) k_temperature_assemble(Physics ph, MeshArgs m, ScalarArgs a)
 {
-    __shared__ double sh[1][MCB_THREADS];
     const int c = grid_stride_start();
-    double v[1] = {0.0};
-    if (c < ph.N) v[0] = temperature_row(ph, m, a, c);
-    if (a.imbalance && publish_partials<1, true>(v, a.partials, a.counter, sh)) {
-        double tot[1];
-        reduce_partials<1, true>(tot, a.partials, a.counter, sh);
-        if (threadIdx.x == 0) *a.imbalance = tot[0];
+    double v = 0.0;
+    if (c < ph.N) v = temperature_row(ph, m, a, c);
+    if (a.imbalance) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+        if ((threadIdx.x & 31) == 0 && v > 0.0)
+            atomicMax((unsigned long long *)a.imbalance, (unsigned long long)__double_as_longlong(v));
     }
 }
 

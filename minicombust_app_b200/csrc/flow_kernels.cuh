@@ -51,10 +51,8 @@ struct ScalarArgs {
     const double *src;
     double *off, *diag, *b;
     // temperature kernel: the pass's mass imbalance max |div(mdot) - mass source|
-    // into *imbalance (null: not computed)
+    // into *imbalance, which must be zero before the launch (null: not computed)
     double *imbalance;
-    double *partials;
-    unsigned int *counter;
     Fp32Rows f32;               // temperature kernel only
 };
 
