@@ -115,7 +115,7 @@ struct UmmaBars {
 __global__ void __launch_bounds__(UM_THREADS, 1)
     k_gnn_layer_umma(const __grid_constant__ CUtensorMap tmap, GnnGraph g, const float *__restrict__ pl,
                      const bf16 *__restrict__ wf, const bf16 *__restrict__ pkl, const bf16 *__restrict__ hin,
-                     bf16 *__restrict__ hout, int ntiles, int *status)
+                     bf16 *__restrict__ hout, int ntiles, int *status, uint32_t wait_polls)
 {
     extern __shared__ unsigned char smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
                 const int tile = blockIdx.x + j * gridDim.x;
                 if (tile >= ntiles) break;
                 const int s = j % UM_STAGES;
-                if (j >= UM_STAGES && !mbar_wait(bars.empty(s), ((j / UM_STAGES) - 1) & 1, abort_flag, WAIT_LIMIT)) {
+                if (j >= UM_STAGES && !mbar_wait(bars.empty(s), ((j / UM_STAGES) - 1) & 1, abort_flag, wait_polls)) {
                     fail(1);
                     break;
                 }
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
                 }
                 if (progressed) {
                     idle = 0;
-                } else if (++idle > 16u * WAIT_LIMIT || *abort_flag) {  // test_wait does not suspend
+                } else if (++idle > 16u * wait_polls || *abort_flag) {  // test_wait does not suspend
                     fail(3);
                     break;
                 }
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
             if (tile >= ntiles) break;
             const int s = j % UM_STAGES, i = tile * GNN_TILE + r;
             const unsigned mk = i < g.n ? g.mask[i] : 0u;
-            const bool ok = mbar_wait(bars.full(s), (j / UM_STAGES) & 1, abort_flag, WAIT_LIMIT);
+            const bool ok = mbar_wait(bars.full(s), (j / UM_STAGES) & 1, abort_flag, wait_polls);
             if (!__all_sync(FULL, ok)) {
                 fail(6);
                 break;
@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
 
             // a = relu(D1 + c1) into the group's K-major a-tile; D1 is
             // released for the group's next tile as soon as it is read
-            bool ok = mbar_wait(bars.d1full(q), (j / UM_GROUPS) & 1, abort_flag, WAIT_LIMIT);
+            bool ok = mbar_wait(bars.d1full(q), (j / UM_GROUPS) & 1, abort_flag, wait_polls);
             if (!__all_sync(FULL, ok)) {
                 fail(7);
                 break;
@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
             mbar_arrive(bars.a1full(q));
 
             // h' = h + (D2 + c2)
-            ok = mbar_wait(bars.d2full(q), (j / UM_GROUPS) & 1, abort_flag, WAIT_LIMIT);
+            ok = mbar_wait(bars.d2full(q), (j / UM_GROUPS) & 1, abort_flag, wait_polls);
             if (!__all_sync(FULL, ok)) {
                 fail(8);
                 break;
@@ -354,6 +354,21 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
 }
 
 } // namespace
+
+// Polls of the layer's pipeline waits before it gives up (the waits that
+// drain copies and products in flight before the block exits keep the full
+// bound).  MC_GNN_WAIT_POLLS overrides the bound, read at every launch, so a
+// test can make the pipeline waits run out (0: the first wait fails) and then
+// restore it on the same handle.
+static uint32_t wait_polls()
+{
+    const char *v = std::getenv("MC_GNN_WAIT_POLLS");
+    if (v && *v) {
+        const long n = std::strtol(v, nullptr, 10);
+        if (n >= 0 && n < (long)WAIT_LIMIT) return (uint32_t)n;
+    }
+    return WAIT_LIMIT;
+}
 
 GnnLayerPath gnn_layer_path()
 {
@@ -418,7 +433,7 @@ void gnn_layer_umma(cudaStream_t s, const GnnGraph &g, const GnnTmaMap &map, con
     std::memcpy(&t, map.raw, sizeof(t));
     const int ntiles = (g.n + GNN_TILE - 1) / GNN_TILE;
     k_gnn_layer_umma<<<std::max(1, std::min(grid, ntiles)), UM_THREADS, UM_SMEM, s>>>(t, g, pl, wf, pkl, hin, hout,
-                                                                                       ntiles, status);
+                                                                                       ntiles, status, wait_polls());
 }
 
 } // namespace mcb
