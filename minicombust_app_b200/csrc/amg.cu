@@ -566,10 +566,10 @@ void set_dense_attributes()
 } // namespace
 
 template <typename T>
-void amg_setup_levels(cudaStream_t s, const AmgHierarchy &H)
+void amg_setup_levels(cudaStream_t s, const AmgHierarchy &H, bool level0_ready)
 {
     const AmgLevelT<T> *lv = levels_of<T>(H);
-    if (sizeof(T) == sizeof(float))
+    if (sizeof(T) == sizeof(float) && !level0_ready)
         k_amg_round_level0<<<blocks(H.lv[0].n), MCB_THREADS, 0, s>>>(H.lv[0].n, H.lv[0].diag, H.lv[0].off,
                                                                      lv[0].dc.dia ? H.lv[0].dc.code : nullptr,
                                                                      (float *)lv[0].diag, (float *)lv[0].off);
@@ -686,8 +686,8 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
     }
 }
 
-template void amg_setup_levels<double>(cudaStream_t, const AmgHierarchy &);
-template void amg_setup_levels<float>(cudaStream_t, const AmgHierarchy &);
+template void amg_setup_levels<double>(cudaStream_t, const AmgHierarchy &, bool);
+template void amg_setup_levels<float>(cudaStream_t, const AmgHierarchy &, bool);
 template void amg_coarsest_inverse<double>(cudaStream_t, const AmgHierarchy &, double *);
 template void amg_coarsest_inverse<float>(cudaStream_t, const AmgHierarchy &, double *);
 template void amg_vcycle<double>(cudaStream_t, const AmgHierarchy &, const double *, void *, PcgState *, double *,

@@ -104,9 +104,10 @@ int amg_build_host(int N, const std::vector<int> &col0, const std::vector<int> &
 
 // Device work, all asynchronous on stream s.
 // Galerkin values of levels 1..L-1 for the FP64 (T = double) or the FP32
-// (T = float; level 0 rounded from FP64 first) hierarchy.
+// (T = float; level 0 rounded from FP64 first, unless the pressure kernel
+// has just written it: level0_ready) hierarchy.
 template <typename T>
-void amg_setup_levels(cudaStream_t s, const AmgHierarchy &H);
+void amg_setup_levels(cudaStream_t s, const AmgHierarchy &H, bool level0_ready = false);
 // Explicit inverse of the coarsest level's current values into `out`
 // (n x n FP64); reads only the coarsest level.
 template <typename T>

@@ -130,6 +130,7 @@ struct mc_flow {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_levels = nullptr, ev_inverse = nullptr;
     bool inverse_ready = false, inverse_pending = false, inverse_deferred = false;
+    bool p32_written = false;  // the pressure kernel wrote the FP32 level 0 since the last AMG setup
     // device-side loops (conditional WHILE graphs) of the same solves
     cudaGraphExec_t l_pcg = nullptr, l_b3 = nullptr, l_b1 = nullptr, l_pcg_amg = nullptr;
     cudaGraphExec_t l_pcg_amg32 = nullptr, l_b3_32 = nullptr, l_b1_32 = nullptr;
@@ -775,13 +776,13 @@ int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const B
         if (line) {
             // x-line sweep steps on the row-scaled FP32 system; the last step
             // writes the inner solution out.e.  A step reduces the residual by
-            // well over 10^2 on the flows this is meant for, so when every open
-            // system is within 10^2 of its tolerance one step is taken (a slower
+            // about 10^3 on the flows this is meant for, so when every open
+            // system is within 10^3 of its tolerance one step is taken (a slower
             // step only costs another outer iteration)
             double need = 1.0;
             for (int j = 0; j < R; j++)
                 if (!hout->done[j] && hout->rr[j] > 0) need = std::min(need, std::sqrt(hout->tol2[j] / hout->rr[j]));
-            const int K = need >= 1e-2 ? 1 : h->prm.ir_line_steps;
+            const int K = need >= 1e-3 ? 1 : h->prm.ir_line_steps;
             float *E[2] = {const_cast<float *>(out.e), h->line_scratch};
             for (int k = 1; k <= K; k++) {
                 float *dst = E[(K - k) % 2];
@@ -967,9 +968,10 @@ int setup_amg_values(mc_flow *h)
         h->inverse_pending = false;
     }
     if (h->refined)
-        amg_setup_levels<float>(h->stream, H);
+        amg_setup_levels<float>(h->stream, H, h->p32_written);
     else
         amg_setup_levels<double>(h->stream, H);
+    h->p32_written = false;
     h->launches += h->refined ? H.levels - 1 : H.levels - 2;  // with the one the caller's launch() counts
     if (h->inverse_ready && h->side && lagged_inverse_enabled()) {
         h->inverse_deferred = true;
@@ -1056,6 +1058,11 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
         a.off = h->off_p;
         a.diag = h->diag_p;
         a.b = h->b_p;
+        h->p32_written = h->use_amg && h->refined;  // the FP32 level 0 of the hierarchy, written by the kernel
+        if (h->p32_written) {
+            const AmgLevelT<float> &L0 = h->amg.lv32[0];
+            a.f32 = Fp32Rows{L0.diag, L0.off, L0.dc.dia ? h->amg.lv[0].dc.code : nullptr, 0};
+        }
         launch(h, K_PRESSURE_ROWS, [&] {
             k_pressure_rows<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a);
         });

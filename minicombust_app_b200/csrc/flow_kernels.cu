@@ -41,14 +41,20 @@ __device__ __forceinline__ void cramer(double A00, double A10, double A20, doubl
 __device__ __forceinline__ int grid_stride_start() { return blockIdx.x * blockDim.x + threadIdx.x; }
 
 // The FP32 copy of an assembled row for the refined solves, written by the
-// assembly kernel itself: the row scaled by 1 / diag (1 when diag is 0) and
-// its six values stored by direction (slot k of code word cw holds
-// direction (cw >> 3k) & 7, or 7 for an unused slot) -- the same values the
-// separate rounding pass (k_round_ell) writes.
+// assembly kernel itself: the row, scaled by 1 / diag (1 when diag is 0) when
+// f.scale_rows is set, with its six values stored by direction (slot k of
+// code word cw holds direction (cw >> 3k) & 7, or 7 for an unused slot), or
+// in slot order without codes -- the same values the separate rounding
+// passes (k_round_ell, k_amg_round_level0) write.
 __device__ __forceinline__ void store_fp32_row(const Fp32Rows &f, int N, int c, double diag, const double (&offv)[6])
 {
-    const double sc = diag != 0.0 ? 1.0 / diag : 1.0;
+    const double sc = f.scale_rows ? (diag != 0.0 ? 1.0 / diag : 1.0) : 1.0;
     f.d32[c] = (float)(diag * sc);
+    if (!f.code) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) f.o32[(size_t)k * N + c] = (float)(offv[k] * sc);
+        return;
+    }
     const uint32_t cw = f.code[c];
     float o[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
@@ -902,6 +908,7 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_pressure_rows(Physics ph, Me
     a.diag[c] = diag;
 #pragma unroll
     for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
+    if (a.f32.d32) store_fp32_row(a.f32, N, c, diag, offv);
 }
 
 // ------------------------------------------------------- corrector updates

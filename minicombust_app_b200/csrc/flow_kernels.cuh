@@ -22,7 +22,8 @@ struct MeshArgs {
 struct Fp32Rows {
     float *d32 = nullptr;        // null: no copy
     float *o32 = nullptr;        // [6][N]
-    const uint32_t *code = nullptr;
+    const uint32_t *code = nullptr;  // null: slot order
+    int scale_rows = 1;          // divide the row by its diagonal
 };
 
 template <int NF>
@@ -89,6 +90,7 @@ struct MassFluxArgs {
 struct PressureRowArgs {
     const double *mdot, *ff0, *ff1, *src;
     double *off, *diag, *b;
+    Fp32Rows f32;               // the FP32 level 0 of the AMG hierarchy (refined path)
 };
 
 struct CorrectArgs {
