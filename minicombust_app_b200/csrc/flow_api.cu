@@ -220,6 +220,7 @@ struct mc_flow {
     double p_bnorm_ref = 0.0;
     long launches = 0;
     Timing timing;
+    bool gp_stale = false;   // grad[G_P] is older than the corrected pressure (see ensure_pressure_gradient)
 };
 
 namespace {
@@ -843,6 +844,7 @@ int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const B
 
 void launch_gradients5(mc_flow *h)
 {
+    h->gp_stale = false;
     GradArgs<5> a{};
     const int fields[5] = {G_U, G_V, G_W, G_P, G_T};
     for (int k = 0; k < 5; k++) {
@@ -868,6 +870,16 @@ void launch_gradient_pressure(mc_flow *h, int g)
     launch(h, K_GRAD1, [&] {
         launch_lsq_gradients1(h->stream, h->N, h->nbr, h->fc1, h->xc, h->yc, h->zc, h->xf, h->yf, h->zf, a);
     });
+}
+
+// The pressure gradient of the corrected pressure, for readers between
+// passes (get_phi_gradient(P) at the end of calculate_pressure,
+// FlowSolver.inl:2454).
+void ensure_pressure_gradient(mc_flow *h)
+{
+    if (!h->gp_stale) return;
+    launch_gradient_pressure(h, G_P);
+    h->gp_stale = false;
 }
 
 void launch_mass_flux(mc_flow *h)
@@ -1151,11 +1163,14 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
         if (!std::isfinite(pc_max)) return fail(h, MC_ERR_NONFINITE, "pressure correction is not finite");
         if (loop >= 4 || pc_max <= 0.25 * pc_ref) break;
     }
-    launch_gradient_pressure(h, G_P);
+    // update_P needs the corrected pressure's gradient in six cells; the
+    // whole field's gradient is formed only if something reads it before
+    // the next pass's gradients replace it (ensure_pressure_gradient)
     launch(h, K_P_BOUNDARY, [&] {
         k_update_p_boundary<<<1, 32, 0, h->stream>>>(h->ph, h->margs, h->phi[G_P], h->grad[G_P][0], h->grad[G_P][1],
-                                                     h->grad[G_P][2]);
+                                                     h->grad[G_P][2], h->nbr);
     });
+    h->gp_stale = true;
     rc = check_launch(h);
     return rc ? rc : worst;
 }
@@ -2521,6 +2536,7 @@ int mc_flow_interpolate_nodes(mc_flow *h, int64_t n_cells, const uint64_t *cells
     if (!node_ids && !node_fields) return MC_OK;  // size query
     if (count > max_nodes) return fail(h, MC_ERR_ARG, "max_nodes is smaller than the number of nodes");
     if (count == 0) return MC_OK;
+    ensure_pressure_gradient(h);
     NodeArgs a{};
     a.U = h->phi[G_U];
     a.V = h->phi[G_V];
@@ -2569,6 +2585,7 @@ int mc_flow_get_gradient(mc_flow *h, int field, double *vals)
 {
     if (!h || !vals) return MC_ERR_ARG;
     if (!grad_ptr(h, field, 0)) return MC_ERR_UNSUPPORTED;
+    if (field == MC_FIELD_P) ensure_pressure_gradient(h);
     std::vector<double> tmp((size_t)h->N);
     for (int d = 0; d < 3; d++) {
         const double *src = grad_ptr(h, field, d);

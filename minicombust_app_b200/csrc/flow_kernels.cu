@@ -78,16 +78,12 @@ __device__ __forceinline__ void store_fp32_row(const Fp32Rows &f, int N, int c, 
 // The five-field form is held to 3 blocks of 256 per SM (80 registers, a few
 // spilled) instead of the 106 registers and 2 blocks it takes unbounded.
 template <int NF>
-__global__ void __launch_bounds__(MCB_THREADS, NF > 1 ? 3 : 0) k_lsq_gradients(int N, const int *__restrict__ nbr,
-                                                              const int *__restrict__ fc1, const double *__restrict__ xc,
-                                                              const double *__restrict__ yc,
-                                                              const double *__restrict__ zc,
-                                                              const double *__restrict__ xf,
-                                                              const double *__restrict__ yf,
-                                                              const double *__restrict__ zf, GradArgs<NF> a)
+__device__ __forceinline__ void lsq_cell(int N, const int *__restrict__ nbr, const int *__restrict__ fc1,
+                                         const double *__restrict__ xc, const double *__restrict__ yc,
+                                         const double *__restrict__ zc, const double *__restrict__ xf,
+                                         const double *__restrict__ yf, const double *__restrict__ zf,
+                                         const GradArgs<NF> &a, int c)
 {
-    const int c = grid_stride_start();
-    if (c >= N) return;
     const double x = xc[c], y = yc[c], z = zc[c];
     double pc[NF];
 #pragma unroll
@@ -136,6 +132,19 @@ __global__ void __launch_bounds__(MCB_THREADS, NF > 1 ? 3 : 0) k_lsq_gradients(i
         a.gy[k][c] = gy;
         a.gz[k][c] = gz;
     }
+}
+
+template <int NF>
+__global__ void __launch_bounds__(MCB_THREADS, NF > 1 ? 3 : 0) k_lsq_gradients(int N, const int *__restrict__ nbr,
+                                                              const int *__restrict__ fc1, const double *__restrict__ xc,
+                                                              const double *__restrict__ yc,
+                                                              const double *__restrict__ zc,
+                                                              const double *__restrict__ xf,
+                                                              const double *__restrict__ yf,
+                                                              const double *__restrict__ zf, GradArgs<NF> a)
+{
+    const int c = grid_stride_start();
+    if (c < N) lsq_cell<NF>(N, nbr, fc1, xc, yc, zc, xf, yf, zf, a, c);
 }
 
 void launch_lsq_gradients5(cudaStream_t s, int N, const int *nbr, const int *fc1, const double *xc,
@@ -212,18 +221,34 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_momentum_assemble(Physics ph
             internal |= 1u << k;
             const double l0 = m.lam[face];
             const double l1 = 1.0 - l0;
-            const double dUx = a.gU[0][c0] * l0 + a.gU[0][c1] * l1;
-            const double dUy = a.gU[1][c0] * l0 + a.gU[1][c1] * l1;
-            const double dUz = a.gU[2][c0] * l0 + a.gU[2][c1] * l1;
-            const double dVx = a.gV[0][c0] * l0 + a.gV[0][c1] * l1;
-            const double dVy = a.gV[1][c0] * l0 + a.gV[1][c1] * l1;
-            const double dVz = a.gV[2][c0] * l0 + a.gV[2][c1] * l1;
-            const double dWx = a.gW[0][c0] * l0 + a.gW[0][c1] * l1;
-            const double dWy = a.gW[1][c0] * l0 + a.gW[1][c1] * l1;
-            const double dWz = a.gW[2][c0] * l0 + a.gW[2][c1] * l1;
+            double g0[9], g1[9], x0[3], x1[3];  // values at c0 and c1
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                g0[d] = a.gU[d][c0];
+                g1[d] = a.gU[d][c1];
+                g0[3 + d] = a.gV[d][c0];
+                g1[3 + d] = a.gV[d][c1];
+                g0[6 + d] = a.gW[d][c0];
+                g1[6 + d] = a.gW[d][c1];
+            }
+            x0[0] = m.xc[c0];
+            x0[1] = m.yc[c0];
+            x0[2] = m.zc[c0];
+            x1[0] = m.xc[c1];
+            x1[1] = m.yc[c1];
+            x1[2] = m.zc[c1];
+            const double dUx = g0[0] * l0 + g1[0] * l1;
+            const double dUy = g0[1] * l0 + g1[1] * l1;
+            const double dUz = g0[2] * l0 + g1[2] * l1;
+            const double dVx = g0[3] * l0 + g1[3] * l1;
+            const double dVy = g0[4] * l0 + g1[4] * l1;
+            const double dVz = g0[5] * l0 + g1[5] * l1;
+            const double dWx = g0[6] * l0 + g1[6] * l1;
+            const double dWy = g0[7] * l0 + g1[7] * l1;
+            const double dWz = g0[8] * l0 + g1[8] * l1;
             const double Visac = mu * l0 + mu * l1;
             const double VisFace = Visac * m.rl[face];
-            const double Xx = m.xc[c1] - m.xc[c0], Xy = m.yc[c1] - m.yc[c0], Xz = m.zc[c1] - m.zc[c0];
+            const double Xx = x1[0] - x0[0], Xy = x1[1] - x0[1], Xz = x1[2] - x0[2];
             const double md = a.mdot[face];
             const double fude = Visac * ((dUx + dUx) * Sx + (dUy + dVx) * Sy + (dUz + dWx) * Sz);
             const double fvde = Visac * ((dUy + dVx) * Sx + (dVy + dVy) * Sy + (dVz + dWy) * Sz);
@@ -347,6 +372,7 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_momentum_assemble(Physics ph
     if (a.f32.d32) store_fp32_row(a.f32, N, c, ac, offv);
 }
 
+
 // ------------------------------------------------------------- temperature
 // FluxScalar(TEMP) (FlowSolver.inl:2516-2744), unsteady term and
 // setup_sparse_matrix of Scalar_solve (:2885-2953).
@@ -375,10 +401,23 @@ __device__ __forceinline__ double temperature_row(const Physics &ph, const MeshA
             double Visac = mu * l0 + mu * l1;
             Visac -= mu;
             Visac = (mu + Visac / 0.9) / 0.6905;
-            const double dx = a.g[0][c0] * l0 + a.g[0][c1] * l1;
-            const double dy = a.g[1][c0] * l0 + a.g[1][c1] * l1;
-            const double dz = a.g[2][c0] * l0 + a.g[2][c1] * l1;
-            const double Xx = m.xc[c1] - m.xc[c0], Xy = m.yc[c1] - m.yc[c0], Xz = m.zc[c1] - m.zc[c0];
+            // the gradient and centre at c0 and at c1, all loaded before use
+            double g0[3], g1[3], x0[3], x1[3];
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                g0[q] = a.g[q][c0];
+                g1[q] = a.g[q][c1];
+            }
+            x0[0] = m.xc[c0];
+            x0[1] = m.yc[c0];
+            x0[2] = m.zc[c0];
+            x1[0] = m.xc[c1];
+            x1[1] = m.yc[c1];
+            x1[2] = m.zc[c1];
+            const double dx = g0[0] * l0 + g1[0] * l1;
+            const double dy = g0[1] * l0 + g1[1] * l1;
+            const double dz = g0[2] * l0 + g1[2] * l1;
+            const double Xx = x1[0] - x0[0], Xy = x1[1] - x0[1], Xz = x1[2] - x0[2];
             const double VisFace = Visac * m.rl[face];
             const double fde1 = Visac * (dx * Sx + dy * Sy + dz * Sz);
             const double fdi = VisFace * (dx * Xx + dy * Xy + dz * Xz);
@@ -989,15 +1028,27 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_pp_correct_cells(Physics ph,
 }
 
 // update_P (FlowSolver.inl:2292-2315): boundary pressure from the last face
-// of each side.
-__global__ void k_update_p_boundary(Physics ph, MeshArgs m, double *P, const double *gPx, const double *gPy,
-                                    const double *gPz)
+// of each side.  Only the cells of those six faces need the pressure
+// gradient here (get_phi_gradient(P) before it, :2454): with `nbr` given,
+// each thread first computes its cell's gradient (the same least-squares
+// arithmetic as k_lsq_gradients, pressure boundary rule) into gPx/gPy/gPz.
+__global__ void k_update_p_boundary(Physics ph, MeshArgs m, double *P, double *gPx, double *gPy, double *gPz,
+                                    const int *nbr)
 {
     const int side = threadIdx.x;
     if (side >= 6) return;
     const int face = ph.last_bface[side];
     if (face < 0) return;
     const int c0 = m.fc0[face];
+    if (nbr) {
+        GradArgs<1> g{};
+        g.phi[0] = P;
+        g.gx[0] = gPx;
+        g.gy[0] = gPy;
+        g.gz[0] = gPz;
+        g.zero_boundary = 1u;
+        lsq_cell<1>(ph.N, nbr, m.fc1, m.xc, m.yc, m.zc, m.xf, m.yf, m.zf, g, c0);
+    }
     if (ph.btype[side] == OUTLET) {
         P[ph.N + side] = P[c0];
     } else {

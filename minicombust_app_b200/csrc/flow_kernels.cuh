@@ -131,8 +131,8 @@ __global__ void k_outlet_fix(Physics ph, MeshArgs m, double *mdot, double *U, do
 __global__ void k_pressure_rows(Physics ph, MeshArgs m, PressureRowArgs a);
 __global__ void k_pp_correct_faces(Physics ph, MeshArgs m, CorrectArgs a);
 __global__ void k_pp_correct_cells(Physics ph, MeshArgs m, CorrectArgs a, int correct_all, int correct_cell0);
-__global__ void k_update_p_boundary(Physics ph, MeshArgs m, double *P, const double *gPx, const double *gPy,
-                                    const double *gPz);
+__global__ void k_update_p_boundary(Physics ph, MeshArgs m, double *P, double *gPx, double *gPy, double *gPz,
+                                    const int *nbr);
 __global__ void k_pp_max(int N, int cell0, const double *PP, double *partials, unsigned int *counter, double *out);
 // Sum of x[0..n) into *out, deterministic (per-block partials, last block reduces in order).
 __global__ void k_sum(int n, const double *x, double *partials, unsigned int *counter, double *out);
