@@ -148,13 +148,16 @@ class ClockSampler:
 def kernel_bytes(name, N, F, nnz_off):
     """Algorithmic (unique-touch) bytes of one launch: each stored input
     element read once, each output written once, at its stored type.  The
-    FP64 solver kernels read a 4-byte direction code per row instead of the
-    six int32 columns (structured box); the FP32 copies are stored by
-    direction and read no column data.  ELL values include the boundary
-    padding."""
+    FP64 momentum and temperature solver kernels read a 4-byte direction code
+    per row instead of the six int32 columns (structured box); the FP32
+    copies are stored by direction and read no column data.  The pressure
+    solvers' copies (FP64 and FP32) are stored by direction in the half form
+    of a symmetric matrix: the diagonal and the +x, +y, +z couplings, the
+    others read as the neighbours' (counted once).  ELL values include the
+    boundary padding."""
     return {
-        "pcg_iter1_spmv": 92 * N,      # diag, 6 off, code, (z, p) pair -> p, q
-        "pcg32_iter1_spmv": 44 * N,    # the same in FP32, no code
+        "pcg_iter1_spmv": 64 * N,      # diag, 3 off, (z, p) pair -> p, q
+        "pcg32_iter1_spmv": 32 * N,    # the same in FP32
         "pcg_iter2_update": 64 * N,    # x rw, r rw, p, q, diag -> z (Jacobi path)
         "bicg3_1_spmv": 204 * N,       # matrix 60 + 3 x (r, p, v gathered; r0; p, v out)
         "bicg3_2_spmv": 156 * N,       # matrix 60 + 3 x (r, v gathered; s, t out)
@@ -163,15 +166,17 @@ def kernel_bytes(name, N, F, nnz_off):
         "bicg3_32_2_spmv": 76 * N,     # FP32: matrix 28 + 3 x 16
         "bicg3_32_3_update": 84 * N,
         "gnn_forward": 708 * N,        # inputs 24 + vhat 4, h0 out 64, 4 layers x (h in 64 + h out 64 + mask 1), decode 64 in + y, x0 out 12
-        # one V-cycle, per fine row.  FP32 (every level's matrix by direction),
-        # level 0: first two sweeps 36, sweep 40, restriction 40, prolongation
-        # + sweep 44, sweep 40, last sweep with r.z 40 = 240; level 1 (1/8 of
-        # the rows, about 241 bytes per row) 30; level 2 and below 4
-        "amg32_vcycle": 274 * N,
-        # FP64 (level 0 direction codes, coarse levels by direction), level 0:
-        # first sweep 24, sweeps 4 x 84, restriction 81, prolongation 21, last
-        # sweep 84 = 546; level 1 66; level 2 and below 9
-        "amg_vcycle": 621 * N,
+        # one V-cycle, per fine row.  FP32 (every level's matrix by direction,
+        # level 0 in the half form: 16 bytes of matrix per row), level 0: first
+        # two sweeps 24, sweep 28, restriction 28, prolongation + sweep 32,
+        # sweep 28, last sweep with r.z 28 = 168; level 1 (1/8 of the rows,
+        # about 241 bytes per row) 30; level 2 and below 4
+        "amg32_vcycle": 202 * N,
+        # FP64 (level 0 in the half form: 32 bytes of matrix per row, coarse
+        # levels by direction), level 0: first sweep 24, sweeps 4 x 56,
+        # restriction 53, prolongation 21, last sweep 56 = 378; level 1 66;
+        # level 2 and below 9
+        "amg_vcycle": 453 * N,
         "lsq_gradients_uvwpt": 208 * N,
         "momentum_assemble": 56 * F + 296 * N,
         "mass_flux": 88 * F + 176 * N,

@@ -64,6 +64,10 @@ using AmgLevel = AmgLevelT<double>;
 struct AmgHierarchy {
     int levels = 0;
     AmgLevelT<double> lv[AMG_MAX_LEVELS];    // FP64 values (level 0 = the pressure-correction matrix)
+    // level 0 with its values in slot order: the source of the Galerkin
+    // lists of level 1 and of the FP32 level 0 (lv[0] itself may be the
+    // half-form copy, DirCodes::sym)
+    AmgLevelT<double> g0;
     AmgLevelT<float> lv32[AMG_MAX_LEVELS];   // FP32 values, when the refined FP32 path is enabled
     bool has32 = false;
     double *dense = nullptr;       // coarsest inverse [n][n] (row-major, exactly symmetric), FP64

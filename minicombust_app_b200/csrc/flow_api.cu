@@ -94,6 +94,10 @@ struct mc_flow {
     std::vector<int> hcol;   // ELL columns with -1 on boundary slots (CSR export)
     uint32_t *dcode = nullptr;  // direction codes of the ELL columns (used when dc.code is set)
     DirCodes dc;
+    // the solvers' copy of the pressure-correction matrix in the half form of
+    // a symmetric matrix (DirCodes::sym), written with the slot-order rows
+    double *p_sym64 = nullptr;
+    DirCodes dc_psym;
     // cell/face renumbering (reorder == MC_REORDER_RCM); host and device copies
     bool reordered = false;
     std::vector<int> cell_n2o, cell_o2n, face_o2n;
@@ -328,7 +332,11 @@ double *grad_ptr(mc_flow *h, int field, int d)
 }
 
 Ell momentum_matrix(mc_flow *h) { return Ell{h->N, h->AU, h->off_m, h->col, h->dc}; }
-Ell pressure_matrix(mc_flow *h) { return Ell{h->N, h->diag_p, h->off_p, h->col, h->dc}; }
+Ell pressure_matrix(mc_flow *h)
+{
+    if (h->p_sym64) return Ell{h->N, h->diag_p, h->p_sym64, h->col, h->dc_psym};
+    return Ell{h->N, h->diag_p, h->off_p, h->col, h->dc};
+}
 Ell temperature_matrix(mc_flow *h) { return Ell{h->N, h->diag_t, h->off_t, h->col, h->dc}; }
 
 // ------------------------------------------------------------ Krylov drivers
@@ -1073,8 +1081,10 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
         h->p32_written = h->use_amg && h->refined;  // the FP32 level 0 of the hierarchy, written by the kernel
         if (h->p32_written) {
             const AmgLevelT<float> &L0 = h->amg.lv32[0];
-            a.f32 = Fp32Rows{L0.diag, L0.off, L0.dc.dia ? h->amg.lv[0].dc.code : nullptr, 0};
+            a.f32 = Fp32Rows{L0.diag, L0.off, L0.dc.dia ? h->dc.code : nullptr, 0, L0.dc.sym};
         }
+        a.sym64 = h->p_sym64;
+        a.code = h->dc.code;
         launch(h, K_PRESSURE_ROWS, [&] {
             k_pressure_rows<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a);
         });
@@ -1616,6 +1626,13 @@ int x_line_length(const std::vector<uint32_t> &code, const int doff[6], int N)
     return ex;
 }
 
+// MC_SYM_PRESSURE=0 keeps the solvers on the slot-order pressure matrix.
+bool sym_pressure_disabled()
+{
+    const char *v = std::getenv("MC_SYM_PRESSURE");
+    return v && v[0] == '0';
+}
+
 bool dir_codes_disabled()
 {
     const char *v = std::getenv("MC_DIR_CODES");
@@ -1743,9 +1760,9 @@ int build_amg(mc_flow *h, const HostMesh &hm)
         AmgLevel &d = H.lv[l];
         if (l == 0) {
             d.diag = h->diag_p;
-            d.off = h->off_p;
+            d.off = h->p_sym64 ? h->p_sym64 : h->off_p;
             d.col = h->col;
-            d.dc = h->dc;
+            d.dc = h->p_sym64 ? h->dc_psym : h->dc;
             d.r = h->pv.r;
         } else {
             int rc = put(d_col[l], lv[l].col);
@@ -1771,6 +1788,9 @@ int build_amg(mc_flow *h, const HostMesh &hm)
             d.mlist = d_mlist[l];
         }
     }
+    H.g0 = H.lv[0];  // the slot-order level 0 (Galerkin lists, FP32 rounding)
+    H.g0.off = h->off_p;
+    H.g0.dc = h->dc;
     if (fp32) {
         for (int l = 0; l < L; l++) {
             AmgLevelT<float> &f = H.lv32[l];
@@ -1778,7 +1798,9 @@ int build_amg(mc_flow *h, const HostMesh &hm)
             f.n = d.n;
             f.k = d.k;
             f.col = d.col;
-            f.dc = l == 0 ? by_direction(d.dc) : d.dc;  // FP32 level 0 values are stored by direction
+            // FP32 level 0 values are stored by direction (in the half form
+            // where the FP64 copy is)
+            f.dc = l == 0 ? (h->p_sym64 ? by_direction_sym(h->dc) : by_direction(h->dc)) : d.dc;
             f.agg = d.agg;
             f.mptr = d.mptr;
             f.mlist = d.mlist;
@@ -1990,6 +2012,12 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
                     h->line_ex = x_line_length(code, doff, (int)N);
                 }
             }
+            if (!rc && sym_applies(h->dc) && !sym_pressure_disabled()) {
+                // the solvers' half-form copy of the pressure-correction matrix
+                const cudaError_t e = cudaMalloc((void **)&h->p_sym64, (size_t)3 * N * sizeof(double));
+                if (e != cudaSuccess) rc = fail(h, MC_ERR_NOMEM, "cudaMalloc (pressure copy)");
+                else h->dc_psym = by_direction_sym(h->dc);
+            }
             if (!rc && params->pressure_solver == MC_PSOLVER_PCG_AMG) rc = build_amg(h, hm);
             if (!rc) rc = setup_guess(h, hm);
             if (!rc && params->precision == MC_PRECISION_FP32_REFINED) rc = setup_bicg_refined(h);
@@ -2050,6 +2078,7 @@ int mc_flow_destroy(mc_flow *h)
                               h->l_pcg, h->l_b3, h->l_b1, h->l_pcg_amg, h->l_pcg_amg32, h->l_b3_32, h->l_b1_32})
         if (g) cudaGraphExecDestroy(g);
     if (h->amg_mem) cudaFree(h->amg_mem);
+    if (h->p_sym64) cudaFree(h->p_sym64);
     for (cudaEvent_t e : h->timing.ev) cudaEventDestroy(e);
     if (h->arena.base) cudaFree(h->arena.base);
     if (h->h_pcg) cudaFreeHost(h->h_pcg);
@@ -2366,6 +2395,9 @@ int mc_flow_checkpoint_read(mc_flow *h, const char *path)
     h->sources_set = hd.sources_set;
     h->mass_source_total = hd.mass_source_total;
     h->mass_source_on_device = false;
+    // the solvers' half-form copy of a carried-over pressure system
+    if (h->p_sym64)
+        k_sym_rows64<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->N, h->off_p, h->dc.code, h->p_sym64);
     // a pressure system carried over from before (compat mode) needs its AMG
     // values; the coarsest inverse is formed in line
     if (h->use_amg && !h->first_pressure) {

@@ -21,9 +21,10 @@ struct MeshArgs {
 // FP32 copy of assembled rows (refined path): scaled by 1 / diag, by direction.
 struct Fp32Rows {
     float *d32 = nullptr;        // null: no copy
-    float *o32 = nullptr;        // [6][N]
+    float *o32 = nullptr;        // [6][N] ([3][N] with sym)
     const uint32_t *code = nullptr;  // null: slot order
     int scale_rows = 1;          // divide the row by its diagonal
+    int sym = 0;                 // symmetric matrix: only directions 1, 3, 5 into slots 0, 1, 2 (DirCodes::sym)
 };
 
 template <int NF>
@@ -91,7 +92,16 @@ struct PressureRowArgs {
     const double *mdot, *ff0, *ff1, *src;
     double *off, *diag, *b;
     Fp32Rows f32;               // the FP32 level 0 of the AMG hierarchy (refined path)
+    // the FP64 copy the solvers read, in the half form of a symmetric matrix
+    // (DirCodes::sym; by the direction codes `code`), or null
+    double *sym64;
+    const uint32_t *code;
 };
+
+// The half-form FP64 copy (DirCodes::sym) of a symmetric matrix stored by
+// slot with direction codes: sym[(d >> 1) N + i] = off[k][i] for the slot k
+// of each direction d = 1, 3, 5 (0 where the row has none).
+__global__ void k_sym_rows64(int N, const double *off, const uint32_t *code, double *sym);
 
 struct CorrectArgs {
     double *PP, *P, *U, *V, *W;

@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_init(Ell A, PcgVectors v, d
             int c_[6];
             row_cols(A, i, c_);
 #pragma unroll
-            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * v.x[c_[k]];
+            for (int k = 0; k < 6; k++) ax += ell_val(A.dc, A.off, N, i, k, c_[k]) * v.x[c_[k]];
             ri = bi - ax;
         } else {
             v.x[i] = 0.0;
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_iter1(EllT<T> A, PcgVectors
 #pragma unroll
                 for (int k = 0; k < 6; k++) {
                     const T2 g = X[c[k]];
-                    q += A.off[(size_t)k * N + i] * (g.x + bt * g.y);
+                    q += ell_val(A.dc, A.off, N, i, k, c[k]) * (g.x + bt * g.y);
                 }
                 return q;
             });
@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_pcg_init_amg(EllT<T> A, PcgVect
             int c_[6];
             row_cols(A, i, c_);
 #pragma unroll
-            for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * N + i] * v.x[c_[k]];
+            for (int k = 0; k < 6; k++) ax += ell_val(A.dc, A.off, N, i, k, c_[k]) * v.x[c_[k]];
             ri = bi - ax;
         } else {
             v.x[i] = (T)0;
@@ -316,7 +316,7 @@ __device__ __forceinline__ double ell_row(const Ell &A, const double *__restrict
     return with_row_cols(A.dc, A.col, A.N, i, [&](const int(&c)[6]) {
         double ax = A.diag[i] * x[i];
 #pragma unroll
-        for (int k = 0; k < 6; k++) ax += A.off[(size_t)k * A.N + i] * x[c[k]];
+        for (int k = 0; k < 6; k++) ax += ell_val(A.dc, A.off, A.N, i, k, c[k]) * x[c[k]];
         return ax;
     });
 }
@@ -332,7 +332,7 @@ __device__ __forceinline__ RowPair ell_row2(const Ell &A, const double *__restri
         RowPair o{xa ? A.diag[i] * xa[i] : 0.0, xb ? A.diag[i] * xb[i] : 0.0};
 #pragma unroll
         for (int k = 0; k < 6; k++) {
-            const double a = A.off[(size_t)k * A.N + i];
+            const double a = ell_val(A.dc, A.off, A.N, i, k, c[k]);
             if (xa) o.u += a * xa[c[k]];
             if (xb) o.w += a * xb[c[k]];
         }
@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_ir_residual(Ell A, const double
         const double ax = with_row_cols(A.dc, A.col, N, i, [&](const int(&c)[6]) {
             double s = A.diag[i] * x[i];
 #pragma unroll
-            for (int k = 0; k < 6; k++) s += A.off[(size_t)k * N + i] * x[c[k]];
+            for (int k = 0; k < 6; k++) s += ell_val(A.dc, A.off, N, i, k, c[k]) * x[c[k]];
             return s;
         });
         const double ri = (b[i] - mean) - ax;

@@ -38,19 +38,54 @@ struct Pair<float> {
 // (slot d = direction d, zero where the row has no neighbour that way): its
 // columns are row + doff[d] (clamped into [0, N), where the value is 0), so
 // the kernels read no column data at all.
+// `sym` (with `dia`) marks the copy of a symmetric matrix that keeps only
+// the couplings of the directions with positive offsets (d = 1, 3, 5 in slot
+// d >> 1): the coupling of row i in direction d - 1 is the one row
+// i + doff[d - 1] keeps for direction d (A_ij = A_ji), and 0 where that row
+// index is below 0.  A row with no neighbour in direction d - 1 reads the
+// stored 0 of the row before it on the x-line, y-column or z-column edge.
+// Half the off-diagonal bytes.
 struct DirCodes {
     const uint32_t *code = nullptr;  // [N]; nullptr: use the column list
     int doff[6] = {0, 0, 0, 0, 0, 0};
     uint32_t canon = 0;
     int coff[6] = {0, 0, 0, 0, 0, 0};
     int dia = 0;
+    int sym = 0;
 };
 
 // The same codes for a copy of the values in direction order (see `dia`).
 inline DirCodes by_direction(DirCodes dc)
 {
     dc.dia = dc.code ? 1 : 0;
+    dc.sym = 0;
     return dc;
+}
+
+// A symmetric matrix's copy in the half form (see `sym`): needs codes whose
+// even directions are the negatives of the odd ones.
+inline bool sym_applies(const DirCodes &dc)
+{
+    if (!dc.code) return false;
+    for (int j = 0; j < 3; j++)
+        if (!(dc.doff[2 * j] < 0 && dc.doff[2 * j] == -dc.doff[2 * j + 1])) return false;
+    return true;
+}
+inline DirCodes by_direction_sym(DirCodes dc)
+{
+    dc = by_direction(dc);
+    dc.sym = dc.dia;
+    return dc;
+}
+
+// Value of slot k of row i (its column ck from row_cols / with_row_cols).
+template <typename T>
+__device__ __forceinline__ T ell_val(const DirCodes &dc, const T *__restrict__ off, int N, int i, int k, int ck)
+{
+    if (!dc.sym) return off[(size_t)k * N + i];
+    const size_t j = (size_t)(k >> 1) * N;
+    if (k & 1) return off[j + i];
+    return (i + dc.doff[k] >= 0) ? off[j + ck] : (T)0;
 }
 
 __device__ __forceinline__ void dia_cols(const DirCodes &dc, int N, int i, int (&c)[6])
