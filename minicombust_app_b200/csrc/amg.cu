@@ -220,21 +220,16 @@ __device__ __forceinline__ T inv_or_zero(T d)
 } // namespace
 
 // FP32 copy of the level-0 values (in direction order when the level has
-// direction codes; with sym only directions 1, 3, 5, DirCodes::sym).
+// direction codes).
 __global__ void k_amg_round_level0(int n, const double *__restrict__ diag, const double *__restrict__ off,
                                    const uint32_t *__restrict__ code, float *__restrict__ diag32,
-                                   float *__restrict__ off32, int sym)
+                                   float *__restrict__ off32)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     diag32[i] = (float)diag[i];
     float o[6];
     round_row_by_direction(off, code, n, i, o);
-    if (sym) {
-#pragma unroll
-        for (int j = 0; j < 3; j++) off32[(size_t)j * n + i] = o[2 * j + 1];
-        return;
-    }
 #pragma unroll
     for (int q = 0; q < 6; q++) off32[(size_t)q * n + i] = o[q];
 }
@@ -577,7 +572,7 @@ void amg_setup_levels(cudaStream_t s, const AmgHierarchy &H, bool level0_ready)
     if (sizeof(T) == sizeof(float) && !level0_ready)
         k_amg_round_level0<<<blocks(H.g0.n), MCB_THREADS, 0, s>>>(H.g0.n, H.g0.diag, H.g0.off,
                                                                   lv[0].dc.dia ? H.g0.dc.code : nullptr,
-                                                                  (float *)lv[0].diag, (float *)lv[0].off, lv[0].dc.sym);
+                                                                  (float *)lv[0].diag, (float *)lv[0].off);
     if (H.levels > 1) k_amg_galerkin<double, T><<<blocks(lv[1].n), MCB_THREADS, 0, s>>>(H.g0, lv[1]);
     for (int l = 2; l < H.levels; l++)
         k_amg_galerkin<T, T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l - 1], lv[l]);

@@ -39,7 +39,7 @@ enum KernelId {
     K_IR, K_PCG_INIT_AMG32, K_PCG_ITER1_32, K_PCG_ITER2_AMG32, K_AMG_VCYCLE32, K_PERMUTE, K_GUESS, K_GNN,
     K_SNAPSHOT, K_BIR, K_ROUND_ELL, K_BICG3_INIT32, K_BICG3_1_32, K_BICG3_2_32, K_BICG3_3_32, K_BICG1_INIT32,
     K_BICG1_1_32, K_BICG1_2_32, K_BICG1_3_32, K_GRAD6, K_SCALAR, K_SCALAR_CLIP, K_EXCHANGE, K_LINE3, K_LINE1,
-    K_COUNT
+    K_GNN_LAYERS, K_COUNT
 };
 
 const char *kKernelNames[K_COUNT] = {
@@ -49,11 +49,11 @@ const char *kKernelNames[K_COUNT] = {
     "pcg_xmean", "pcg_sub_xmean", "bicg3_init", "bicg3_1_spmv", "bicg3_2_spmv", "bicg3_3_update",
     "bicg1_init", "bicg1_1_spmv", "bicg1_2_spmv", "bicg1_3_update", "amg_setup_galerkin_factor",
     "pcg_init_amg", "pcg_iter2_amg_update", "amg_vcycle", "ir_fp64_residual_update", "pcg32_init_amg",
-    "pcg32_iter1_spmv", "pcg32_iter2_amg_update", "amg32_vcycle", "permute", "guess_select", "gnn_forward",
+    "pcg32_iter1_spmv", "pcg32_iter2_amg_update", "amg32_vcycle", "permute", "guess_select", "gnn_encode_decode",
     "snapshot_pack", "bicg_refine_fp64_residual", "round_fp32", "bicg3_32_init", "bicg3_32_1_spmv",
     "bicg3_32_2_spmv", "bicg3_32_3_update", "bicg1_32_init", "bicg1_32_1_spmv", "bicg1_32_2_spmv",
     "bicg1_32_3_update", "lsq_gradients_scalars", "scalar_assemble", "scalar_clip_negative", "particle_exchange",
-    "line_sweep3_32", "line_sweep1_32"};
+    "line_sweep3_32", "line_sweep1_32", "gnn_layers"};
 
 constexpr int PCG_BATCH = 16;   // iterations per status read (even: ping-pong buffers)
 constexpr int PCG_AMG_BATCH = 4;
@@ -94,10 +94,11 @@ struct mc_flow {
     std::vector<int> hcol;   // ELL columns with -1 on boundary slots (CSR export)
     uint32_t *dcode = nullptr;  // direction codes of the ELL columns (used when dc.code is set)
     DirCodes dc;
-    // the solvers' copy of the pressure-correction matrix in the half form of
-    // a symmetric matrix (DirCodes::sym), written with the slot-order rows
-    double *p_sym64 = nullptr;
-    DirCodes dc_psym;
+    // the solvers' copy of the pressure-correction matrix stored by direction
+    // (DirCodes::dia; with dc_pdir.sym in the half form of a symmetric
+    // matrix), written with the slot-order rows; null: the solvers read those
+    double *p_dir64 = nullptr;
+    DirCodes dc_pdir;
     // cell/face renumbering (reorder == MC_REORDER_RCM); host and device copies
     bool reordered = false;
     std::vector<int> cell_n2o, cell_o2n, face_o2n;
@@ -334,7 +335,7 @@ double *grad_ptr(mc_flow *h, int field, int d)
 Ell momentum_matrix(mc_flow *h) { return Ell{h->N, h->AU, h->off_m, h->col, h->dc}; }
 Ell pressure_matrix(mc_flow *h)
 {
-    if (h->p_sym64) return Ell{h->N, h->diag_p, h->p_sym64, h->col, h->dc_psym};
+    if (h->p_dir64) return Ell{h->N, h->diag_p, h->p_dir64, h->col, h->dc_pdir};
     return Ell{h->N, h->diag_p, h->off_p, h->col, h->dc};
 }
 Ell temperature_matrix(mc_flow *h) { return Ell{h->N, h->diag_t, h->off_t, h->col, h->dc}; }
@@ -487,10 +488,13 @@ int select_guess(mc_flow *h, const Ell &A, const double *b, const PcgState *st, 
     if (h->prm.initial_guess == MC_GUESS_ZERO || h->corrector > 1) return 0;
     const bool learned = h->prm.initial_guess == MC_GUESS_LEARNED;
     if (learned) {
-        launch(h, K_GNN, [&] {
-            GnnInput<double> in{b, &st->mean, A.diag, h->pp_prev};
-            gnn_forward<double>(h->stream, h->gnn_g, in, h->gnn_p, h->gnn_pk, h->gnn_w, h->x0_learned);
-        });
+        // the network's layers are timed apart from its encoder and decoder
+        const GnnInput<double> in{b, &st->mean, A.diag, h->pp_prev};
+        for (const int part : {GNN_FWD_BEGIN, GNN_FWD_LAYERS, GNN_FWD_END})
+            launch(h, part == GNN_FWD_LAYERS ? K_GNN_LAYERS : K_GNN, [&] {
+                gnn_forward<double>(h->stream, h->gnn_g, in, h->gnn_p, h->gnn_pk, h->gnn_w, h->x0_learned, part);
+            });
+        h->launches -= 2;
         CUDA_TRY(h, cudaMemcpyAsync(&h->gs->net_status, h->gnn_w.status, sizeof(int), cudaMemcpyDeviceToDevice,
                                     h->stream));
         h->launches += gnn_forward_launches() - 1;
@@ -1081,9 +1085,10 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
         h->p32_written = h->use_amg && h->refined;  // the FP32 level 0 of the hierarchy, written by the kernel
         if (h->p32_written) {
             const AmgLevelT<float> &L0 = h->amg.lv32[0];
-            a.f32 = Fp32Rows{L0.diag, L0.off, L0.dc.dia ? h->dc.code : nullptr, 0, L0.dc.sym};
+            a.f32 = Fp32Rows{L0.diag, L0.off, L0.dc.dia ? h->dc.code : nullptr, 0};
         }
-        a.sym64 = h->p_sym64;
+        a.dir64 = h->p_dir64;
+        a.dir64_sym = h->dc_pdir.sym;
         a.code = h->dc.code;
         launch(h, K_PRESSURE_ROWS, [&] {
             k_pressure_rows<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->ph, h->margs, a);
@@ -1626,11 +1631,13 @@ int x_line_length(const std::vector<uint32_t> &code, const int doff[6], int N)
     return ex;
 }
 
-// MC_SYM_PRESSURE=0 keeps the solvers on the slot-order pressure matrix.
-bool sym_pressure_disabled()
+// Form of the pressure solvers' FP64 copy: 1 (default) the half form of the
+// symmetric matrix, 2 all six directions, 0 none (the slot-order matrix);
+// MC_PRESSURE_COPY overrides.  The FP32 level 0 keeps all six directions.
+int pressure_copy_form()
 {
-    const char *v = std::getenv("MC_SYM_PRESSURE");
-    return v && v[0] == '0';
+    const char *v = std::getenv("MC_PRESSURE_COPY");
+    return (v && *v) ? std::atoi(v) : 1;
 }
 
 bool dir_codes_disabled()
@@ -1760,9 +1767,9 @@ int build_amg(mc_flow *h, const HostMesh &hm)
         AmgLevel &d = H.lv[l];
         if (l == 0) {
             d.diag = h->diag_p;
-            d.off = h->p_sym64 ? h->p_sym64 : h->off_p;
+            d.off = h->p_dir64 ? h->p_dir64 : h->off_p;
             d.col = h->col;
-            d.dc = h->p_sym64 ? h->dc_psym : h->dc;
+            d.dc = h->p_dir64 ? h->dc_pdir : h->dc;
             d.r = h->pv.r;
         } else {
             int rc = put(d_col[l], lv[l].col);
@@ -1798,9 +1805,7 @@ int build_amg(mc_flow *h, const HostMesh &hm)
             f.n = d.n;
             f.k = d.k;
             f.col = d.col;
-            // FP32 level 0 values are stored by direction (in the half form
-            // where the FP64 copy is)
-            f.dc = l == 0 ? (h->p_sym64 ? by_direction_sym(h->dc) : by_direction(h->dc)) : d.dc;
+            f.dc = l == 0 ? by_direction(h->dc) : d.dc;  // FP32 level 0 values are stored by direction
             f.agg = d.agg;
             f.mptr = d.mptr;
             f.mlist = d.mlist;
@@ -2012,11 +2017,14 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
                     h->line_ex = x_line_length(code, doff, (int)N);
                 }
             }
-            if (!rc && sym_applies(h->dc) && !sym_pressure_disabled()) {
-                // the solvers' half-form copy of the pressure-correction matrix
-                const cudaError_t e = cudaMalloc((void **)&h->p_sym64, (size_t)3 * N * sizeof(double));
+            const int form = pressure_copy_form();
+            if (!rc && h->dc.code && form > 0 && (form == 2 || sym_applies(h->dc))) {
+                // the solvers' by-direction copy of the pressure-correction matrix
+                const bool sym = form != 2;
+                const cudaError_t e =
+                    cudaMalloc((void **)&h->p_dir64, (size_t)(sym ? 3 : 6) * N * sizeof(double));
                 if (e != cudaSuccess) rc = fail(h, MC_ERR_NOMEM, "cudaMalloc (pressure copy)");
-                else h->dc_psym = by_direction_sym(h->dc);
+                else h->dc_pdir = sym ? by_direction_sym(h->dc) : by_direction(h->dc);
             }
             if (!rc && params->pressure_solver == MC_PSOLVER_PCG_AMG) rc = build_amg(h, hm);
             if (!rc) rc = setup_guess(h, hm);
@@ -2078,7 +2086,7 @@ int mc_flow_destroy(mc_flow *h)
                               h->l_pcg, h->l_b3, h->l_b1, h->l_pcg_amg, h->l_pcg_amg32, h->l_b3_32, h->l_b1_32})
         if (g) cudaGraphExecDestroy(g);
     if (h->amg_mem) cudaFree(h->amg_mem);
-    if (h->p_sym64) cudaFree(h->p_sym64);
+    if (h->p_dir64) cudaFree(h->p_dir64);
     for (cudaEvent_t e : h->timing.ev) cudaEventDestroy(e);
     if (h->arena.base) cudaFree(h->arena.base);
     if (h->h_pcg) cudaFreeHost(h->h_pcg);
@@ -2395,9 +2403,10 @@ int mc_flow_checkpoint_read(mc_flow *h, const char *path)
     h->sources_set = hd.sources_set;
     h->mass_source_total = hd.mass_source_total;
     h->mass_source_on_device = false;
-    // the solvers' half-form copy of a carried-over pressure system
-    if (h->p_sym64)
-        k_sym_rows64<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->N, h->off_p, h->dc.code, h->p_sym64);
+    // the solvers' by-direction copy of a carried-over pressure system
+    if (h->p_dir64)
+        k_dir_rows64<<<blocks_for(h->N), MCB_THREADS, 0, h->stream>>>(h->N, h->off_p, h->dc.code, h->p_dir64,
+                                                                     h->dc_pdir.sym);
     // a pressure system carried over from before (compat mode) needs its AMG
     // values; the coarsest inverse is formed in line
     if (h->use_amg && !h->first_pressure) {

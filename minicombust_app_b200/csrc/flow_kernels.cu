@@ -64,25 +64,29 @@ __device__ __forceinline__ void store_fp32_row(const Fp32Rows &f, int N, int c, 
 #pragma unroll
         for (int q = 0; q < 6; q++) o[q] = (d == (unsigned)q) ? v : o[q];
     }
-    if (f.sym) {
-#pragma unroll
-        for (int j = 0; j < 3; j++) f.o32[(size_t)j * N + c] = o[2 * j + 1];
-        return;
-    }
 #pragma unroll
     for (int q = 0; q < 6; q++) f.o32[(size_t)q * N + c] = o[q];
 }
 
-// The couplings of directions 1, 3, 5 of row c (0 where the row has none).
-__device__ __forceinline__ void sym_row(const uint32_t cw, const double (&offv)[6], double (&o)[3])
+// Row c stored by direction into out (see k_dir_rows64).
+__device__ __forceinline__ void store_dir_row(const uint32_t cw, const double (&offv)[6], double *out, int N, int c,
+                                              int sym)
 {
+    double o[6];
 #pragma unroll
-    for (int j = 0; j < 3; j++) o[j] = 0.0;
+    for (int d = 0; d < 6; d++) o[d] = 0.0;
 #pragma unroll
     for (int k = 0; k < 6; k++) {
         const unsigned d = (cw >> (3 * k)) & 7u;
 #pragma unroll
-        for (int j = 0; j < 3; j++) o[j] = (d == (unsigned)(2 * j + 1)) ? offv[k] : o[j];
+        for (int q = 0; q < 6; q++) o[q] = (d == (unsigned)q) ? offv[k] : o[q];
+    }
+    if (sym) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) out[(size_t)j * N + c] = o[2 * j + 1];
+    } else {
+#pragma unroll
+        for (int q = 0; q < 6; q++) out[(size_t)q * N + c] = o[q];
     }
 }
 
@@ -966,25 +970,19 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_pressure_rows(Physics ph, Me
 #pragma unroll
     for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
     if (a.f32.d32) store_fp32_row(a.f32, N, c, diag, offv);
-    if (a.sym64) {
-        double o[3];
-        sym_row(a.code[c], offv, o);
-#pragma unroll
-        for (int j = 0; j < 3; j++) a.sym64[(size_t)j * N + c] = o[j];
-    }
+    if (a.dir64) store_dir_row(a.code[c], offv, a.dir64, N, c, a.dir64_sym);
 }
 
-__global__ void __launch_bounds__(MCB_THREADS) k_sym_rows64(int N, const double *__restrict__ off,
-                                                           const uint32_t *__restrict__ code, double *__restrict__ sym)
+__global__ void __launch_bounds__(MCB_THREADS) k_dir_rows64(int N, const double *__restrict__ off,
+                                                           const uint32_t *__restrict__ code, double *__restrict__ out,
+                                                           int sym)
 {
     const int c = grid_stride_start();
     if (c >= N) return;
-    double offv[6], o[3];
+    double offv[6];
 #pragma unroll
     for (int k = 0; k < 6; k++) offv[k] = off[(size_t)k * N + c];
-    sym_row(code[c], offv, o);
-#pragma unroll
-    for (int j = 0; j < 3; j++) sym[(size_t)j * N + c] = o[j];
+    store_dir_row(code[c], offv, out, N, c, sym);
 }
 
 // ------------------------------------------------------- corrector updates

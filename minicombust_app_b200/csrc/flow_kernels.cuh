@@ -21,10 +21,9 @@ struct MeshArgs {
 // FP32 copy of assembled rows (refined path): scaled by 1 / diag, by direction.
 struct Fp32Rows {
     float *d32 = nullptr;        // null: no copy
-    float *o32 = nullptr;        // [6][N] ([3][N] with sym)
+    float *o32 = nullptr;        // [6][N]
     const uint32_t *code = nullptr;  // null: slot order
     int scale_rows = 1;          // divide the row by its diagonal
-    int sym = 0;                 // symmetric matrix: only directions 1, 3, 5 into slots 0, 1, 2 (DirCodes::sym)
 };
 
 template <int NF>
@@ -92,16 +91,19 @@ struct PressureRowArgs {
     const double *mdot, *ff0, *ff1, *src;
     double *off, *diag, *b;
     Fp32Rows f32;               // the FP32 level 0 of the AMG hierarchy (refined path)
-    // the FP64 copy the solvers read, in the half form of a symmetric matrix
-    // (DirCodes::sym; by the direction codes `code`), or null
-    double *sym64;
+    // the FP64 copy the solvers read, stored by direction (by the direction
+    // codes `code`): all six directions, or with dir64_sym the half form of
+    // a symmetric matrix (DirCodes::sym); null: none
+    double *dir64;
+    int dir64_sym;
     const uint32_t *code;
 };
 
-// The half-form FP64 copy (DirCodes::sym) of a symmetric matrix stored by
-// slot with direction codes: sym[(d >> 1) N + i] = off[k][i] for the slot k
-// of each direction d = 1, 3, 5 (0 where the row has none).
-__global__ void k_sym_rows64(int N, const double *off, const uint32_t *code, double *sym);
+// The by-direction FP64 copy of a matrix stored by slot with direction
+// codes: out[d N + i] = off[k][i] for the slot k of direction d (0 where the
+// row has none), or with sym (DirCodes::sym) only d = 1, 3, 5 into
+// out[(d >> 1) N + i].
+__global__ void k_dir_rows64(int N, const double *off, const uint32_t *code, double *out, int sym);
 
 struct CorrectArgs {
     double *PP, *P, *U, *V, *W;

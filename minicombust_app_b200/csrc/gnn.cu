@@ -1184,7 +1184,7 @@ void gnn_pack(cudaStream_t s, const float *p, bf16 *pk) { k_gnn_pack<<<32, 256, 
 // h[1] and uses the offset-form weights where the graph allows.
 template <typename T>
 static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &in, const float *p, const bf16 *pk,
-                         GnnWork &w, double *x0, bool train)
+                         GnnWork &w, double *x0, bool train, int parts = GNN_FWD_ALL)
 {
     const int nb = gnn_blocks(g.n);
     const bool folded = !train && g.affine;
@@ -1192,18 +1192,20 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
     GnnTmaMap maps[2];
     const bool umma = folded && path != GnnLayerPath::Mma && gnn_umma_map(&maps[0], w.h[0], g.n) &&
                       gnn_umma_map(&maps[1], w.h[1], g.n) && gnn_umma_ready();
-    cudaMemsetAsync(w.status, 0, sizeof(int), s);
-    if (folded && !umma && path == GnnLayerPath::UmmaRequired) cudaMemsetAsync(w.status, 0x7f, sizeof(int), s);
-    k_gnn_scales<T><<<reduce_grid(g.n), MCB_THREADS, 0, s>>>(g.n, in, w.partials, w.counter, w.scales);
-    k_gnn_encode<T><<<nb, GNN_TILE, 0, s>>>(g, in, p, w.scales, w.h[0]);
+    if (parts & GNN_FWD_BEGIN) {
+        cudaMemsetAsync(w.status, 0, sizeof(int), s);
+        if (folded && !umma && path == GnnLayerPath::UmmaRequired) cudaMemsetAsync(w.status, 0x7f, sizeof(int), s);
+        k_gnn_scales<T><<<reduce_grid(g.n), MCB_THREADS, 0, s>>>(g.n, in, w.partials, w.counter, w.scales);
+        k_gnn_encode<T><<<nb, GNN_TILE, 0, s>>>(g, in, p, w.scales, w.h[0]);
+        if (folded) k_gnn_fold<<<(GNN_L * 7 * GNN_H * GNN_H + 255) / 256, 256, 0, s>>>(p, g, w.fold);
+    }
     if (folded) {
-        k_gnn_fold<<<(GNN_L * 7 * GNN_H * GNN_H + 255) / 256, 256, 0, s>>>(p, g, w.fold);
         cudaFuncSetAttribute(k_gnn_layer_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FOLD_SMEM);
     } else {
         cudaFuncSetAttribute(k_gnn_layer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LAYER_SMEM);
         cudaFuncSetAttribute(k_gnn_layer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LAYER_SMEM);
     }
-    for (int l = 0; l < GNN_L; l++) {
+    for (int l = 0; (parts & GNN_FWD_LAYERS) && l < GNN_L; l++) {
         const float *pl = p + GP_LAYER0 + l * GPL_SIZE;
         const bf16 *pkl = pk + GK_LAYER0 + l * GKL_SIZE;
         if (train)
@@ -1218,6 +1220,7 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
         } else
             k_gnn_layer<false><<<nb, LAYER_THREADS, LAYER_SMEM, s>>>(g, pl, pkl, w.h[l & 1], w.h[(l + 1) & 1], nullptr);
     }
+    if (!(parts & GNN_FWD_END)) return;
     const bf16 *hl = train ? w.h[GNN_L] : w.h[GNN_L & 1];
     const int gd = std::min(nb, 16 * sm_count());  // the decoder loops over tiles
     if (train)
@@ -1229,14 +1232,14 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
 
 template <typename T>
 void gnn_forward(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &in, const float *p, const bf16 *pk, GnnWork &w,
-                 double *x0)
+                 double *x0, int parts)
 {
-    forward_impl<T>(s, g, in, p, pk, w, x0, false);
+    forward_impl<T>(s, g, in, p, pk, w, x0, false, parts);
 }
 template void gnn_forward<double>(cudaStream_t, const GnnGraph &, const GnnInput<double> &, const float *,
-                                  const bf16 *, GnnWork &, double *);
+                                  const bf16 *, GnnWork &, double *, int);
 template void gnn_forward<float>(cudaStream_t, const GnnGraph &, const GnnInput<float> &, const float *, const bf16 *,
-                                 GnnWork &, double *);
+                                 GnnWork &, double *, int);
 
 int gnn_forward_launches() { return 4 + GNN_L; }
 

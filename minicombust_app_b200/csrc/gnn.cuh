@@ -133,9 +133,13 @@ void gnn_pack(cudaStream_t s, const float *p, __nv_bfloat16 *pk);
 // offset form the per-direction gates are folded into the first weight
 // matrix, [W1h | W1m diag(g_1) | ... | W1m diag(g_6)], so that each layer is
 // one tensor-core product over the seven staged row tiles.
+// `parts` selects the launches (for timing them apart): the scales and the
+// encoder (GNN_FWD_BEGIN), the GNN_L layers (GNN_FWD_LAYERS), the decoder
+// (GNN_FWD_END); called in that order on one stream.
+enum { GNN_FWD_BEGIN = 1, GNN_FWD_LAYERS = 2, GNN_FWD_END = 4, GNN_FWD_ALL = 7 };
 template <typename T>
 void gnn_forward(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &in, const float *p, const __nv_bfloat16 *pk,
-                 GnnWork &w, double *x0);
+                 GnnWork &w, double *x0, int parts = GNN_FWD_ALL);
 int gnn_forward_launches();
 
 // Layer kernel of the offset form: the tcgen05 kernel (default), the same

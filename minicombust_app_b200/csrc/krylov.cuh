@@ -79,10 +79,12 @@ inline DirCodes by_direction_sym(DirCodes dc)
 }
 
 // Value of slot k of row i (its column ck from row_cols / with_row_cols).
+// Only FP64 copies come in the half form (the FP32 kernels compile without
+// it: the extra path cost them registers and time).
 template <typename T>
 __device__ __forceinline__ T ell_val(const DirCodes &dc, const T *__restrict__ off, int N, int i, int k, int ck)
 {
-    if (!dc.sym) return off[(size_t)k * N + i];
+    if (sizeof(T) == sizeof(float) || !dc.sym) return off[(size_t)k * N + i];
     const size_t j = (size_t)(k >> 1) * N;
     if (k & 1) return off[j + i];
     return (i + dc.doff[k] >= 0) ? off[j + ck] : (T)0;
