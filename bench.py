@@ -450,7 +450,8 @@ def roofline_of(solver, mesh, N):
             continue
         work = working_launches(name, st, cnt)
         avg_s = ms / work / 1e3
-        per_kernel[name] = {"ms": round(ms, 4), "launches": cnt, "working_launches": work,
+        launches = cnt * KERNELS_PER_GROUP.get(name, 1)
+        per_kernel[name] = {"ms": round(ms, 4), "launches": launches, "working_launches": work,
                             "bytes_per_launch": b, "avg_launch_us": round(avg_s * 1e6, 2),
                             "achieved_gbs": round(b / avg_s / 1e9, 1), "frac": round(b / avg_s / 1e9 / peak, 3),
                             "share_of_step": round(ms / total, 4)}
