@@ -1080,11 +1080,15 @@ void bicg_init_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, 
 {
     k_bicg_init<T, R><<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, v, rtol, max_iters);
 }
-// FP32 systems run the first product and the update in the split form (one
-// block range per right-hand side; with one right-hand side the split form
-// is the fused one with the register cap of full occupancy).
+// The first product and the update run in the split form (one block range
+// per right-hand side; with one right-hand side the split form is the fused
+// one with the register cap of full occupancy): 32 registers, 8 blocks of
+// 256 per SM.  The update is a streaming kernel that the 70-register fused
+// FP64 form held to 3 blocks per SM and 31 % of the DRAM bandwidth (same-box
+// A/B at 2 x 128^3, plain pass: update 2.36 -> 1.42 ms, first product 2.77
+// -> 2.65 ms).
 template <typename T, int R>
-constexpr bool bicg_split() { return sizeof(T) == 4; }
+constexpr bool bicg_split() { return true; }
 
 template <typename T, int R>
 void bicg_1_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int pin)
@@ -1094,12 +1098,12 @@ void bicg_1_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int
                v.p[pin ^ 1], v.v[pin ^ 1]);
 }
 // The second product gathers two vectors per right-hand side: one pass over
-// the matrix for all of them is faster than the split form here (which FP32
-// uses with one right-hand side, for its occupancy).
+// the matrix for all of them is faster than the split form here (which a
+// single right-hand side uses, for its occupancy).
 template <typename T, int R>
 void bicg_2_t(cudaStream_t s, const EllT<T> &A, const BicgVectorsT<T, R> &v, int vnew)
 {
-    constexpr bool S = sizeof(T) == 4 && R == 1;
+    constexpr bool S = R == 1;
     pdl_launch(k_bicg_2<T, R, S>, krylov_grid(A.N), MCB_THREADS, 0, s, A, v, v.v[vnew]);
 }
 template <typename T, int R>
