@@ -242,7 +242,8 @@ def test_fp32_refined_pressure_solver_matches_oracle(gpu, dims, line_steps):
     for p in range(5):
         solver.simple_iteration()
         assert orc.step() == 0
-        assert solver.last_stats.pressure_rel_residual <= 1e-12
+        # every solve that did work, relative to the first corrector's right-hand side
+        assert 0.0 < solver.last_stats.pressure_rel_residual <= 1e-12
     for name in FIELDS:
         err = rel_err(solver.field(name), orc.field(name))
         assert err <= PARITY, (name, err)
