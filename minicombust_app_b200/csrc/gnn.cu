@@ -713,6 +713,19 @@ __global__ void __launch_bounds__(GNN_TILE) k_gnn_decode(GnnGraph g, const float
     }
 }
 
+// After the tcgen05 layers, whose last one writes the prediction: a pipeline
+// wait that ran out (status set) leaves tiles unwritten, so the prediction
+// is zero then, as k_gnn_decode writes it.
+__global__ void __launch_bounds__(MCB_THREADS) k_gnn_zero_on_fail(int n, const int *__restrict__ status,
+                                                                  float *__restrict__ y, double *__restrict__ x0)
+{
+    if (*status == 0) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        y[i] = 0.f;
+        if (x0) x0[i] = 0.0;
+    }
+}
+
 // ---------------------------------------------------------------- training
 
 // Mean of (y - t / s_x) over the cells.
@@ -1205,6 +1218,8 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
         cudaFuncSetAttribute(k_gnn_layer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LAYER_SMEM);
         cudaFuncSetAttribute(k_gnn_layer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LAYER_SMEM);
     }
+    // the tcgen05 path runs the decoder inside the last layer
+    const GnnUmmaDecode dec{pk + GK_WD, p + GP_DEC, w.scales, w.y, x0};
     for (int l = 0; (parts & GNN_FWD_LAYERS) && l < GNN_L; l++) {
         const float *pl = p + GP_LAYER0 + l * GPL_SIZE;
         const bf16 *pkl = pk + GK_LAYER0 + l * GKL_SIZE;
@@ -1213,7 +1228,8 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
         else if (folded) {
             const bf16 *wf = w.fold + (size_t)l * 7 * GNN_H * GNN_H;
             if (umma)
-                gnn_layer_umma(s, g, maps[l & 1], pl, wf, pkl, w.h[l & 1], w.h[(l + 1) & 1], w.status, sm_count());
+                gnn_layer_umma(s, g, maps[l & 1], pl, wf, pkl, w.h[l & 1], w.h[(l + 1) & 1], w.status, sm_count(),
+                               l == GNN_L - 1 ? &dec : nullptr);
             else
                 k_gnn_layer_fold<<<std::min(nb, sm_count()), LAYER_THREADS, FOLD_SMEM, s>>>(
                     g, pl, wf, pkl, w.h[l & 1], w.h[(l + 1) & 1], nb);
@@ -1221,6 +1237,10 @@ static void forward_impl(cudaStream_t s, const GnnGraph &g, const GnnInput<T> &i
             k_gnn_layer<false><<<nb, LAYER_THREADS, LAYER_SMEM, s>>>(g, pl, pkl, w.h[l & 1], w.h[(l + 1) & 1], nullptr);
     }
     if (!(parts & GNN_FWD_END)) return;
+    if (umma) {
+        k_gnn_zero_on_fail<<<reduce_grid(g.n), MCB_THREADS, 0, s>>>(g.n, w.status, w.y, x0);
+        return;
+    }
     const bf16 *hl = train ? w.h[GNN_L] : w.h[GNN_L & 1];
     const int gd = std::min(nb, 16 * sm_count());  // the decoder loops over tiles
     if (train)

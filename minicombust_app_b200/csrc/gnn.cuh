@@ -156,11 +156,20 @@ struct alignas(64) GnnTmaMap {
 bool gnn_umma_map(GnnTmaMap *m, const __nv_bfloat16 *h, int n);
 // Launch attributes of the layer kernel (false: the kernel cannot run).
 bool gnn_umma_ready();
+// The decoder fused into the last layer: y = wo . relu(Wd h' + cd) + co and
+// x0 = s_x y (x0 may be null) instead of storing h'.
+struct GnnUmmaDecode {
+    const __nv_bfloat16 *pkd;  // Wd, BF16 [32][32]
+    const float *pd;           // the decoder's FP32 parameters
+    const GnnScales *scales;
+    float *y;
+    double *x0;
+};
 // One offset-form layer on the tcgen05 tensor cores, `grid` persistent
-// blocks, hin (described by `map`) -> hout.
+// blocks, hin (described by `map`) -> hout, or with dec the network's output.
 void gnn_layer_umma(cudaStream_t s, const GnnGraph &g, const GnnTmaMap &map, const float *pl,
                     const __nv_bfloat16 *wf, const __nv_bfloat16 *pkl, const __nv_bfloat16 *hin,
-                    __nv_bfloat16 *hout, int *status, int grid);
+                    __nv_bfloat16 *hout, int *status, int grid, const GnnUmmaDecode *dec = nullptr);
 
 // Training: forward, loss against `target` (units of the solution), backward;
 // adds this sample's gradient, scaled by `weight`, into grad[NPARAM] and

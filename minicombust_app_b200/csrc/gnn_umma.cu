@@ -58,17 +58,22 @@ constexpr int UM_B2 = GNN_H * GNN_H * 2;            // 2048 B
 constexpr int UM_A1 = GNN_TILE * GNN_H * 2;         // 8192 B per epilogue group
 constexpr int UM_GROUPS = 3;  // one copy stage per group
 constexpr int UM_THREADS = 128 * UM_GROUPS + 64 + 128;
-constexpr uint32_t UM_TMEM_COLS = 256;  // >= 64 per group (D1 and D2, 32 columns each), a power of two
+// TMEM columns of a group: D1 and D2 (and for the last layer D3 of the
+// decoder), 32 columns each, at 128-column group strides; a power of two
+constexpr uint32_t UM_TMEM_COLS = 512;
+constexpr uint32_t UM_GROUP_COLS = 128;
 constexpr int WARP_TMA = 4 * UM_GROUPS, WARP_MMA = 4 * UM_GROUPS + 1, WARP_MASK = 4 * UM_GROUPS + 2;
 
 constexpr int OFF_STAGE = 0;
 constexpr int OFF_B1 = OFF_STAGE + UM_STAGES * UM_STAGE;
 constexpr int OFF_B2 = OFF_B1 + UM_B1;
-constexpr int OFF_A1 = OFF_B2 + UM_B2;
-constexpr int OFF_BIAS = OFF_A1 + UM_GROUPS * UM_A1;
-constexpr int OFF_BAR = OFF_BIAS + 2 * GNN_H * 4;
-// barriers: full[3], masked[3], empty[3], d1full[3], a1full[3], d2full[3], d1free[3], fin
-constexpr int NBAR = 3 * UM_STAGES + 4 * UM_GROUPS + 1;
+constexpr int OFF_B3 = OFF_B2 + UM_B2;                // the decoder's Wd (last layer)
+constexpr int OFF_A1 = OFF_B3 + UM_B2;
+constexpr int OFF_BIAS = OFF_A1 + UM_GROUPS * UM_A1;  // c1, c2, cd, wo
+constexpr int OFF_BAR = OFF_BIAS + 4 * GNN_H * 4;
+// barriers: full[3], masked[3], empty[3], d1full[3], a1full[3], d2full[3],
+// d1free[3], hfull[3], d3full[3], fin
+constexpr int NBAR = 3 * UM_STAGES + 6 * UM_GROUPS + 1;
 constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
 constexpr int UM_SMEM_USED = OFF_MISC + 16;
 constexpr int UM_SMEM = UM_SMEM_USED + 1024;        // slack for the 1024-byte alignment of the base
@@ -77,7 +82,7 @@ constexpr uint32_t WAIT_LIMIT = 1u << 22;
 constexpr unsigned FULL = 0xffffffffu;
 
 static_assert(UM_SMEM <= 227 * 1024, "shared memory of the tensor-core layer");
-static_assert(UM_STAGES == UM_GROUPS && 64 * UM_GROUPS <= (int)UM_TMEM_COLS, "stage and TMEM set per group");
+static_assert(UM_STAGES == UM_GROUPS && UM_GROUP_COLS * UM_GROUPS <= UM_TMEM_COLS, "stage and TMEM set per group");
 static_assert(OFF_B1 % 1024 == 0 && OFF_A1 % 1024 == 0, "operand alignment");
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
@@ -109,13 +114,27 @@ struct UmmaBars {
     __device__ uint32_t a1full(int g) const { return base + 8 * (3 * UM_STAGES + UM_GROUPS + g); }
     __device__ uint32_t d2full(int g) const { return base + 8 * (3 * UM_STAGES + 2 * UM_GROUPS + g); }
     __device__ uint32_t d1free(int g) const { return base + 8 * (3 * UM_STAGES + 3 * UM_GROUPS + g); }
-    __device__ uint32_t fin() const { return base + 8 * (3 * UM_STAGES + 4 * UM_GROUPS); }
+    __device__ uint32_t hfull(int g) const { return base + 8 * (3 * UM_STAGES + 4 * UM_GROUPS + g); }
+    __device__ uint32_t d3full(int g) const { return base + 8 * (3 * UM_STAGES + 5 * UM_GROUPS + g); }
+    __device__ uint32_t fin() const { return base + 8 * (3 * UM_STAGES + 6 * UM_GROUPS); }
 };
 
+// The decoder fused into the last layer (LAST): y = wo . relu(Wd h' + cd) + co
+// and x0 = s_x y, with D3 = h' Wd^T a third product per tile (h' in BF16, as
+// the layer stores it for k_gnn_decode).
+struct UmmaDecode {
+    const bf16 *pkd;     // Wd, BF16 [32][32]
+    const float *pd;     // the decoder's FP32 parameters (cd, wo, co)
+    const GnnScales *scales;
+    float *y;
+    double *x0;          // may be null
+};
+
+template <bool LAST>
 __global__ void __launch_bounds__(UM_THREADS, 1)
     k_gnn_layer_umma(const __grid_constant__ CUtensorMap tmap, GnnGraph g, const float *__restrict__ pl,
                      const bf16 *__restrict__ wf, const bf16 *__restrict__ pkl, const bf16 *__restrict__ hin,
-                     bf16 *__restrict__ hout, int ntiles, int *status, uint32_t wait_polls)
+                     bf16 *__restrict__ hout, int ntiles, int *status, uint32_t wait_polls, UmmaDecode dec)
 {
     extern __shared__ unsigned char smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
@@ -123,6 +142,8 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
     unsigned char *sgen = smem_raw + (sbase - raw);
     float *sC1 = reinterpret_cast<float *>(sgen + OFF_BIAS);
     float *sC2 = sC1 + GNN_H;
+    float *sCD = sC2 + GNN_H;
+    float *sWO = sCD + GNN_H;
     volatile int *abort_flag = reinterpret_cast<volatile int *>(sgen + OFF_MISC);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sgen + OFF_MISC + 4);
     const UmmaBars bars{sbase + OFF_BAR};
@@ -139,6 +160,8 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
             mbar_init(bars.a1full(q), 128);
             mbar_init(bars.d2full(q), 1);
             mbar_init(bars.d1free(q), 128);
+            mbar_init(bars.hfull(q), 128);
+            mbar_init(bars.d3full(q), 1);
         }
         mbar_init(bars.fin(), 1);
         *abort_flag = 0;
@@ -151,16 +174,23 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
     // B operands, K-major without swizzle: element (n, k) at
     // (k / 8) * 512 + n * 16 + (k % 8) * 2 -- core matrices of 8 rows x 16 B,
     // 8-row groups 128 B apart, K groups 512 B apart.
-    for (int e = tid; e < 8 * GNN_H * 4; e += UM_THREADS) {
+    for (int e = tid; e < (LAST ? 9 : 8) * GNN_H * 4; e += UM_THREADS) {
         const int slot = e >> 7, rem = e & 127, n = rem >> 2, c = rem & 3;
-        const uint4 v = slot < 7 ? *reinterpret_cast<const uint4 *>(wf + ((size_t)slot * GNN_H + n) * GNN_H + c * 8)
-                                 : *reinterpret_cast<const uint4 *>(pkl + GKL_W2 + n * GNN_H + c * 8);
-        const uint32_t dst = slot < 7 ? sbase + OFF_B1 + (slot * 4 + c) * 512 + n * 16 : sbase + OFF_B2 + c * 512 + n * 16;
+        const uint4 v = slot < 7  ? *reinterpret_cast<const uint4 *>(wf + ((size_t)slot * GNN_H + n) * GNN_H + c * 8)
+                        : slot == 7 ? *reinterpret_cast<const uint4 *>(pkl + GKL_W2 + n * GNN_H + c * 8)
+                                    : *reinterpret_cast<const uint4 *>(dec.pkd + n * GNN_H + c * 8);
+        const uint32_t dst = slot < 7  ? sbase + OFF_B1 + (slot * 4 + c) * 512 + n * 16
+                             : slot == 7 ? sbase + OFF_B2 + c * 512 + n * 16
+                                         : sbase + OFF_B3 + c * 512 + n * 16;
         st_shared_v4(dst, v.x, v.y, v.z, v.w);
     }
     if (tid < GNN_H) {
         sC1[tid] = pl[GPL_C1 + tid];
         sC2[tid] = pl[GPL_C2 + tid];
+        if (LAST) {
+            sCD[tid] = dec.pd[GPD_CD + tid];
+            sWO[tid] = dec.pd[GPD_WO + tid];
+        }
     }
     fence_proxy_async_smem();
     tc_fence_before();
@@ -206,9 +236,9 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
         if (lane == 0) {
             constexpr uint32_t idesc = idesc_bf16_f32(GNN_TILE, GNN_H);
             const int nj = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
-            int j1 = 0, j2 = 0;  // next tile of the first / second product
+            int j1 = 0, j2 = 0, j3 = 0;  // next tile of the first / second / decoder product
             uint32_t idle = 0;
-            while (j2 < nj) {
+            while (LAST ? j3 < nj : j2 < nj) {
                 bool progressed = false;
                 if (j1 < nj && mbar_test_wait(bars.masked(j1 % UM_STAGES), (j1 / UM_STAGES) & 1) &&
                     (j1 < UM_GROUPS || mbar_test_wait(bars.d1free(j1 % UM_GROUPS), ((j1 / UM_GROUPS) - 1) & 1))) {
@@ -220,7 +250,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
                         const uint64_t ad = smem_desc(a0 + (ks >> 1) * UM_SLICE + (ks & 1) * 32, 16, 512,
                                                       DESC_SWIZZLE_64B);
                         const uint64_t bd = smem_desc(sbase + OFF_B1 + ks * 1024, 512, 128, DESC_SWIZZLE_NONE);
-                        umma_f16(tmem + q * 64, ad, bd, idesc, ks > 0);
+                        umma_f16(tmem + q * UM_GROUP_COLS, ad, bd, idesc, ks > 0);
                     }
                     umma_commit(bars.empty(s));
                     umma_commit(bars.d1full(q));
@@ -234,10 +264,23 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
                     for (int ks = 0; ks < 2; ks++) {
                         const uint64_t ad = smem_desc(sbase + OFF_A1 + q * UM_A1 + ks * 4096, 2048, 128, DESC_SWIZZLE_NONE);
                         const uint64_t bd = smem_desc(sbase + OFF_B2 + ks * 1024, 512, 128, DESC_SWIZZLE_NONE);
-                        umma_f16(tmem + q * 64 + 32, ad, bd, idesc, ks > 0);
+                        umma_f16(tmem + q * UM_GROUP_COLS + 32, ad, bd, idesc, ks > 0);
                     }
                     umma_commit(bars.d2full(q));
                     j2++;
+                    progressed = true;
+                }
+                if (LAST && j3 < j2 && mbar_test_wait(bars.hfull(j3 % UM_GROUPS), (j3 / UM_GROUPS) & 1)) {
+                    tc_fence_after();
+                    const int q = j3 % UM_GROUPS;
+#pragma unroll
+                    for (int ks = 0; ks < 2; ks++) {  // h' of the tile, in the group's a-tile
+                        const uint64_t ad = smem_desc(sbase + OFF_A1 + q * UM_A1 + ks * 4096, 2048, 128, DESC_SWIZZLE_NONE);
+                        const uint64_t bd = smem_desc(sbase + OFF_B3 + ks * 1024, 512, 128, DESC_SWIZZLE_NONE);
+                        umma_f16(tmem + q * UM_GROUP_COLS + 64, ad, bd, idesc, ks > 0);
+                    }
+                    umma_commit(bars.d3full(q));
+                    j3++;
                     progressed = true;
                 }
                 if (progressed) {
@@ -300,7 +343,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
             }
             tc_fence_after();
             uint32_t v[32];
-            tmem_ld32(tmem + q * 64 + lane_base, v);
+            tmem_ld32(tmem + q * UM_GROUP_COLS + lane_base, v);
             tc_fence_before();
             mbar_arrive(bars.d1free(q));
 #pragma unroll
@@ -325,22 +368,56 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
                 break;
             }
             tc_fence_after();
-            tmem_ld32(tmem + q * 64 + 32 + lane_base, v);
+            tmem_ld32(tmem + q * UM_GROUP_COLS + 32 + lane_base, v);
             tc_fence_before();
-            if (in) {
+            uint32_t o[4][4];
 #pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    const uint32_t hw[4] = {hv[c].x, hv[c].y, hv[c].z, hv[c].w};
-                    uint32_t o[4];
+            for (int c = 0; c < 4; c++) {
+                const uint32_t hw[4] = {hv[c].x, hv[c].y, hv[c].z, hv[c].w};
 #pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const int col = 8 * c + 2 * e;
-                        const float2 h2 = unpack_bf16(hw[e]);
-                        o[e] = pack_bf16(h2.x + (__uint_as_float(v[col]) + sC2[col]),
-                                         h2.y + (__uint_as_float(v[col + 1]) + sC2[col + 1]));
-                    }
-                    *reinterpret_cast<uint4 *>(hout + (size_t)i * GNN_H + c * 8) = make_uint4(o[0], o[1], o[2], o[3]);
+                for (int e = 0; e < 4; e++) {
+                    const int col = 8 * c + 2 * e;
+                    const float2 h2 = unpack_bf16(hw[e]);
+                    o[c][e] = pack_bf16(h2.x + (__uint_as_float(v[col]) + sC2[col]),
+                                        h2.y + (__uint_as_float(v[col + 1]) + sC2[col + 1]));
                 }
+            }
+            if (!LAST) {
+                if (in) {
+#pragma unroll
+                    for (int c = 0; c < 4; c++)
+                        *reinterpret_cast<uint4 *>(hout + (size_t)i * GNN_H + c * 8) =
+                            make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
+                }
+                continue;
+            }
+            // the decoder: h' (rows outside the mesh are zeros) into the
+            // group's a-tile, whose second product has completed
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                st_shared_v4(a1 + c * 2048, in ? o[c][0] : 0u, in ? o[c][1] : 0u, in ? o[c][2] : 0u, in ? o[c][3] : 0u);
+            fence_proxy_async_smem();
+            tc_fence_before();
+            mbar_arrive(bars.hfull(q));
+            ok = mbar_wait(bars.d3full(q), (j / UM_GROUPS) & 1, abort_flag, wait_polls);
+            if (!__all_sync(FULL, ok)) {
+                fail(9);
+                break;
+            }
+            tc_fence_after();
+            tmem_ld32(tmem + q * UM_GROUP_COLS + 64 + lane_base, v);
+            tc_fence_before();
+            float ys = 0.f;
+#pragma unroll
+            for (int col = 0; col < GNN_H; col += 2) {  // q = relu(Wd h' + cd), rounded to BF16 as stored
+                const float2 qr = unpack_bf16(pack_bf16(fmaxf(__uint_as_float(v[col]) + sCD[col], 0.f),
+                                                        fmaxf(__uint_as_float(v[col + 1]) + sCD[col + 1], 0.f)));
+                ys += sWO[col] * qr.x + sWO[col + 1] * qr.y;
+            }
+            if (in) {
+                const float yi = ys + dec.pd[GPD_CO];
+                dec.y[i] = yi;
+                if (dec.x0) dec.x0[i] = dec.scales->sx * (double)yi;
             }
         }
     }
@@ -419,21 +496,30 @@ bool gnn_umma_ready()
 {
     static int state = 0;  // 0 unknown, 1 ready, -1 failed
     if (state == 0)
-        state = cudaFuncSetAttribute(k_gnn_layer_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, UM_SMEM) ==
-                        cudaSuccess
+        state = (cudaFuncSetAttribute(k_gnn_layer_umma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, UM_SMEM) ==
+                     cudaSuccess &&
+                 cudaFuncSetAttribute(k_gnn_layer_umma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, UM_SMEM) ==
+                     cudaSuccess)
                     ? 1
                     : -1;
     return state > 0;
 }
 
 void gnn_layer_umma(cudaStream_t s, const GnnGraph &g, const GnnTmaMap &map, const float *pl, const bf16 *wf,
-                    const bf16 *pkl, const bf16 *hin, bf16 *hout, int *status, int grid)
+                    const bf16 *pkl, const bf16 *hin, bf16 *hout, int *status, int grid, const GnnUmmaDecode *dec)
 {
     CUtensorMap t;
     std::memcpy(&t, map.raw, sizeof(t));
     const int ntiles = (g.n + GNN_TILE - 1) / GNN_TILE;
-    k_gnn_layer_umma<<<std::max(1, std::min(grid, ntiles)), UM_THREADS, UM_SMEM, s>>>(t, g, pl, wf, pkl, hin, hout,
-                                                                                       ntiles, status, wait_polls());
+    const int blocks = std::max(1, std::min(grid, ntiles));
+    if (dec) {
+        const UmmaDecode d{dec->pkd, dec->pd, dec->scales, dec->y, dec->x0};
+        k_gnn_layer_umma<true><<<blocks, UM_THREADS, UM_SMEM, s>>>(t, g, pl, wf, pkl, hin, hout, ntiles, status,
+                                                                  wait_polls(), d);
+    } else {
+        k_gnn_layer_umma<false><<<blocks, UM_THREADS, UM_SMEM, s>>>(t, g, pl, wf, pkl, hin, hout, ntiles, status,
+                                                                   wait_polls(), UmmaDecode{});
+    }
 }
 
 } // namespace mcb
