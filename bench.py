@@ -147,10 +147,10 @@ class ClockSampler:
 
 def kernel_bytes(name, N, F, nnz_off):
     """Algorithmic (unique-touch) bytes of one launch: each stored input
-    element read once, each output written once, at its stored type.  The
-    FP64 momentum and temperature solver kernels read a 4-byte direction code
-    per row instead of the six int32 columns (structured box); the FP32
-    copies are stored by direction and read no column data.  The pressure
+    element read once, each output written once, at its stored type.  On a
+    structured box the FP64 momentum and temperature rows and the FP32
+    copies are stored by direction and the solver kernels read no column
+    data (the assembly reads a 4-byte direction code per row).  The pressure
     solvers' FP64 copy is stored by direction in the half form of a
     symmetric matrix: the diagonal and the +x, +y, +z couplings, the others
     read as the neighbours' (counted once).  ELL values include the boundary
@@ -159,8 +159,8 @@ def kernel_bytes(name, N, F, nnz_off):
         "pcg_iter1_spmv": 64 * N,      # diag, 3 off, (z, p) pair -> p, q
         "pcg32_iter1_spmv": 44 * N,    # FP32: diag, 6 off by direction, (z, p) pair -> p, q
         "pcg_iter2_update": 64 * N,    # x rw, r rw, p, q, diag -> z (Jacobi path)
-        "bicg3_1_spmv": 204 * N,       # matrix 60 + 3 x (r, p, v gathered; r0; p, v out)
-        "bicg3_2_spmv": 156 * N,       # matrix 60 + 3 x (r, v gathered; s, t out)
+        "bicg3_1_spmv": 200 * N,       # matrix 56 + 3 x (r, p, v gathered; r0; p, v out)
+        "bicg3_2_spmv": 152 * N,       # matrix 56 + 3 x (r, v gathered; s, t out)
         "bicg3_3_update": 168 * N,     # 3 x (s, p, t, r0, x rw, r out)
         "bicg3_32_1_spmv": 100 * N,    # FP32: matrix 28 + 3 x 24
         "bicg3_32_2_spmv": 76 * N,     # FP32: matrix 28 + 3 x 16
@@ -177,10 +177,16 @@ def kernel_bytes(name, N, F, nnz_off):
         # level 2 and below 9
         "amg_vcycle": 453 * N,
         "lsq_gradients_uvwpt": 208 * N,
-        "momentum_assemble": 56 * F + 296 * N,
+        # a cell's faces: face index, other cell (col) and owner bits per
+        # cell instead of each face's two cell indices
+        "momentum_assemble": 48 * F + 325 * N,
         "mass_flux": 88 * F + 176 * N,
-        "pressure_rows": 24 * F + 120 * N,
-        "temperature_assemble": 40 * F + 168 * N,
+        # faces: mdot, ff0, ff1; cells: face index, other cell, owner bits,
+        # code -> b, diag, six values, the FP64 copy in the half form (the
+        # FP32 level 0 the refined configuration also writes, 28 N, is not
+        # counted)
+        "pressure_rows": 24 * F + 141 * N,
+        "temperature_assemble": 40 * F + 172 * N,
     }.get(name)
 
 

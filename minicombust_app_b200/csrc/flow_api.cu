@@ -94,6 +94,12 @@ struct mc_flow {
     std::vector<int> hcol;   // ELL columns with -1 on boundary slots (CSR export)
     uint32_t *dcode = nullptr;  // direction codes of the ELL columns (used when dc.code is set)
     DirCodes dc;
+    // FP64 momentum, temperature and scalar rows stored by direction
+    // (rows.code set; see RowStore) and the codes the solvers read them with;
+    // hcode: the direction codes on the host (CSR export)
+    RowStore rows;
+    DirCodes dc_rows;
+    std::vector<uint32_t> hcode;
     // the solvers' copy of the pressure-correction matrix stored by direction
     // (DirCodes::dia; with dc_pdir.sym in the half form of a symmetric
     // matrix), written with the slot-order rows; null: the solvers read those
@@ -107,6 +113,7 @@ struct mc_flow {
 
     // mesh
     int *fc0, *fc1, *nbr, *sface, *col, *outlet_faces;
+    uint8_t *sown;  // [N] bit k: the cell is cell0 of its slot-k face
     double *area, *lam, *rl, *Sx, *Sy, *Sz, *xf, *yf, *zf, *xc, *yc, *zc, *vol, *rho;
     // fields and gradients (G_U..G_T x 3 components)
     double *phi[G_NFIELDS];
@@ -332,13 +339,13 @@ double *grad_ptr(mc_flow *h, int field, int d)
     return (h->has_scalars && is_scalar_field(field) && field != MC_FIELD_TP) ? h->sgrad[field][d] : nullptr;
 }
 
-Ell momentum_matrix(mc_flow *h) { return Ell{h->N, h->AU, h->off_m, h->col, h->dc}; }
+Ell momentum_matrix(mc_flow *h) { return Ell{h->N, h->AU, h->off_m, h->col, h->rows.code ? h->dc_rows : h->dc}; }
 Ell pressure_matrix(mc_flow *h)
 {
     if (h->p_dir64) return Ell{h->N, h->diag_p, h->p_dir64, h->col, h->dc_pdir};
     return Ell{h->N, h->diag_p, h->off_p, h->col, h->dc};
 }
-Ell temperature_matrix(mc_flow *h) { return Ell{h->N, h->diag_t, h->off_t, h->col, h->dc}; }
+Ell temperature_matrix(mc_flow *h) { return Ell{h->N, h->diag_t, h->off_t, h->col, h->rows.code ? h->dc_rows : h->dc}; }
 
 // ------------------------------------------------------------ Krylov drivers
 
@@ -1044,6 +1051,7 @@ int stage_momentum(mc_flow *h, mc_iter_stats *st)
     a.mdot = h->mdot;
     a.src = h->sources_set ? h->src : nullptr;
     a.off = h->off_m;
+    a.store = h->rows;
     a.AU = h->AU;
     a.b = h->b_m;
     const bool fused32 = h->bir_mem && h->dc.code;  // the FP32 copy written by the assembly itself
@@ -1198,6 +1206,7 @@ int stage_temperature(mc_flow *h, mc_iter_stats *st)
     a.mdot = h->mdot;
     a.src = h->sources_set ? h->src : nullptr;
     a.off = h->off_t;
+    a.store = h->rows;
     a.diag = h->diag_t;
     a.b = h->b_t;
     a.imbalance = h->scalars + 1;
@@ -1250,6 +1259,7 @@ int stage_scalar(mc_flow *h, int field, mc_iter_stats *st)
     a.mdot = h->mdot;
     a.src = nullptr;
     a.off = h->off_t;
+    a.store = h->rows;
     a.diag = h->diag_t;
     a.b = h->b_t;
     TurbArgs t{};
@@ -1317,6 +1327,7 @@ int allocate(mc_flow *h)
     auto add = [&](void *pp, size_t bytes) { items.push_back({(void **)pp, bytes}); };
     add(&h->fc0, F * 4); add(&h->fc1, F * 4);
     add(&h->nbr, 6 * N * 4); add(&h->sface, 6 * N * 4); add(&h->col, 6 * N * 4);
+    add(&h->sown, N);
     add(&h->outlet_faces, std::max<size_t>(1, (size_t)h->margs.n_outlet) * 4);
     for (double **p : {&h->area, &h->lam, &h->rl, &h->Sx, &h->Sy, &h->Sz, &h->xf, &h->yf, &h->zf}) add(p, F * 8);
     for (double **p : {&h->xc, &h->yc, &h->zc, &h->vol, &h->rho}) add(p, N * 8);
@@ -1646,6 +1657,49 @@ bool dir_codes_disabled()
     return v && v[0] == '0';
 }
 
+bool row_store_disabled()
+{
+    const char *v = std::getenv("MC_ROW_STORE");
+    return v && v[0] == '0';
+}
+
+// Positions of the six directions in rows stored by direction (RowStore):
+// an order in which the directions occur in the slots of every row, so that
+// a row summed by position sums its terms in slot order.  False when the
+// rows disagree (no such order).
+bool row_direction_order(const std::vector<uint32_t> &code, uint32_t &pos)
+{
+    bool before[6][6] = {};
+    std::unordered_map<uint32_t, int> seen;
+    for (uint32_t cw : code) {
+        if (seen.count(cw)) continue;
+        seen[cw] = 1;
+        int last[6], n = 0;
+        for (int k = 0; k < 6; k++) {
+            const unsigned d = (cw >> (3 * k)) & 7u;
+            if (d < 6) last[n++] = (int)d;
+        }
+        for (int a = 0; a < n; a++)
+            for (int b = a + 1; b < n; b++) before[last[a]][last[b]] = true;
+    }
+    bool placed[6] = {};
+    pos = 0;
+    for (int q = 0; q < 6; q++) {  // Kahn's order, ties by direction index
+        int pick = -1;
+        for (int d = 0; d < 6 && pick < 0; d++) {
+            if (placed[d]) continue;
+            bool free = true;
+            for (int e = 0; e < 6; e++)
+                if (!placed[e] && e != d && before[e][d]) free = false;
+            if (free) pick = d;
+        }
+        if (pick < 0) return false;  // a cycle: the rows disagree
+        placed[pick] = true;
+        pos |= (uint32_t)q << (3 * pick);
+    }
+    return true;
+}
+
 // Direction codes of the ELL columns (DirCodes): slot k of row i holds the
 // direction d with nbr[d][i] == col[k][i] (7: unused slot).  Returns false
 // when some direction's neighbour offset is not the same for every row (RCM
@@ -1961,6 +2015,12 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
             rc = rc ? rc : upload(h, h->nbr, hm.nbr.data(), 6 * N);
             rc = rc ? rc : upload(h, h->sface, hm.sface.data(), 6 * N);
             rc = rc ? rc : upload(h, h->col, hm.col.data(), 6 * N);
+            // kept until the stream synchronisation below
+            std::vector<uint8_t> own(N, 0);
+            for (size_t c = 0; c < N; c++)
+                for (int k = 0; k < 6; k++)
+                    if (hm.fc0[hm.sface[(size_t)k * N + c]] == (int)c) own[c] |= (uint8_t)(1u << k);
+            rc = rc ? rc : upload(h, h->sown, own.data(), N);
             if (!rc && !hm.outlet_faces.empty()) rc = upload(h, h->outlet_faces, hm.outlet_faces.data(), hm.outlet_faces.size());
             rc = rc ? rc : upload(h, h->area, hm.area.data(), F);
             rc = rc ? rc : upload(h, h->lam, hm.lam.data(), F);
@@ -2015,6 +2075,14 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
                         h->dc.coff[k] = d < 6 ? doff[d] : 0;
                     }
                     h->line_ex = x_line_length(code, doff, (int)N);
+                    uint32_t pos = 0;
+                    if (!row_store_disabled() && row_direction_order(code, pos)) {
+                        h->rows.code = h->dcode;
+                        h->rows.pos = pos;
+                        h->dc_rows = by_direction(h->dc);
+                        for (int d = 0; d < 6; d++) h->dc_rows.doff[(pos >> (3 * d)) & 7u] = doff[d];
+                        h->hcode.swap(code);
+                    }
                 }
             }
             const int form = pressure_copy_form();
@@ -2057,7 +2125,7 @@ int mc_flow_create(const mc_mesh_view *mesh, const mc_flow_params *params, mc_fl
             ph.flux_corr = params->flux_corr;
             MeshArgs &m = h->margs;
             m.F = hm.F;
-            m.fc0 = h->fc0; m.fc1 = h->fc1; m.sface = h->sface;
+            m.fc0 = h->fc0; m.fc1 = h->fc1; m.sface = h->sface; m.col = h->col; m.own = h->sown;
             m.area = h->area; m.lam = h->lam; m.rl = h->rl;
             m.Sx = h->Sx; m.Sy = h->Sy; m.Sz = h->Sz;
             m.xf = h->xf; m.yf = h->yf; m.zf = h->zf;
@@ -2746,6 +2814,14 @@ int mc_flow_get_csr(mc_flow *h, int system, int *n, int *nnz, int *row_ptr, int 
     CUDA_TRY(h, cudaMemcpyAsync(off.data(), d_off, 6 * N * 8, cudaMemcpyDeviceToHost, h->stream));
     if (rhs) CUDA_TRY(h, cudaMemcpyAsync(b.data(), d_rhs, N * 8, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (h->rows.code && system != MC_SYSTEM_PRESSURE) {  // rows stored by direction: back to slot order
+        std::vector<double> dir(off);
+        for (size_t i = 0; i < N; i++)
+            for (int k = 0; k < 6; k++) {
+                const unsigned d = (h->hcode[i] >> (3 * k)) & 7u;
+                off[k * N + i] = d < 6 ? dir[(size_t)((h->rows.pos >> (3 * d)) & 7u) * N + i] : 0.0;
+            }
+    }
     size_t pos = 0;
     std::vector<std::pair<int, double>> row;
     // rows and columns in the caller's numbering

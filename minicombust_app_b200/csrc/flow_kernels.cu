@@ -69,6 +69,29 @@ __device__ __forceinline__ void store_fp32_row(const Fp32Rows &f, int N, int c, 
 }
 
 // Row c stored by direction into out (see k_dir_rows64).
+// Off-diagonal values of row c as RowStore says.
+__device__ __forceinline__ void store_row(const RowStore &rs, double *out, int N, int c, const double (&offv)[6])
+{
+    if (!rs.code) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) out[(size_t)k * N + c] = offv[k];
+        return;
+    }
+    const uint32_t cw = rs.code[c];
+    double o[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) o[q] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        const unsigned d = (cw >> (3 * k)) & 7u;
+        const unsigned p = d < 6 ? (rs.pos >> (3 * d)) & 7u : 7u;
+#pragma unroll
+        for (int q = 0; q < 6; q++) o[q] = (p == (unsigned)q) ? offv[k] : o[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) out[(size_t)q * N + c] = o[q];
+}
+
 __device__ __forceinline__ void store_dir_row(const uint32_t cw, const double (&offv)[6], double *out, int N, int c,
                                               int sym)
 {
@@ -231,15 +254,18 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_momentum_assemble(Physics ph
     if (c >= N) return;
     const double xcc = m.xc[c], ycc = m.yc[c], zcc = m.zc[c];
     const double Uc = a.U[c], Vc = a.V[c], Wc = a.W[c];
+    const unsigned own = m.own[c];
     double su = 0.0, sv = 0.0, sw = 0.0, ac = 0.0;
     double offv[6];
     unsigned internal = 0u;
     const double mu = ph.mu;
     for (int k = 0; k < 6; k++) {
         const int face = m.sface[(size_t)k * N + c];
-        const int c0 = m.fc0[face], c1 = m.fc1[face];
+        const int nb = m.col[(size_t)k * N + c];
         const double Sx = m.Sx[face], Sy = m.Sy[face], Sz = m.Sz[face];
-        if (c1 < N) {
+        if (nb != c) {
+            const bool c_is_c0 = (own >> k) & 1u;
+            const int c0 = c_is_c0 ? c : nb, c1 = c_is_c0 ? nb : c;
             internal |= 1u << k;
             const double l0 = m.lam[face];
             const double l1 = 1.0 - l0;
@@ -292,6 +318,7 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_momentum_assemble(Physics ph
             }
         } else {
             offv[k] = 0.0;
+            const int c1 = m.fc1[face];
             const int side = c1 - N;
             const int t = ph.btype[side];
             const double Xx = m.xf[face] - xcc, Xy = m.yf[face] - ycc, Xz = m.zf[face] - zcc;
@@ -389,8 +416,7 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_momentum_assemble(Physics ph
     a.b[(size_t)N + c] = sv + (1.0 - URF) * ac * Vc;
     a.b[2 * (size_t)N + c] = sw + (1.0 - URF) * ac * Wc;
     a.AU[c] = ac;
-#pragma unroll
-    for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
+    store_row(a.store, a.off, N, c, offv);
     if (a.f32.d32) store_fp32_row(a.f32, N, c, ac, offv);
 }
 
@@ -494,8 +520,7 @@ __device__ __forceinline__ double temperature_row(const Physics &ph, const MeshA
     at *= RURF;
     a.b[c] = st + (1.0 - URF) * at * Tc;
     a.diag[c] = at;
-#pragma unroll
-    for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
+    store_row(a.store, a.off, N, c, offv);
     if (a.f32.d32) store_fp32_row(a.f32, N, c, at, offv);
     if (ph.mode == 1 && a.src) div -= a.src[4 * (size_t)N + c];
     return fabs(div);
@@ -700,8 +725,7 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_scalar_assemble(Physics ph, 
     at *= RURF;
     a.b[c] = st + (1.0 - URF) * at * phic;
     a.diag[c] = at;
-#pragma unroll
-    for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
+    store_row(a.store, a.off, N, c, offv);
 }
 
 void launch_scalar_assemble(cudaStream_t s, int type, const Physics &ph, const MeshArgs &m, const ScalarArgs &a,
@@ -931,19 +955,23 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_pressure_rows(Physics ph, Me
     const int N = ph.N;
     const int c = grid_stride_start();
     if (c >= N) return;
-    int faces[6];
+    const unsigned own = m.own[c];
+    int faces[6], nbs[6];
 #pragma unroll
-    for (int k = 0; k < 6; k++) faces[k] = m.sface[(size_t)k * N + c];
+    for (int k = 0; k < 6; k++) {
+        faces[k] = m.sface[(size_t)k * N + c];
+        nbs[k] = m.col[(size_t)k * N + c];
+    }
     double s = 0.0;
 #pragma unroll
     for (int k = 0; k < 6; k++) {
-        const int c1 = m.fc1[faces[k]];
-        if (c1 >= N && ph.btype[c1 - N] == INLET) s = s - a.mdot[faces[k]];
+        if (nbs[k] != c) continue;
+        if (ph.btype[m.fc1[faces[k]] - N] == INLET) s = s - a.mdot[faces[k]];
     }
 #pragma unroll
     for (int k = 0; k < 6; k++) {
-        const int c1 = m.fc1[faces[k]];
-        if (c1 >= N && ph.btype[c1 - N] == OUTLET) s -= a.mdot[faces[k]];
+        if (nbs[k] != c) continue;
+        if (ph.btype[m.fc1[faces[k]] - N] == OUTLET) s -= a.mdot[faces[k]];
     }
     if (ph.mode == 1 && a.src) s += a.src[4 * (size_t)N + c];
     double diag = 0.0;
@@ -951,11 +979,10 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_pressure_rows(Physics ph, Me
 #pragma unroll
     for (int k = 0; k < 6; k++) {
         const int face = faces[k];
-        const int c0 = m.fc0[face], c1 = m.fc1[face];
         offv[k] = 0.0;
-        if (c1 >= N) continue;
+        if (nbs[k] == c) continue;
         const double md = a.mdot[face];
-        if (c == c0) {
+        if ((own >> k) & 1u) {
             s -= md;
             offv[k] = a.ff1[face];
             diag -= offv[k];

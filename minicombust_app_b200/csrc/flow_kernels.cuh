@@ -12,10 +12,27 @@ namespace mcb {
 struct MeshArgs {
     int F;
     const int *fc0, *fc1, *sface;
+    // Both cells of a cell's faces without reading them through the face
+    // index: col[k][c] is the other cell of face sface[k][c] (c itself on a
+    // boundary face) and bit k of own[c] is set when c is that face's cell0.
+    const int *col;
+    const uint8_t *own;
     const double *area, *lam, *rl, *Sx, *Sy, *Sz, *xf, *yf, *zf;
     const double *xc, *yc, *zc, *vol, *rho;
     const int *outlet_faces;
     int n_outlet;
+};
+
+// Storage of the FP64 momentum, temperature and scalar rows for the solvers.
+// code null: slot order (slot k = the k-th face of the cell in reference
+// order).  Otherwise by direction: the value of slot k goes to position
+// (pos >> 3d) & 7 of the row, d = (code[c] >> 3k) & 7 its direction (7: no
+// value), 0 where the row has no neighbour that way; the solvers then read no
+// column data.  The positions follow the order in which the directions occur
+// in every row's slots, so each row sums its terms in slot order.
+struct RowStore {
+    const uint32_t *code = nullptr;
+    uint32_t pos = 0;
 };
 
 // FP32 copy of assembled rows (refined path): scaled by 1 / diag, by direction.
@@ -42,6 +59,7 @@ struct MomentumArgs {
     double *off;                // [6][N]
     double *AU;                 // diagonal after under-relaxation (A_phi.U)
     double *b;                  // [3][N]
+    RowStore store;
     Fp32Rows f32;
 };
 
@@ -54,6 +72,7 @@ struct ScalarArgs {
     // temperature kernel: the pass's mass imbalance max |div(mdot) - mass source|
     // into *imbalance, which must be zero before the launch (null: not computed)
     double *imbalance;
+    RowStore store;
     Fp32Rows f32;               // temperature kernel only
 };
 
