@@ -804,15 +804,16 @@ int solve_bicg_refined(mc_flow *h, const Ell &A, const EllT<float> &A32, const B
                 if (!hout->done[j] && hout->rr[j] > 0) need = std::min(need, std::sqrt(hout->tol2[j] / hout->rr[j]));
             const int K = need >= 1e-3 ? 1 : h->prm.ir_line_steps;
             float *E[2] = {const_cast<float *>(out.e), h->line_scratch};
+            // the last step adds its result to x (the refinement update)
             for (int k = 1; k <= K; k++) {
                 float *dst = E[(K - k) % 2];
                 const float *prev = E[(K - k + 1) % 2];
-                launch(h, R == 3 ? K_LINE3 : K_LINE1,
-                       [&] { line_step<R>(h->stream, *line, out.r32, prev, dst, k == 1 ? 1 : 0); });
+                launch(h, R == 3 ? K_LINE3 : K_LINE1, [&] {
+                    line_step<R>(h->stream, *line, out.r32, prev, dst, k == 1 ? 1 : 0, k == K ? &out : nullptr);
+                });
             }
             for (int j = 0; j < R; j++)
                 if (!hout->done[j]) iters_out[j] += K;
-            launch(h, K_BIR, [&] { bir_add<R>(h->stream, A.N, out); });
             launch(h, K_BIR, [&] { bir_residual<R>(h->stream, A, out); });
             rc = check_launch(h);
             if (rc) return rc;

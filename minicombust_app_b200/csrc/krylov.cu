@@ -1166,8 +1166,15 @@ void bir_residual(cudaStream_t s, const Ell &A, const BirVectors<R> &v)
 // the chunk's maps, the value entering the chunk is applied, and the chunk's
 // last value is carried into the next chunk.
 template <int R>
+struct LineAdd {
+    double *x[R];
+    const BirState<R> *st = nullptr;  // null: store e_new
+};
+
+template <int R>
 __global__ void __launch_bounds__(256, R == 1 ? 8 : 6) k_line_sweep(LineSystem L, const float *__restrict__ r,
-                                                    const float *__restrict__ ep, float *__restrict__ en, int first)
+                                                    const float *__restrict__ ep, float *__restrict__ en, int first,
+                                                    LineAdd<R> add)
 {
     extern __shared__ float sline[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1205,6 +1212,9 @@ __global__ void __launch_bounds__(256, R == 1 ? 8 : 6) k_line_sweep(LineSystem L
         for (int j = 0; j < R; j++) sp[j * ex + c] = rhs[j] * rb;
     }
     __syncwarp();
+    bool act[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) act[j] = add.st && !add.st->done[j];
     float carry[R];
 #pragma unroll
     for (int j = 0; j < R; j++) carry[j] = 0.f;
@@ -1233,25 +1243,38 @@ __global__ void __launch_bounds__(256, R == 1 ? 8 : 6) k_line_sweep(LineSystem L
 #pragma unroll
         for (int j = 0; j < R; j++) {
             const float x = p[j] + q * carry[j];
-            if (c < ex) en[(size_t)j * N + base + c] = x;
+            if (c < ex) {
+                if (!add.st)
+                    en[(size_t)j * N + base + c] = x;
+                else if (act[j])
+                    add.x[j][base + c] += (double)x;
+            }
             carry[j] = __shfl_sync(0xffffffffu, x, 31);
         }
     }
 }
 
 template <int R>
-void line_step(cudaStream_t s, const LineSystem &L, const float *r, const float *e_prev, float *e_new, int first)
+void line_step(cudaStream_t s, const LineSystem &L, const float *r, const float *e_prev, float *e_new, int first,
+               const BirVectors<R> *add)
 {
+    LineAdd<R> la{};
+    if (add) {
+        for (int j = 0; j < R; j++) la.x[j] = add->x[j];
+        la.st = add->st;
+    }
     const int lines = L.N / L.ex;
     const size_t per_warp = (size_t)L.ex * (R + 1) * sizeof(float);
     int warps = 8;
     while (warps > 1 && warps * per_warp > 48 * 1024) warps >>= 1;
     const int threads = 32 * warps;
     const int grid = (lines + warps - 1) / warps;
-    k_line_sweep<R><<<grid, threads, warps * per_warp, s>>>(L, r, e_prev, e_new, first);
+    k_line_sweep<R><<<grid, threads, warps * per_warp, s>>>(L, r, e_prev, e_new, first, la);
 }
-template void line_step<1>(cudaStream_t, const LineSystem &, const float *, const float *, float *, int);
-template void line_step<3>(cudaStream_t, const LineSystem &, const float *, const float *, float *, int);
+template void line_step<1>(cudaStream_t, const LineSystem &, const float *, const float *, float *, int,
+                           const BirVectors<1> *);
+template void line_step<3>(cudaStream_t, const LineSystem &, const float *, const float *, float *, int,
+                           const BirVectors<3> *);
 
 void round_ell(cudaStream_t s, int N, const double *diag, const double *off, const uint32_t *code, float *diag32,
                float *off32)

@@ -285,9 +285,13 @@ struct LineSystem {
     const float *off = nullptr; // [6][N] by direction
 };
 // One sweep step for R right-hand sides [R][N]: with first set, M e_new = r;
-// otherwise M e_new = r - (M - A) e_prev.
+// otherwise M e_new = r - (M - A) e_prev.  With add set (the last step of an
+// inner solve) the step's result is added to the FP64 solutions add->x of
+// the systems still open instead of being stored (e_new unused): the
+// refinement update x += e without a kernel of its own.
 template <int R>
-void line_step(cudaStream_t s, const LineSystem &L, const float *r, const float *e_prev, float *e_new, int first);
+void line_step(cudaStream_t s, const LineSystem &L, const float *r, const float *e_prev, float *e_new, int first,
+               const BirVectors<R> *add = nullptr);
 
 enum { KRYLOV_OK = 0, KRYLOV_NOT_CONVERGED = 1, KRYLOV_NONFINITE = 2 };
 
