@@ -166,11 +166,12 @@ def kernel_bytes(name, N, F, nnz_off):
         "bicg3_32_2_spmv": 76 * N,     # FP32: matrix 28 + 3 x 16
         "bicg3_32_3_update": 84 * N,
         "gnn_layers": 129 * N,         # one tcgen05 layer launch: h in 64, h out 64, mask 1 (four per pass)
-        # one V-cycle, per fine row.  FP32 (every level's matrix by direction),
-        # level 0: first two sweeps 36, sweep 40, restriction 40, prolongation
-        # + sweep 44, sweep 40, last sweep with r.z 40 = 240; level 1 (1/8 of
-        # the rows, about 241 bytes per row) 30; level 2 and below 4
-        "amg32_vcycle": 274 * N,
+        # one V-cycle, per fine row.  FP32 (every level's matrix by direction;
+        # level 0's off-diagonal values read in FP16, 12 bytes), level 0:
+        # first two sweeps 24, sweep 28, restriction 28, prolongation + sweep
+        # 32, sweep 28, last sweep with r.z 28 = 168; level 1 (1/8 of the
+        # rows, about 241 bytes per row) 30; level 2 and below 4
+        "amg32_vcycle": 202 * N,
         # FP64 (level 0 in the half form: 32 bytes of matrix per row, coarse
         # levels by direction), level 0: first sweep 24, sweeps 4 x 56,
         # restriction 53, prolongation 21, last sweep 56 = 378; level 1 66;

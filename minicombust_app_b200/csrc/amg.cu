@@ -188,10 +188,18 @@ namespace {
 
 // (A v)_i where v(j) yields the vector's value at row j (a stored vector, or
 // one evaluated where it is needed).
-template <typename T, typename V>
+template <bool H = false, typename T, typename V>
 __device__ __forceinline__ T row_apply_v(const AmgLevelT<T> &L, int i, V &&v)
 {
     const T s0 = L.diag[i] * v(i);
+    if constexpr (H) {  // FP16 off-diagonal values by direction (FP32 level 0)
+        int c[6];
+        dia_cols(L.dc, L.n, i, c);
+        T t = (T)0;
+#pragma unroll
+        for (int q = 0; q < 6; q++) t += (T)__half2float(L.off16[(size_t)q * L.n + i]) * v(c[q]);
+        return s0 + t * (T)__ldg(L.scale16 + 1);
+    }
     if (L.dc.code || L.dc.dia) {
         return with_row_cols(L.dc, L.col, L.n, i, [&](const int(&c)[6]) {
             T s = s0;
@@ -205,10 +213,10 @@ __device__ __forceinline__ T row_apply_v(const AmgLevelT<T> &L, int i, V &&v)
     return s;
 }
 
-template <typename T>
+template <bool H = false, typename T>
 __device__ __forceinline__ T row_apply(const AmgLevelT<T> &L, int i, const T *__restrict__ e)
 {
-    return row_apply_v(L, i, [&](int j) { return e[j]; });
+    return row_apply_v<H>(L, i, [&](int j) { return e[j]; });
 }
 
 template <typename T>
@@ -232,6 +240,59 @@ __global__ void k_amg_round_level0(int n, const double *__restrict__ diag, const
     round_row_by_direction(off, code, n, i, o);
 #pragma unroll
     for (int q = 0; q < 6; q++) off32[(size_t)q * n + i] = o[q];
+}
+
+// max |diag| of the FP32 level 0 into *dmax (when the pressure-row kernel
+// has not formed it).
+__global__ void __launch_bounds__(MCB_THREADS) k_amg_half_max(int n, const float *__restrict__ diag, double *dmax,
+                                                              double *partials, unsigned int *counter)
+{
+    __shared__ double sh[1][MCB_THREADS];
+    double m[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        m[0] = fmax(m[0], (double)fabsf(diag[i]));
+    if (publish_partials<1, true>(m, partials, counter, sh)) {
+        double tot[1];
+        reduce_partials<1, true>(tot, partials, counter, sh);
+        if (threadIdx.x == 0) *dmax = tot[0];
+    }
+}
+
+// FP16 copy of the FP32 level-0 off-diagonal values (by direction), times
+// the power of two 2^(14 - e) with max |diag| = *dmax < 2^e, saturated at
+// the largest finite FP16 value.  The rows are weakly diagonally dominant,
+// so every scaled value is below 2^14 (FP16 reaches 65504) and values down
+// to 2^-28 of the largest diagonal stay normal FP16 numbers.  The scale and
+// its reciprocal go to scale16[0..1] for the V-cycle.
+__global__ void __launch_bounds__(MCB_THREADS) k_amg_half_level0(int n, const float *__restrict__ off,
+                                                                 const double *__restrict__ dmax,
+                                                                 float *__restrict__ scale16,
+                                                                 __half *__restrict__ off16)
+{
+    const double d = *dmax;
+    int e = 0;
+    if (d > 0.0 && isfinite(d)) frexp(d, &e);
+    e = max(-100, min(100, e));
+    const float sc = ldexpf(1.f, 14 - e);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scale16[0] = sc;
+        scale16[1] = ldexpf(1.f, e - 14);
+    }
+    auto h = [&](float v) { return __float2half_rn(fminf(fmaxf(v * sc, -65504.f), 65504.f)); };
+    const size_t total = (size_t)6 * n, quads = total / 4;  // both arrays 256-byte aligned
+    const float4 *o4 = reinterpret_cast<const float4 *>(off);
+    uint2 *h4 = reinterpret_cast<uint2 *>(off16);
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < quads; t += (size_t)gridDim.x * blockDim.x) {
+        const float4 v = o4[t];
+        const __half2 a = __halves2half2(h(v.x), h(v.y)), b = __halves2half2(h(v.z), h(v.w));
+        uint2 u;
+        memcpy(&u.x, &a, 4);
+        memcpy(&u.y, &b, 4);
+        h4[t] = u;
+    }
+    for (size_t t = 4 * quads + (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (size_t)gridDim.x * blockDim.x)
+        off16[t] = h(off[t]);
 }
 
 // Coarse values as sums of fine values (the Galerkin lists index the fine
@@ -345,7 +406,7 @@ __global__ void k_amg_smooth_first(AmgLevelT<T> L, T omega, T *__restrict__ e, c
 
 // The first two sweeps from e = 0 in one pass: e1 = e0 + omega D^-1 (r - A e0)
 // with e0 = omega D^-1 r evaluated at each row where it is needed.
-template <typename T>
+template <typename T, bool H = false>
 __global__ void k_amg_smooth_first2(AmgLevelT<T> L, T omega, T omega2, T *__restrict__ eout, const PcgState *st)
 {
     pdl_wait();
@@ -353,7 +414,7 @@ __global__ void k_amg_smooth_first2(AmgLevelT<T> L, T omega, T omega2, T *__rest
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= L.n) return;
     auto e0 = [&](int j) { return omega * L.r[j] * inv_or_zero(L.diag[j]); };
-    eout[i] = e0(i) + omega2 * (L.r[i] - row_apply_v(L, i, e0)) * inv_or_zero(L.diag[i]);
+    eout[i] = e0(i) + omega2 * (L.r[i] - row_apply_v<H>(L, i, e0)) * inv_or_zero(L.diag[i]);
 }
 
 // Prolongation and the first post-smoothing sweep in one pass: the
@@ -362,7 +423,7 @@ __global__ void k_amg_smooth_first2(AmgLevelT<T> L, T omega, T omega2, T *__rest
 // The FP32 forms of this kernel, the restriction and the last sweep are held
 // to 32 registers (8 blocks of 256 per SM: full occupancy); 0 leaves the FP64
 // forms to the compiler.
-template <typename T>
+template <typename T, bool H = false>
 __global__ void __launch_bounds__(MCB_THREADS, sizeof(T) == 4 ? 8 : 0)
     k_amg_prolong_jacobi(AmgLevelT<T> L, T omega, T alpha, const T *__restrict__ ec,
                                      const T *__restrict__ e, T *__restrict__ eout, const PcgState *st)
@@ -372,10 +433,10 @@ __global__ void __launch_bounds__(MCB_THREADS, sizeof(T) == 4 ? 8 : 0)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= L.n) return;
     auto ein = [&](int j) { return e[j] + alpha * ec[L.agg[j]]; };
-    eout[i] = ein(i) + omega * (L.r[i] - row_apply_v(L, i, ein)) * inv_or_zero(L.diag[i]);
+    eout[i] = ein(i) + omega * (L.r[i] - row_apply_v<H>(L, i, ein)) * inv_or_zero(L.diag[i]);
 }
 
-template <typename T>
+template <typename T, bool H = false>
 __global__ void k_amg_jacobi(AmgLevelT<T> L, T omega, const T *__restrict__ ein, T *__restrict__ eout,
                              const PcgState *st)
 {
@@ -383,13 +444,13 @@ __global__ void k_amg_jacobi(AmgLevelT<T> L, T omega, const T *__restrict__ ein,
     if (st->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= L.n) return;
-    eout[i] = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
+    eout[i] = ein[i] + omega * (L.r[i] - row_apply<H>(L, i, ein)) * inv_or_zero(L.diag[i]);
 }
 
 // Residual of the fine rows of coarse row I, summed: 8 lanes per coarse
 // row (an aggregate has at most 8 rows; larger ones loop), each lane one
 // fine row, then a fixed-order shuffle sum.  Every lane of the warp must call.
-template <typename T>
+template <bool H, typename T>
 __device__ __forceinline__ void restrict_row8(const AmgLevelT<T> &fine, const AmgLevelT<T> &coarse,
                                               const T *__restrict__ e, int I, int m)
 {
@@ -397,7 +458,7 @@ __device__ __forceinline__ void restrict_row8(const AmgLevelT<T> &fine, const Am
     if (I < coarse.n)
         for (int t = fine.mptr[I] + m; t < fine.mptr[I + 1]; t += 8) {
             const int i = fine.mlist[t];
-            s += fine.r[i] - row_apply(fine, i, e);
+            s += fine.r[i] - row_apply<H>(fine, i, e);
         }
     s += __shfl_xor_sync(0xffffffffu, s, 1);
     s += __shfl_xor_sync(0xffffffffu, s, 2);
@@ -405,14 +466,14 @@ __device__ __forceinline__ void restrict_row8(const AmgLevelT<T> &fine, const Am
     if (I < coarse.n && m == 0) coarse.r[I] = s;
 }
 
-template <typename T>
+template <typename T, bool H = false>
 __global__ void __launch_bounds__(MCB_THREADS, sizeof(T) == 4 ? 8 : 0)
     k_amg_restrict(AmgLevelT<T> fine, AmgLevelT<T> coarse, const T *__restrict__ e, const PcgState *st)
 {
     pdl_wait();
     if (st->done) return;
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    restrict_row8(fine, coarse, e, g >> 3, g & 7);
+    restrict_row8<H>(fine, coarse, e, g >> 3, g & 7);
 }
 
 template <typename T>
@@ -427,7 +488,7 @@ __global__ void k_amg_prolong(AmgLevelT<T> fine, T alpha, const T *__restrict__ 
 }
 
 // Last post-smoothing sweep on level 0: z into zp[i].x and the PCG's r . z (FP64 sum).
-template <typename T>
+template <typename T, bool H = false>
 __global__ void __launch_bounds__(MCB_THREADS, sizeof(T) == 4 ? 8 : 0) k_amg_final(AmgLevelT<T> L, T omega, const T *__restrict__ ein,
                                                            typename Pair<T>::type *__restrict__ zp, PcgState *st,
                                                            double *partials, unsigned int *counter, int is_init)
@@ -437,7 +498,7 @@ __global__ void __launch_bounds__(MCB_THREADS, sizeof(T) == 4 ? 8 : 0) k_amg_fin
     if (st->done) return;
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x) {
-        const T z = ein[i] + omega * (L.r[i] - row_apply(L, i, ein)) * inv_or_zero(L.diag[i]);
+        const T z = ein[i] + omega * (L.r[i] - row_apply<H>(L, i, ein)) * inv_or_zero(L.diag[i]);
         zp[i].x = z;
         acc[0] += (double)L.r[i] * (double)z;
     }
@@ -498,7 +559,7 @@ __global__ void __launch_bounds__(AMG_FUSED_THREADS)
             __syncthreads();
         }
         const AmgLevelT<T> &Cl = C.lv[l + 1];
-        for (int g = t; g < ((Cl.n + 3) & ~3) * 8; g += nt) restrict_row8(L, Cl, L.e[c], g >> 3, g & 7);
+        for (int g = t; g < ((Cl.n + 3) & ~3) * 8; g += nt) restrict_row8<false>(L, Cl, L.e[c], g >> 3, g & 7);
         __syncthreads();
     }
     {  // dense solve on the coarsest level
@@ -566,13 +627,22 @@ void set_dense_attributes()
 } // namespace
 
 template <typename T>
-void amg_setup_levels(cudaStream_t s, const AmgHierarchy &H, bool level0_ready)
+void amg_setup_levels(cudaStream_t s, const AmgHierarchy &H, bool level0_ready, double *partials,
+                      unsigned int *counter, double *dmax)
 {
     const AmgLevelT<T> *lv = levels_of<T>(H);
     if (sizeof(T) == sizeof(float) && !level0_ready)
         k_amg_round_level0<<<blocks(H.g0.n), MCB_THREADS, 0, s>>>(H.g0.n, H.g0.diag, H.g0.off,
                                                                   lv[0].dc.dia ? H.g0.dc.code : nullptr,
                                                                   (float *)lv[0].diag, (float *)lv[0].off);
+    if (sizeof(T) == sizeof(float) && lv[0].off16) {
+        const int n = lv[0].n;
+        if (!level0_ready)
+            k_amg_half_max<<<krylov_grid(n), MCB_THREADS, 0, s>>>(n, (const float *)lv[0].diag, dmax, partials,
+                                                                   counter);
+        k_amg_half_level0<<<krylov_grid(n), MCB_THREADS, 0, s>>>(n, (const float *)lv[0].off, dmax, lv[0].scale16,
+                                                                 lv[0].off16);
+    }
     if (H.levels > 1) k_amg_galerkin<double, T><<<blocks(lv[1].n), MCB_THREADS, 0, s>>>(H.g0, lv[1]);
     for (int l = 2; l < H.levels; l++)
         k_amg_galerkin<T, T><<<blocks(lv[l].n), MCB_THREADS, 0, s>>>(lv[l - 1], lv[l]);
@@ -637,23 +707,29 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
     lv[0].r = const_cast<T *>(r0);
     const bool pair = amg_paired_sweeps(H, sizeof(T) == sizeof(float));
     const dim3 nt(MCB_THREADS);
+    // level 0 with FP16 off-diagonal values: the kernels' H forms
+    const bool h0 = sizeof(T) == sizeof(float) && lv[0].off16;
     for (int l = 0; l < F; l++) {
         const AmgLevelT<T> &V = lv[l];
         const dim3 g(blocks(V.n));
+        const bool hv = h0 && l == 0;
         int c = 0, sw = 1;
         if (pair) {
-            pdl_launch(k_amg_smooth_first2<T>, g, nt, 0, s, V, w(0), w(1), V.e[1], st);
+            pdl_launch(hv ? k_amg_smooth_first2<T, true> : k_amg_smooth_first2<T, false>, g, nt, 0, s, V, w(0), w(1),
+                       V.e[1], st);
             c = 1;
             sw = 2;
         } else {
             pdl_launch(k_amg_smooth_first<T>, g, nt, 0, s, V, w(0), V.e[0], st);
         }
         for (; sw < H.sweeps; sw++) {
-            pdl_launch(k_amg_jacobi<T>, g, nt, 0, s, V, w(sw), V.e[c], V.e[c ^ 1], st);
+            pdl_launch(hv ? k_amg_jacobi<T, true> : k_amg_jacobi<T, false>, g, nt, 0, s, V, w(sw), V.e[c], V.e[c ^ 1],
+                       st);
             c ^= 1;
         }
         cur[l] = c;
-        pdl_launch(k_amg_restrict<T>, dim3(blocks8(lv[l + 1].n)), nt, 0, s, V, lv[l + 1], V.e[c], st);
+        pdl_launch(hv ? k_amg_restrict<T, true> : k_amg_restrict<T, false>, dim3(blocks8(lv[l + 1].n)), nt, 0, s, V,
+                   lv[l + 1], V.e[c], st);
     }
     AmgCoarse<T> C;
     C.nl = L - F;
@@ -664,10 +740,12 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
     for (int l = F - 1; l >= 0; l--) {
         const AmgLevelT<T> &V = lv[l];
         const dim3 g(blocks(V.n));
+        const bool hv = h0 && l == 0;
         const T *ec = lv[l + 1].e[cur[l + 1]];
         int c = cur[l], sw = 1;
         if (pair) {
-            pdl_launch(k_amg_prolong_jacobi<T>, g, nt, 0, s, V, w(H.sweeps - 1), alpha, ec, V.e[c], V.e[c ^ 1], st);
+            pdl_launch(hv ? k_amg_prolong_jacobi<T, true> : k_amg_prolong_jacobi<T, false>, g, nt, 0, s, V,
+                       w(H.sweeps - 1), alpha, ec, V.e[c], V.e[c ^ 1], st);
             c ^= 1;
             sw = 2;
         } else {
@@ -675,10 +753,11 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
         }
         for (; sw <= H.sweeps; sw++) {
             if (l == 0 && sw == H.sweeps) {
-                pdl_launch(k_amg_final<T>, dim3(krylov_grid(V.n)), nt, 0, s, V, w(H.sweeps - sw), V.e[c], zp_out, st,
-                           partials, counter, is_init);
+                pdl_launch(hv ? k_amg_final<T, true> : k_amg_final<T, false>, dim3(krylov_grid(V.n)), nt, 0, s, V,
+                           w(H.sweeps - sw), V.e[c], zp_out, st, partials, counter, is_init);
             } else {
-                pdl_launch(k_amg_jacobi<T>, g, nt, 0, s, V, w(H.sweeps - sw), V.e[c], V.e[c ^ 1], st);
+                pdl_launch(hv ? k_amg_jacobi<T, true> : k_amg_jacobi<T, false>, g, nt, 0, s, V, w(H.sweeps - sw),
+                           V.e[c], V.e[c ^ 1], st);
                 c ^= 1;
             }
         }
@@ -686,8 +765,8 @@ void amg_vcycle(cudaStream_t s, const AmgHierarchy &H, const T *r0, void *zp_out
     }
 }
 
-template void amg_setup_levels<double>(cudaStream_t, const AmgHierarchy &, bool);
-template void amg_setup_levels<float>(cudaStream_t, const AmgHierarchy &, bool);
+template void amg_setup_levels<double>(cudaStream_t, const AmgHierarchy &, bool, double *, unsigned int *, double *);
+template void amg_setup_levels<float>(cudaStream_t, const AmgHierarchy &, bool, double *, unsigned int *, double *);
 template void amg_coarsest_inverse<double>(cudaStream_t, const AmgHierarchy &, double *);
 template void amg_coarsest_inverse<float>(cudaStream_t, const AmgHierarchy &, double *);
 template void amg_vcycle<double>(cudaStream_t, const AmgHierarchy &, const double *, void *, PcgState *, double *,

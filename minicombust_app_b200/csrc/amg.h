@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "krylov.cuh"
@@ -58,6 +59,13 @@ struct AmgLevelT {
     const int *gidx;
     T *r;           // right-hand side of the level
     T *e[2];        // ping-pong iterates
+    // FP32 level 0 stored by direction: its off-diagonal values also in FP16,
+    // times scale16[0] (a power of two chosen each time the values change);
+    // the sweeps and the restriction of the V-cycle read these (and multiply
+    // by scale16[1] = 1 / scale16[0]), the PCG product keeps the FP32 values.
+    // Null: every kernel reads off.
+    __half *off16 = nullptr;
+    float *scale16 = nullptr;
 };
 using AmgLevel = AmgLevelT<double>;
 
@@ -109,9 +117,13 @@ int amg_build_host(int N, const std::vector<int> &col0, const std::vector<int> &
 // Device work, all asynchronous on stream s.
 // Galerkin values of levels 1..L-1 for the FP64 (T = double) or the FP32
 // (T = float; level 0 rounded from FP64 first, unless the pressure kernel
-// has just written it: level0_ready) hierarchy.
+// has just written it: level0_ready) hierarchy, and the FP16 copy of the
+// FP32 level 0 where there is one, scaled by max |diag| in *dmax (formed by
+// the pressure kernel with level0_ready, else here through partials and
+// counter).
 template <typename T>
-void amg_setup_levels(cudaStream_t s, const AmgHierarchy &H, bool level0_ready = false);
+void amg_setup_levels(cudaStream_t s, const AmgHierarchy &H, bool level0_ready, double *partials,
+                      unsigned int *counter, double *dmax);
 // Explicit inverse of the coarsest level's current values into `out`
 // (n x n FP64); reads only the coarsest level.
 template <typename T>

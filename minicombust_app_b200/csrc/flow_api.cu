@@ -127,7 +127,7 @@ struct mc_flow {
     double *partials;
     unsigned int *counter;
     FluxBalance *balance;
-    double *scalars;   // [0] max|PP|, [1] mass imbalance
+    double *scalars;   // [0] max|PP|, [1] mass imbalance, [2] max |diag| of the pressure rows (FP16 level 0)
     // Krylov
     PcgVectors pv{};
     BicgVectors<3> b3{};
@@ -1000,11 +1000,12 @@ int setup_amg_values(mc_flow *h)
         h->inverse_pending = false;
     }
     if (h->refined)
-        amg_setup_levels<float>(h->stream, H, h->p32_written);
+        amg_setup_levels<float>(h->stream, H, h->p32_written, h->partials, h->counter, h->scalars + 2);
     else
-        amg_setup_levels<double>(h->stream, H);
-    h->p32_written = false;
+        amg_setup_levels<double>(h->stream, H, false, h->partials, h->counter, h->scalars + 2);
     h->launches += h->refined ? H.levels - 1 : H.levels - 2;  // with the one the caller's launch() counts
+    if (h->refined && H.lv32[0].off16) h->launches += h->p32_written ? 1 : 2;  // the FP16 level 0 (and its scale)
+    h->p32_written = false;
     if (h->inverse_ready && h->side && lagged_inverse_enabled()) {
         h->inverse_deferred = true;
         return MC_OK;
@@ -1095,6 +1096,10 @@ int stage_pressure(mc_flow *h, mc_iter_stats *st)
         if (h->p32_written) {
             const AmgLevelT<float> &L0 = h->amg.lv32[0];
             a.f32 = Fp32Rows{L0.diag, L0.off, L0.dc.dia ? h->dc.code : nullptr, 0};
+            if (L0.off16) {  // the scale of its FP16 copy
+                a.diag_max = h->scalars + 2;
+                CUDA_TRY(h, cudaMemsetAsync(a.diag_max, 0, sizeof(double), h->stream));
+            }
         }
         a.dir64 = h->p_dir64;
         a.dir64_sym = h->dc_pdir.sym;
@@ -1658,6 +1663,12 @@ bool dir_codes_disabled()
     return v && v[0] == '0';
 }
 
+bool amg_half_disabled()
+{
+    const char *v = std::getenv("MC_AMG_HALF");
+    return v && v[0] == '0';
+}
+
 bool row_store_disabled()
 {
     const char *v = std::getenv("MC_ROW_STORE");
@@ -1791,6 +1802,8 @@ int build_amg(mc_flow *h, const HostMesh &hm)
     add(&H.dense_next, (size_t)nc * nc * 8);
     const bool fp32 = h->prm.precision == MC_PRECISION_FP32_REFINED;
     PcgState *inner_state = nullptr;
+    // the FP16 copy of the FP32 level 0 (values by direction) for the V-cycle
+    const bool half0 = fp32 && h->dc.code && !amg_half_disabled();
     if (fp32) {
         for (int l = 0; l < L; l++) {
             AmgLevelT<float> &f = H.lv32[l];
@@ -1799,6 +1812,10 @@ int build_amg(mc_flow *h, const HostMesh &hm)
             add(&f.r, (size_t)lv[l].n * 4);
             add(&f.e[0], (size_t)lv[l].n * 4);
             add(&f.e[1], (size_t)lv[l].n * 4);
+            if (l == 0 && half0) {
+                add(&f.off16, (size_t)6 * lv[l].n * 2);
+                add(&f.scale16, 2 * sizeof(float));
+            }
         }
         add(&h->pv32.x, (size_t)N * 4);
         add(&h->pv32.r, (size_t)N * 4);

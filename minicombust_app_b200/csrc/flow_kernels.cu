@@ -950,11 +950,10 @@ __global__ void k_outlet_fix(Physics ph, MeshArgs m, double *__restrict__ mdot, 
 
 // Pressure-correction rows (the S_U accumulation of calculate_mass_flux,
 // :1964 and :2101, and setup_pressure_matrix, :2139-2189).
-__global__ void __launch_bounds__(MCB_THREADS, 4) k_pressure_rows(Physics ph, MeshArgs m, PressureRowArgs a)
+// One cell's row; returns its diagonal.
+__device__ __forceinline__ double pressure_row(const Physics &ph, const MeshArgs &m, const PressureRowArgs &a, int c)
 {
     const int N = ph.N;
-    const int c = grid_stride_start();
-    if (c >= N) return;
     const unsigned own = m.own[c];
     int faces[6], nbs[6];
 #pragma unroll
@@ -998,6 +997,23 @@ __global__ void __launch_bounds__(MCB_THREADS, 4) k_pressure_rows(Physics ph, Me
     for (int k = 0; k < 6; k++) a.off[(size_t)k * N + c] = offv[k];
     if (a.f32.d32) store_fp32_row(a.f32, N, c, diag, offv);
     if (a.dir64) store_dir_row(a.code[c], offv, a.dir64, N, c, a.dir64_sym);
+    return diag;
+}
+
+// With diag_max set, also max |diag| (for the scale of the FP16 copy of the
+// FP32 level 0): a warp maximum, then one atomicMax per warp on the bits of
+// the non-negative value; *diag_max must be zero before the launch.
+__global__ void __launch_bounds__(MCB_THREADS, 4) k_pressure_rows(Physics ph, MeshArgs m, PressureRowArgs a)
+{
+    const int c = grid_stride_start();
+    double v = 0.0;
+    if (c < ph.N) v = fabs(pressure_row(ph, m, a, c));
+    if (a.diag_max) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+        if ((threadIdx.x & 31) == 0 && v > 0.0)
+            atomicMax((unsigned long long *)a.diag_max, (unsigned long long)__double_as_longlong(v));
+    }
 }
 
 __global__ void __launch_bounds__(MCB_THREADS) k_dir_rows64(int N, const double *__restrict__ off,

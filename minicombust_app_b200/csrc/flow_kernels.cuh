@@ -116,6 +116,7 @@ struct PressureRowArgs {
     double *dir64;
     int dir64_sym;
     const uint32_t *code;
+    double *diag_max;           // max |diag| (zero before the launch); null: not formed
 };
 
 // The by-direction FP64 copy of a matrix stored by slot with direction
