@@ -195,7 +195,7 @@ def kernel_bytes(name, N, F, nnz_off):
 # 2 x 96^3 case (a full capture of the 2 x 128^3 case is too large); scaled by
 # rows to the bench size for the roofline's `traffic`.
 NCU_DRAM_BYTES_PER_ROW = {
-    "bicg3_1_spmv": 211.9,   # k_bicg_1<double,3>
+    "bicg3_1_spmv": 217.2,   # k_bicg_1<double,3>: 384.3 MB read + written on 1,769,472 cells
     "gnn_layers": 103.6,     # k_gnn_layer_umma: 115.1 + 68.2 MB read + written on 1,769,472 cells
 }
 
