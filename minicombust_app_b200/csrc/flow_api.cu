@@ -97,6 +97,7 @@ struct mc_flow {
     // FP64 momentum, temperature and scalar rows stored by direction
     // (rows.code set; see RowStore) and the codes the solvers read them with;
     // hcode: the direction codes on the host (CSR export)
+    double *ir_x2 = nullptr;  // the refined pressure solve's second FP64 solution buffer
     RowStore rows;
     DirCodes dc_rows;
     std::vector<uint32_t> hcode;
@@ -623,7 +624,7 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
     h->guess_used = use_x0 != 0;
     if (const int rl = launch_deferred_inverse(h)) return rl;
     launch(h, K_IR, [&] {
-        ir_init(h->stream, A, o.b, o.x, o.r, h->r32, o.st, o.partials, o.counter, h->prm.p_rtol, abs_floor, kMaxOuter,
+        ir_init(h->stream, A, o.b, o.x, nullptr, h->r32, o.st, o.partials, o.counter, h->prm.p_rtol, abs_floor, kMaxOuter,
                 use_x0);
     });
     int rc = check_launch(h);
@@ -631,6 +632,7 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
     const int per_iter = 2 + amg_kernels_per_vcycle(h->amg, true);
     const long max_batches = h->prm.max_iters / PCG_AMG_BATCH + 2;
     int inner_total = 0, worst = MC_OK;
+    double *xcur = o.x;  // the FP64 solution alternates between o.x and ir_x2
     // A device-looped inner solve is followed at once by the outer update;
     // its state is read together with the next outer check (one
     // synchronisation per outer iteration).
@@ -694,11 +696,16 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
             }
             if ((rc = account_inner(false))) return rc;
         }
-        launch(h, K_IR, [&] { ir_add(h->stream, h->N, o.x, in.x, o.st); });
-        launch(h, K_IR, [&] { ir_residual(h->stream, A, o.b, o.x, o.r, h->r32, o.st, o.partials, o.counter); });
+        // x + e and the new FP64 residual in one pass, into the other buffer
+        double *const xn = (xcur == o.x) ? h->ir_x2 : o.x;
+        launch(h, K_IR, [&] {
+            ir_residual(h->stream, A, o.b, xcur, nullptr, h->r32, o.st, o.partials, o.counter, in.x, xn);
+        });
+        xcur = xn;
         rc = check_launch(h);
         if (rc) return rc;
     }
+    if (xcur != o.x) CUDA_TRY(h, cudaMemcpyAsync(o.x, xcur, (size_t)h->N * 8, cudaMemcpyDeviceToDevice, h->stream));
     launch(h, K_PCG_XMEAN, [&] { pcg_xmean(h->stream, h->N, o); });
     launch(h, K_PCG_SUBMEAN, [&] { pcg_sub_xmean(h->stream, h->N, o); });
     rc = check_launch(h);
@@ -1823,6 +1830,7 @@ int build_amg(mc_flow *h, const HostMesh &hm)
         add(&h->pv32.zp[0], (size_t)N * 8);
         add(&h->pv32.zp[1], (size_t)N * 8);
         add(&h->r32, (size_t)N * 4);
+        add(&h->ir_x2, (size_t)N * 8);
         add(&inner_state, sizeof(PcgState));
     }
     std::vector<size_t> offs;

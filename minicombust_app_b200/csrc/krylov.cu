@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(MCB_THREADS) k_ir_init(Ell A, const double *__
         } else {
             x[i] = 0.0;
         }
-        r[i] = ri;
+        if (r) r[i] = ri;
         r32[i] = (float)ri;
         acc[0] += bi * bi;
         acc[1] += ri * ri;
@@ -465,26 +465,38 @@ __global__ void __launch_bounds__(MCB_THREADS) k_ir_add(int N, double *__restric
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) x[i] += (double)e[i];
 }
 
+// With e set: the update x' = x + e (the inner solution) in the same pass,
+// evaluated at each row where the product needs it and stored in xout (not
+// in x, which neighbouring rows still read); without e, x' = x.  r may be
+// null (the FP64 residual is then not stored).
 __global__ void __launch_bounds__(MCB_THREADS) k_ir_residual(Ell A, const double *__restrict__ b,
-                                                             const double *__restrict__ x, double *__restrict__ r,
+                                                             const double *__restrict__ x, const float *__restrict__ e,
+                                                             double *__restrict__ xout, double *__restrict__ r,
                                                              float *__restrict__ r32, PcgState *st, double *partials,
                                                              unsigned int *counter)
 {
     pdl_wait();
     __shared__ double sh[1][MCB_THREADS];
-    if (st->done) return;
     const int N = A.N;
+    if (st->done) {  // nothing to add: xout still has to hold the solution
+        if (e)
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) xout[i] = x[i];
+        return;
+    }
     const double mean = st->mean;
     double acc[1] = {0.0};
+    auto xv = [&](int j) { return e ? x[j] + (double)e[j] : x[j]; };
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double xi = xv(i);
         const double ax = with_row_cols(A.dc, A.col, N, i, [&](const int(&c)[6]) {
-            double s = A.diag[i] * x[i];
+            double s = A.diag[i] * xi;
 #pragma unroll
-            for (int k = 0; k < 6; k++) s += ell_val(A.dc, A.off, N, i, k, c[k]) * x[c[k]];
+            for (int k = 0; k < 6; k++) s += ell_val(A.dc, A.off, N, i, k, c[k]) * xv(c[k]);
             return s;
         });
+        if (e) xout[i] = xi;
         const double ri = (b[i] - mean) - ax;
-        r[i] = ri;
+        if (r) r[i] = ri;
         r32[i] = (float)ri;
         acc[0] += ri * ri;
     }
@@ -581,9 +593,9 @@ void ir_add(cudaStream_t s, int N, double *x, const float *e, const PcgState *st
     k_ir_add<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, x, e, st);
 }
 void ir_residual(cudaStream_t s, const Ell &A, const double *b, const double *x, double *r, float *r32, PcgState *st,
-                 double *partials, unsigned int *counter)
+                 double *partials, unsigned int *counter, const float *e, double *xout)
 {
-    k_ir_residual<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, b, x, r, r32, st, partials, counter);
+    k_ir_residual<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, b, x, e, xout, r, r32, st, partials, counter);
 }
 void pcg_xmean(cudaStream_t s, int N, const PcgVectors &v) { k_pcg_xmean<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, v); }
 void pcg_sub_xmean(cudaStream_t s, int N, const PcgVectors &v)

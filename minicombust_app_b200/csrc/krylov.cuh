@@ -342,7 +342,9 @@ void pcg_iter2_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, in
 // FP64 iterative refinement around an FP32 inner solve: the state's mean
 // (from pcg_mean) defines b' = b - mean; ir_init sets x = 0, r = b', r32 =
 // (float) r and the tolerance; ir_add accumulates x += e in FP64; ir_residual
-// recomputes the FP64 true residual, its norm, r32, and the convergence flag.
+// recomputes the FP64 true residual, its norm, r32, and the convergence flag
+// (with e given, of x + e, which it stores in xout != x: the update and the
+// residual in one pass).  r may be null in both.
 void ir_init(cudaStream_t s, const Ell &A, const double *b, double *x, double *r, float *r32, PcgState *st,
              double *partials, unsigned int *counter, double rtol, double abs_floor, int max_outer, int use_x0 = 0);
 
@@ -362,7 +364,7 @@ void guess_residuals(cudaStream_t s, const Ell &A, const double *b, const PcgSta
 void guess_apply(cudaStream_t s, int N, double *x, const double *xa, const double *xb, const GuessState *gs);
 void ir_add(cudaStream_t s, int N, double *x, const float *e, const PcgState *st);
 void ir_residual(cudaStream_t s, const Ell &A, const double *b, const double *x, double *r, float *r32, PcgState *st,
-                 double *partials, unsigned int *counter);
+                 double *partials, unsigned int *counter, const float *e = nullptr, double *xout = nullptr);
 void pcg_xmean(cudaStream_t s, int N, const PcgVectors &v);
 void pcg_sub_xmean(cudaStream_t s, int N, const PcgVectors &v);
 
