@@ -487,7 +487,10 @@ __global__ void k_snapshot_pack(int N, const double *__restrict__ b, const PcgSt
 // previous converged correction and, with MC_GUESS_LEARNED, the network's
 // prediction compete with the zero guess on ||b' - A x0||; the winner is
 // written into x.  Returns 1 when x holds the guess (0: start from zero).
-int select_guess(mc_flow *h, const Ell &A, const double *b, const PcgState *st, double *x)
+// With fuse set the guess is not written to x here: A xa and A xb are kept
+// (in the FP64 PCG's r and q, unused by the refined solve) and ir_init
+// applies the combination (guess_ir).
+int select_guess(mc_flow *h, const Ell &A, const double *b, const PcgState *st, double *x, bool fuse = false)
 {
     // Only the first corrector of a pass starts from a guess: the later ones
     // solve for the small non-orthogonal remainder, which on the benchmark box
@@ -509,9 +512,11 @@ int select_guess(mc_flow *h, const Ell &A, const double *b, const PcgState *st, 
     }
     launch(h, K_GUESS, [&] {
         guess_residuals(h->stream, A, b, st, h->pp_prev, learned ? h->x0_learned : nullptr, h->gs, h->partials,
-                        h->counter);
+                        h->counter, fuse ? h->pv.r : nullptr, fuse ? h->pv.q : nullptr);
     });
-    launch(h, K_GUESS, [&] { guess_apply(h->stream, h->N, x, h->pp_prev, learned ? h->x0_learned : nullptr, h->gs); });
+    if (!fuse)
+        launch(h, K_GUESS,
+               [&] { guess_apply(h->stream, h->N, x, h->pp_prev, learned ? h->x0_learned : nullptr, h->gs); });
     CUDA_TRY(h, cudaMemcpyAsync(h->h_gs, h->gs, sizeof(GuessState), cudaMemcpyDeviceToHost, h->stream));
     return 1;
 }
@@ -620,12 +625,16 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
     PcgVectorsT<float> in = h->pv32;
     constexpr int kMaxOuter = 50;
     launch(h, K_PCG_MEAN, [&] { pcg_mean(h->stream, A, o); });
-    const int use_x0 = select_guess(h, A, o.b, o.st, o.x);
+    const int use_x0 = select_guess(h, A, o.b, o.st, o.x, true);
     h->guess_used = use_x0 != 0;
     if (const int rl = launch_deferred_inverse(h)) return rl;
+    IrGuess g{};
+    if (use_x0)
+        g = IrGuess{h->gs, h->pp_prev,
+                    h->prm.initial_guess == MC_GUESS_LEARNED ? h->x0_learned : nullptr, h->pv.r, h->pv.q};
     launch(h, K_IR, [&] {
         ir_init(h->stream, A, o.b, o.x, nullptr, h->r32, o.st, o.partials, o.counter, h->prm.p_rtol, abs_floor, kMaxOuter,
-                use_x0);
+                0, g);
     });
     int rc = check_launch(h);
     if (rc) return rc;

@@ -343,16 +343,23 @@ __device__ __forceinline__ RowPair ell_row2(const Ell &A, const double *__restri
 __global__ void __launch_bounds__(MCB_THREADS) k_ir_init(Ell A, const double *__restrict__ b, double *__restrict__ x,
                                                          double *__restrict__ r, float *__restrict__ r32, PcgState *st,
                                                          double *partials, unsigned int *counter, double rtol,
-                                                         double abs_floor, int max_outer, int use_x0)
+                                                         double abs_floor, int max_outer, int use_x0,
+                                                         IrGuess g)
 {
     __shared__ double sh[2][MCB_THREADS];
     const int N = A.N;
     const double mean = st->mean;
+    // the guess's combination (see GuessState), applied here
+    const double al = g.gs ? g.gs->coef[0] : 0.0, be = g.gs ? g.gs->coef[1] : 0.0;
+    const bool ua = g.gs && g.xa && al != 0.0, ub = g.gs && g.xb && be != 0.0;
     double acc[2] = {0.0, 0.0};  // b'.b', r.r
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const double bi = b[i] - mean;
         double ri = bi;
-        if (use_x0) {
+        if (g.gs) {
+            x[i] = (ua ? al * g.xa[i] : 0.0) + (ub ? be * g.xb[i] : 0.0);
+            ri = bi - ((ua ? al * g.u[i] : 0.0) + (ub ? be * g.w[i] : 0.0));
+        } else if (use_x0) {
             ri = bi - ell_row(A, x, i);
         } else {
             x[i] = 0.0;
@@ -390,34 +397,35 @@ __global__ void __launch_bounds__(MCB_THREADS) k_guess_residuals(Ell A, const do
                                                                  const PcgState *__restrict__ st,
                                                                  const double *__restrict__ xa,
                                                                  const double *__restrict__ xb, GuessState *gs,
-                                                                 double *partials, unsigned int *counter)
+                                                                 double *partials, unsigned int *counter,
+                                                                 double *__restrict__ uo, double *__restrict__ wo)
 {
-    __shared__ double sh[8][MCB_THREADS];
+    __shared__ double sh[6][MCB_THREADS];
     const int N = A.N;
     const double mean = st->mean;
-    // bb, bu, bw, uu, uw, ww, |b'-u|^2, |b'-w|^2
-    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    // bb, bu, bw, uu, uw, ww
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const double bi = b[i] - mean;
         const RowPair uw = ell_row2(A, xa, xb, i);
         const double u = uw.u, w = uw.w;
+        if (uo && xa) uo[i] = u;
+        if (wo && xb) wo[i] = w;
         acc[0] += bi * bi;
         acc[1] += bi * u;
         acc[2] += bi * w;
         acc[3] += u * u;
         acc[4] += u * w;
         acc[5] += w * w;
-        acc[6] += (bi - u) * (bi - u);
-        acc[7] += (bi - w) * (bi - w);
     }
-    if (publish_partials<8>(acc, partials, counter, sh)) {
-        double t[8];
-        reduce_partials<8>(t, partials, counter, sh);
+    if (publish_partials<6>(acc, partials, counter, sh)) {
+        double t[6];
+        reduce_partials<6>(t, partials, counter, sh);
         if (threadIdx.x == 0) {
             const double bb = t[0], bu = t[1], bw = t[2], uu = t[3], uw = t[4], ww = t[5];
             gs->bb = bb;
-            gs->rr[0] = xa ? t[6] : -1.0;
-            gs->rr[1] = xb ? t[7] : -1.0;
+            gs->rr[0] = xa ? fmax(bb - 2.0 * bu + uu, 0.0) : -1.0;
+            gs->rr[1] = xb ? fmax(bb - 2.0 * bw + ww, 0.0) : -1.0;
             double al = 0.0, be = 0.0;
             const bool ha = xa && uu > 0 && finite(uu), hb = xb && ww > 0 && finite(ww);
             const double det = uu * ww - uw * uw;
@@ -574,15 +582,17 @@ void pcg_iter2_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, in
 MCB_INSTANTIATE_PCG(double)
 MCB_INSTANTIATE_PCG(float)
 void ir_init(cudaStream_t s, const Ell &A, const double *b, double *x, double *r, float *r32, PcgState *st,
-             double *partials, unsigned int *counter, double rtol, double abs_floor, int max_outer, int use_x0)
+             double *partials, unsigned int *counter, double rtol, double abs_floor, int max_outer, int use_x0,
+             const IrGuess &g)
 {
     k_ir_init<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, b, x, r, r32, st, partials, counter, rtol, abs_floor,
-                                                       max_outer, use_x0);
+                                                       max_outer, use_x0, g);
 }
 void guess_residuals(cudaStream_t s, const Ell &A, const double *b, const PcgState *st, const double *xa,
-                     const double *xb, GuessState *gs, double *partials, unsigned int *counter)
+                     const double *xb, GuessState *gs, double *partials, unsigned int *counter, double *uo,
+                     double *wo)
 {
-    k_guess_residuals<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, b, st, xa, xb, gs, partials, counter);
+    k_guess_residuals<<<krylov_grid(A.N), MCB_THREADS, 0, s>>>(A, b, st, xa, xb, gs, partials, counter, uo, wo);
 }
 void guess_apply(cudaStream_t s, int N, double *x, const double *xa, const double *xb, const GuessState *gs)
 {

@@ -345,9 +345,6 @@ void pcg_iter2_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, in
 // recomputes the FP64 true residual, its norm, r32, and the convergence flag
 // (with e given, of x + e, which it stores in xout != x: the update and the
 // residual in one pass).  r may be null in both.
-void ir_init(cudaStream_t s, const Ell &A, const double *b, double *x, double *r, float *r32, PcgState *st,
-             double *partials, unsigned int *counter, double rtol, double abs_floor, int max_outer, int use_x0 = 0);
-
 // Initial guess of the pressure correction from up to two candidates xa, xb
 // (a null candidate is skipped): the combination x0 = alpha xa + beta xb
 // that minimises ||b' - A x0|| (b' = b - st->mean).  Zero lies in the span,
@@ -359,8 +356,20 @@ struct GuessState {
     int choice;      // -1 zero, 2 combination
     int net_status;  // copy of the network's status (nonzero: its prediction was zeroed)
 };
+// The guess applied by ir_init itself: x0 = alpha xa + beta xb (coefficients
+// in *gs) and r = b' - (alpha u + beta w) with u = A xa, w = A xb as
+// guess_residuals stored them.  gs null: not used.
+struct IrGuess {
+    const GuessState *gs = nullptr;
+    const double *xa = nullptr, *xb = nullptr, *u = nullptr, *w = nullptr;
+};
+void ir_init(cudaStream_t s, const Ell &A, const double *b, double *x, double *r, float *r32, PcgState *st,
+             double *partials, unsigned int *counter, double rtol, double abs_floor, int max_outer, int use_x0 = 0,
+             const IrGuess &g = IrGuess{});
+// uo, wo (optional): A xa and A xb are also stored there.
 void guess_residuals(cudaStream_t s, const Ell &A, const double *b, const PcgState *st, const double *xa,
-                     const double *xb, GuessState *gs, double *partials, unsigned int *counter);
+                     const double *xb, GuessState *gs, double *partials, unsigned int *counter,
+                     double *uo = nullptr, double *wo = nullptr);
 void guess_apply(cudaStream_t s, int N, double *x, const double *xa, const double *xb, const GuessState *gs);
 void ir_add(cudaStream_t s, int N, double *x, const float *e, const PcgState *st);
 void ir_residual(cudaStream_t s, const Ell &A, const double *b, const double *x, double *r, float *r32, PcgState *st,
