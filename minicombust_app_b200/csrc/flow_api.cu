@@ -603,8 +603,12 @@ int solve_pressure(mc_flow *h, double abs_floor, int *iters, double *relres, dou
         if (rc) return rc;
     }
     if (looped) h->launches += loop_launches(h->h_pcg->iter, per_iter);
-    launch(h, K_PCG_XMEAN, [&] { pcg_xmean(h->stream, h->N, v); });
-    launch(h, K_PCG_SUBMEAN, [&] { pcg_sub_xmean(h->stream, h->N, v); });
+    // a solve that stopped at its initial check from x = 0 left x = 0, whose
+    // mean removal changes nothing
+    if (h->h_pcg->iter > 0 || use_x0) {
+        launch(h, K_PCG_XMEAN, [&] { pcg_xmean(h->stream, h->N, v); });
+        launch(h, K_PCG_SUBMEAN, [&] { pcg_sub_xmean(h->stream, h->N, v); });
+    }
     rc = check_launch(h);
     if (rc) return rc;
     const PcgState &s = *h->h_pcg;
@@ -642,6 +646,7 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
     const long max_batches = h->prm.max_iters / PCG_AMG_BATCH + 2;
     int inner_total = 0, worst = MC_OK;
     double *xcur = o.x;  // the FP64 solution alternates between o.x and ir_x2
+    int outers = 0;      // outer iterations that ran an inner solve
     // A device-looped inner solve is followed at once by the outer update;
     // its state is read together with the next outer check (one
     // synchronisation per outer iteration).
@@ -670,6 +675,7 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
         // each inner solve asks for the reduction still missing (with a
         // margin of 2), but never for less than ir_inner_rtol
         const PcgState &os = *h->h_pcg;
+        outers++;
         double inner_rtol = os.rr > 0 ? 0.5 * std::sqrt(os.tol2 / os.rr) : h->prm.ir_inner_rtol;
         inner_rtol = std::min(0.5, std::max(h->prm.ir_inner_rtol, inner_rtol));
         launch(h, K_PCG_INIT_AMG32,
@@ -715,8 +721,12 @@ int solve_pressure_refined(mc_flow *h, double abs_floor, int *iters, double *rel
         if (rc) return rc;
     }
     if (xcur != o.x) CUDA_TRY(h, cudaMemcpyAsync(o.x, xcur, (size_t)h->N * 8, cudaMemcpyDeviceToDevice, h->stream));
-    launch(h, K_PCG_XMEAN, [&] { pcg_xmean(h->stream, h->N, o); });
-    launch(h, K_PCG_SUBMEAN, [&] { pcg_sub_xmean(h->stream, h->N, o); });
+    // a solve that stopped at its initial check from x = 0 left x = 0, whose
+    // mean removal changes nothing
+    if (xcur != o.x || outers > 0 || use_x0) {
+        launch(h, K_PCG_XMEAN, [&] { pcg_xmean(h->stream, h->N, o); });
+        launch(h, K_PCG_SUBMEAN, [&] { pcg_sub_xmean(h->stream, h->N, o); });
+    }
     rc = check_launch(h);
     if (rc) return rc;
     const PcgState &st = *h->h_pcg;
