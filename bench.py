@@ -2,7 +2,7 @@
 learned initial guess + FP32-refined pressure solve against the plain FP64
 path, both to the same 1e-8 pressure residual.
 
-Workload (BASELINE metric configuration): box of 2*128 x 128 x 128 =
+Workload (the headline metric's configuration): box of 2*128 x 128 x 128 =
 4,194,304 hexahedral cells on a 0.2 x 0.1 x 0.1 m domain, inlet u = 50 m/s on
 x-min, zero-gradient outlet on x-max, walls elsewhere, rho 1.2, mu 1.8e-5,
 T0 1500 K; initial u, v, w, p, T = inlet state + seeded uniform noise +-1%;
