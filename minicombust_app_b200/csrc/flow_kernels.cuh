@@ -29,7 +29,7 @@ struct MeshArgs {
 // (pos >> 3d) & 7 of the row, d = (code[c] >> 3k) & 7 its direction (7: no
 // value), 0 where the row has no neighbour that way; the solvers then read no
 // column data.  The positions follow the order in which the directions occur
-// in every row's slots, so each row sums its terms in slot order.
+// in every row's slots, so each row sums its nonzero terms in slot order.
 struct RowStore {
     const uint32_t *code = nullptr;
     uint32_t pos = 0;
