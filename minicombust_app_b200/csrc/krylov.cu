@@ -465,14 +465,6 @@ __global__ void __launch_bounds__(MCB_THREADS) k_guess_apply(int N, double *__re
         x[i] = (ua ? al * xa[i] : 0.0) + (ub ? be * xb[i] : 0.0);
 }
 
-__global__ void __launch_bounds__(MCB_THREADS) k_ir_add(int N, double *__restrict__ x, const float *__restrict__ e,
-                                                        const PcgState *st)
-{
-    pdl_wait();
-    if (st->done) return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) x[i] += (double)e[i];
-}
-
 // With e set: the update x' = x + e (the inner solution) in the same pass,
 // evaluated at each row where the product needs it and stored in xout (not
 // in x, which neighbouring rows still read); without e, x' = x.  r may be
@@ -597,10 +589,6 @@ void guess_residuals(cudaStream_t s, const Ell &A, const double *b, const PcgSta
 void guess_apply(cudaStream_t s, int N, double *x, const double *xa, const double *xb, const GuessState *gs)
 {
     k_guess_apply<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, x, xa, xb, gs);
-}
-void ir_add(cudaStream_t s, int N, double *x, const float *e, const PcgState *st)
-{
-    k_ir_add<<<krylov_grid(N), MCB_THREADS, 0, s>>>(N, x, e, st);
 }
 void ir_residual(cudaStream_t s, const Ell &A, const double *b, const double *x, double *r, float *r32, PcgState *st,
                  double *partials, unsigned int *counter, const float *e, double *xout)

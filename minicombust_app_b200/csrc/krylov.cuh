@@ -341,10 +341,10 @@ template <typename T>
 void pcg_iter2_amg(cudaStream_t s, const EllT<T> &A, const PcgVectorsT<T> &v, int pnew);
 // FP64 iterative refinement around an FP32 inner solve: the state's mean
 // (from pcg_mean) defines b' = b - mean; ir_init sets x = 0, r = b', r32 =
-// (float) r and the tolerance; ir_add accumulates x += e in FP64; ir_residual
+// (float) r and the tolerance (or applies a guess, IrGuess); ir_residual
 // recomputes the FP64 true residual, its norm, r32, and the convergence flag
-// (with e given, of x + e, which it stores in xout != x: the update and the
-// residual in one pass).  r may be null in both.
+// (with e given, of x + e, which it stores in xout != x: the update x += e
+// and the residual in one pass).  r may be null in both.
 // Initial guess of the pressure correction from up to two candidates xa, xb
 // (a null candidate is skipped): the combination x0 = alpha xa + beta xb
 // that minimises ||b' - A x0|| (b' = b - st->mean).  Zero lies in the span,
@@ -371,7 +371,6 @@ void guess_residuals(cudaStream_t s, const Ell &A, const double *b, const PcgSta
                      const double *xb, GuessState *gs, double *partials, unsigned int *counter,
                      double *uo = nullptr, double *wo = nullptr);
 void guess_apply(cudaStream_t s, int N, double *x, const double *xa, const double *xb, const GuessState *gs);
-void ir_add(cudaStream_t s, int N, double *x, const float *e, const PcgState *st);
 void ir_residual(cudaStream_t s, const Ell &A, const double *b, const double *x, double *r, float *r32, PcgState *st,
                  double *partials, unsigned int *counter, const float *e = nullptr, double *xout = nullptr);
 void pcg_xmean(cudaStream_t s, int N, const PcgVectors &v);
